@@ -1,0 +1,247 @@
+"""dvr3d_b200 -- B200-native DVR3DRJZ hot path behind a C ABI.
+
+Python mirror of the library's C entry points (include/dvr3d_b200.h). The numerical work
+runs in ``libdvr3d_b200.so`` (CUDA kernels for sm_100a); this module only marshals
+arguments. Importing it does not need a GPU; creating a :class:`Context` does, and fails
+with an error when no usable device or no built library is present (there is no CPU
+fallback of the hot path).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _abi
+from ._abi import (DVR3D_PES_GRID, DVR3D_PES_MORSE_SUM, DVR3D_PES_MORSE_SUM_NPARAM,
+                   DVR3D_PREC_FP64, DVR3D_PREC_MIXED_DAVIDSON, Deck, Options, Result)
+
+AUTOCM = 2.19474624e5  # hartree -> cm-1, as diag3d (:2681)
+
+__all__ = ["Context", "Deck", "DVR3DError", "SolveResult", "parse_deck", "AUTOCM",
+           "DVR3D_PES_MORSE_SUM", "DVR3D_PES_GRID", "DVR3D_PREC_FP64",
+           "DVR3D_PREC_MIXED_DAVIDSON", "k_blocks", "host_grid"]
+
+
+class DVR3DError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"[{code}] {msg}")
+        self.code = code
+
+
+def _strerror(code: int) -> str:
+    return _abi.load_library().dvr3d_b200_strerror(code).decode()
+
+
+def parse_deck(text: str) -> Deck:
+    """Read a DVR3DRJZ job deck (namelist PRT + cards) into a :class:`Deck`."""
+    lib = _abi.load_library()
+    d = Deck()
+    rc = lib.dvr3d_b200_parse_deck(text.encode(), C.byref(d))
+    if rc != 0:
+        raise DVR3DError(rc, _strerror(rc))
+    return d
+
+
+def k_blocks(deck: Deck) -> list[int]:
+    """k-loop indices of ccmain (:811-819) for a deck: [kd .. ku]."""
+    jrot, kmin = abs(deck.jrot), deck.kmin
+    zrot = bool(deck.zrot) and jrot != 0
+    if jrot == 0:
+        kmin = 0
+    if zrot:
+        zbisc = deck.idia == -2
+        if kmin != 0 and not zbisc:
+            kmin = 1
+        if kmin not in (0, 1):
+            kmin = 2
+        kd, ku = 1 - min(kmin, 1), jrot + (1 if kmin == 2 else 0)
+    else:
+        kd = ku = kmin
+    return list(range(kd, ku + 1))
+
+
+def host_grid(deck: Deck, kk: int = 0):
+    """DVR grid (r1, r2, cos theta) of one k block from the library's host set-up
+    (dvr3d_b200_grid with no device context; needs no GPU)."""
+    lib = _abi.load_library()
+    r1 = np.zeros(256)
+    r2 = np.zeros(256)
+    xa = np.zeros(512)
+    dp = C.POINTER(C.c_double)
+    rc = lib.dvr3d_b200_grid(None, C.byref(deck), kk, r1.ctypes.data_as(dp), 256, r2.ctypes.data_as(dp), 256,
+                             xa.ctypes.data_as(dp), 512)
+    if rc != 0:
+        raise DVR3DError(rc, _strerror(rc))
+    n1 = deck.npnt2 if deck.idia == -2 else deck.npnt1
+    na = deck.nalf // 2 if deck.idia == 2 else deck.nalf
+    return r1[:n1].copy(), r2[:deck.npnt2].copy(), xa[:na].copy()
+
+
+@dataclass
+class SolveResult:
+    eval: np.ndarray                 # levels (Eh), ascending, length meval
+    nham3: int
+    iv2: np.ndarray                  # per-block selection counts
+    kz: int
+    ipar: int
+    stage_ms: np.ndarray
+    max_resid: float
+    iterations: int = 0
+    fallback: int = 0
+    resid: np.ndarray | None = None
+    evec: np.ndarray | None = None
+    h3: np.ndarray | None = None
+    extra: dict = field(default_factory=dict)
+
+    @property
+    def eval_cm(self) -> np.ndarray:
+        return self.eval * AUTOCM
+
+
+class Context:
+    """One CUDA device context of the library (dvr3d_b200_init)."""
+
+    def __init__(self, device: int = 0):
+        self._lib = _abi.load_library()
+        h = C.c_void_p()
+        rc = self._lib.dvr3d_b200_init(int(device), C.byref(h))
+        if rc != 0:
+            raise DVR3DError(rc, _strerror(rc) + " (the CUDA path is required; no CPU fallback)")
+        self._h = h
+
+    def close(self) -> None:
+        if getattr(self, "_h", None):
+            self._lib.dvr3d_b200_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _check(self, rc: int) -> None:
+        if rc != 0:
+            msg = self._lib.dvr3d_b200_last_error(self._h).decode()
+            raise DVR3DError(rc, _strerror(rc) + (": " + msg if msg else ""))
+
+    def set_stream(self, stream_ptr: int) -> None:
+        self._check(self._lib.dvr3d_b200_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    def set_pes(self, params) -> None:
+        p = np.ascontiguousarray(np.asarray(params, dtype=np.float64))
+        if p.size != DVR3D_PES_MORSE_SUM_NPARAM:
+            raise ValueError("MORSE_SUM takes 13 parameters")
+        self._check(self._lib.dvr3d_b200_set_pes(
+            self._h, DVR3D_PES_MORSE_SUM, p.ctypes.data_as(C.POINTER(C.c_double)), p.size))
+
+    def set_pes_grid(self, table) -> None:
+        t = np.ascontiguousarray(np.asarray(table, dtype=np.float64).ravel())
+        self._check(self._lib.dvr3d_b200_set_pes_grid(
+            self._h, t.ctypes.data_as(C.POINTER(C.c_double)), t.size))
+
+    def grid(self, deck: Deck, kk: int = 0):
+        r1 = np.zeros(256)
+        r2 = np.zeros(256)
+        xa = np.zeros(512)
+        dp = C.POINTER(C.c_double)
+        self._check(self._lib.dvr3d_b200_grid(self._h, C.byref(deck), kk, r1.ctypes.data_as(dp), 256,
+                                              r2.ctypes.data_as(dp), 256, xa.ctypes.data_as(dp), 512))
+        n1 = deck.npnt2 if deck.idia == -2 else deck.npnt1
+        n2 = deck.npnt2
+        na = deck.nalf // 2 if deck.idia == 2 else deck.nalf
+        return r1[:n1].copy(), r2[:n2].copy(), xa[:na].copy()
+
+    def solve(self, deck: Deck, kk: int | None = None, *, precision: int = DVR3D_PREC_FP64,
+              nlevels: int = 0, tol_cm: float = 0.0, max_iter: int = 0, block: int = 0,
+              learned_precond: bool = False, want_vectors: bool = False, want_h3: bool = False,
+              want_resid: bool = False) -> SolveResult:
+        """Solve one k block (dvr3d_b200_solve_block)."""
+        if kk is None:
+            kk = k_blocks(deck)[0]
+        neval = max(int(deck.neval), 10, int(nlevels))
+        nalf = max(int(deck.nalf), int(deck.npnt1), int(deck.npnt2), 1)
+        ev = np.zeros(neval + 8)
+        iv2 = np.zeros(nalf + 8, dtype=np.int32)
+        r = Result()
+        r.eval = ev.ctypes.data_as(C.POINTER(C.c_double))
+        r.eval_cap = ev.size
+        r.iv2 = iv2.ctypes.data_as(C.POINTER(C.c_int))
+        r.iv2_cap = iv2.size
+        rs = None
+        if want_resid:
+            rs = np.zeros(neval + 8)
+            r.resid = rs.ctypes.data_as(C.POINTER(C.c_double))
+            r.resid_cap = rs.size
+        o = Options(precision=precision, nlevels=nlevels, tol_cm=tol_cm, max_iter=max_iter,
+                    block=block, learned_precond=int(learned_precond),
+                    want_vectors=int(want_vectors), want_h3=int(want_h3))
+        h3 = evec = None
+        if want_h3 or want_vectors:
+            # size is only known after the 2D stage: solve once to learn N, then allocate
+            probe = self.solve(deck, kk, precision=precision, nlevels=nlevels, tol_cm=tol_cm,
+                               max_iter=max_iter, block=block, learned_precond=learned_precond)
+            n = probe.nham3
+            m = len(probe.eval)
+            if want_h3:
+                h3 = np.zeros((n, n), order="F")
+                r.h3 = h3.ctypes.data_as(C.POINTER(C.c_double))
+                r.h3_cap = h3.size
+            if want_vectors:
+                evec = np.zeros((n, max(m, 1)), order="F")
+                r.evec = evec.ctypes.data_as(C.POINTER(C.c_double))
+                r.evec_cap = evec.size
+        self._check(self._lib.dvr3d_b200_solve_block(self._h, C.byref(deck), kk, C.byref(o), C.byref(r)))
+        m = r.meval
+        return SolveResult(eval=ev[:m].copy(), nham3=r.nham3, iv2=iv2[:r.nblocks].copy(), kz=r.kz,
+                           ipar=r.ipar, stage_ms=np.array(r.stage_ms[:]), max_resid=r.max_resid,
+                           iterations=r.iterations, fallback=r.fallback,
+                           resid=None if rs is None else rs[:m].copy(),
+                           evec=None if evec is None else evec[:, :m], h3=h3)
+
+    def solve_batch(self, decks: list[Deck], pes_rows) -> list[SolveResult]:
+        n = len(decks)
+        arr = (Deck * n)(*decks)
+        P = np.ascontiguousarray(np.asarray(pes_rows, dtype=np.float64).reshape(n, DVR3D_PES_MORSE_SUM_NPARAM))
+        res = (Result * n)()
+        bufs = []
+        for i, d in enumerate(decks):
+            ev = np.zeros(max(d.neval, 10) + 8)
+            iv2 = np.zeros(max(d.nalf, d.npnt1, d.npnt2) + 8, dtype=np.int32)
+            bufs.append((ev, iv2))
+            res[i].eval = ev.ctypes.data_as(C.POINTER(C.c_double))
+            res[i].eval_cap = ev.size
+            res[i].iv2 = iv2.ctypes.data_as(C.POINTER(C.c_int))
+            res[i].iv2_cap = iv2.size
+        o = Options()
+        self._check(self._lib.dvr3d_b200_solve_batch(self._h, arr, P.ctypes.data_as(C.POINTER(C.c_double)), n,
+                                                     C.byref(o), res))
+        out = []
+        for i in range(n):
+            ev, iv2 = bufs[i]
+            r = res[i]
+            out.append(SolveResult(eval=ev[:r.meval].copy(), nham3=r.nham3, iv2=iv2[:r.nblocks].copy(),
+                                   kz=r.kz, ipar=r.ipar, stage_ms=np.array(r.stage_ms[:]),
+                                   max_resid=r.max_resid))
+        return out
+
+    def run_deck(self, text: str, precision: int = DVR3D_PREC_FP64) -> tuple[str, str]:
+        """Run a job like program DVR3DRJZ; returns (printed output, fort.14 levels text)."""
+        o = Options(precision=precision)
+        need = C.c_size_t(0)
+        needl = C.c_size_t(0)
+        self._check(self._lib.dvr3d_b200_run_deck(self._h, text.encode(), C.byref(o), None, 0, C.byref(need),
+                                                  None, 0, C.byref(needl)))
+        out = C.create_string_buffer(need.value + 1)
+        lev = C.create_string_buffer(needl.value + 1)
+        self._check(self._lib.dvr3d_b200_run_deck(self._h, text.encode(), C.byref(o), out, len(out), C.byref(need),
+                                                  lev, len(lev), C.byref(needl)))
+        return out.value.decode(), lev.value.decode()

@@ -1,0 +1,410 @@
+// capi.cu -- extern "C" entry points declared in include/dvr3d_b200.h.
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/dvr3d_b200.h"
+#include "eig_batched.cuh"
+#include "eig_dense.cuh"
+#include "pipeline.cuh"
+
+using dvr3d::CudaFail;
+using dvr3d::HostError;
+
+namespace {
+
+int fail_ctx(dvr3d_ctx *ctx, int code, const std::string &msg) {
+    if (ctx) ctx->last_error = msg;
+    return code;
+}
+
+template <class F>
+int guarded(dvr3d_ctx *ctx, F &&f) {
+    try {
+        return f();
+    } catch (HostError &e) {
+        return fail_ctx(ctx, e.code, e.msg);
+    } catch (CudaFail &e) {
+        cudaGetLastError();
+        return fail_ctx(ctx, DVR3D_ERR_CUDA, e.where + ": " + cudaGetErrorString(e.err));
+    } catch (std::bad_alloc &) {
+        return fail_ctx(ctx, DVR3D_ERR_NOMEM, "host allocation failed");
+    }
+}
+
+void appendf(std::string &s, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    s += buf;
+}
+
+// Fortran Dw.d edit descriptor (0.ddddD+ee form) for the level tables of diag3d.
+std::string fortran_d(double v, int w, int d) {
+    char buf[64];
+    if (v == 0.0) {
+        snprintf(buf, sizeof(buf), "0.%0*dD+00", d, 0);
+    } else {
+        int ex = (int)std::floor(std::log10(std::fabs(v))) + 1;
+        double mant = std::fabs(v) / std::pow(10.0, ex);
+        // rounding may carry into the next decade
+        double scale = std::pow(10.0, d);
+        double rm = std::round(mant * scale);
+        if (rm >= scale) {
+            rm /= 10.0;
+            ex += 1;
+        }
+        if (rm < scale / 10.0) {
+            rm *= 10.0;
+            ex -= 1;
+        }
+        snprintf(buf, sizeof(buf), "%s0.%0*.0fD%c%02d", v < 0 ? "-" : "", d, rm, ex < 0 ? '-' : '+', std::abs(ex));
+    }
+    std::string s(buf);
+    if ((int)s.size() < w) s = std::string(w - s.size(), ' ') + s;
+    return s;
+}
+
+void copy_out(const std::string &s, char *out, size_t cap, size_t *len) {
+    if (len) *len = s.size() + 1;
+    if (out && cap > 0) {
+        const size_t n = std::min(cap - 1, s.size());
+        std::memcpy(out, s.data(), n);
+        out[n] = '\0';
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *dvr3d_b200_strerror(int code) {
+    switch (code) {
+    case DVR3D_OK: return "ok";
+    case DVR3D_ERR_ARG: return "invalid argument or inconsistent input";
+    case DVR3D_ERR_CORE_MAX2D: return "core exceeded: reduce cut-off emax1 (MAX2D)";
+    case DVR3D_ERR_CORE_MAX3D: return "core exceeded: increase max3d or reduce emax2 (MAX3D)";
+    case DVR3D_ERR_QUADRATURE: return "points & weights in error (quadrature self-check failed)";
+    case DVR3D_ERR_NOCONV: return "eigensolver did not converge within its limits";
+    case DVR3D_ERR_CUDA: return "CUDA runtime error";
+    case DVR3D_ERR_NOMEM: return "out of memory";
+    case DVR3D_ERR_UNSUPPORTED: return "option not supported on this path";
+    case DVR3D_ERR_THETA0: return "bisector embedding: wavefunction has amplitude for theta = 0";
+    case DVR3D_ERR_PES: return "potential returned a non-finite value";
+    case DVR3D_ERR_DECK: return "job deck could not be parsed";
+    case DVR3D_ERR_NO_DEVICE: return "no usable CUDA device";
+    case DVR3D_ERR_BUFFER: return "caller buffer too small";
+    default: return "unknown error";
+    }
+}
+
+const char *dvr3d_b200_last_error(const dvr3d_ctx *ctx) { return ctx ? ctx->last_error.c_str() : ""; }
+
+int dvr3d_b200_init(int device, dvr3d_ctx **out) {
+    if (!out) return DVR3D_ERR_ARG;
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev <= device || device < 0) {
+        cudaGetLastError();
+        return DVR3D_ERR_NO_DEVICE;
+    }
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device) != cudaSuccess || prop.major < 10) {
+        cudaGetLastError();
+        return DVR3D_ERR_NO_DEVICE;
+    }
+    if (cudaSetDevice(device) != cudaSuccess) {
+        cudaGetLastError();
+        return DVR3D_ERR_NO_DEVICE;
+    }
+    dvr3d_ctx *ctx = new dvr3d_ctx();
+    ctx->device = device;
+    ctx->sm_count = prop.multiProcessorCount;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        delete ctx;
+        return DVR3D_ERR_CUDA;
+    }
+    ctx->own_stream = true;
+    for (auto &e : ctx->ev) cudaEventCreate(&e);
+    ctx->dense_grid = dvr3d::dense_tridiag_grid(device);
+    ctx->pes.kind = DVR3D_PES_NONE;
+    *out = ctx;
+    return DVR3D_OK;
+}
+
+void dvr3d_b200_destroy(dvr3d_ctx *ctx) {
+    if (!ctx) return;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    ctx->arena.release_all();
+    for (auto &e : ctx->ev)
+        if (e) cudaEventDestroy(e);
+    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+}
+
+int dvr3d_b200_set_stream(dvr3d_ctx *ctx, void *stream) {
+    if (!ctx) return DVR3D_ERR_ARG;
+    if (stream) {
+        ctx->stream = (cudaStream_t)stream;
+    } else {
+        return DVR3D_ERR_ARG;
+    }
+    return DVR3D_OK;
+}
+
+int dvr3d_b200_parse_deck(const char *text, dvr3d_deck *out) {
+    if (!text || !out) return DVR3D_ERR_ARG;
+    try {
+        dvr3d::parse_deck(text, *out);
+        return DVR3D_OK;
+    } catch (HostError &e) {
+        return e.code;
+    }
+}
+
+int dvr3d_b200_set_pes(dvr3d_ctx *ctx, int kind, const double *params, int nparams) {
+    if (!ctx) return DVR3D_ERR_ARG;
+    if (kind == DVR3D_PES_MORSE_SUM) {
+        if (!params || nparams < DVR3D_PES_MORSE_SUM_NPARAM) return fail_ctx(ctx, DVR3D_ERR_ARG, "MORSE_SUM needs 13 parameters");
+        for (int i = 0; i < DVR3D_PES_MORSE_SUM_NPARAM; ++i) {
+            if (!std::isfinite(params[i])) return fail_ctx(ctx, DVR3D_ERR_PES, "non-finite PES parameter");
+            ctx->pes.p[i] = params[i];
+        }
+        ctx->pes.kind = kind;
+        return DVR3D_OK;
+    }
+    if (kind == DVR3D_PES_GRID) {
+        if (ctx->pes_grid.empty()) return fail_ctx(ctx, DVR3D_ERR_ARG, "call dvr3d_b200_set_pes_grid first");
+        ctx->pes.kind = kind;
+        return DVR3D_OK;
+    }
+    return fail_ctx(ctx, DVR3D_ERR_ARG, "unknown PES kind");
+}
+
+int dvr3d_b200_set_pes_grid(dvr3d_ctx *ctx, const double *v, size_t n) {
+    if (!ctx || !v || n == 0) return DVR3D_ERR_ARG;
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(v[i])) return fail_ctx(ctx, DVR3D_ERR_PES, "non-finite value in the PES table");
+    ctx->pes_grid.assign(v, v + n);
+    ctx->pes.kind = DVR3D_PES_GRID;
+    return DVR3D_OK;
+}
+
+int dvr3d_b200_grid(dvr3d_ctx *ctx, const dvr3d_deck *deck, int kz, double *r1, int n1cap, double *r2,
+                    int n2cap, double *xalf, int nacap) {
+    if (!deck) return DVR3D_ERR_ARG;
+    return guarded(ctx, [&]() -> int {
+        dvr3d::BlockPlan p;
+        dvr3d::plan_block(*deck, kz, p);
+        if ((r1 && n1cap < p.npnt1) || (r2 && n2cap < p.npnt2) || (xalf && nacap < (int)p.xalf.size()))
+            return fail_ctx(ctx, DVR3D_ERR_BUFFER, "grid buffers too small");
+        if (r1) std::memcpy(r1, p.r1.data(), sizeof(double) * p.npnt1);
+        if (r2) std::memcpy(r2, p.r2.data(), sizeof(double) * p.r2.size());
+        if (xalf) std::memcpy(xalf, p.xalf.data(), sizeof(double) * p.xalf.size());
+        return DVR3D_OK;
+    });
+}
+
+int dvr3d_b200_solve_block(dvr3d_ctx *ctx, const dvr3d_deck *deck, int kz, const dvr3d_options *opt,
+                           dvr3d_result *res) {
+    if (!ctx || !deck || !res) return DVR3D_ERR_ARG;
+    dvr3d_options o{};
+    if (opt) o = *opt;
+    return guarded(ctx, [&]() -> int {
+        cudaSetDevice(ctx->device);
+        dvr3d::solve_block(ctx, *deck, kz, o, *res);
+        return DVR3D_OK;
+    });
+}
+
+int dvr3d_b200_solve_batch(dvr3d_ctx *ctx, const dvr3d_deck *decks, const double *pes_params, int nprob,
+                           const dvr3d_options *opt, dvr3d_result *res) {
+    if (!ctx || !decks || !pes_params || !res || nprob <= 0) return DVR3D_ERR_ARG;
+    dvr3d_options o{};
+    if (opt) o = *opt;
+    return guarded(ctx, [&]() -> int {
+        cudaSetDevice(ctx->device);
+        const dvr3d::PesParams saved = ctx->pes;
+        for (int i = 0; i < nprob; ++i) {
+            ctx->pes.kind = DVR3D_PES_MORSE_SUM;
+            for (int k = 0; k < DVR3D_PES_MORSE_SUM_NPARAM; ++k)
+                ctx->pes.p[k] = pes_params[(size_t)i * DVR3D_PES_MORSE_SUM_NPARAM + k];
+            int kd, ku;
+            dvr3d::k_range(decks[i], kd, ku);
+            dvr3d::solve_block(ctx, decks[i], kd, o, res[i]);
+        }
+        ctx->pes = saved;
+        return DVR3D_OK;
+    });
+}
+
+int dvr3d_b200_diag_batched(dvr3d_ctx *ctx, int nblk, const int *n_host, const long long *off_host,
+                            const long long *woff_host, double *a_dev, double *w_dev, int vecs) {
+    if (!ctx || nblk <= 0 || !n_host || !off_host || !woff_host || !a_dev || !w_dev) return DVR3D_ERR_ARG;
+    return guarded(ctx, [&]() -> int {
+        cudaSetDevice(ctx->device);
+        cudaStream_t st = ctx->stream;
+        std::vector<int> n(n_host, n_host + nblk);
+        std::vector<long long> aoff(off_host, off_host + nblk), voff(nblk);
+        int nmax = 0;
+        long long vt = 0;
+        for (int b = 0; b < nblk; ++b) {
+            if (n[b] < 1 || n[b] > 1024) return fail_ctx(ctx, DVR3D_ERR_ARG, "block dimension must be 1..1024");
+            nmax = std::max(nmax, n[b]);
+            voff[b] = vt;
+            vt += n[b];
+        }
+        auto up = [&](const char *name, const auto &v) {
+            using T = typename std::decay_t<decltype(v)>::value_type;
+            T *p = ctx->arena.get_t<T>(name, v.size());
+            cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+            return p;
+        };
+        dvr3d::BatchDesc bd{nblk, up("dg_n", n), up("dg_aoff", aoff), up("dg_voff", voff)};
+        double *d = ctx->arena.get_t<double>("dg_d", vt), *e = ctx->arena.get_t<double>("dg_e", vt);
+        double *tau = ctx->arena.get_t<double>("dg_tau", vt), *w = ctx->arena.get_t<double>("dg_w", vt);
+        int *cnt = ctx->arena.get_t<int>("dg_cnt", nblk);
+        // the reflectors overwrite a copy of the blocks; eigenvectors are written back to a
+        std::vector<long long> asz(nblk);
+        long long at = 0;
+        for (int b = 0; b < nblk; ++b) {
+            asz[b] = at;
+            at += (long long)n[b] * n[b];
+        }
+        double *ac = ctx->arena.get_t<double>("dg_a", at);
+        for (int b = 0; b < nblk; ++b)
+            cudaMemcpyAsync(ac + asz[b], a_dev + aoff[b], sizeof(double) * n[b] * n[b], cudaMemcpyDeviceToDevice, st);
+        // the reference reads the lower triangle only: mirror it into full storage
+        std::vector<int> dummy;
+        (void)dummy;
+        dvr3d::BatchDesc bdc{nblk, bd.n, up("dg_asz", asz), bd.voff};
+        extern void dvr3d_symmetrize_lower(const dvr3d::BatchDesc &, double *, int, cudaStream_t);
+        dvr3d_symmetrize_lower(bdc, ac, nmax, st);
+        dvr3d::launch_tridiag_batched(bdc, ac, d, e, tau, nmax, st);
+        dvr3d::launch_eigvals_batched(bdc, d, e, w, cnt, 0, 0.0, st);
+        for (int b = 0; b < nblk; ++b)
+            cudaMemcpyAsync(w_dev + woff_host[b], w + voff[b], sizeof(double) * n[b], cudaMemcpyDeviceToDevice, st);
+        if (vecs) {
+            std::vector<int> zld(n);
+            std::vector<long long> woff(nblk);
+            long long wt = 0;
+            for (int b = 0; b < nblk; ++b) {
+                woff[b] = wt;
+                wt += 5LL * n[b] * std::min(128, n[b]) + (long long)n[b] * n[b];
+            }
+            double *work = ctx->arena.get_t<double>("dg_work", wt);
+            int *err = ctx->arena.get_t<int>("err", 1);
+            cudaMemsetAsync(err, 0, sizeof(int), st);
+            dvr3d::launch_eigvecs_batched(bdc, ac, d, e, tau, w, bd.n, up("dg_zoff", aoff), up("dg_zld", n), a_dev,
+                                          work, up("dg_woff", woff), nmax, err, st);
+        }
+        cudaError_t ce = cudaStreamSynchronize(st);
+        if (ce != cudaSuccess) throw CudaFail{ce, "diag_batched"};
+        return DVR3D_OK;
+    });
+}
+
+int dvr3d_b200_run_deck(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_options *opt, char *out, size_t outcap,
+                        size_t *outlen, char *lev, size_t levcap, size_t *levlen) {
+    if (!ctx || !deck_text) return DVR3D_ERR_ARG;
+    dvr3d_options o{};
+    if (opt) o = *opt;
+    return guarded(ctx, [&]() -> int {
+        cudaSetDevice(ctx->device);
+        dvr3d_deck d;
+        dvr3d::parse_deck(deck_text, d);
+        int kd, ku;
+        dvr3d::k_range(d, kd, ku);
+        const double autocm = 2.19474624e+05;
+        std::string s, lv;
+        appendf(s, "     Program DVR3DRJZ (B200 hot path)\n\n     Title: %s\n", d.title);
+        for (int kk = kd; kk <= ku; ++kk) {
+            dvr3d::BlockPlan p;
+            dvr3d::plan_block(d, kk, p);
+            std::vector<double> ev(std::max(p.neval, 1));
+            std::vector<int> iv2(std::max(p.radau ? p.nalf : p.npntc, 1));
+            dvr3d_result r{};
+            r.eval = ev.data();
+            r.eval_cap = (int)ev.size();
+            r.iv2 = iv2.data();
+            r.iv2_cap = (int)iv2.size();
+            dvr3d::solve_block(ctx, d, kk, o, r);
+            if (d.jrot != 0 && p.zrot) appendf(s, "\n     Solutions with J =%3d k =%3d\n", p.jrot, p.kz);
+            if (p.radau && d.jrot != 0 && p.zrot)
+                appendf(s, p.ipar == 0 ? "\n     even parity solutions\n" : "\n     odd parity solutions\n");
+            for (int b = 0; b < r.nblocks && p.radau; ++b)
+                appendf(s, "     for gamma = %2d selected %3d energies.\n", b + 1, iv2[b]);
+            appendf(s, "                         total = %5d\n", r.nham3);
+            const int meval = r.meval;
+            if (!d.zpmin) {
+                appendf(s, "\n     lowest%4d eigenvalues in hartrees:\n\n", meval);
+                for (int i = 0; i < meval; ++i) {
+                    s += fortran_d(ev[i], 24, 12);
+                    if (i % 5 == 4 || i == meval - 1) s += "\n\n";
+                }
+            }
+            appendf(s, "\n\n     Lowest%4d eigenvalues in wavenumbers:\n\n", meval);
+            for (int i = 0; i < meval; ++i) {
+                s += fortran_d(ev[i] * autocm, 24, 12);
+                if (i % 5 == 4 || i == meval - 1) s += "\n\n";
+            }
+            // zpfun levels file (:2708-2719): header 6i4, then 4d20.12
+            const int ip = d.jrot - p.kmin;
+            if (d.zpfun && std::abs(d.jrot) <= 1 && (d.jrot == 0 || ip == 1)) {
+                const int jdia = std::max(0, d.idia), jpar = std::min(jdia, p.ipar);
+                int isym = std::abs(std::min(0, d.idia));
+                if (p.ipar == 1) isym = -isym;
+                appendf(lv, "%4d%4d%4d%4d%4d%4d\n", d.jrot, ip, jdia, jpar, isym, meval);
+                for (int i = 0; i < meval; ++i) {
+                    lv += fortran_d(ev[i], 20, 12);
+                    if (i % 4 == 3 || i == meval - 1) lv += "\n";
+                }
+            }
+            if (d.jrot == 0 && meval > 0) {  // band origins (:2748-2761)
+                double ezero;
+                int ii;
+                if (std::abs(d.idia) == 2 && p.ipar == 1) {
+                    ezero = d.have_ezero ? d.ezero : 0.0;
+                    ii = 0;
+                } else {
+                    ezero = ev[0] * autocm;
+                    ii = 1;
+                }
+                appendf(s, "\n  Band origins in wavenumbers:\n\n");
+                int c = 0;
+                for (int i = ii; i < meval; ++i, ++c) {
+                    appendf(s, "%15.6f", ev[i] * autocm - ezero);
+                    if (c % 5 == 4 || i == meval - 1) s += "\n\n";
+                }
+            }
+        }
+        copy_out(s, out, outcap, outlen);
+        copy_out(lv, lev, levcap, levlen);
+        return DVR3D_OK;
+    });
+}
+
+}  // extern "C"
+
+// mirror the lower triangle of each block into the upper one (dsyev('V','L') semantics)
+namespace {
+__global__ void symmetrize_lower_kernel(dvr3d::BatchDesc bd, double *A) {
+    const int b = blockIdx.y;
+    const int n = bd.n[b];
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * n) return;
+    const int i = (int)(idx % n), j = (int)(idx / n);
+    if (j > i) A[bd.aoff[b] + idx] = A[bd.aoff[b] + (long long)i * n + j];
+}
+}  // namespace
+
+void dvr3d_symmetrize_lower(const dvr3d::BatchDesc &bd, double *A, int nmax, cudaStream_t st) {
+    dim3 grid((unsigned)(((long long)nmax * nmax + 255) / 256), bd.nblk);
+    symmetrize_lower_kernel<<<grid, 256, 0, st>>>(bd, A);
+}

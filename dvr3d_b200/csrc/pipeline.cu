@@ -1,0 +1,667 @@
+// pipeline.cu -- the per-k-block solve on one GPU.
+//
+// Stage order follows nfmain (:3006-3121) for Radau idia=-2 and jhmain (:1915-2118) for
+// the Jacobi / idia=-1 orderings; the reference's scratch units (ivecs1, ieigs1, intvec,
+// ivint, iband ...) become device buffers that stay resident between stages. The host
+// only plans sizes (selection counts come back as a few integers per block).
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstring>
+#include <numeric>
+
+#include "blocks.cuh"
+#include "eig_batched.cuh"
+#include "eig_dense.cuh"
+#include "gemm64.cuh"
+#include "pipeline.cuh"
+
+#define CK(x)                                          \
+    do {                                               \
+        cudaError_t e_ = (x);                          \
+        if (e_ != cudaSuccess) throw CudaFail{e_, #x}; \
+    } while (0)
+
+namespace dvr3d {
+
+// ---------------------------------------------------------------- arena
+DeviceArena::~DeviceArena() { release_all(); }
+
+void *DeviceArena::get(const std::string &name, size_t bytes) {
+    if (bytes == 0) bytes = 16;
+    Buf &b = bufs_[name];
+    if (b.bytes < bytes) {
+        if (b.p) cudaFree(b.p);
+        b.p = nullptr;
+        b.bytes = 0;
+        size_t nb = std::max(bytes, b.bytes + b.bytes / 4);
+        nb = (nb + 255) & ~(size_t)255;
+        cudaError_t e = cudaMalloc(&b.p, nb);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            throw HostError{DVR3D_ERR_NOMEM, "device allocation of " + std::to_string(nb) + " bytes for " + name + " failed"};
+        }
+        b.bytes = nb;
+    }
+    return b.p;
+}
+
+size_t DeviceArena::bytes_held() const {
+    size_t s = 0;
+    for (auto &kv : bufs_) s += kv.second.bytes;
+    return s;
+}
+
+void DeviceArena::release_all() {
+    for (auto &kv : bufs_)
+        if (kv.second.p) cudaFree(kv.second.p);
+    bufs_.clear();
+}
+
+namespace {
+
+template <class T>
+T *upload(dvr3d_ctx *ctx, const std::string &name, const std::vector<T> &v) {
+    T *p = ctx->arena.get_t<T>(name, std::max<size_t>(v.size(), 1));
+    if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    return p;
+}
+
+template <class T>
+std::vector<T> download(dvr3d_ctx *ctx, const T *p, size_t n) {
+    std::vector<T> v(n);
+    if (n) CK(cudaMemcpyAsync(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    return v;
+}
+
+inline long long round_up(long long x, long long m) { return (x + m - 1) / m * m; }
+
+void check_dev_err(dvr3d_ctx *ctx, const int *err_dev, const char *stage) {
+    int e = 0;
+    CK(cudaMemcpyAsync(&e, err_dev, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    CK(cudaStreamSynchronize(ctx->stream));
+    if (e == kDevBarrierTimeout) throw HostError{DVR3D_ERR_NOCONV, std::string(stage) + ": grid barrier wait exceeded its limit"};
+    if (e != 0) throw HostError{DVR3D_ERR_NOCONV, std::string(stage) + ": device error flag " + std::to_string(e)};
+}
+
+// Output of the 2D stage: the contracted basis, ready for assembly.
+struct Contracted {
+    double *Vt = nullptr;   // ldv x ncol (zero padded)
+    long long ldv = 0;
+    int P = 0, N = 0;
+    int *g = nullptr;       // [N] block of each column
+    double *e2 = nullptr;   // [N] 2D eigenvalues
+    const double *T = nullptr;
+    int ldt = 0;
+    std::vector<int> iv2;   // per block selected counts
+    int nblocks = 0;
+};
+
+void eigvecs_work(const std::vector<int> &n, const std::vector<int> &sel, std::vector<long long> &off,
+                  long long &total) {
+    off.resize(n.size());
+    total = 0;
+    for (size_t b = 0; b < n.size(); ++b) {
+        off[b] = total;
+        const long long T = std::min(128, std::max(sel[b], 1));
+        total += 5LL * n[b] * T + (long long)n[b] * std::max(sel[b], 0);
+    }
+}
+
+// ---------------------------------------------------------------- Radau (nfmain)
+void radau_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
+    cudaStream_t st = ctx->stream;
+    const int npnt = p.npnt1, ipar = p.ipar, nalf = p.nalf;
+    const int n = npnt * (npnt + 1 - 2 * ipar) / 2;
+    if (n > 1024) throw HostError{DVR3D_ERR_UNSUPPORTED, "Radau 2D block larger than 1024"};
+    std::vector<int> pa, pb;
+    for (int beta = 1; beta <= npnt; ++beta)
+        for (int alpha = 1; alpha <= beta - ipar; ++alpha) {
+            pa.push_back(alpha - 1);
+            pb.push_back(beta - 1);
+        }
+    double *r = upload(ctx, "r1", p.r1);
+    double *hr = upload(ctx, "xk1", p.xk1);
+    double *xalf = upload(ctx, "xalf", p.xalf);
+    double *xl = upload(ctx, "xlmatr", p.xlmatr);
+    int *dpa = upload(ctx, "pa", pa);
+    int *dpb = upload(ctx, "pb", pb);
+    double *H = ctx->arena.get_t<double>("blk2", (size_t)nalf * n * n);
+    RadauBuild rb{};
+    rb.n = n;
+    rb.npnt = npnt;
+    rb.ipar = ipar;
+    rb.jrot = p.jrot;
+    rb.kz = p.kz;
+    rb.pa = dpa;
+    rb.pb = dpb;
+    rb.r = r;
+    rb.hr = hr;
+    rb.xalf = xalf;
+    rb.term = p.nf_term;
+    rb.term2 = p.nf_term2;
+    rb.term3 = p.nf_term3;
+    rb.urr1 = p.urr1;
+    rb.pes = ctx->pes;
+    if (rb.pes.kind == DVR3D_PES_GRID) {
+        if (ctx->pes_grid.size() < (size_t)nalf * p.npnt1 * p.npnt1)
+            throw HostError{DVR3D_ERR_ARG, "tabulated PES smaller than the DVR grid"};
+        rb.pes.grid = upload(ctx, "pesgrid", ctx->pes_grid);
+        rb.pes.npnt1 = p.npnt1;
+        rb.pes.npnt2 = p.npnt1;
+    }
+    launch_radau_build(rb, nalf, H, st);
+    CK(cudaGetLastError());
+    std::vector<int> nv(nalf, n);
+    std::vector<long long> aoff(nalf), voff(nalf);
+    for (int b = 0; b < nalf; ++b) {
+        aoff[b] = (long long)b * n * n;
+        voff[b] = (long long)b * n;
+    }
+    BatchDesc bd{nalf, upload(ctx, "bd_n", nv), upload(ctx, "bd_aoff", aoff), upload(ctx, "bd_voff", voff)};
+    double *d = ctx->arena.get_t<double>("bd_d", (size_t)nalf * n);
+    double *e = ctx->arena.get_t<double>("bd_e", (size_t)nalf * n);
+    double *tau = ctx->arena.get_t<double>("bd_tau", (size_t)nalf * n);
+    double *w = ctx->arena.get_t<double>("bd_w", (size_t)nalf * n);
+    int *cnt = ctx->arena.get_t<int>("bd_cnt", nalf);
+    launch_tridiag_batched(bd, H, d, e, tau, n, st);
+    launch_eigvals_batched(bd, d, e, w, cnt, p.zcut ? 1 : 0, p.emax2_au, st);
+    CK(cudaGetLastError());
+    // selection: cut2dr (:3323-3377) or choosr (:3223-3319), then testiv (:3380-3451)
+    std::vector<int> sel = download(ctx, cnt, nalf);
+    if (p.zcut) {
+        long long tot = 0;
+        for (int b = 0; b < nalf; ++b) {
+            tot += sel[b];
+            if (tot > p.max3d) throw HostError{DVR3D_ERR_CORE_MAX3D, "number of 2d eigenvalues greater than max3d"};
+        }
+    } else {
+        std::vector<double> all = download(ctx, w, (size_t)nalf * n);
+        std::vector<double> srt = all;
+        std::sort(srt.begin(), srt.end());
+        const double emax = ((long long)srt.size() <= p.max3d) ? srt.back() : srt[p.max3d - 1];
+        for (int b = 0; b < nalf; ++b) {
+            int c = 0;
+            while (c < n && all[(size_t)b * n + c] <= emax) ++c;
+            sel[b] = c;
+        }
+    }
+    if (p.jrot > 0) {
+        int iend = nalf;
+        for (int i = nalf / 2; i <= nalf; ++i)
+            if (i >= 1 && sel[i - 1] == 0) {
+                iend = i;
+                break;
+            }
+        for (int i = iend + 1; i <= nalf; ++i) sel[i - 1] = 0;
+        if (sel[nalf - 1] > 0) {
+            if (p.zlin) sel[nalf - 1] = 0;
+            else throw HostError{DVR3D_ERR_THETA0, "bisector embedding: wavefunction has amplitude for theta = 0"};
+        }
+    }
+    const int N = std::accumulate(sel.begin(), sel.end(), 0);
+    out.iv2 = sel;
+    out.nblocks = nalf;
+    out.N = N;
+    out.P = n;
+    out.ldv = round_up(n, 16);
+    if (N == 0) return;
+    const long long ncol = round_up(N, 64);
+    out.Vt = ctx->arena.get_t<double>("vt", (size_t)out.ldv * ncol);
+    CK(cudaMemsetAsync(out.Vt, 0, sizeof(double) * out.ldv * ncol, st));
+    std::vector<long long> zoff(nalf);
+    std::vector<int> zld(nalf, (int)out.ldv);
+    std::vector<int> gcol(N);
+    std::vector<long long> emap(N);
+    long long col = 0;
+    for (int b = 0; b < nalf; ++b) {
+        zoff[b] = col * out.ldv;
+        for (int j = 0; j < sel[b]; ++j) {
+            gcol[col + j] = b;
+            emap[col + j] = voff[b] + j;
+        }
+        col += sel[b];
+    }
+    std::vector<long long> woff;
+    long long wtot;
+    eigvecs_work(nv, sel, woff, wtot);
+    double *work = ctx->arena.get_t<double>("evwork", (size_t)wtot);
+    int *err = ctx->arena.get_t<int>("err", 1);
+    CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+    launch_eigvecs_batched(bd, H, d, e, tau, w, upload(ctx, "sel", sel), upload(ctx, "zoff", zoff),
+                           upload(ctx, "zld", zld), out.Vt, work, upload(ctx, "woff", woff), n, err, st);
+    CK(cudaGetLastError());
+    // sqrt of the pair weight w_p = 1/(2 mu r_a^2) + 1/(2 mu r_b^2) (blc2d2 :3537-3539)
+    std::vector<double> sw(out.ldv, 0.0);
+    for (int q = 0; q < n; ++q) {
+        const double ra = p.r1[pa[q]], rbv = p.r1[pb[q]];
+        sw[q] = std::sqrt(0.5 / (ra * ra * p.ur1) + 0.5 / (rbv * rbv * p.ur1));
+    }
+    launch_scale_rows(out.Vt, (int)out.ldv, N, upload(ctx, "sw", sw), st);
+    out.g = upload(ctx, "gcol", gcol);
+    out.e2 = ctx->arena.get_t<double>("e2", N);
+    launch_gather(w, upload(ctx, "emap", emap), out.e2, N, st);
+    out.T = xl;
+    out.ldt = p.idvr;
+    CK(cudaGetLastError());
+}
+
+// ---------------------------------------------------------------- Jacobi (jhmain)
+void jacobi_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
+    cudaStream_t st = ctx->stream;
+    const int na = p.npnta, nbp = p.npntb, ncp = p.npntc;
+    if (na > 1024) throw HostError{DVR3D_ERR_UNSUPPORTED, "1D block larger than 1024"};
+    double *r1 = upload(ctx, "r1", p.r1);
+    double *r2 = upload(ctx, "r2", p.r2);
+    double *xalf = upload(ctx, "xalf", p.xalf);
+    double *xk1 = upload(ctx, "xk1", p.xk1);
+    double *xk2 = upload(ctx, "xk2", p.xk2);
+    double *xl = upload(ctx, "xlmatr", p.xlmatr);
+    // ---- 1D stage (mkham1 / diag / cut1d, :1975-2003)
+    Jacobi1D j1{};
+    j1.npnta = na;
+    j1.npntb = nbp;
+    j1.npntc = ncp;
+    j1.ztheta = p.ztheta;
+    j1.zr2r1 = p.zr2r1;
+    j1.zembed = p.zembed;
+    j1.jrot = p.jrot;
+    j1.r1 = r1;
+    j1.r2 = r2;
+    j1.xalf = xalf;
+    if (p.ztheta) {
+        j1.ta = xl;
+        j1.lda = p.idvr;
+    } else {
+        j1.ta = p.zr2r1 ? xk2 : xk1;
+        j1.lda = p.zr2r1 ? p.npnt2 : p.npnt1;
+    }
+    j1.ur1 = p.ur1;
+    j1.ur2 = p.ur2;
+    j1.urr1 = p.urr1;
+    j1.urr2 = p.urr2;
+    j1.term = p.term;
+    j1.pes = ctx->pes;
+    if (j1.pes.kind == DVR3D_PES_GRID) {
+        if (ctx->pes_grid.size() < (size_t)p.idvr * p.npnt1 * p.npnt2)
+            throw HostError{DVR3D_ERR_ARG, "tabulated PES smaller than the DVR grid"};
+        j1.pes.grid = upload(ctx, "pesgrid", ctx->pes_grid);
+        j1.pes.npnt1 = p.npnt1;
+        j1.pes.npnt2 = p.npnt2;
+    }
+    const int nb1 = ncp * nbp;
+    double *H1 = ctx->arena.get_t<double>("blk1", (size_t)nb1 * na * na);
+    launch_jacobi_build1d(j1, nb1, H1, st);
+    std::vector<int> nv1(nb1, na);
+    std::vector<long long> aoff1(nb1), voff1(nb1);
+    for (int b = 0; b < nb1; ++b) {
+        aoff1[b] = (long long)b * na * na;
+        voff1[b] = (long long)b * na;
+    }
+    BatchDesc bd1{nb1, upload(ctx, "bd1_n", nv1), upload(ctx, "bd1_aoff", aoff1), upload(ctx, "bd1_voff", voff1)};
+    double *d1 = ctx->arena.get_t<double>("bd1_d", (size_t)nb1 * na);
+    double *e1 = ctx->arena.get_t<double>("bd1_e", (size_t)nb1 * na);
+    double *t1 = ctx->arena.get_t<double>("bd1_tau", (size_t)nb1 * na);
+    double *w1 = ctx->arena.get_t<double>("bd1_w", (size_t)nb1 * na);
+    int *c1 = ctx->arena.get_t<int>("bd1_cnt", nb1);
+    launch_tridiag_batched(bd1, H1, d1, e1, t1, na, st);
+    launch_eigvals_batched(bd1, d1, e1, w1, c1, p.zall ? 0 : 2, p.emax1_au, st);
+    CK(cudaGetLastError());
+    std::vector<int> iv1 = download(ctx, c1, nb1);
+    std::vector<int> n2(ncp, 0);
+    std::vector<long long> uoff(ncp), zoff1(nb1), e1off(ncp);
+    long long ut = 0, et = 0;
+    for (int ic = 0; ic < ncp; ++ic) {
+        uoff[ic] = ut;
+        e1off[ic] = et;
+        int s = 0;
+        for (int ib = 0; ib < nbp; ++ib) {
+            zoff1[ic * nbp + ib] = ut + (long long)na * s;
+            s += iv1[ic * nbp + ib];
+            if (s > p.max2d && !p.zall) throw HostError{DVR3D_ERR_CORE_MAX2D, "core exceeded: reduce cut-off emax1"};
+        }
+        n2[ic] = s;
+        ut += (long long)na * s;
+        et += s;
+    }
+    double *U = ctx->arena.get_t<double>("u1", (size_t)std::max<long long>(ut, 1));
+    {
+        std::vector<long long> woff;
+        long long wtot;
+        eigvecs_work(nv1, iv1, woff, wtot);
+        double *work = ctx->arena.get_t<double>("evwork", (size_t)wtot);
+        int *err = ctx->arena.get_t<int>("err", 1);
+        CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+        std::vector<int> zld1(nb1, na);
+        launch_eigvecs_batched(bd1, H1, d1, e1, t1, w1, upload(ctx, "sel1", iv1), upload(ctx, "zoff1", zoff1),
+                               upload(ctx, "zld1", zld1), U, work, upload(ctx, "woff1", woff), na, err, st);
+        CK(cudaGetLastError());
+    }
+    // 1D eigenvalues and coordinate-b index of each 2D basis function
+    std::vector<long long> e1map(std::max<long long>(et, 1));
+    std::vector<int> bidx(std::max<long long>(et, 1));
+    for (int ic = 0; ic < ncp; ++ic) {
+        long long q = e1off[ic];
+        for (int ib = 0; ib < nbp; ++ib)
+            for (int jj = 0; jj < iv1[ic * nbp + ib]; ++jj) {
+                e1map[q] = voff1[ic * nbp + ib] + jj;
+                bidx[q] = ib;
+                ++q;
+            }
+    }
+    double *e1v = ctx->arena.get_t<double>("e1v", (size_t)std::max<long long>(et, 1));
+    launch_gather(w1, upload(ctx, "e1map", e1map), e1v, et, st);
+    // ---- 2D stage (mkham2 / diag / cut2d | choose, :2019-2053)
+    std::vector<int> blocks;  // ic with n2 > 0
+    for (int ic = 0; ic < ncp; ++ic)
+        if (n2[ic] > 0) blocks.push_back(ic);
+    const int nb2 = (int)blocks.size();
+    int n2max = 0;
+    std::vector<long long> hoff(ncp, 0), aoff2, voff2;
+    std::vector<int> nv2;
+    long long ht = 0, vt = 0;
+    for (int ic = 0; ic < ncp; ++ic) {
+        hoff[ic] = ht;
+        ht += (long long)n2[ic] * n2[ic];
+        n2max = std::max(n2max, n2[ic]);
+    }
+    for (int ic : blocks) {
+        nv2.push_back(n2[ic]);
+        aoff2.push_back(hoff[ic]);
+        voff2.push_back(vt);
+        vt += n2[ic];
+    }
+    if (n2max > 1024) throw HostError{DVR3D_ERR_UNSUPPORTED, "2D block larger than 1024"};
+    Jacobi2D j2{};
+    j2.npnta = na;
+    j2.npntb = nbp;
+    j2.n2 = upload(ctx, "n2", n2);
+    j2.uoff = upload(ctx, "uoff", uoff);
+    j2.U = U;
+    j2.bidx = upload(ctx, "bidx", bidx);
+    j2.e1off = upload(ctx, "e1off", e1off);
+    j2.e1 = e1v;
+    if (p.ztheta) {
+        j2.tb = p.zr2r1 ? xk2 : xk1;
+        j2.ldb = p.zr2r1 ? p.npnt2 : p.npnt1;
+    } else {
+        j2.tb = p.zr2r1 ? xk1 : xk2;
+        j2.ldb = p.zr2r1 ? p.npnt1 : p.npnt2;
+    }
+    j2.hoff = upload(ctx, "hoff", hoff);
+    double *H2 = ctx->arena.get_t<double>("blk2", (size_t)std::max<long long>(ht, 1));
+    std::vector<int> sel2(nb2, 0);
+    std::vector<int> s2(ncp, 0);
+    double *d2 = nullptr, *e2d = nullptr, *t2 = nullptr, *w2 = nullptr;
+    BatchDesc bd2{};
+    if (nb2 > 0) {
+        launch_jacobi_build2d(j2, ncp, n2max, H2, st);
+        bd2 = BatchDesc{nb2, upload(ctx, "bd2_n", nv2), upload(ctx, "bd2_aoff", aoff2), upload(ctx, "bd2_voff", voff2)};
+        d2 = ctx->arena.get_t<double>("bd2_d", (size_t)vt);
+        e2d = ctx->arena.get_t<double>("bd2_e", (size_t)vt);
+        t2 = ctx->arena.get_t<double>("bd2_tau", (size_t)vt);
+        w2 = ctx->arena.get_t<double>("bd2_w", (size_t)vt);
+        int *c2 = ctx->arena.get_t<int>("bd2_cnt", nb2);
+        launch_tridiag_batched(bd2, H2, d2, e2d, t2, n2max, st);
+        const bool zcut = p.zcut;
+        launch_eigvals_batched(bd2, d2, e2d, w2, c2, zcut ? 2 : 0, p.emax2_au, st);
+        CK(cudaGetLastError());
+        sel2 = download(ctx, c2, nb2);
+        if (zcut) {
+            long long tot = 0;
+            for (int q = 0; q < nb2; ++q) {
+                tot += sel2[q];
+                if (tot > p.max3d && !p.zall) throw HostError{DVR3D_ERR_CORE_MAX3D, "core exceeded: reduce cut-off emax2"};
+            }
+        } else {
+            // choose (:2767-2867): the max3d lowest over all blocks, ties to the lower block
+            std::vector<double> all = download(ctx, w2, (size_t)vt);
+            long long nhamsm = vt;
+            long long low3d = std::min<long long>(p.max3d, nhamsm);
+            std::vector<int> ptr(nb2, 0);
+            for (long long q = 0; q < low3d; ++q) {
+                int best = -1;
+                double bv = 0.0;
+                for (int bb = 0; bb < nb2; ++bb) {
+                    if (ptr[bb] >= nv2[bb]) continue;
+                    const double v = all[voff2[bb] + ptr[bb]];
+                    if (best < 0 || v < bv) {
+                        best = bb;
+                        bv = v;
+                    }
+                }
+                ptr[best] += 1;
+            }
+            sel2 = ptr;
+        }
+        for (int q = 0; q < nb2; ++q) s2[blocks[q]] = sel2[q];
+    }
+    const int N = std::accumulate(s2.begin(), s2.end(), 0);
+    out.iv2 = s2;
+    out.nblocks = ncp;
+    out.N = N;
+    out.P = na * nbp;
+    out.ldv = round_up(out.P, 16);
+    if (N == 0) return;
+    // 2D eigenvectors of the selected levels
+    std::vector<long long> v2off(ncp, 0), zoff2(nb2);
+    std::vector<int> zld2(nb2);
+    long long v2t = 0;
+    for (int q = 0; q < nb2; ++q) {
+        const int ic = blocks[q];
+        v2off[ic] = v2t;
+        zoff2[q] = v2t;
+        zld2[q] = n2[ic];
+        v2t += (long long)n2[ic] * sel2[q];
+    }
+    double *V2 = ctx->arena.get_t<double>("v2", (size_t)std::max<long long>(v2t, 1));
+    {
+        std::vector<long long> woff;
+        long long wtot;
+        eigvecs_work(nv2, sel2, woff, wtot);
+        double *work = ctx->arena.get_t<double>("evwork", (size_t)wtot);
+        int *err = ctx->arena.get_t<int>("err", 1);
+        CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+        launch_eigvecs_batched(bd2, H2, d2, e2d, t2, w2, upload(ctx, "sel2", sel2), upload(ctx, "zoff2", zoff2),
+                               upload(ctx, "zld2", zld2), V2, work, upload(ctx, "woff2", woff), n2max, err, st);
+        CK(cudaGetLastError());
+    }
+    // contracted basis (mkham3 first part :2362-2411)
+    const long long ncol = round_up(N, 64);
+    out.Vt = ctx->arena.get_t<double>("vt", (size_t)out.ldv * ncol);
+    CK(cudaMemsetAsync(out.Vt, 0, sizeof(double) * out.ldv * ncol, st));
+    std::vector<int> gstart((size_t)ncp * (nbp + 1));
+    std::vector<long long> col0(ncp);
+    std::vector<int> gcol(N);
+    std::vector<long long> emap(N);
+    long long col = 0;
+    int s2max = 0;
+    for (int ic = 0; ic < ncp; ++ic) {
+        int s = 0;
+        for (int ib = 0; ib < nbp; ++ib) {
+            gstart[(size_t)ic * (nbp + 1) + ib] = s;
+            s += iv1[ic * nbp + ib];
+        }
+        gstart[(size_t)ic * (nbp + 1) + nbp] = s;
+        col0[ic] = col;
+        s2max = std::max(s2max, s2[ic]);
+        col += s2[ic];
+    }
+    for (int q = 0; q < nb2; ++q) {
+        const int ic = blocks[q];
+        for (int j = 0; j < sel2[q]; ++j) {
+            gcol[col0[ic] + j] = ic;
+            emap[col0[ic] + j] = voff2[q] + j;
+        }
+    }
+    std::vector<double> sw(out.P, 1.0);
+    if (!p.ztheta) {
+        for (int ia = 0; ia < na; ++ia)
+            for (int ib = 0; ib < nbp; ++ib) {
+                const int i1 = p.zr2r1 ? ib : ia, i2 = p.zr2r1 ? ia : ib;
+                const double wsum = 0.5 / (p.r1[i1] * p.r1[i1] * p.ur1) + 0.5 / (p.r2[i2] * p.r2[i2] * p.ur2);
+                sw[(size_t)ia * nbp + ib] = std::sqrt(wsum);
+            }
+    }
+    CTrans ct{};
+    ct.s2 = upload(ctx, "s2", s2);
+    ct.v2off = upload(ctx, "v2off", v2off);
+    ct.gstart = upload(ctx, "gstart", gstart);
+    ct.col0 = upload(ctx, "col0", col0);
+    ct.sw = upload(ctx, "sw", sw);
+    ct.ldv = out.ldv;
+    launch_jacobi_ctrans(j2, ct, ncp, s2max, V2, out.Vt, st);
+    out.g = upload(ctx, "gcol", gcol);
+    out.e2 = ctx->arena.get_t<double>("e2", N);
+    launch_gather(w2, upload(ctx, "emap", emap), out.e2, N, st);
+    if (p.ztheta) {
+        out.T = p.zr2r1 ? xk1 : xk2;
+        out.ldt = p.zr2r1 ? p.npnt1 : p.npnt2;
+    } else {
+        out.T = xl;
+        out.ldt = p.idvr;
+    }
+    CK(cudaGetLastError());
+}
+
+__global__ void resid_kernel(const double *R, const double *Z, const double *w, int n, long long ld, int nev,
+                             double *res) {
+    const int j = blockIdx.x;
+    if (j >= nev) return;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < n; i += blockDim.x) {
+        const double r = R[(size_t)j * ld + i] - w[j] * Z[(size_t)j * ld + i];
+        s += r * r;
+    }
+    __shared__ double red[32];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) res[j] = sqrt(s);
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------- one k block
+void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_options &opt,
+                 dvr3d_result &res) {
+    auto th0 = std::chrono::steady_clock::now();
+    if (ctx->pes.kind != DVR3D_PES_MORSE_SUM && ctx->pes.kind != DVR3D_PES_GRID)
+        throw HostError{DVR3D_ERR_ARG, "no potential selected (dvr3d_b200_set_pes)"};
+    BlockPlan p;
+    plan_block(deck, kk, p);
+    auto th1 = std::chrono::steady_clock::now();
+    cudaStream_t st = ctx->stream;
+    CK(cudaEventRecord(ctx->ev[0], st));
+    Contracted C;
+    if (p.radau) radau_stage(ctx, p, C);
+    else jacobi_stage(ctx, p, C);
+    CK(cudaEventRecord(ctx->ev[1], st));
+    const int N = C.N;
+    res.kz = p.kz;
+    res.ipar = p.ipar;
+    res.nham3 = N;
+    res.nblocks = C.nblocks;
+    res.iterations = 0;
+    res.fallback = 0;
+    if (res.iv2 && res.iv2_cap >= C.nblocks)
+        for (int b = 0; b < C.nblocks; ++b) res.iv2[b] = C.iv2[b];
+    const int meval = std::min(p.neval, N);
+    res.meval = meval;
+    if (N == 0) {
+        res.max_resid = 0.0;
+        return;
+    }
+    if (res.eval && res.eval_cap < meval) throw HostError{DVR3D_ERR_BUFFER, "eval buffer smaller than min(neval, N)"};
+    // ---- assembly (bloc3d / mkham3+loadh)
+    double *H3 = ctx->arena.get_t<double>("h3", (size_t)N * N);
+    AsmParams ap{};
+    ap.Vt = C.Vt;
+    ap.ldv = C.ldv;
+    ap.n = N;
+    ap.g = C.g;
+    ap.T = C.T;
+    ap.ldt = C.ldt;
+    ap.e2 = C.e2;
+    ap.H = H3;
+    ap.ldh = N;
+    launch_assemble_h3(ap, st);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ctx->ev[2], st));
+    if (opt.want_h3 && res.h3) {
+        if (res.h3_cap < (size_t)N * N) throw HostError{DVR3D_ERR_BUFFER, "h3 buffer too small"};
+        CK(cudaMemcpyAsync(res.h3, H3, sizeof(double) * N * N, cudaMemcpyDeviceToHost, st));
+    }
+    // ---- final eigensolve (diag3d), plain FP64 path
+    double *Hw = ctx->arena.get_t<double>("h3w", (size_t)N * N);
+    CK(cudaMemcpyAsync(Hw, H3, sizeof(double) * N * N, cudaMemcpyDeviceToDevice, st));
+    DenseTri dt{};
+    dt.A = Hw;
+    dt.lda = N;
+    dt.n = N;
+    dt.d = ctx->arena.get_t<double>("dt_d", N);
+    dt.e = ctx->arena.get_t<double>("dt_e", N);
+    dt.tau = ctx->arena.get_t<double>("dt_tau", N);
+    dt.scal = ctx->arena.get_t<double>("dt_scal", N);
+    dt.vp = ctx->arena.get_t<double>("dt_vp", N);
+    dt.wp = ctx->arena.get_t<double>("dt_wp", N);
+    dt.pbuf = ctx->arena.get_t<double>("dt_p", N);
+    const int G = ctx->dense_grid;
+    if ((long long)N > (long long)G * 256)
+        throw HostError{DVR3D_ERR_UNSUPPORTED, "final Hamiltonian larger than 256 rows per SM"};
+    dt.part = ctx->arena.get_t<double>("dt_part", 2 * (size_t)G);
+    dt.bar = ctx->arena.get_t<GridBarrier>("dt_bar", 1);
+    dt.err = ctx->arena.get_t<int>("dt_err", 1);
+    CK(cudaMemsetAsync(dt.bar, 0, sizeof(GridBarrier), st));
+    CK(cudaMemsetAsync(dt.err, 0, sizeof(int), st));
+    CK(launch_dense_tridiag(dt, G, st));
+    double *e2s = ctx->arena.get_t<double>("dt_e2", N);
+    double *info = ctx->arena.get_t<double>("dt_info", 4);
+    double *wv = ctx->arena.get_t<double>("dt_w", meval);
+    launch_dense_eigvals(dt.d, dt.e, N, meval, e2s, info, wv, st);
+    CK(cudaGetLastError());
+    const bool vecs = opt.want_vectors || res.evec || res.resid;
+    double *Z = nullptr;
+    if (vecs) {
+        const int T = std::min(meval, 1024);
+        double *fac = ctx->arena.get_t<double>("dv_fac", (size_t)5 * N * T);
+        double *X = ctx->arena.get_t<double>("dv_x", (size_t)N * meval);
+        Z = ctx->arena.get_t<double>("dv_z", (size_t)N * meval);
+        int *cs = ctx->arena.get_t<int>("dv_cs", meval + 1);
+        int *ncl = ctx->arena.get_t<int>("dv_ncl", 1);
+        launch_dense_eigvecs(Hw, N, N, dt.d, dt.e, dt.tau, dt.scal, wv, meval, info, cs, ncl, fac, T, X, Z, N, st);
+        CK(cudaGetLastError());
+    }
+    CK(cudaEventRecord(ctx->ev[3], st));
+    check_dev_err(ctx, dt.err, "final tridiagonal reduction");
+    if (res.eval) CK(cudaMemcpyAsync(res.eval, wv, sizeof(double) * meval, cudaMemcpyDeviceToHost, st));
+    res.max_resid = -1.0;
+    if (vecs && (res.resid || opt.want_vectors)) {
+        double *R = ctx->arena.get_t<double>("dv_r", (size_t)N * meval);
+        double *rn = ctx->arena.get_t<double>("dv_rn", meval);
+        launch_dgemm(false, false, N, meval, N, 1.0, H3, N, Z, N, 0.0, R, N, st);
+        resid_kernel<<<meval, 256, 0, st>>>(R, Z, wv, N, N, meval, rn);
+        CK(cudaGetLastError());
+        std::vector<double> rv = download(ctx, rn, meval);
+        res.max_resid = 0.0;
+        for (double v : rv) res.max_resid = std::max(res.max_resid, v);
+        if (res.resid)
+            for (int j = 0; j < std::min(meval, res.resid_cap); ++j) res.resid[j] = rv[j];
+    }
+    if (res.evec && Z) {
+        if (res.evec_cap < (size_t)N * meval) throw HostError{DVR3D_ERR_BUFFER, "evec buffer too small"};
+        CK(cudaMemcpyAsync(res.evec, Z, sizeof(double) * N * meval, cudaMemcpyDeviceToHost, st));
+    }
+    CK(cudaStreamSynchronize(st));
+    float ms1 = 0, ms2 = 0, ms3 = 0;
+    CK(cudaEventElapsedTime(&ms1, ctx->ev[0], ctx->ev[1]));
+    CK(cudaEventElapsedTime(&ms2, ctx->ev[1], ctx->ev[2]));
+    CK(cudaEventElapsedTime(&ms3, ctx->ev[2], ctx->ev[3]));
+    res.stage_ms[0] = std::chrono::duration<double, std::milli>(th1 - th0).count();
+    res.stage_ms[1] = ms1;
+    res.stage_ms[2] = ms2;
+    res.stage_ms[3] = ms3;
+    res.stage_ms[4] = ms1 + ms2 + ms3;
+    res.stage_ms[5] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - th0).count();
+}
+
+}  // namespace dvr3d

@@ -1,0 +1,192 @@
+/*
+ * dvr3d_b200.h -- C ABI of the B200-native DVR3DRJZ hot path.
+ *
+ * The library replaces, for one GPU, the numerical core of the DVR3DRJZ program of the
+ * DVR3D suite (reference file source/dvr3drjz_segmented.f90):
+ *
+ *   radial / angular DVR set-up  ->  per-angle 2D (or 1D+2D) block builds and FP64
+ *   eigensolves with energy-cut-off truncation  ->  contracted 3D Hamiltonian assembly
+ *   ->  final eigensolve for the lowest levels.
+ *
+ * Conventions (they follow the Fortran reference so a Fortran/ISO_C_BINDING or ctypes
+ * host can bind the entry points directly):
+ *   - plain C types and pointers only; every array is caller-owned host memory unless
+ *     stated; matrices are column-major FP64 (Fortran order);
+ *   - energies are in hartree (Eh) unless the name says _cm (wavenumbers);
+ *   - every entry point returns 0 on success or a negative DVR3D_ERR_* code; the library
+ *     never calls exit() or stop (the reference's STOP conditions become error codes);
+ *   - one dvr3d_ctx per host thread; the library owns all device memory in the ctx.
+ */
+#ifndef DVR3D_B200_H
+#define DVR3D_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DVR3D_B200_ABI_VERSION 1
+
+/* ---- error codes ------------------------------------------------------------------ */
+enum dvr3d_status {
+    DVR3D_OK = 0,
+    DVR3D_ERR_ARG = -1,          /* invalid argument or inconsistent input cards          */
+    DVR3D_ERR_CORE_MAX2D = -2,   /* cut1d: "core exceeded: reduce cut-off emax1"  (:2925) */
+    DVR3D_ERR_CORE_MAX3D = -3,   /* cut2d/cut2dr: "core exceeded ... emax2" (:2981,:3359) */
+    DVR3D_ERR_QUADRATURE = -4,   /* lagpt/jacobi: "points & weights in error" (:1360,:939) */
+    DVR3D_ERR_NOCONV = -5,       /* an eigensolver did not converge within its limits     */
+    DVR3D_ERR_CUDA = -6,         /* CUDA runtime error (message via strerror of the ctx)  */
+    DVR3D_ERR_NOMEM = -7,        /* device allocation failed                              */
+    DVR3D_ERR_UNSUPPORTED = -8,  /* option of the reference not implemented on this path */
+    DVR3D_ERR_THETA0 = -9,       /* testiv: wavefunction amplitude at theta = 0 (:3430)  */
+    DVR3D_ERR_PES = -10,         /* potential returned a non-finite value                 */
+    DVR3D_ERR_DECK = -11,        /* job deck could not be parsed                          */
+    DVR3D_ERR_NO_DEVICE = -12,   /* no CUDA device / extension not usable                 */
+    DVR3D_ERR_BUFFER = -13       /* caller buffer too small                               */
+};
+
+typedef struct dvr3d_ctx dvr3d_ctx;
+
+/* ---- job deck: the reference's stdin input (namelist PRT + fixed-format cards) -------- */
+/* Field meaning, defaults and card order follow block data (:83-168), insize (:171-638)
+ * and setcon (:1016-1188). Logical flags are 0/1. */
+typedef struct dvr3d_deck {
+    /* Line 1: namelist /PRT/ */
+    int zpham, zprad, zp1d, zp2d, zpmin, zpvec, zlmat, zcut, zrot, zperp, zembed, zlin;
+    int zmors1, zmors2, zladd, ztwod, zvec, zall, ztheta, zr2r1, ztran, zquad2, zdiag;
+    int zpfun, zx, zs0, zs1;
+    /* Line 2 */
+    int ncoord;
+    /* Line 3: NPNT2,JROT,NEVAL,NALF,MAX2D,MAX3D,IDIA,KMIN,NPNT1,IPAR,MAX3D2 (11I5) */
+    int npnt2, jrot, neval, nalf, max2d, max3d, idia, kmin, npnt1, ipar, max3d2;
+    /* Line 4 */
+    char title[80];
+    /* Lines 5-10 (F20.0 fields) */
+    double fixcos;
+    double xmass[3], xmassr[3];
+    double emax1, emax2;                 /* cm-1 */
+    double re1, diss1, we1, re2, diss2, we2;
+    /* optional trailing card read by diag3d for odd-parity band origins (:2751) */
+    double ezero;
+    int have_ezero;
+} dvr3d_deck;
+
+/* ---- potential energy surface ------------------------------------------------------ */
+/* The reference's plugin is SUBROUTINE POTV(V,R1,R2,XCOS) (docum.tex:30-47; called from
+ * mkham1 :2178-2183 and blc2d1 :3199,:3204). A host callback cannot run on the GPU, so a
+ * potential is either one of the device-built families below, or a table of V that the
+ * host evaluated with its own POTV at the DVR grid returned by dvr3d_b200_grid(). */
+typedef enum dvr3d_pes_kind {
+    DVR3D_PES_NONE = 0,
+    /* V = D1 (1-exp(-a1 (r1-re1)))^2 + D2 (1-exp(-a2 (r2-re2)))^2
+     *   + kb (cos t - c0)^2 + c12 (r1-re1)(r2-re2) + sum_{l=1..4} cl P_l(cos t)
+     * params[13] = {D1, a1, re1, D2, a2, re2, kb, c0, c12, c1, c2, c3, c4} (Eh, bohr) */
+    DVR3D_PES_MORSE_SUM = 1,
+    /* V tabulated on the grid: v[(ic*npnt2 + i2)*npnt1 + i1] = V(r1[i1], r2[i2], xalf[ic]);
+     * for Radau (idia=-2) r2 == r1. Set with dvr3d_b200_set_pes_grid(). */
+    DVR3D_PES_GRID = 2
+} dvr3d_pes_kind;
+
+#define DVR3D_PES_MORSE_SUM_NPARAM 13
+
+/* ---- solve options and results ------------------------------------------------------- */
+typedef enum dvr3d_precision {
+    DVR3D_PREC_FP64 = 0,             /* plain FP64 GPU path: dense FP64 final eigensolve  */
+    DVR3D_PREC_MIXED_DAVIDSON = 1    /* BF16x3/FP32 tensor-core H*v, FP64 Rayleigh-Ritz,
+                                        block-Davidson, optional learned preconditioner   */
+} dvr3d_precision;
+
+typedef struct dvr3d_options {
+    int precision;          /* dvr3d_precision                                              */
+    int nlevels;            /* levels wanted (0: NEVAL of the deck)                         */
+    double tol_cm;          /* Davidson: max eigenvalue error target in cm-1 (0: 1e-4)      */
+    int max_iter;           /* Davidson iteration limit (0: 200)                            */
+    int block;              /* Davidson block size (0: automatic)                           */
+    int learned_precond;    /* 1: use the trained preconditioner network if one is loaded  */
+    int want_vectors;       /* 1: return eigenvectors of the final Hamiltonian in evec      */
+    int want_h3;            /* 1: copy the assembled final Hamiltonian (lower) into h3      */
+} dvr3d_options;
+
+typedef struct dvr3d_result {
+    /* outputs */
+    int kz, ipar;           /* k block and parity solved                                    */
+    int nham3;              /* dimension of the final contracted Hamiltonian                */
+    int meval;              /* levels written to eval (min(neval, nham3))                   */
+    int nblocks;            /* number of angular (Radau) / last-coordinate (Jacobi) blocks  */
+    int iterations;         /* Davidson iterations (0 on the dense path)                    */
+    int fallback;           /* 1 if the Davidson path fell back to the dense FP64 solve     */
+    double stage_ms[6];     /* device time: 0 set-up, 1 block builds+eigensolves+selection,
+                               2 assembly, 3 final eigensolve, 4 total, 5 host set-up       */
+    double max_resid;       /* max FP64 residual ||H x - e x|| over returned levels (Eh)    */
+    /* caller-provided buffers (may be NULL / 0) */
+    double *eval;   int eval_cap;     /* levels (Eh), ascending                               */
+    int *iv2;       int iv2_cap;      /* per-block selection counts (blocks in solve order)   */
+    double *resid;  int resid_cap;    /* per-level FP64 residual norms (Eh)                   */
+    double *evec;   size_t evec_cap;  /* nham3 x meval, column-major                          */
+    double *h3;     size_t h3_cap;    /* nham3 x nham3, column-major, lower triangle valid    */
+} dvr3d_result;
+
+/* ---- entry points ----------------------------------------------------------------- */
+
+/* Create a context on CUDA device `device`. Fails with DVR3D_ERR_NO_DEVICE when no
+ * usable sm_100 device is present (no CPU fallback exists). */
+int dvr3d_b200_init(int device, dvr3d_ctx **out);
+void dvr3d_b200_destroy(dvr3d_ctx *ctx);
+const char *dvr3d_b200_strerror(int code);
+/* Last detailed error message of this context (CUDA error text, offending sizes). */
+const char *dvr3d_b200_last_error(const dvr3d_ctx *ctx);
+/* Use `stream` (a cudaStream_t) for all work of this context; NULL = the ctx's own. */
+int dvr3d_b200_set_stream(dvr3d_ctx *ctx, void *stream);
+
+/* Reads a job deck in the reference's stdin format: namelist PRT (dvr3d :65, defaults of
+ * block data :158-167), card 2 (insize :232), card 3 (:238), title (:372) and the setcon
+ * cards (:1042-1095, in the source's order FIXCOS, XMASS, XMASSR, EMAX1/EMAX2, r1 Morse,
+ * r2 Morse), plus the optional EZERO card (:2751). Host-only; needs no GPU. */
+int dvr3d_b200_parse_deck(const char *text, dvr3d_deck *out);
+
+/* Select the potential. Replaces linking a POTV routine (docum.tex:30-47). */
+int dvr3d_b200_set_pes(dvr3d_ctx *ctx, int kind, const double *params, int nparams);
+/* Table of V for DVR3D_PES_GRID (layout documented at DVR3D_PES_GRID). */
+int dvr3d_b200_set_pes_grid(dvr3d_ctx *ctx, const double *v, size_t n);
+
+/* DVR grid of one k block, so a host can evaluate its own POTV there: r1[npnt1],
+ * r2[npnt2] (bohr; r2 = r1 for Radau idia=-2) and xalf[nalf] (cos theta, full range),
+ * as computed by lagpt (:1290-1366), jacobi/allpts (:1635-1772). */
+int dvr3d_b200_grid(dvr3d_ctx *ctx, const dvr3d_deck *deck, int kz,
+                    double *r1, int n1cap, double *r2, int n2cap, double *xalf, int nacap);
+
+/* Solve one k block of one deck. Replaces, for that block, the per-k driver call of
+ * ccmain (:988-1006): nfmain(hr,htheta,r,theta,kz) (:3006, Radau idia=-2 in-plane) or
+ * jhmain(xk1,xk2,xlmatr,r1,r2,xalf,r2m2t,kz) (:1915, Jacobi/scattering and idia=-1),
+ * including their calls of diag -> dsyev (:2638-2659) and diag3d (:2661-2764). */
+int dvr3d_b200_solve_block(dvr3d_ctx *ctx, const dvr3d_deck *deck, int kz,
+                           const dvr3d_options *opt, dvr3d_result *res);
+
+/* Solve `nprob` independent J=0 decks, each with its own PES parameter row
+ * (pes_params[i*DVR3D_PES_MORSE_SUM_NPARAM ...]), as one batched device workload. This is
+ * the repeated-caller pattern of the reference's fitting driver (SFIT_DVR3D runs DVR3DRJZ
+ * once per trial surface, SFIT_DVR3D/H2S/dvr3d_sfit.f90:746-832). */
+int dvr3d_b200_solve_batch(dvr3d_ctx *ctx, const dvr3d_deck *decks, const double *pes_params,
+                           int nprob, const dvr3d_options *opt, dvr3d_result *res);
+
+/* Run a whole job like `program DVR3DRJZ` (:1-80): parse, loop over k blocks as ccmain
+ * (:857-1007) does, and write the level tables of diag3d (:2703-2761) into `out` (NUL-
+ * terminated; *outlen receives the length needed). Levels in the fort.14 layout of zpfun
+ * (:2708-2719) go to `lev` when non-NULL. */
+int dvr3d_b200_run_deck(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_options *opt,
+                        char *out, size_t outcap, size_t *outlen,
+                        char *lev, size_t levcap, size_t *levlen);
+
+/* Batched replacement of diag(ham,maxham,nham,eig) -> dsyev('V','L',...) (:2638-2659) for
+ * many independent symmetric blocks already on the device: block b is n[b] x n[b] at
+ * a + off[b] with leading dimension n[b] (lower triangle read). Eigenvalues ascending go
+ * to w + woff[b]; when vecs != 0 the eigenvectors overwrite the blocks. Device pointers. */
+int dvr3d_b200_diag_batched(dvr3d_ctx *ctx, int nblk, const int *n_host,
+                            const long long *off_host, const long long *woff_host,
+                            double *a_dev, double *w_dev, int vecs);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* DVR3D_B200_H */

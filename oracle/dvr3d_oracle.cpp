@@ -1,0 +1,1411 @@
+// dvr3d_oracle.cpp -- CPU FP64 restatement of the DVR3DRJZ hot path (the oracle).
+//
+// TEST INFRASTRUCTURE ONLY: the checker used by tests/, __graft_entry__.smoke() and the
+// CPU-baseline leg of bench.py. The product library never links or calls it.
+//
+// Every routine below restates the routine of the reference file
+// source/dvr3drjz_segmented.f90 named in its comment (line numbers of that file), keeping
+// its loop order and arithmetic so its FP64 results agree with the reference to rounding.
+// Scratch Fortran units of the reference (ivecs1, ieigs1, ivint, iband, intvec ...) are
+// replaced by in-memory arrays holding the same records. LAPACK dsyev is resolved at run
+// time from a shared object (scipy's OpenBLAS), as the reference links LAPACK.
+
+#include "dvr3d_oracle.h"
+
+#include <dlfcn.h>
+
+#include <algorithm>
+#include <chrono>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <random>
+#include <stdexcept>
+#include <vector>
+
+namespace {
+
+// ------------------------------------------------------------------ LAPACK binding
+typedef void (*dsyev_t)(const char *, const char *, const int *, double *, const int *,
+                        double *, double *, const int *, int *, size_t, size_t);
+typedef void (*dsyevd_t)(const char *, const char *, const int *, double *, const int *,
+                         double *, double *, const int *, int *, const int *, int *, size_t,
+                         size_t);
+dsyev_t g_dsyev = nullptr;
+dsyevd_t g_dsyevd = nullptr;
+
+struct Fail {
+    int code;
+};
+[[noreturn]] void fail(int code) { throw Fail{code}; }
+
+const double autocm = 2.19474624e+05;  // diag3d :2681, cut1d :2895
+const double amtoau = 1.8228883e03;    // setcon :1037
+
+// diag(ham,maxham,nham,eig) :2638-2659: dsyev('V','L',nham,ham,maxham,eig,work,3*maxham)
+void diag(double *ham, int maxham, int nham, double *eig, int mode = 0) {
+    if (nham <= 0) return;
+    int info = 0;
+    if (mode == 1 && g_dsyevd) {
+        int lwork = 1 + 6 * nham + 2 * nham * nham, liwork = 3 + 5 * nham;
+        std::vector<double> work(lwork);
+        std::vector<int> iwork(liwork);
+        g_dsyevd("V", "L", &nham, ham, &maxham, eig, work.data(), &lwork, iwork.data(),
+                 &liwork, &info, 1, 1);
+    } else {
+        if (!g_dsyev) fail(DVR3D_ERR_ARG);
+        int lwork = 3 * maxham;
+        std::vector<double> work(lwork);
+        g_dsyev("V", "L", &nham, ham, &maxham, eig, work.data(), &lwork, &info, 1, 1);
+    }
+    // the reference only prints ifail (:2656); a failed LAPACK call is reported here
+    if (info != 0) fail(DVR3D_ERR_NOCONV);
+}
+
+// ------------------------------------------------------------------ problem state
+struct Run {
+    // COMMON /size/
+    int npnt1, npnt2, nalf, nmax1, nmax2, maxleg, nalf2, idvr, npnt, nlim1, nlim2, neval;
+    int ncoord, jrot, kmin, idia, ipar, max2d, max3d, max2d2, max3d2, npnta, npntb, npntc;
+    int ndima, ndimb, ndimc;
+    double emax1, emax2;
+    // COMMON /outp/ (hot-path subset)
+    bool zrot, zembed, zmors1, zmors2, zcut, zall, zlin, zladd, zquad2, ztheta, zr2r1;
+    bool zbisc, zperp, ztwod, zladd_;
+    // COMMON /oupb/
+    double xp0, xp1, xp2;
+    // COMMON /split1/, /split2/, /mass/
+    double re1, diss1, we1, beta1, ur1, urr1, a1;
+    int iu1;
+    double re2, diss2, we2, beta2, ur2, urr2, a2;
+    int iu2;
+    double xmass[3], xmassr[3], g1, g2;
+    // ccmain arrays
+    std::vector<double> r1, r2, wt1, wt2, y1, y2, xk1, xk2;  // xk column-major npnt x npnt
+    double csx1 = 0, csa1 = 0, tsx1 = 0, tsa1 = 0, csx2 = 0, csa2 = 0, tsx2 = 0, tsa2 = 0;
+    // per-k
+    int kz, kd, ku, nidvr, nang, nang2, lincr;
+    std::vector<double> xalf, walf, xhalf, whalf, xlmatr, pleg;  // xlmatr idvr x idvr
+    double cswalf = 0, tswalf = 0;
+    // potential
+    int pes_kind = 0;
+    std::vector<double> pes;
+    const double *vgrid = nullptr;
+    size_t nvgrid = 0;
+};
+
+double pes_morse_sum(const double *p, double r1, double r2, double x) {
+    double d1 = r1 - p[2], d2 = r2 - p[5];
+    double m1 = 1.0 - std::exp(-p[1] * d1);
+    double m2 = 1.0 - std::exp(-p[4] * d2);
+    double x2 = x * x;
+    double P1 = x, P2 = 0.5 * (3.0 * x2 - 1.0), P3 = 0.5 * (5.0 * x2 - 3.0) * x;
+    double P4 = (35.0 * x2 * x2 - 30.0 * x2 + 3.0) / 8.0;
+    double dc = x - p[7];
+    return p[0] * m1 * m1 + p[3] * m2 * m2 + p[6] * dc * dc + p[8] * d1 * d2 + p[9] * P1 +
+           p[10] * P2 + p[11] * P3 + p[12] * P4;
+}
+
+// POTV(V,R1,R2,XCOS) plugin (docum.tex:30-47). For a tabulated surface the point is
+// identified by its grid indices.
+double potv(const Run &R, double r1, double r2, double x, int i1, int i2, int ia) {
+    double v;
+    if (R.pes_kind == DVR3D_PES_MORSE_SUM) {
+        v = pes_morse_sum(R.pes.data(), r1, r2, x);
+    } else if (R.pes_kind == DVR3D_PES_GRID) {
+        size_t idx = ((size_t)ia * R.npnt2 + i2) * R.npnt1 + i1;
+        if (!R.vgrid || idx >= R.nvgrid) fail(DVR3D_ERR_ARG);
+        v = R.vgrid[idx];
+    } else {
+        fail(DVR3D_ERR_ARG);
+    }
+    if (!std::isfinite(v)) fail(DVR3D_ERR_PES);
+    return v;
+}
+
+// insize :171-638 (derived sizes only; the printing is omitted) and setcon :1016-1188.
+void insize_setcon(Run &R, const dvr3d_deck &d) {
+    R.zrot = d.zrot;
+    R.zembed = d.zembed;
+    R.zmors1 = d.zmors1;
+    R.zmors2 = d.zmors2;
+    R.zcut = d.zcut;
+    R.zall = d.zall;
+    R.zlin = d.zlin;
+    R.zladd = d.zladd;
+    R.zquad2 = d.zquad2;
+    R.ztheta = d.ztheta;
+    R.zr2r1 = d.zr2r1;
+    R.zperp = d.zperp;
+    R.ztwod = d.ztwod;
+    R.ncoord = d.ncoord;
+    R.npnt2 = d.npnt2;
+    R.jrot = d.jrot;
+    R.neval = d.neval;
+    R.nalf = d.nalf;
+    R.max2d = d.max2d;
+    R.max3d = d.max3d;
+    R.idia = d.idia;
+    R.kmin = d.kmin;
+    R.npnt1 = d.npnt1;
+    R.ipar = d.ipar;
+    R.max3d2 = d.max3d2;
+    R.emax1 = d.emax1;
+    R.emax2 = d.emax2;
+    for (int i = 0; i < 3; ++i) {
+        R.xmass[i] = d.xmass[i];
+        R.xmassr[i] = d.xmassr[i];
+    }
+    if (R.ztwod || R.zperp || d.ncoord == 2) fail(DVR3D_ERR_UNSUPPORTED);
+    if (!R.zmors1 || !R.zmors2) fail(DVR3D_ERR_UNSUPPORTED);  // keint2 path not restated
+    // :241-264
+    R.zbisc = false;
+    if (R.jrot == 0) {
+        R.zembed = true;
+        R.kmin = 0;
+        R.zrot = false;
+    }
+    if (R.idia == -2) {
+        R.ncoord = 3;
+        R.npnt1 = R.npnt2;
+        R.idvr = R.nalf;
+        R.zmors1 = R.zmors2;
+        R.ztheta = false;
+        if (R.jrot != 0) R.zbisc = true;
+    }
+    R.nalf2 = (R.nalf + 1) / 2;  // :281
+    R.ncoord = 3;
+    R.maxleg = R.nalf - 1;  // :306-308
+    R.nmax2 = R.npnt2 - 1;
+    R.nmax1 = R.npnt1 - 1;
+    int mi = std::max(1, R.idia);
+    if (R.ztheta) {  // :310-328
+        R.npnta = R.nalf / mi;
+        if (R.zr2r1) {
+            R.npntb = R.npnt2;
+            R.npntc = R.npnt1;
+        } else {
+            R.npntb = R.npnt1;
+            R.npntc = R.npnt2;
+        }
+    } else {
+        if (R.zr2r1) {
+            R.npnta = R.npnt2;
+            R.npntb = R.npnt1;
+        } else {
+            R.npnta = R.npnt1;
+            R.npntb = R.npnt2;
+        }
+        R.npntc = R.nalf / mi;
+    }
+    if (R.idia == -2) {  // :330-352
+        if (R.zrot && (R.jrot + R.kmin) > 1) {
+            R.max2d = R.npnt1 * (R.npnt1 + 1) / 2;
+            R.max2d2 = R.npnt1 * (R.npnt1 - 1) / 2;
+        } else {
+            R.max2d = R.npnt1 * (R.npnt1 + 1 - (R.ipar * 2)) / 2;
+            R.max2d2 = 0;
+        }
+        if (!R.zall) R.max3d = std::min(R.max3d, R.max2d * R.nalf);
+        if (R.zall) R.max3d = R.max2d * R.nalf;
+        if (R.zrot) {
+            if (R.max3d2 <= 0) R.max3d2 = R.max3d;
+            R.max3d2 = std::min(std::min(R.max3d, R.max2d2 * R.nalf), R.max3d2);
+        }
+    } else {
+        if (R.zall) {
+            R.max2d = R.npnta * R.npntb;
+            R.max3d = R.max2d * R.npntc;
+        } else {
+            R.max2d = std::min(R.max2d, R.npnta * R.npntb);
+            R.max3d = std::min(R.max3d, R.npnta * R.npntb * R.npntc);
+        }
+    }
+    if (R.neval <= 0) R.neval = 10;  // :354-355
+    R.neval = std::min(R.max3d, R.neval);
+    if (std::abs(R.idia) == 2) {  // :499-522
+        if (R.ipar != 0 && R.ipar != 1) fail(DVR3D_ERR_ARG);
+        if (R.idia == 2) {
+            R.idvr = R.nalf2;
+            if (2 * R.idvr != R.nalf) fail(DVR3D_ERR_ARG);
+        }
+    } else {
+        R.idvr = R.nalf;
+        R.ipar = 0;
+    }
+    if (R.jrot != 0) {  // :523-565
+        R.jrot = std::abs(R.jrot);
+        if (R.zrot) {
+            if (R.kmin != 0 && !R.zbisc) R.kmin = 1;
+            if (R.kmin != 0 && R.kmin != 1) R.kmin = 2;
+        } else if (std::abs(R.kmin) > std::abs(R.jrot)) {
+            fail(DVR3D_ERR_ARG);
+        }
+        if (R.zbisc) R.zembed = false;
+    }
+    R.xp0 = d.zx ? 1.0 : 0.0;  // :571-595
+    R.xp1 = d.zs0 ? 1.0 : 0.0;
+    R.xp2 = d.zs1 ? 1.0 : 0.0;
+    R.npnt = std::max(R.npnt1, R.npnt2);  // :602-612
+    R.nlim1 = R.npnt1 * (R.npnt1 + 1) / 2;
+    R.nlim2 = R.npnt2 * (R.npnt2 + 1) / 2;
+    R.ndima = R.npnta;
+    if (R.idia <= -2 && !R.zrot) R.ndima = R.ndima - R.ipar;
+    R.ndimb = R.npntb;
+    R.ndimc = R.npntc;
+    if (!R.zquad2) fail(DVR3D_ERR_UNSUPPORTED);  // :618-620 (zquad2=F needs keint2 path)
+    if (R.npnt1 < 1 || R.npnt2 < 1 || R.nalf < 1 || R.npnt1 > 120 || R.npnt2 > 120 ||
+        R.nalf > 250)
+        fail(DVR3D_ERR_ARG);
+
+    // setcon :1070-1160
+    if (R.idia >= 1) {
+        R.g1 = R.xmass[1] / (R.xmass[1] + R.xmass[2]);
+        R.g2 = 0.0;
+    } else {
+        double a = std::sqrt(R.xmass[2] / (R.xmass[0] + R.xmass[1] + R.xmass[2]));
+        double b = R.xmass[1] / (R.xmass[0] + R.xmass[1]);
+        R.g1 = 1.0 - a / (a + b - a * b);
+        R.g2 = 1.0 - a / (1.0 - b + a * b);
+    }
+    if (R.xmassr[0] <= 0.0)
+        for (int i = 0; i < 3; ++i) R.xmassr[i] = R.xmass[i];  // :1054
+    const double *xm = R.xmass, *xr = R.xmassr;
+    R.ur1 = amtoau / (R.g2 * R.g2 / xm[0] + 1.0 / xm[1] + (1.0 - R.g2) * (1.0 - R.g2) / xm[2]);
+    R.ur2 = amtoau / (1.0 / xm[0] + R.g1 * R.g1 / xm[1] + (1.0 - R.g1) * (1.0 - R.g1) / xm[2]);
+    R.urr1 = amtoau / (R.g2 * R.g2 / xr[0] + 1.0 / xr[1] + (1.0 - R.g2) * (1.0 - R.g2) / xr[2]);
+    R.urr2 = amtoau / (1.0 / xr[0] + R.g1 * R.g1 / xr[1] + (1.0 - R.g1) * (1.0 - R.g1) / xr[2]);
+    R.re1 = d.re1;
+    R.diss1 = d.diss1;
+    R.we1 = d.we1;
+    R.re2 = d.re2;
+    R.diss2 = d.diss2;
+    R.we2 = d.we2;
+    if (R.diss1 <= 0.0 || R.we1 <= 0.0) fail(DVR3D_ERR_ARG);
+    R.beta1 = R.we1 * std::sqrt(0.5 * R.ur1 / R.diss1);  // :1123-1125
+    R.a1 = 4.0 * R.diss1 / R.we1;
+    R.iu1 = (int)(R.a1 + 0.5);
+    if (R.idia != -2) {  // :1142-1149
+        if (R.diss2 <= 0.0 || R.we2 <= 0.0) fail(DVR3D_ERR_ARG);
+        R.beta2 = R.we2 * std::sqrt(0.5 * R.ur2 / R.diss2);
+        R.a2 = 4.0 * R.diss2 / R.we2;
+        R.iu2 = (int)(R.a2 + 0.5);
+    }
+}
+
+// norms :1261-1287
+void norms(std::vector<double> &dnorm, const std::vector<double> &fact, double &cc,
+           double alf, int npnt, int nmax) {
+    double count = (double)npnt + alf;
+    cc = fact[npnt] / count;  // fact is 1-based in the reference: fact(i) -> fact[i]
+    std::vector<double> bin(npnt + 2);
+    int npt1 = npnt + 1;
+    bin[npt1] = 1.0;
+    for (int i = 1; i <= npnt; ++i) {
+        int n = npt1 - i;
+        bin[n] = bin[n + 1] * count / (double)i;
+        count = count - 1.0;
+    }
+    npt1 = npt1 + 1;
+    dnorm.assign(nmax + 1, 0.0);
+    for (int i = 0; i <= nmax; ++i) dnorm[i] = std::sqrt(bin[i + 1] * fact[i + 1] * fact[npt1 - i - 1]);
+}
+
+// lgrecr :1466-1492 (b, c 1-based)
+void lgrecr(double &pn, double &dpn, double &pn1, double x, int nn, double alf,
+            const std::vector<double> &b, const std::vector<double> &c) {
+    double p1 = 1.0, p = x - alf - 1.0, dp1 = 0.0, dp = 1.0;
+    for (int j = 2; j <= nn; ++j) {
+        double q = (x - b[j]) * p - c[j] * p1;
+        double dq = (x - b[j]) * dp - c[j] * dp1 + p;
+        p1 = p;
+        p = q;
+        dp1 = dp;
+        dp = dq;
+    }
+    pn = p;
+    dpn = dp;
+    pn1 = p1;
+}
+
+// lgroot :1439-1463
+void lgroot(double &x, int nn, double alf, double &dpn, double &pn1,
+            const std::vector<double> &b, const std::vector<double> &c, double eps) {
+    const int itmax = 10;
+    int iter = 0;
+    for (;;) {
+        ++iter;
+        double p;
+        lgrecr(p, dpn, pn1, x, nn, alf, b, c);
+        double d = p / dpn;
+        x = x - d;
+        if (std::fabs(d / x) <= eps) return;
+        if (iter >= itmax) return;  // the reference warns and returns (:1459)
+    }
+}
+
+static inline double fsign1(double v) { return v >= 0.0 ? 1.0 : -1.0; }
+
+// laguer :1369-1436
+void laguer(int nn, std::vector<double> &x, std::vector<double> &a, double alf, double &csx,
+            double &csa, double &tsx, double cc) {
+    const double eps = 1.0e-12;
+    std::vector<double> b(nn + 2), c(nn + 2);
+    csx = 0.0;
+    csa = 0.0;
+    double fa = alf + 1.0;
+    b[1] = fa;
+    c[1] = 0.0;
+    double fn = 1.0;
+    for (int j = 2; j <= nn; ++j) {
+        fa = fa + 2.0;
+        b[j] = fa;
+        c[j] = fn * (alf + fn);
+        fn = fn + 1.0;
+    }
+    tsx = fn * (alf + fn);
+    double xt1 = 0.0, xt2 = 0.0;
+    double xt = (1.0 + alf) * (2.0 + alf) / (1.0 + 3.0 * fn + 2.0 * alf);
+    double step = 3.0 * (1.0 + alf) / (1.0 + 3.0 * fn + alf);
+    double pt, pt2, dpn, pn1;
+    lgrecr(pt, dpn, pn1, xt, nn, alf, b, c);
+    x.assign(nn, 0.0);
+    a.assign(nn, 0.0);
+    for (int i = 1; i <= nn; ++i) {
+        if (i <= 2) {
+            // smallest two zeros by brute-force search (:1410-1419)
+            for (;;) {
+                xt2 = xt + step;
+                lgrecr(pt2, dpn, pn1, xt2, nn, alf, b, c);
+                if (fsign1(pt) * fsign1(pt2) > 0.0) {
+                    pt = pt2;
+                    xt = xt2;
+                    continue;
+                }
+                pt = pt2;
+                xt = 0.5 * (xt + xt2);
+                break;
+            }
+        } else {
+            // Stroud & Secrest formula for the other zeros (:1421-1425)
+            double fi = (double)(i - 2);
+            double rr1 = (1.0 + 2.55 * fi) / (1.9 * fi);
+            double rr2 = 1.26 * fi * alf / (1.0 + 3.5 * fi);
+            double ratio = (rr1 + rr2) / (1.0 + 0.3 * alf);
+            xt = xt + ratio * (xt - xt2);
+        }
+        lgroot(xt, nn, alf, dpn, pn1, b, c, eps);  // :1427
+        xt2 = xt1;
+        xt1 = xt;
+        x[i - 1] = xt;
+        a[i - 1] = cc / dpn / pn1;
+        csx = csx + xt;
+        csa = csa + a[i - 1];
+    }
+}
+
+// lagpt :1290-1366 (Morse branch)
+void lagpt(std::vector<double> &y, std::vector<double> &r, std::vector<double> &wt,
+           std::vector<double> &bass, const std::vector<double> &dnorm, double cc, int npnt,
+           int nmax, double re, double beta, double a, int iu, double &csx, double &csa,
+           double &tsx, double &tsa) {
+    double alf = (double)iu;
+    double alfm1 = alf - 1.0;
+    laguer(npnt, y, wt, alf, csx, csa, tsx, cc);
+    tsa = 1.0 / (dnorm[0] * dnorm[0]);
+    r.assign(npnt, 0.0);
+    bass.assign((size_t)(nmax + 1) * npnt, 0.0);  // bass(0:nmax, npnt)
+    for (int i = 0; i < npnt; ++i) {
+        r[i] = re + std::log(a / y[i]) / beta;  // :1322
+        double *bs = &bass[(size_t)i * (nmax + 1)];
+        bs[0] = 1.0;
+        if (nmax >= 1) {
+            double amx = alf + 1.0 - y[i];
+            bs[1] = amx;
+            double en = 1.0;
+            for (int n = 2; n <= nmax; ++n) {
+                en = en + 1.0;
+                amx = amx + 2.0;
+                bs[n] = (amx * bs[n - 1] - (alfm1 + en) * bs[n - 2]) / en;
+            }
+        }
+        for (int n2 = 0; n2 <= nmax; ++n2) bs[n2] = bs[n2] * dnorm[n2];
+    }
+    const double toler = 1.0e-8;  // :1360-1361
+    if (std::fabs((csx - tsx) / tsx) > toler) fail(DVR3D_ERR_QUADRATURE);
+    if (std::fabs((csa - tsa) / tsa) > toler) fail(DVR3D_ERR_QUADRATURE);
+}
+
+// keints :1495-1535 (packed triangle, 0-based)
+void keints(std::vector<double> &hbl, double fke, int nmax, int iu) {
+    int nlim = (nmax + 1) * (nmax + 2) / 2;
+    hbl.assign(nlim, 0.0);
+    int index = 0;
+    for (int n2 = 1; n2 <= nmax + 1; ++n2) {
+        for (int n1 = 1; n1 <= n2; ++n1) {
+            if (n1 == n2) {
+                hbl[index] = fke * (double)(2 * (n2 - 1) * (n2 + iu) + iu + 1);
+            } else if (n1 + 2 == n2) {
+                hbl[index] = -fke * std::sqrt((double)((long long)(iu + n1 + 1) * (iu + n1)) *
+                                              (double)((n1 + 1) * n1));
+            } else {
+                hbl[index] = 0.0;
+            }
+            ++index;
+        }
+    }
+}
+
+// k1k2 :1603-1632 -> xk column-major npnt x npnt
+void k1k2(std::vector<double> &xk, const std::vector<double> &hbl,
+          const std::vector<double> &bass, const std::vector<double> &wt, int npnt, int nmax) {
+    xk.assign((size_t)npnt * npnt, 0.0);
+    auto B = [&](int m, int k) { return bass[(size_t)k * (nmax + 1) + m]; };
+    for (int k = 0; k < npnt; ++k) {
+        for (int kp = 0; kp <= k; ++kp) {
+            double wtkkp = wt[k] * wt[kp];
+            double acc = 0.0;
+            for (int m = 0; m <= nmax; ++m) {
+                double t = B(m, k) * wtkkp;
+                for (int mp = 0; mp <= nmax; ++mp) {
+                    int mx = std::max(m, mp), mn = std::min(m, mp);
+                    int in = mx * (mx + 1) / 2 + mn;
+                    acc = acc + (hbl[in] * t * B(mp, kp));
+                }
+            }
+            xk[(size_t)kp * npnt + k] = acc;
+            xk[(size_t)k * npnt + kp] = acc;
+        }
+    }
+}
+
+// recur :1722-1744 (b, c 1-based)
+void recur(double &pn, double &dpn, double &pn1, double x, int nn, double alf, double bta,
+           const std::vector<double> &b, const std::vector<double> &c) {
+    double p1 = 1.0, p = x + (alf - bta) / (alf + bta + 2.0), dp1 = 0.0, dp = 1.0;
+    for (int j = 2; j <= nn; ++j) {
+        double q = (x - b[j]) * p - c[j] * p1;
+        double dq = (x - b[j]) * dp + p - c[j] * dp1;
+        p1 = p;
+        p = q;
+        dp1 = dp;
+        dp = dq;
+    }
+    pn = p;
+    dpn = dp;
+    pn1 = p1;
+}
+
+// root :1702-1721
+void root(double &x, int nn, double alf, double bta, double &dpn, double &pn1,
+          const std::vector<double> &b, const std::vector<double> &c, double eps) {
+    int iter = 0;
+    double p, dp;
+    for (;;) {
+        ++iter;
+        recur(p, dp, pn1, x, nn, alf, bta, b, c);
+        double d = p / dp;
+        x = x - d;
+        if (std::fabs(d) <= eps) break;
+        if (iter >= 10) break;
+    }
+    dpn = dp;
+}
+
+// jacobi :1635-1699. The scan step and lower limit are REAL*4 literals in the reference.
+void jacobi(int nn, int nn2, std::vector<double> &x, std::vector<double> &a, double alf,
+            double bta, double &csa, double tsa) {
+    const double eps = 1.0e-12;
+    std::vector<double> b(nn + 2), c(nn + 2), xt(nn + 2);
+    csa = 0.0;
+    c[1] = 0.0;
+    b[1] = 0.0;
+    for (int i = 2; i <= nn; ++i) {
+        double xi = (double)(float)i;
+        b[i] = 0.0;
+        c[i] = 4.0 * (xi - 1.0) * (alf + xi - 1.0) * (bta + xi - 1.0) * (alf + bta + xi - 1.0) /
+               ((alf + bta + 2.0 * xi - 1.0) * (alf + bta + 2.0 * xi - 2.0) *
+                (alf + bta + 2.0 * xi - 2.0) * (alf + bta + 2.0 * xi - 3.0));
+    }
+    double cc = tsa;
+    for (int i = 2; i <= nn; ++i) cc = cc * c[i];
+    const double step = (double)0.0001f, xstop = (double)(-0.002f);
+    int ii = 0;
+    double pm1 = 1.0, xxx = 1.0, p, dp, pn1;
+    for (;;) {
+        recur(p, dp, pn1, xxx, nn, alf, bta, b, c);
+        if (pm1 * p < 0.0) {
+            pm1 = -pm1;
+            ++ii;
+            xt[ii] = xxx;
+        }
+        if (ii == nn2) break;
+        xxx = xxx - step;
+        if (!(xxx > xstop)) fail(DVR3D_ERR_QUADRATURE);  // :1687-1688
+    }
+    x.assign(nn2, 0.0);
+    a.assign(nn2, 0.0);
+    for (int i = 1; i <= nn2; ++i) {
+        double dpn;
+        root(xt[i], nn, alf, bta, dpn, pn1, b, c, eps);
+        x[i - 1] = xt[i];
+        a[i - 1] = cc / (dpn * pn1);
+        csa = csa + a[i - 1] + a[i - 1];
+    }
+    if (2 * nn2 != nn) csa = csa - a[nn2 - 1];
+}
+
+// allpts :1747-1772
+void allpts(Run &R) {
+    double scale = (double)std::max(1, R.idia);
+    R.xalf.assign(R.idvr, 0.0);
+    R.walf.assign(R.idvr, 0.0);
+    for (int i = 0; i < R.nang2; ++i) {
+        R.xalf[i] = R.xhalf[i];
+        R.walf[i] = R.whalf[i];
+    }
+    for (int i = 1; i <= R.nang2; ++i) {
+        R.walf[i - 1] = std::sqrt(scale * R.walf[i - 1]);
+        if (R.idia == 2) continue;
+        R.xalf[R.nang + 1 - i - 1] = R.xalf[i - 1];
+        R.xalf[i - 1] = -R.xalf[i - 1];
+        R.walf[R.nang + 1 - i - 1] = R.walf[i - 1];
+    }
+}
+
+// asleg :1775-1843 -> pleg(0:maxleg, nn2) column-major
+void asleg(Run &R) {
+    int lmax = R.maxleg, m = R.kz, nn2 = R.nidvr, lincr = R.lincr;
+    R.pleg.assign((size_t)(lmax + 1) * nn2, 0.0);
+    auto P = [&](int l, int i) -> double & { return R.pleg[(size_t)i * (lmax + 1) + l]; };
+    for (int i = 0; i < nn2; ++i) {
+        double pmm = 1.0, fact = 1.0;
+        for (int j = 1; j <= m; ++j) {
+            pmm = -pmm * fact;
+            fact = fact + 2.0;
+        }
+        P(0, i) = pmm;
+        double pmmp1 = R.xalf[i] * (m + m + 1) * pmm;
+        if (lmax >= 1) P(1, i) = pmmp1;
+        int ll = 1;
+        for (int l = 2 + m; l <= lmax + lincr; ++l) {
+            double r2lm1 = (double)(l + l - 1), rlpmm1 = (double)(l + m - 1), rlmm = (double)(l - m);
+            double pll = (R.xalf[i] * r2lm1 * pmmp1 - rlpmm1 * pmm) / rlmm;
+            pmm = pmmp1;
+            pmmp1 = pll;
+            ++ll;
+            P(ll, i) = pll;
+        }
+    }
+    std::vector<double> pnorm(lmax + 1);
+    int jj = -1;
+    for (int j = m; j <= lmax + lincr; ++j) {
+        double fact = 1.0;
+        for (int i = j - m + 1; i <= j + m; ++i) fact = fact * (double)i;
+        double rj = (double)j;
+        ++jj;
+        pnorm[jj] = std::sqrt((rj + rj + 1.0) / (fact + fact));
+    }
+    for (int i = 0; i < nn2; ++i) {
+        jj = -1;
+        for (int j = m; j <= lmax + lincr; ++j) {
+            ++jj;
+            P(jj, i) = P(jj, i) * pnorm[jj];
+        }
+    }
+}
+
+// lmatrx :1846-1911 (in-plane branch) -> xlmatr(idvr,idvr) column-major
+void lmatrx(Run &R, int ipar0) {
+    int idvr = R.idvr, nidvr = R.nidvr, lmax = R.maxleg;
+    R.xlmatr.assign((size_t)idvr * idvr, 0.0);
+    int jstart = R.kz, iparam = R.lincr;
+    int jdia = std::max(1, R.idia);
+    int jj0 = -jdia;
+    if (jstart % jdia != ipar0) {
+        ++jj0;
+        ++jstart;
+    }
+    auto P = [&](int l, int i) { return R.pleg[(size_t)i * (lmax + 1) + l]; };
+    for (int k = 0; k < nidvr; ++k) {
+        double term = R.walf[k];
+        for (int kp = k; kp < nidvr; ++kp) {
+            double sumj1 = 0.0;
+            int jj = jj0;
+            for (int j = jstart; j <= lmax + iparam; j += jdia) {
+                jj = jj + jdia;
+                sumj1 = sumj1 + P(jj, k) * P(jj, kp) * (double)((j + 1) * j);
+            }
+            double v = sumj1 * term * R.walf[kp];
+            R.xlmatr[(size_t)k * idvr + kp] = v;
+            R.xlmatr[(size_t)kp * idvr + k] = v;
+        }
+    }
+}
+
+// ccmain :641-1013 up to the driver dispatch, for loop index kk.
+void ccmain_setup(Run &R, int kk) {
+    // setfac :1191-1258
+    std::vector<double> fact(R.npnt + 2);
+    fact[1] = 1.0;
+    double count = 1.0;
+    for (int i = 1; i <= R.npnt; ++i) {
+        fact[i + 1] = count * fact[i];
+        count = count + 1.0;
+    }
+    std::vector<double> dnorm1, dnorm2, bass1, bass2, hbl1, hbl2;
+    double cc1, cc2;
+    norms(dnorm1, fact, cc1, (double)R.iu1, R.npnt1, R.nmax1);
+    if (R.idia > -2) norms(dnorm2, fact, cc2, (double)R.iu2, R.npnt2, R.nmax2);
+    // :764-785
+    lagpt(R.y1, R.r1, R.wt1, bass1, dnorm1, cc1, R.npnt1, R.nmax1, R.re1, R.beta1, R.a1, R.iu1,
+          R.csx1, R.csa1, R.tsx1, R.tsa1);
+    if (R.idia > -2) {
+        lagpt(R.y2, R.r2, R.wt2, bass2, dnorm2, cc2, R.npnt2, R.nmax2, R.re2, R.beta2, R.a2,
+              R.iu2, R.csx2, R.csa2, R.tsx2, R.tsa2);
+        keints(hbl2, R.beta2 * R.beta2 / (8.0 * R.ur2), R.nmax2, R.iu2);
+    }
+    keints(hbl1, R.beta1 * R.beta1 / (8.0 * R.ur1), R.nmax1, R.iu1);
+    std::vector<double> w1 = R.wt1, w2 = R.wt2;  // :797-798 take square roots
+    for (auto &w : w1) w = std::sqrt(w);
+    for (auto &w : w2) w = std::sqrt(w);
+    k1k2(R.xk1, hbl1, bass1, w1, R.npnt1, R.nmax1);  // :802-804
+    if (R.idia > -2) k1k2(R.xk2, hbl2, bass2, w2, R.npnt2, R.nmax2);
+
+    // k-loop state of :810-819 and :857-916, replayed up to kk
+    if (R.zrot) {
+        R.kd = 1 - std::min(R.kmin, 1);
+        R.ku = R.jrot;
+        if (R.kmin == 2) R.ku = R.ku + 1;
+    } else {
+        R.kd = R.kmin;
+        R.ku = R.kmin;
+    }
+    if (kk < R.kd || kk > R.ku) fail(DVR3D_ERR_ARG);
+    int max2d1 = R.max2d, max3d1 = R.max3d;
+    int kkz12 = 0, kkz0 = 0;
+    for (int k = R.kd; k <= kk; ++k) {
+        if (k <= R.jrot) {
+            R.kz = k;
+        } else {
+            R.kz = 1;
+            R.kmin = 0;
+            R.ipar = (R.ipar + R.jrot) % 2;
+        }
+        if (R.zladd || R.kz == R.kd) {
+            R.nidvr = R.idvr;
+            R.nang = R.nalf;
+            R.nang2 = R.nalf2;
+            R.lincr = R.kz;
+        } else {
+            R.lincr = 0;
+            if (R.idia != 2) {
+                R.nidvr = R.idvr - R.kz;
+                R.nang = R.nalf - R.kz;
+                R.nang2 = (R.nang + 1) / 2;
+            } else if (R.ipar == 0) {
+                if (R.kz % 2 == 1) kkz0 += 2;
+                R.nidvr = R.idvr - kkz0 / 2;
+                R.nang = R.nalf - kkz0;
+                R.nang2 = (R.nang + 1) / 2;
+            } else {
+                if (R.kz % 2 == 0 && R.kz > 0) kkz12 += 2;
+                R.nidvr = R.idvr - kkz12 / 2;
+                R.nang = R.nalf - kkz12;
+                R.nang2 = (R.nang + 1) / 2;
+            }
+        }
+        if (!R.zladd) {
+            if (R.ztheta) R.npnta = R.nidvr;
+            else R.npntc = R.nidvr;
+        }
+        if (R.idia <= -2 && R.zrot) {  // :989-998
+            if (R.kz > R.kd) R.ipar = (R.ipar + 1) % 2;
+            if (R.ipar > 0) {
+                R.max2d = R.max2d2;
+                R.max3d = R.max3d2;
+            } else {
+                R.max2d = max2d1;
+                R.max3d = max3d1;
+            }
+        }
+    }
+    // Gauss-(associated) Legendre points for this k (:887-944)
+    double realkz = (double)R.kz;
+    R.tswalf = std::pow(2.0, R.kz + R.kz + 1) / (double)(R.kz + 1);
+    for (int ia = 1; ia <= R.kz; ++ia) R.tswalf = R.tswalf * (double)ia / (double)(R.kz + ia + 1);
+    jacobi(R.nang, R.nang2, R.xhalf, R.whalf, realkz, realkz, R.cswalf, R.tswalf);
+    if (std::fabs((R.cswalf - R.tswalf) / R.tswalf) > 1.0e-8) fail(DVR3D_ERR_QUADRATURE);
+    allpts(R);
+    asleg(R);
+    int ipar0 = (R.idia == 2 && R.ipar == 1) ? 1 : 0;
+    lmatrx(R, ipar0);
+}
+
+// ------------------------------------------------------------------ Radau: nfmain
+struct Selected {
+    std::vector<double> eigs2d;       // selected 2D eigenvalues (final basis order)
+    std::vector<std::vector<double>> vec;  // per block: n2 x count (column-major)
+    std::vector<int> count, n2;
+};
+
+// blc2d1 :3125-3219 -> ham2 (nham2 x nham2 column-major, full)
+void blc2d1(const Run &R, int ig, double xcos, std::vector<double> &ham2, int nham2,
+            double term, double term2, double term3, double xtscw) {
+    int npnt = R.npnt, ipar = R.ipar;
+    const double factr2 = std::sqrt(0.5);
+    ham2.assign((size_t)nham2 * nham2, 0.0);
+    auto H = [&](int i, int j) -> double & { return ham2[(size_t)(j - 1) * nham2 + (i - 1)]; };
+    double xsen2 = 1.0 - xcos * xcos;
+    double hfac = 1.0 - R.xp1 * 0.4150706813595e-3 * 1.25;
+    auto hrpb = [&](int i, int j) { return R.xk1[(size_t)(j - 1) * R.npnt1 + (i - 1)] * hfac; };
+    const std::vector<double> &r = R.r1;
+    if (R.jrot != 0) {
+        double fact = term + term2 / (1.0 - xcos);
+        if (R.kz == 1) fact = fact + term3 * (1.0 + xcos) / (1.0 - xcos);
+        int ia = 0;
+        double wsum = 0.0, wsum2 = 0.0;
+        for (int ibeta = 1; ibeta <= npnt; ++ibeta) {
+            for (int ialpha = 1; ialpha <= ibeta - ipar; ++ialpha) {
+                double walpha = 0.5 / (r[ialpha - 1] * r[ialpha - 1]);
+                double wbeta = 0.5 / (r[ibeta - 1] * r[ibeta - 1]);
+                wsum = (walpha + wbeta) * fact / R.urr1 - xtscw;
+                wsum2 = R.kz * R.kz * (walpha + wbeta) * (1.0 / R.ur1 - 1.0 / R.urr1) * R.xp0 / xsen2;
+                H(ialpha + ia, ialpha + ia) += wsum - wsum2;
+            }
+            ia = ia + ibeta - ipar;
+            if (ipar == 0) H(ia, ia) += wsum - wsum2;
+        }
+    }
+    double q = (ipar == 1) ? -1.0 : 1.0;
+    int iap = 0;
+    for (int ibetap = 1; ibetap <= npnt; ++ibetap) {
+        int ia = 0;
+        for (int ibeta = 1; ibeta <= npnt; ++ibeta) {
+            for (int ialphp = 1; ialphp <= ibetap - ipar; ++ialphp) {
+                for (int ialpha = 1; ialpha <= ibeta - ipar; ++ialpha) {
+                    double &h = H(ialphp + iap, ialpha + ia);
+                    if (ibeta == ibetap) h = h + hrpb(ialphp, ialpha);
+                    if (ibeta == ialphp) h = h + q * hrpb(ibetap, ialpha);
+                    if (ialpha == ibetap) h = h + q * hrpb(ialphp, ibeta);
+                    if (ialpha == ialphp) h = h + hrpb(ibetap, ibeta);
+                    if (ialpha == ialphp && ibeta == ibetap)
+                        h = h + potv(R, r[ialpha - 1], r[ibeta - 1], xcos, ialpha - 1, ibeta - 1, ig);
+                    if (ialpha == ibetap && ibeta == ialphp)
+                        h = h + q * potv(R, r[ibeta - 1], r[ialpha - 1], xcos, ibeta - 1, ialpha - 1, ig);
+                    if (ialphp == ibetap) h = h * factr2;
+                    if (ialpha == ibeta) h = h * factr2;
+                }
+            }
+            ia = ia + ibeta - ipar;
+        }
+        iap = iap + ibetap - ipar;
+    }
+}
+
+// nfmain :3006-3121 with cut2dr :3323-3377, choosr :3223-3319, testiv :3380-3451,
+// bloc3d :3455-3505, blc2d2 :3509-3566, vecmul :3570-3595, diag3d :2661-2764.
+void nfmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
+    auto t0 = std::chrono::steady_clock::now();
+    int nalf = R.nalf, npnt = R.npnt, ipar = R.ipar, jrot = R.jrot, kz = R.kz;
+    double asw = 0.98205515e-8 * (1.10) * (0.06);
+    double bsw = 7.3757478e-9 * (1.10) * (0.06);
+    double csw = 1.7082113e-8 * (1.10) * (-0.21);
+    double xtscw = ((double)(jrot * jrot + jrot) * (asw + bsw) * 0.5 +
+                    (double)(kz * kz) * (csw - (bsw + asw) * 0.5)) * R.xp2;
+    double term = 0, term2 = 0, term3 = 0;
+    if (jrot != 0) {
+        term = (double)(jrot * jrot + jrot - kz * kz) / 8.0;
+        term2 = (double)(jrot * jrot + jrot - 3 * kz * kz) / 4.0;
+        if (std::abs(kz) == 1) {
+            term3 = (double)(jrot * jrot + jrot) / 16.0;
+            if (R.kmin >= 1 && R.zrot) term3 = -term3;
+        }
+    }
+    int nham2 = (npnt * (npnt + 1 - ipar * 2)) / 2;
+    std::vector<int> nv2(nalf, nham2), iv2a(nalf, 0), iv2b(nalf, 0);  // iv2(1,:), iv2(2,:)
+    std::vector<double> ham2, eig2(nham2);
+    std::vector<double> eigs2d;
+    std::vector<double> vecs2d;  // max2d x (columns), column-major, leading dim nham2
+    std::vector<double> eigtmp;
+    std::vector<std::vector<double>> allv(nalf), alle(nalf);  // unit intvec (choosr)
+    double emaxau = R.emax2 / autocm;
+    int npos = 1;
+    for (int ig = 0; ig < nalf; ++ig) {
+        blc2d1(R, ig, R.xalf[ig], ham2, nham2, term, term2, term3, xtscw);
+        diag(ham2.data(), nham2, nham2, eig2.data());
+        if (tr && tr->eig2all && (size_t)(ig + 1) * nham2 <= (size_t)tr->eig2all_cap)
+            std::memcpy(tr->eig2all + (size_t)ig * nham2, eig2.data(), sizeof(double) * nham2);
+        if (!R.zcut) {
+            allv[ig] = ham2;
+            alle[ig] = eig2;
+            // merge (:3260-3280): equivalent to keeping all eigenvalues sorted
+            eigtmp.insert(eigtmp.end(), eig2.begin(), eig2.end());
+            std::sort(eigtmp.begin(), eigtmp.end());
+        } else {
+            int nvec = 0;
+            for (int ia = 0; ia < nham2; ++ia) {
+                if (eig2[ia] < emaxau) {
+                    int ntot = npos + nvec;
+                    if (ntot > R.max3d) fail(DVR3D_ERR_CORE_MAX3D);
+                    eigs2d.push_back(eig2[ia]);
+                    vecs2d.insert(vecs2d.end(), ham2.begin() + (size_t)ia * nham2,
+                                  ham2.begin() + (size_t)(ia + 1) * nham2);
+                    ++nvec;
+                }
+            }
+            iv2a[ig] = npos;
+            iv2b[ig] = nvec;
+            npos += nvec;
+        }
+    }
+    if (!R.zcut) {  // choosr final selection (:3284-3311)
+        int itotal = (int)eigtmp.size();
+        double emax = (itotal <= R.max3d) ? eigtmp[itotal - 1] : eigtmp[R.max3d - 1];
+        int it = 1;
+        for (int ig = 0; ig < nalf; ++ig) {
+            iv2a[ig] = it;
+            int ichose = 0;
+            for (int j = 0; j < nv2[ig]; ++j) {
+                double e = alle[ig][j];
+                if (e <= emax) {
+                    eigs2d.push_back(e);
+                    vecs2d.insert(vecs2d.end(), allv[ig].begin() + (size_t)j * nham2,
+                                  allv[ig].begin() + (size_t)(j + 1) * nham2);
+                    ++ichose;
+                    ++it;
+                }
+            }
+            iv2b[ig] = ichose;
+        }
+    }
+    // testiv :3380-3451
+    if (jrot > 0) {
+        int iend = nalf;
+        for (int i = nalf / 2; i <= nalf; ++i) {
+            if (iv2b[i - 1] == 0) {
+                iend = i;
+                break;
+            }
+        }
+        for (int i = iend + 1; i <= nalf; ++i) {
+            if (iv2b[i - 1] > 0) {
+                iv2b[i - 1] = 0;
+                iv2a[i - 1] = iv2a[i - 2];
+            }
+        }
+        if (iv2b[nalf - 1] > 0) {
+            if (R.zlin) iv2b[nalf - 1] = 0;
+            else fail(DVR3D_ERR_THETA0);
+        }
+    }
+    int nham3 = iv2a[nalf - 1] + iv2b[nalf - 1] - 1;  // :3092
+    auto t1 = std::chrono::steady_clock::now();
+    // bloc3d :3455-3505
+    std::vector<double> ham3((size_t)nham3 * nham3, 0.0);
+    auto V = [&](int col) { return &vecs2d[(size_t)col * nham2]; };
+    std::vector<double> hama(nham2);
+    int ndim1g = 1;
+    for (int ig = 0; ig < nalf; ++ig) {
+        if (iv2b[ig] <= 0) continue;
+        int ndim2g = 1;
+        for (int igp = 0; igp <= ig; ++igp) {
+            if (iv2b[igp] <= 0) continue;
+            // blc2d2 :3509-3566 -- nonzero only on the diagonal of the pair basis
+            double L = R.xlmatr[(size_t)ig * R.idvr + igp];  // htheta(igammp,igamma)
+            const double factr2 = std::sqrt(0.5);
+            double q = (ipar == 1) ? -1.0 : 1.0;
+            int idx = 0;
+            for (int ib = 1; ib <= npnt; ++ib) {
+                for (int iaa = 1; iaa <= ib - ipar; ++iaa) {
+                    double walpha = 0.5 / (R.r1[iaa - 1] * R.r1[iaa - 1] * R.ur1);
+                    double wbeta = 0.5 / (R.r1[ib - 1] * R.r1[ib - 1] * R.ur1);
+                    double h = 0.0;
+                    double wsum = walpha + wbeta - R.xp1 * 1.5468847900e-8 * 1.250;
+                    h = h + L * wsum;
+                    if (iaa == ib) h = h + q * L * (walpha + wbeta);
+                    if (iaa == ib) h = h * factr2;  // ialphp == ibetap
+                    if (iaa == ib) h = h * factr2;  // ialpha == ibeta
+                    hama[idx++] = h;
+                }
+            }
+            // vecmul :3570-3595: hamb += va^T hama vb (hama diagonal here)
+            int ja0 = ndim1g - 1, jb0 = ndim2g - 1;
+            int ca = iv2a[ig] - 1, cb = iv2a[igp] - 1;
+            for (int ib = 0; ib < nham2; ++ib) {
+                double temp1 = hama[ib];
+                if (temp1 == 0.0) continue;
+                int ia = ib;
+                for (int ja = 0; ja < iv2b[ig]; ++ja) {
+                    double temp2 = V(ca + ja)[ia] * temp1;
+                    for (int jb = 0; jb < iv2b[igp]; ++jb)
+                        ham3[(size_t)(jb0 + jb) * nham3 + (ja0 + ja)] += V(cb + jb)[ib] * temp2;
+                }
+            }
+            ndim2g += iv2b[igp];
+        }
+        ndim1g += iv2b[ig];
+    }
+    for (int i = 0; i < nham3; ++i) ham3[(size_t)i * nham3 + i] += eigs2d[i];
+    auto t2 = std::chrono::steady_clock::now();
+    if (tr) {
+        tr->nblocks = nalf;
+        tr->nham3 = nham3;
+        if (tr->iv2 && tr->iv2_cap >= nalf)
+            for (int i = 0; i < nalf; ++i) tr->iv2[i] = iv2b[i];
+        if (tr->n2d && tr->n2d_cap >= nalf)
+            for (int i = 0; i < nalf; ++i) tr->n2d[i] = nv2[i];
+        if (tr->eigs2d && tr->eigs2d_cap >= nham3)
+            std::memcpy(tr->eigs2d, eigs2d.data(), sizeof(double) * nham3);
+        if (tr->h3 && tr->h3_cap >= (size_t)nham3 * nham3)
+            std::memcpy(tr->h3, ham3.data(), sizeof(double) * nham3 * nham3);
+    }
+    // diag3d :2661-2764
+    int meval = std::min(R.neval, nham3);
+    std::vector<double> eval(nham3);
+    if (final_mode != 2) diag(ham3.data(), nham3, nham3, eval.data(), final_mode);
+    auto t3 = std::chrono::steady_clock::now();
+    if (tr) {
+        tr->stage_s[0] = std::chrono::duration<double>(t1 - t0).count();
+        tr->stage_s[1] = std::chrono::duration<double>(t2 - t1).count();
+        tr->stage_s[2] = std::chrono::duration<double>(t3 - t2).count();
+        tr->stage_s[3] = std::chrono::duration<double>(t3 - t0).count();
+    }
+    if (res) {
+        res->nham3 = nham3;
+        res->meval = (final_mode == 2) ? 0 : meval;
+        res->nblocks = nalf;
+        res->kz = R.kz;
+        res->ipar = R.ipar;
+        if (res->eval && final_mode != 2) {
+            if (res->eval_cap < meval) fail(DVR3D_ERR_BUFFER);
+            std::memcpy(res->eval, eval.data(), sizeof(double) * meval);
+        }
+        if (res->iv2 && res->iv2_cap >= nalf)
+            for (int i = 0; i < nalf; ++i) res->iv2[i] = iv2b[i];
+    }
+}
+
+// ------------------------------------------------------------------ Jacobi: jhmain
+// mkham1 :2121-2225 -> ham1 (npnta x npnta, column-major, lower filled)
+void mkham1(const Run &R, std::vector<double> &ham1, int i1, int i2, double term) {
+    int n = R.npnta;
+    ham1.assign((size_t)n * n, 0.0);
+    auto H = [&](int i, int j) -> double & { return ham1[(size_t)j * n + i]; };
+    double wterm = 0.0, w1gama = 0, w2beta = 0, wsum = 0, w3 = 0;
+    if (R.ztheta) {
+        w1gama = 0.5 / (R.r1[i1] * R.r1[i1] * R.ur1);
+        w2beta = 0.5 / (R.r2[i2] * R.r2[i2] * R.ur2);
+        wsum = w1gama + w2beta;
+        if (R.jrot > 0) {
+            if (R.zembed) wterm = term * w2beta * R.ur2 / R.urr2;
+            else wterm = term * w1gama * R.ur1 / R.urr1;
+            if (R.kz > 0) {
+                double s1 = R.ur1 / R.urr1 - 1.0, s2 = R.ur2 / R.urr2 - 1.0;
+                w3 = (double)(R.kz * R.kz) * (s1 * w1gama + s2 * w2beta) * R.xp0;
+            }
+        }
+    }
+    for (int k = 0; k < n; ++k) {
+        double v;
+        if (R.ztheta) {
+            v = potv(R, R.r1[i1], R.r2[i2], R.xalf[k], i1, i2, k);
+        } else if (R.zr2r1) {
+            v = potv(R, R.r1[i2], R.r2[k], R.xalf[i1], i2, k, i1);
+        } else {
+            v = potv(R, R.r1[k], R.r2[i1], R.xalf[i2], k, i1, i2);
+        }
+        if (R.ztheta) {
+            if (R.kz > 0) v = v + w3 / (1.0 - R.xalf[k] * R.xalf[k]);
+            H(k, k) = v + wterm;
+            for (int kp = 0; kp <= k; ++kp) H(k, kp) = H(k, kp) + R.xlmatr[(size_t)kp * R.idvr + k] * wsum;
+        } else {
+            if (R.jrot > 0) {
+                if (R.zembed) {
+                    if (R.zr2r1) wterm = (term * 0.5) / (R.r2[k] * R.r2[k] * R.ur2);
+                    else wterm = (term * 0.5) / (R.r2[i1] * R.r2[i1] * R.ur2);
+                } else {
+                    if (R.zr2r1) wterm = (term * 0.5) / (R.r1[i2] * R.r1[i2] * R.ur1);
+                    else wterm = (term * 0.5) / (R.r1[k] * R.r1[k] * R.ur1);
+                }
+            }
+            H(k, k) = v + wterm;
+            const std::vector<double> &xk = R.zr2r1 ? R.xk2 : R.xk1;
+            int np = R.zr2r1 ? R.npnt2 : R.npnt1;
+            for (int kp = 0; kp <= k; ++kp) H(k, kp) = H(k, kp) + xk[(size_t)kp * np + k];
+        }
+    }
+}
+
+// jhmain :1915-2118 with cut1d :2870-2938, mkham2 :2228-2298, cut2d :2941-3003,
+// choose :2767-2867, mkham3 :2301-2552, loadh :2554-2609, diag3d :2661-2764.
+void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
+    auto t0 = std::chrono::steady_clock::now();
+    int npnta = R.npnta, npntb = R.npntb, npntc = R.npntc;
+    double term = (double)(R.jrot * R.jrot + R.jrot - (2 * R.kz * R.kz));
+    // 1D stage (:1973-2003): per ione the selected 1D eigenpairs (units ieigs1/ivecs1)
+    std::vector<std::vector<double>> eigs1d(npntc), vecs1d(npntc);  // vecs1d: nham2 x npnta
+    std::vector<int> iv1((size_t)npntc * npntb, 0);
+    std::vector<double> ham1, eig1(npnta);
+    double emax1au = R.emax1 / autocm;
+    for (int ione = 0; ione < npntc; ++ione) {
+        std::vector<double> e1;
+        std::vector<std::vector<double>> cols;  // each selected vector over npnta
+        for (int itwo = 0; itwo < npntb; ++itwo) {
+            mkham1(R, ham1, R.zr2r1 ? ione : itwo, R.zr2r1 ? itwo : ione, term);
+            diag(ham1.data(), npnta, npnta, eig1.data());
+            int ivn = 0;
+            if (!R.zall) {
+                for (int n = 0; n < npnta; ++n) {
+                    if (eig1[n] > emax1au) break;
+                    ++ivn;
+                }
+            } else {
+                ivn = npnta;
+            }
+            iv1[(size_t)ione * npntb + itwo] = ivn;
+            for (int i = 0; i < ivn; ++i) {
+                if ((int)e1.size() + 1 > R.max2d && !R.zall) fail(DVR3D_ERR_CORE_MAX2D);
+                e1.push_back(eig1[i]);
+                cols.emplace_back(ham1.begin() + (size_t)i * npnta,
+                                  ham1.begin() + (size_t)(i + 1) * npnta);
+            }
+        }
+        int nh = (int)e1.size();
+        eigs1d[ione] = e1;
+        vecs1d[ione].assign((size_t)nh * npnta, 0.0);  // vecs1d(nham2, ka) column-major
+        for (int j = 0; j < nh; ++j)
+            for (int ka = 0; ka < npnta; ++ka) vecs1d[ione][(size_t)ka * nh + j] = cols[j][ka];
+    }
+    // 2D stage (:2019-2053)
+    bool zcut = R.zcut || R.zall;
+    std::vector<int> ndim2d(npntc, 0), iv2(npntc, 0);
+    std::vector<std::vector<double>> eig2s(npntc), vec2s(npntc);  // per block: all or selected
+    int low3d = 0;
+    double emax2au = R.emax2 / autocm;
+    size_t eoff = 0;
+    for (int ione = 0; ione < npntc; ++ione) {
+        int nham2 = 0;
+        for (int itwo = 0; itwo < npntb; ++itwo) nham2 += iv1[(size_t)ione * npntb + itwo];
+        ndim2d[ione] = nham2;
+        if (nham2 == 0) continue;
+        // mkham2 :2228-2298
+        std::vector<double> ham2((size_t)nham2 * nham2, 0.0);
+        const std::vector<double> &V1 = vecs1d[ione];
+        for (int i3 = 0; i3 < npnta; ++i3)
+            for (int j = 0; j < nham2; ++j)
+                for (int k = 0; k <= j; ++k)
+                    ham2[(size_t)k * nham2 + j] += V1[(size_t)i3 * nham2 + j] * V1[(size_t)i3 * nham2 + k];
+        const std::vector<double> *xkb;
+        int npb;
+        if (R.ztheta) {
+            xkb = R.zr2r1 ? &R.xk2 : &R.xk1;
+            npb = R.zr2r1 ? R.npnt2 : R.npnt1;
+        } else {
+            xkb = R.zr2r1 ? &R.xk1 : &R.xk2;
+            npb = R.zr2r1 ? R.npnt1 : R.npnt2;
+        }
+        int ivbsm = 0;
+        for (int itwo = 0; itwo < npntb; ++itwo) {
+            int ivbpsm = 0, ivb = iv1[(size_t)ione * npntb + itwo];
+            for (int itwop = 0; itwop <= itwo; ++itwop) {
+                double xkterm = (*xkb)[(size_t)itwop * npb + itwo];
+                int ivbp = iv1[(size_t)ione * npntb + itwop];
+                for (int j = 0; j < ivb; ++j)
+                    for (int jp = 0; jp < ivbp; ++jp)
+                        ham2[(size_t)(ivbpsm + jp) * nham2 + (ivbsm + j)] *= xkterm;
+                ivbpsm += ivbp;
+            }
+            ivbsm += ivb;
+        }
+        for (int nn = 0; nn < nham2; ++nn) ham2[(size_t)nn * nham2 + nn] += eigs1d[ione][nn];
+        std::vector<double> eig2(nham2);
+        diag(ham2.data(), nham2, nham2, eig2.data());
+        if (tr && tr->eig2all && eoff + nham2 <= (size_t)tr->eig2all_cap)
+            std::memcpy(tr->eig2all + eoff, eig2.data(), sizeof(double) * nham2);
+        eoff += nham2;
+        if (zcut) {  // cut2d :2941-3003
+            int ivm = 0;
+            if (!R.zall) {
+                for (int n = 0; n < nham2; ++n) {
+                    if (eig2[n] > emax2au) break;
+                    ++ivm;
+                }
+            } else {
+                ivm = nham2;
+            }
+            low3d += ivm;
+            if (low3d > R.max3d && !R.zall) fail(DVR3D_ERR_CORE_MAX3D);
+            iv2[ione] = ivm;
+            eig2s[ione].assign(eig2.begin(), eig2.begin() + ivm);
+            vec2s[ione].assign(ham2.begin(), ham2.begin() + (size_t)ivm * nham2);
+        } else {
+            eig2s[ione] = eig2;
+            vec2s[ione] = ham2;
+            low3d = R.max3d;
+        }
+    }
+    if (!zcut) {  // choose :2767-2867
+        int nhamsm = 0;
+        std::vector<int> ptr(npntc, 1);
+        for (int i = 0; i < npntc; ++i) nhamsm += ndim2d[i];
+        if (nhamsm < R.max3d) low3d = nhamsm;
+        int ipt = 0;
+        for (int n = 0; n < low3d; ++n) {
+            while (ptr[ipt] > ndim2d[ipt]) ++ipt;
+            double eigvib = eig2s[ipt][ptr[ipt] - 1];
+            int jpt = ipt;
+            for (int j = ipt + 1; j < npntc; ++j) {
+                if (ptr[j] > ndim2d[j]) continue;
+                if (eig2s[j][ptr[j] - 1] >= eigvib) continue;
+                eigvib = eig2s[j][ptr[j] - 1];
+                jpt = j;
+            }
+            ptr[jpt] += 1;
+        }
+        for (int i = 0; i < npntc; ++i) {
+            iv2[i] = ptr[i] - 1;
+            eig2s[i].resize(iv2[i]);
+            vec2s[i].resize((size_t)iv2[i] * ndim2d[i]);
+        }
+    }
+    int nham3 = low3d;
+    auto t1 = std::chrono::steady_clock::now();
+    // mkham3 :2301-2552, first part: cint per block (P x iv2), P = npnta*npntb
+    int ncint = npnta * npntb;
+    std::vector<std::vector<double>> cint(npntc);
+    for (int ione = 0; ione < npntc; ++ione) {
+        int nham2 = ndim2d[ione];
+        if (nham2 == 0 || iv2[ione] == 0) continue;
+        std::vector<double> &C = cint[ione];
+        C.assign((size_t)ncint * iv2[ione], 0.0);
+        const std::vector<double> &V1 = vecs1d[ione];
+        for (int j = 0; j < iv2[ione]; ++j) {
+            const double *h2 = &vec2s[ione][(size_t)j * nham2];
+            int ind2 = 0;
+            for (int k = 0; k < npnta; ++k) {
+                int ind1 = 0;
+                for (int itwo = 0; itwo < npntb; ++itwo) {
+                    for (int i = 0; i < iv1[(size_t)ione * npntb + itwo]; ++i) {
+                        C[(size_t)j * ncint + ind2] += h2[ind1] * V1[(size_t)k * nham2 + ind1];
+                        ++ind1;
+                    }
+                    ++ind2;
+                }
+            }
+            if (!R.ztheta) {
+                int in2 = 0;
+                for (int ia = 0; ia < npnta; ++ia) {
+                    for (int ib = 0; ib < npntb; ++ib) {
+                        int ii1 = R.zr2r1 ? ib : ia, ii2 = R.zr2r1 ? ia : ib;
+                        double w1 = 0.5 / (R.r1[ii1] * R.r1[ii1] * R.ur1);
+                        double w2 = 0.5 / (R.r2[ii2] * R.r2[ii2] * R.ur2);
+                        double wsum = w1 + w2;
+                        C[(size_t)j * ncint + in2] *= std::sqrt(wsum);
+                        ++in2;
+                    }
+                }
+            }
+        }
+    }
+    // second part: hband = T(ione,ionep) C_ione^T C_ionep; loadh puts it in ham3 (lower)
+    std::vector<double> ham3((size_t)nham3 * nham3, 0.0);
+    int ivsm = 0;
+    for (int ione = 0; ione < npntc; ++ione) {
+        int iv = iv2[ione];
+        if (ndim2d[ione] == 0) continue;
+        int ivpsm = 0;
+        for (int ionep = 0; ionep <= ione; ++ionep) {
+            double xkterm;
+            if (R.ztheta) {
+                xkterm = R.zr2r1 ? R.xk1[(size_t)ionep * R.npnt1 + ione]
+                                 : R.xk2[(size_t)ionep * R.npnt2 + ione];
+            } else {
+                xkterm = R.xlmatr[(size_t)ionep * R.idvr + ione];
+            }
+            int ivp = iv2[ionep];
+            for (int j = 0; j < iv; ++j) {
+                const double *cj = &cint[ione][(size_t)j * ncint];
+                for (int jp = 0; jp < ivp; ++jp) {
+                    const double *cp = &cint[ionep][(size_t)jp * ncint];
+                    double h = 0.0;
+                    for (int k = 0; k < ncint; ++k) h = h + cj[k] * cp[k] * xkterm;
+                    ham3[(size_t)(ivpsm + jp) * nham3 + (ivsm + j)] = h;
+                }
+            }
+            ivpsm += ivp;
+        }
+        ivsm += iv;
+    }
+    std::vector<double> eigs2d;
+    for (int ione = 0; ione < npntc; ++ione)
+        for (int i = 0; i < iv2[ione]; ++i) eigs2d.push_back(eig2s[ione][i]);
+    for (int nn = 0; nn < nham3; ++nn) ham3[(size_t)nn * nham3 + nn] += eigs2d[nn];
+    auto t2 = std::chrono::steady_clock::now();
+    if (tr) {
+        tr->nblocks = npntc;
+        tr->nham3 = nham3;
+        if (tr->iv1 && tr->iv1_cap >= npntc * npntb)
+            std::memcpy(tr->iv1, iv1.data(), sizeof(int) * npntc * npntb);
+        if (tr->iv2 && tr->iv2_cap >= npntc)
+            for (int i = 0; i < npntc; ++i) tr->iv2[i] = iv2[i];
+        if (tr->n2d && tr->n2d_cap >= npntc)
+            for (int i = 0; i < npntc; ++i) tr->n2d[i] = ndim2d[i];
+        if (tr->eigs2d && tr->eigs2d_cap >= nham3)
+            std::memcpy(tr->eigs2d, eigs2d.data(), sizeof(double) * nham3);
+        if (tr->h3 && tr->h3_cap >= (size_t)nham3 * nham3)
+            std::memcpy(tr->h3, ham3.data(), sizeof(double) * nham3 * nham3);
+    }
+    int meval = std::min(R.neval, nham3);
+    std::vector<double> eval(nham3);
+    if (final_mode != 2) diag(ham3.data(), nham3, nham3, eval.data(), final_mode);
+    auto t3 = std::chrono::steady_clock::now();
+    if (tr) {
+        tr->stage_s[0] = std::chrono::duration<double>(t1 - t0).count();
+        tr->stage_s[1] = std::chrono::duration<double>(t2 - t1).count();
+        tr->stage_s[2] = std::chrono::duration<double>(t3 - t2).count();
+        tr->stage_s[3] = std::chrono::duration<double>(t3 - t0).count();
+    }
+    if (res) {
+        res->nham3 = nham3;
+        res->meval = (final_mode == 2) ? 0 : meval;
+        res->nblocks = npntc;
+        res->kz = R.kz;
+        res->ipar = R.ipar;
+        if (res->eval && final_mode != 2) {
+            if (res->eval_cap < meval) fail(DVR3D_ERR_BUFFER);
+            std::memcpy(res->eval, eval.data(), sizeof(double) * meval);
+        }
+        if (res->iv2 && res->iv2_cap >= npntc)
+            for (int i = 0; i < npntc; ++i) res->iv2[i] = iv2[i];
+    }
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_load_lapack(const char *path, const char *prefix) {
+    void *h = dlopen(path, RTLD_NOW | RTLD_LOCAL);
+    if (!h) return DVR3D_ERR_ARG;
+    std::string p(prefix ? prefix : "");
+    g_dsyev = (dsyev_t)dlsym(h, (p + "dsyev_").c_str());
+    g_dsyevd = (dsyevd_t)dlsym(h, (p + "dsyevd_").c_str());
+    return g_dsyev ? DVR3D_OK : DVR3D_ERR_ARG;
+}
+
+double oracle_pes_morse_sum(const double *p, double r1, double r2, double xcos) {
+    return pes_morse_sum(p, r1, r2, xcos);
+}
+
+int oracle_sizes(const dvr3d_deck *deck, int kk, int *o) {
+    try {
+        Run R;
+        insize_setcon(R, *deck);
+        ccmain_setup(R, kk);
+        int v[16] = {R.npnt1, R.npnt2, R.nalf, R.idvr, R.npnta, R.npntb, R.npntc, R.max2d,
+                     R.max3d, R.neval, R.kz, R.ipar, R.nidvr, R.lincr, R.kd, R.ku};
+        std::memcpy(o, v, sizeof(v));
+        return DVR3D_OK;
+    } catch (Fail &f) {
+        return f.code;
+    }
+}
+
+int oracle_quadrature(const dvr3d_deck *deck, int kk, oracle_quad *q) {
+    std::memset(q, 0, sizeof(*q));
+    Run R;
+    int status = DVR3D_OK;
+    try {
+        insize_setcon(R, *deck);
+        ccmain_setup(R, kk);
+    } catch (Fail &f) {
+        status = f.code;
+    }
+    q->status = status;
+    q->npnt1 = (int)R.y1.size();
+    q->npnt2 = (int)R.y2.size();
+    for (size_t i = 0; i < R.y1.size() && i < 128; ++i) {
+        q->y1[i] = R.y1[i];
+        q->wt1[i] = R.wt1[i];
+        q->r1[i] = R.r1.size() > i ? R.r1[i] : 0.0;
+    }
+    for (size_t i = 0; i < R.y2.size() && i < 128; ++i) {
+        q->y2[i] = R.y2[i];
+        q->wt2[i] = R.wt2[i];
+        q->r2[i] = R.r2.size() > i ? R.r2[i] : 0.0;
+    }
+    q->csx1 = R.csx1; q->csa1 = R.csa1; q->tsx1 = R.tsx1; q->tsa1 = R.tsa1;
+    q->csx2 = R.csx2; q->csa2 = R.csa2; q->tsx2 = R.tsx2; q->tsa2 = R.tsa2;
+    q->nang2 = (int)R.xhalf.size();
+    for (size_t i = 0; i < R.xhalf.size() && i < 128; ++i) {
+        q->xhalf[i] = R.xhalf[i];
+        q->whalf[i] = R.whalf[i];
+    }
+    q->cswalf = R.cswalf;
+    q->tswalf = R.tswalf;
+    q->nidvr = (int)R.xalf.size();
+    for (size_t i = 0; i < R.xalf.size() && i < 256; ++i) {
+        q->xalf[i] = R.xalf[i];
+        q->walf[i] = R.walf[i];
+    }
+    q->ur1 = R.ur1; q->ur2 = R.ur2; q->urr1 = R.urr1; q->urr2 = R.urr2;
+    q->beta1 = R.beta1; q->beta2 = R.beta2; q->a1 = R.a1; q->a2 = R.a2;
+    q->g1 = R.g1; q->g2 = R.g2; q->iu1 = R.iu1; q->iu2 = R.iu2;
+    return status;
+}
+
+int oracle_solve_block(const dvr3d_deck *deck, int kk, int pes_kind, const double *pes,
+                       int npes, const double *vgrid, size_t nvgrid, int final_mode,
+                       oracle_trace *trace, dvr3d_result *res) {
+    try {
+        Run R;
+        insize_setcon(R, *deck);
+        R.pes_kind = pes_kind;
+        if (pes_kind == DVR3D_PES_MORSE_SUM) {
+            if (!pes || npes < DVR3D_PES_MORSE_SUM_NPARAM) return DVR3D_ERR_ARG;
+            R.pes.assign(pes, pes + DVR3D_PES_MORSE_SUM_NPARAM);
+        }
+        R.vgrid = vgrid;
+        R.nvgrid = nvgrid;
+        ccmain_setup(R, kk);
+        if (trace) {
+            trace->npnta = R.npnta;
+            trace->npntb = R.npntb;
+            trace->npntc = R.npntc;
+            trace->max2d = R.max2d;
+            trace->max3d = R.max3d;
+            trace->kz = R.kz;
+            trace->ipar = R.ipar;
+        }
+        if (R.idia <= -2) nfmain(R, final_mode, trace, res);
+        else jhmain(R, final_mode, trace, res);
+        return DVR3D_OK;
+    } catch (Fail &f) {
+        return f.code;
+    } catch (std::exception &) {
+        return DVR3D_ERR_NOMEM;
+    }
+}
+
+double oracle_time_dsyev(int n, int reps, int mode) {
+    std::mt19937_64 rng(12345);
+    std::uniform_real_distribution<double> u(-1.0, 1.0);
+    std::vector<double> a0((size_t)n * n), a((size_t)n * n), w(n);
+    for (int j = 0; j < n; ++j)
+        for (int i = j; i < n; ++i) a0[(size_t)j * n + i] = a0[(size_t)i * n + j] = u(rng);
+    double tot = 0.0;
+    for (int r = 0; r < reps; ++r) {
+        a = a0;
+        auto t0 = std::chrono::steady_clock::now();
+        try {
+            diag(a.data(), n, n, w.data(), mode);
+        } catch (Fail &) {
+            return -1.0;
+        }
+        tot += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+    }
+    return tot / reps;
+}
+
+}  // extern "C"

@@ -1,0 +1,73 @@
+/*
+ * dvr3d_oracle.h -- CPU FP64 restatement of the DVR3DRJZ hot path.
+ *
+ * TEST INFRASTRUCTURE ONLY. This is the checker: it is loaded by tests/, by
+ * __graft_entry__.smoke() and by bench.py's CPU-baseline leg, never by the product
+ * library. It restates source/dvr3drjz_segmented.f90 of the reference routine by routine
+ * (each function cites the lines it follows) and calls LAPACK dsyev like the reference.
+ */
+#ifndef DVR3D_ORACLE_H
+#define DVR3D_ORACLE_H
+#include <stddef.h>
+#include "../include/dvr3d_b200.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Resolve dsyev/dsyevd/dgemm from a LAPACK shared object (scipy's OpenBLAS exports them
+ * as scipy_dsyev_ ...). `prefix` is the symbol prefix ("scipy_" or ""). */
+int oracle_load_lapack(const char *path, const char *prefix);
+
+/* Quadrature known-answer data of one k block (what lagpt / jacobi print). */
+typedef struct oracle_quad {
+    int npnt1, npnt2, nang2, nidvr;
+    double y1[128], wt1[128], r1[128];   /* Gauss-Laguerre points, weights, r (r1) */
+    double csx1, csa1, tsx1, tsa1;
+    double y2[128], wt2[128], r2[128];   /* same for r2 (idia > -2) */
+    double csx2, csa2, tsx2, tsa2;
+    double xhalf[128], whalf[128];       /* jacobi() output before allpts (printed)  */
+    double cswalf, tswalf;
+    double xalf[256], walf[256];         /* after allpts (walf = sqrt(scale w))      */
+    double ur1, ur2, urr1, urr2, beta1, beta2, a1, a2, g1, g2;
+    int iu1, iu2;
+    int status;                          /* 0 or DVR3D_ERR_QUADRATURE                */
+} oracle_quad;
+
+int oracle_quadrature(const dvr3d_deck *deck, int kk, oracle_quad *q);
+
+/* Optional intermediate outputs of one k block. All pointers may be NULL. */
+typedef struct oracle_trace {
+    int nblocks;                 /* nalf (Radau) or npntc (Jacobi)                        */
+    int npnta, npntb, npntc, max2d, max3d, kz, ipar;
+    int *iv1; int iv1_cap;       /* Jacobi: 1D counts iv1(ione,itwo) as [ione*npntb+itwo]  */
+    int *iv2; int iv2_cap;       /* per-block 2D selection counts                          */
+    int *n2d; int n2d_cap;       /* per-block 2D Hamiltonian dimension                     */
+    double *eig2all; int eig2all_cap;   /* all 2D eigenvalues, blocks concatenated         */
+    double *eigs2d; int eigs2d_cap;     /* selected 2D eigenvalues in final-basis order     */
+    double *h3; size_t h3_cap;          /* assembled final Hamiltonian (lower valid)        */
+    double stage_s[4];           /* wall seconds: 1D/2D stage, assembly, final diag, total */
+    int nham3;
+} oracle_trace;
+
+/* final_mode: 0 = dsyev('V','L') with lwork = 3*N as diag() does (:2650-2654);
+ *             1 = dsyevd (the divide-and-conquer variant kept commented in :2612-2636);
+ *             2 = stop after assembly (no final diagonalisation). */
+int oracle_solve_block(const dvr3d_deck *deck, int kk, int pes_kind, const double *pes,
+                       int npes, const double *vgrid, size_t nvgrid, int final_mode,
+                       oracle_trace *trace, dvr3d_result *res);
+
+/* Derived sizes of insize (:171-638) for one k block (kk = loop index of ccmain :857). */
+int oracle_sizes(const dvr3d_deck *deck, int kk, int *out16);
+
+/* Potential family DVR3D_PES_MORSE_SUM at one point (for fixtures). */
+double oracle_pes_morse_sum(const double *p, double r1, double r2, double xcos);
+
+/* Time `reps` dsyev('V','L') calls on a seeded random symmetric n x n (CPU baseline
+ * samples of the final eigensolve). Returns seconds per call. */
+double oracle_time_dsyev(int n, int reps, int mode);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

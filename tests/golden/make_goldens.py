@@ -1,0 +1,105 @@
+"""Extract the PES-independent known-answer data of the reference's example runs.
+
+Reads the job decks and printed outputs shipped with the reference (ExoMol/dvr3d) and
+writes ``quadrature_kat.json`` next to this script: for each example the deck text and,
+per k block, the printed Gauss-Laguerre points / r values / check sums (lagpt :1315-1361)
+and Gauss-(associated) Legendre points / weights / check sums (ccmain :932-938).
+
+The printed Laguerre "weights" column of these outputs comes from a later build of the
+program (outputs say "version of June 2010", the source "March 2002") that prints a
+different weight normalisation, so only points, r values and point sums are kept for the
+radial quadrature; the angular weights and sums are those of the source's routine.
+
+Run from the repository root:  python tests/golden/make_goldens.py /path/to/reference
+"""
+from __future__ import annotations
+
+import json
+import re
+import sys
+from pathlib import Path
+
+HERE = Path(__file__).resolve().parent
+
+CASES = {
+    "water_J0": ("water/jobs/dvr0.job", "water/results/result-0.water.dvr"),
+    "h3p_jacobi_J0": ("H3+Jacobi/jobs/dvrJ0.job", "H3+Jacobi/results/result.H3p.J0.dvr"),
+    "hcn_J2": ("HCN/jobs/dvr.job", "HCN/results/result.HCN.dvr"),
+}
+
+FNUM = r"[-+]?\d*\.\d+(?:[DdEe][-+]?\d+)?"
+
+
+def fnum(s: str) -> float:
+    return float(s.replace("D", "E").replace("d", "e"))
+
+
+def parse_output(text: str) -> dict:
+    lines = text.splitlines()
+    lag = []
+    leg = []
+    i = 0
+    while i < len(lines):
+        ln = lines[i]
+        m = re.search(r"(\d+) POINT GAUSS-LAGUERRE INTEGRATION", ln, re.I)
+        if m:
+            npt = int(m.group(1))
+            which = "r1" if "R1" in lines[i + 1].upper() else "r2"
+            pts = []
+            j = i + 2
+            while len(pts) < npt:
+                t = lines[j].split()
+                if len(t) == 3:
+                    try:
+                        pts.append((fnum(t[0]), fnum(t[2])))
+                    except ValueError:
+                        pass
+                j += 1
+            # sums: "COMPUTED SUM OF POINTS x & WEIGHTS y" then "EXACT ..."
+            while "SUM OF POINTS" not in lines[j].upper():
+                j += 1
+            comp = re.findall(FNUM, lines[j])
+            exact = re.findall(FNUM, lines[j + 1])
+            lag.append({"coord": which, "n": npt, "y": [p[0] for p in pts], "r": [p[1] for p in pts],
+                        "sum_points": fnum(comp[0]), "exact_sum_points": fnum(exact[0])})
+            i = j + 2
+            continue
+        m = re.search(r"(\d+) point Gauss-associated Legendre integration with k =\s*(\d+)", ln)
+        if m:
+            nang, k = int(m.group(1)), int(m.group(2))
+            xs, ws = [], []
+            j = i + 1
+            while not lines[j].strip().startswith("Computed sum of weights"):
+                t = lines[j].split()
+                if len(t) == 2:
+                    try:
+                        xs.append(fnum(t[0]))
+                        ws.append(fnum(t[1]))
+                    except ValueError:
+                        pass
+                j += 1
+            comp = fnum(re.findall(FNUM, lines[j])[0])
+            exact = fnum(re.findall(FNUM, lines[j + 1])[0])
+            leg.append({"nang": nang, "k": k, "x": xs, "w": ws, "computed_sum": comp, "exact_sum": exact})
+            i = j + 2
+            continue
+        i += 1
+    return {"laguerre": lag, "legendre": leg}
+
+
+def main(ref: str) -> None:
+    root = Path(ref)
+    out = {"source": "ExoMol/dvr3d example decks and printed outputs", "cases": {}}
+    for name, (job, res) in CASES.items():
+        deck = (root / job).read_text()
+        data = parse_output((root / res).read_text())
+        data["deck"] = deck
+        data["deck_file"] = job
+        data["output_file"] = res
+        out["cases"][name] = data
+    (HERE / "quadrature_kat.json").write_text(json.dumps(out, indent=1))
+    print("wrote", HERE / "quadrature_kat.json")
+
+
+if __name__ == "__main__":
+    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")

@@ -1,0 +1,115 @@
+"""The oracle and the product's host set-up against the reference's printed quadrature.
+
+Known answers: tests/golden/quadrature_kat.json, extracted by make_goldens.py from the
+example outputs shipped with the reference (water J=0 Radau, H3+ Jacobi J=0, HCN J=2).
+"""
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+import dvr3d_b200
+from dvr3d_b200 import parse_deck
+
+CASES = ["water_J0", "h3p_jacobi_J0", "hcn_J2"]
+
+
+def _deck(kat, name):
+    return parse_deck(kat["cases"][name]["deck"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_laguerre_points_match_reference(kat, oracle_mod, name):
+    d = _deck(kat, name)
+    q = oracle_mod.quadrature(d, dvr3d_b200.k_blocks(d)[0])
+    assert q.status == 0
+    for lag in kat["cases"][name]["laguerre"]:
+        n = lag["n"]
+        if lag["coord"] == "r1":
+            y, r, csx, tsx = np.array(q.y1[:n]), np.array(q.r1[:n]), q.csx1, q.tsx1
+        else:
+            y, r, csx, tsx = np.array(q.y2[:n]), np.array(q.r2[:n]), q.csx2, q.tsx2
+        ref_y, ref_r = np.array(lag["y"]), np.array(lag["r"])
+        # points printed with 15 decimals (f23.15), r with 5 (f13.5)
+        np.testing.assert_allclose(y, ref_y, rtol=2e-14, atol=2e-13)
+        np.testing.assert_allclose(r, ref_r, rtol=0, atol=5.1e-6)
+        assert abs(csx - lag["sum_points"]) <= 1e-9 * lag["sum_points"]
+        assert abs(tsx - lag["exact_sum_points"]) <= 1e-12 * lag["exact_sum_points"]
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_legendre_points_weights_and_sums_match_reference(kat, oracle_mod, name):
+    d = _deck(kat, name)
+    ks = dvr3d_b200.k_blocks(d)
+    legs = kat["cases"][name]["legendre"]
+    assert len(legs) == len(ks)
+    for kk, leg in zip(ks, legs):
+        q = oracle_mod.quadrature(d, kk)
+        assert q.status == 0
+        n2 = q.nang2
+        assert n2 == len(leg["x"])
+        np.testing.assert_allclose(np.array(q.xhalf[:n2]), leg["x"], rtol=0, atol=1.01e-15)
+        np.testing.assert_allclose(np.array(q.whalf[:n2]), leg["w"], rtol=1e-11, atol=0)
+        # the reference's printed sum carries its iteration history (e.g. 1.99999999999202):
+        # reproducing it to the printed 15 digits pins the root finder step for step
+        assert abs(q.cswalf - leg["computed_sum"]) <= 1.5e-14 * abs(leg["computed_sum"])
+        assert abs(q.tswalf - leg["exact_sum"]) <= 1e-14 * abs(leg["exact_sum"])
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_product_host_grid_matches_reference(kat, name):
+    """The library's own set-up (dvr3d_b200_grid, host-only) gives the same grid."""
+    d = _deck(kat, name)
+    ks = dvr3d_b200.k_blocks(d)
+    for kk, leg in zip(ks, kat["cases"][name]["legendre"]):
+        r1, r2, xa = dvr3d_b200.host_grid(d, kk)
+        n2 = len(leg["x"])
+        if d.idia == 2:
+            np.testing.assert_allclose(xa[:n2], leg["x"], rtol=0, atol=1.01e-15)
+        else:
+            np.testing.assert_allclose(xa[-n2:][::-1], leg["x"], rtol=0, atol=1.01e-15)
+            np.testing.assert_allclose(xa[:n2], -np.array(leg["x"]), rtol=0, atol=1.01e-15)
+        for lag in kat["cases"][name]["laguerre"]:
+            r = r1 if lag["coord"] == "r1" else r2
+            np.testing.assert_allclose(r[:lag["n"]], lag["r"], rtol=0, atol=5.1e-6)
+
+
+@pytest.mark.parametrize("name", CASES)
+def test_product_host_grid_equals_oracle(kat, oracle_mod, name):
+    d = _deck(kat, name)
+    for kk in dvr3d_b200.k_blocks(d):
+        q = oracle_mod.quadrature(d, kk)
+        r1, r2, xa = dvr3d_b200.host_grid(d, kk)
+        np.testing.assert_array_equal(r1, np.array(q.r1[:len(r1)]))
+        if d.idia != -2:
+            np.testing.assert_array_equal(r2, np.array(q.r2[:len(r2)]))
+        np.testing.assert_array_equal(xa, np.array(q.xalf[:len(xa)]))
+
+
+def test_water_deck_card_order_quirk(kat):
+    """setcon reads EMAX1/EMAX2 before the Morse cards (:1058-1095); the water deck has no
+    separate EMAX card, so its first Morse line is consumed as EMAX1, EMAX2."""
+    d = _deck(kat, "water_J0")
+    assert (d.npnt2, d.jrot, d.neval, d.nalf, d.max2d, d.max3d, d.idia, d.kmin) == (21, 0, 25, 40, 500, 500, -2, 2)
+    assert (d.emax1, d.emax2) == (2.55, 0.25)
+    assert (d.re1, d.diss1, d.we1) == (2.55, 0.25, 0.007)
+    assert d.zrot == 1 and d.zlin == 1 and d.ztran == 1 and d.zpfun == 1 and d.zcut == 0
+    assert list(d.xmass) == [1.007825, 1.007825, 15.990726]
+
+
+def test_hcn_deck_namelist_spanning_lines(kat):
+    d = _deck(kat, "hcn_J2")
+    assert d.ztheta == 0 and d.zr2r1 == 0 and d.zembed == 0 and d.zp1d == 0 and d.zp2d == 0
+    assert (d.npnt2, d.jrot, d.neval, d.nalf, d.idia, d.kmin, d.npnt1) == (30, 2, 40, 45, 1, 2, 16)
+    assert d.emax1 == 45000.0
+    assert dvr3d_b200.k_blocks(d) == [0, 1, 2]
+
+
+def test_reduced_masses_match_printed(kat, oracle_mod):
+    # water output: reduced mass 0.1732801D+04, beta 0.4121, a 0.1428571D+03, u 143
+    q = oracle_mod.quadrature(_deck(kat, "water_J0"), 0)
+    assert abs(q.ur1 - 1732.801) < 5e-4 and abs(q.beta1 - 0.4121) < 5e-5 and q.iu1 == 143
+    # H3+ Jacobi: 0.9183139D+03 / 0.7996 / u=34 ; 0.1224419D+04 / 0.4367 / u=116
+    q = oracle_mod.quadrature(_deck(kat, "h3p_jacobi_J0"), 0)
+    assert abs(q.ur1 - 918.3139) < 5e-5 and abs(q.beta1 - 0.7996) < 5e-5 and q.iu1 == 34
+    assert abs(q.ur2 - 1224.419) < 5e-4 and abs(q.beta2 - 0.4367) < 5e-5 and q.iu2 == 116
