@@ -100,6 +100,12 @@ class SolveResult:
         return self.eval * AUTOCM
 
 
+def _counters(r: Result) -> dict:
+    return {"dom_ms": r.dom_ms, "dom_bytes": r.dom_bytes, "dom_flops": r.dom_flops,
+            "dom_launches": r.dom_launches, "launches": r.launches, "h2d_bytes": r.h2d_bytes,
+            "d2h_bytes": r.d2h_bytes, "dom_kernel": r.dom_kernel.decode()}
+
+
 class Context:
     """One CUDA device context of the library (dvr3d_b200_init)."""
 
@@ -205,7 +211,7 @@ class Context:
                            ipar=r.ipar, stage_ms=np.array(r.stage_ms[:]), max_resid=r.max_resid,
                            iterations=r.iterations, fallback=r.fallback,
                            resid=None if rs is None else rs[:m].copy(),
-                           evec=None if evec is None else evec[:, :m], h3=h3)
+                           evec=None if evec is None else evec[:, :m], h3=h3, extra=_counters(r))
 
     def solve_batch(self, decks: list[Deck], pes_rows) -> list[SolveResult]:
         n = len(decks)

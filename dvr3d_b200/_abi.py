@@ -75,6 +75,10 @@ class Result(C.Structure):
     _fields_ = [("kz", C.c_int), ("ipar", C.c_int), ("nham3", C.c_int), ("meval", C.c_int),
                 ("nblocks", C.c_int), ("iterations", C.c_int), ("fallback", C.c_int),
                 ("stage_ms", C.c_double * 6), ("max_resid", C.c_double),
+                ("dom_ms", C.c_double), ("dom_bytes", C.c_double), ("dom_flops", C.c_double),
+                ("dom_launches", C.c_int), ("launches", C.c_int),
+                ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong),
+                ("dom_kernel", C.c_char * 48),
                 ("eval", C.POINTER(C.c_double)), ("eval_cap", C.c_int),
                 ("iv2", C.POINTER(C.c_int)), ("iv2_cap", C.c_int),
                 ("resid", C.POINTER(C.c_double)), ("resid_cap", C.c_int),

@@ -91,7 +91,7 @@ def config1() -> Workload:
 
 def config2() -> Workload:
     """Same family at NPNT=30, NALF=64; 2D cut-off chosen for a final basis of ~4000."""
-    return radau_water_like(30, 64, 40000.0, 300, title="cfg2 Radau NPNT=30 NALF=64")
+    return radau_water_like(30, 64, 62000.0, 300, title="cfg2 Radau NPNT=30 NALF=64")
 
 
 def config3(seed: int = 2024, nprob: int = 64) -> list[Workload]:
@@ -133,8 +133,8 @@ def jacobi_h3p_like(npnt1: int, npnt2: int, nalf: int, emax1_cm: float, emax2_cm
 
 
 # cut-offs of the headline workload, fixed once against the oracle's 1D/2D stages
-CFG4_EMAX1 = 60000.0
-CFG4_EMAX2 = 60000.0
+CFG4_EMAX1 = 50000.0
+CFG4_EMAX2 = 40000.0
 
 
 def config4(emax1: float = CFG4_EMAX1, emax2: float = CFG4_EMAX2) -> Workload:

@@ -144,18 +144,21 @@ __global__ void gather_kernel(const double *src, const long long *map, double *d
 void launch_radau_build(const RadauBuild &rb, int nalf, double *H, cudaStream_t st) {
     const long long nn = (long long)rb.n * rb.n;
     dim3 grid((unsigned)((nn + 255) / 256), nalf);
+    DVR3D_COUNT_LAUNCH(1);
     radau_build_kernel<<<grid, 256, 0, st>>>(rb, H);
 }
 
 void launch_jacobi_build1d(const Jacobi1D &jb, int nblk, double *H, cudaStream_t st) {
     const int nn = jb.npnta * jb.npnta;
     dim3 grid((nn + 127) / 128, nblk);
+    DVR3D_COUNT_LAUNCH(1);
     jacobi_build1d_kernel<<<grid, 128, 0, st>>>(jb, H);
 }
 
 void launch_jacobi_build2d(const Jacobi2D &jb, int nblk, int n2max, double *H2, cudaStream_t st) {
     const long long nn = (long long)n2max * n2max;
     dim3 grid((unsigned)((nn + 255) / 256), nblk);
+    DVR3D_COUNT_LAUNCH(1);
     jacobi_build2d_kernel<<<grid, 256, 0, st>>>(jb, H2);
 }
 
@@ -165,17 +168,20 @@ void launch_jacobi_ctrans(const Jacobi2D &jb, const CTrans &ct, int nblk, int s2
     const long long tot = P * s2max;
     if (tot == 0) return;
     dim3 grid((unsigned)((tot + 255) / 256), nblk);
+    DVR3D_COUNT_LAUNCH(1);
     jacobi_ctrans_kernel<<<grid, 256, 0, st>>>(jb, ct, V2, Vt);
 }
 
 void launch_scale_rows(double *Vt, int P, long long ncol, const double *sw, cudaStream_t st) {
     const long long tot = (long long)P * ncol;
     if (tot == 0) return;
+    DVR3D_COUNT_LAUNCH(1);
     scale_rows_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(Vt, P, ncol, sw);
 }
 
 void launch_gather(const double *src, const long long *map, double *dst, long long n, cudaStream_t st) {
     if (n == 0) return;
+    DVR3D_COUNT_LAUNCH(1);
     gather_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(src, map, dst, n);
 }
 

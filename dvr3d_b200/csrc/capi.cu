@@ -125,11 +125,11 @@ int dvr3d_b200_init(int device, dvr3d_ctx **out) {
     dvr3d_ctx *ctx = new dvr3d_ctx();
     ctx->device = device;
     ctx->sm_count = prop.multiProcessorCount;
-    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) {
+    if (cudaStreamCreateWithFlags(&ctx->own_stream, cudaStreamNonBlocking) != cudaSuccess) {
         delete ctx;
         return DVR3D_ERR_CUDA;
     }
-    ctx->own_stream = true;
+    ctx->stream = ctx->own_stream;
     for (auto &e : ctx->ev) cudaEventCreate(&e);
     ctx->dense_grid = dvr3d::dense_tridiag_grid(device);
     ctx->pes.kind = DVR3D_PES_NONE;
@@ -144,17 +144,14 @@ void dvr3d_b200_destroy(dvr3d_ctx *ctx) {
     ctx->arena.release_all();
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
-    if (ctx->own_stream && ctx->stream) cudaStreamDestroy(ctx->stream);
+    for (auto &e : ctx->panel_ev) cudaEventDestroy(e);
+    if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
 }
 
 int dvr3d_b200_set_stream(dvr3d_ctx *ctx, void *stream) {
     if (!ctx) return DVR3D_ERR_ARG;
-    if (stream) {
-        ctx->stream = (cudaStream_t)stream;
-    } else {
-        return DVR3D_ERR_ARG;
-    }
+    ctx->stream = stream ? (cudaStream_t)stream : ctx->own_stream;
     return DVR3D_OK;
 }
 
@@ -406,5 +403,6 @@ __global__ void symmetrize_lower_kernel(dvr3d::BatchDesc bd, double *A) {
 
 void dvr3d_symmetrize_lower(const dvr3d::BatchDesc &bd, double *A, int nmax, cudaStream_t st) {
     dim3 grid((unsigned)(((long long)nmax * nmax + 255) / 256), bd.nblk);
+    DVR3D_COUNT_LAUNCH(1);
     symmetrize_lower_kernel<<<grid, 256, 0, st>>>(bd, A);
 }

@@ -6,6 +6,11 @@
 
 namespace dvr3d {
 
+// Number of kernels this library has launched (host side; read by the solve entry
+// points to report the launches of one solve).
+extern long long g_kernel_launches;
+#define DVR3D_COUNT_LAUNCH(k) (::dvr3d::g_kernel_launches += (k))
+
 // Device-side error flags written by kernels (never __trap): the host reads them after a
 // stage and turns them into DVR3D_ERR_* codes.
 enum DeviceErr : int {
@@ -74,7 +79,7 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, int *err, unsigned lon
                     atomicExch(err, (int)kDevBarrierTimeout);
                     break;
                 }
-                if (spins > 64) __nanosleep(64);
+                if (spins > 4096) __nanosleep(32);
             }
         }
         __threadfence();

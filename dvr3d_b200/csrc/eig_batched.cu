@@ -299,6 +299,7 @@ void launch_tridiag_batched(const BatchDesc &bd, double *A, double *d, double *e
                             int nmax, cudaStream_t st) {
     if (bd.nblk <= 0) return;
     const size_t smem = (size_t)3 * nmax * sizeof(double);
+    DVR3D_COUNT_LAUNCH(1);
     tridiag_kernel<<<bd.nblk, kTriThreads, smem, st>>>(bd, A, d, e, tau);
 }
 
@@ -308,6 +309,7 @@ void launch_eigvals_batched(const BatchDesc &bd, const double *d, const double *
     int nmax = 0;
     (void)nmax;
     // dynamic shared memory: d and e^2 of the largest block (caller guarantees <= 1024)
+    DVR3D_COUNT_LAUNCH(1);
     eigvals_kernel<<<bd.nblk, kEvThreads, 2 * 1024 * sizeof(double), st>>>(bd, d, e, w, cnt, mode, cut);
 }
 
@@ -320,6 +322,7 @@ void launch_eigvecs_batched(const BatchDesc &bd, const double *A, const double *
     size_t smem = (size_t)nmax * sizeof(double);
     const size_t smem_cl = (size_t)(nmax + 2) * sizeof(int);
     if (smem_cl > smem) smem = smem_cl;
+    DVR3D_COUNT_LAUNCH(1);
     eigvecs_kernel<<<bd.nblk, kVecThreads, smem, st>>>(bd, A, d, e, tau, w, sel, zoff, zld, Z, work,
                                                        workoff, err);
 }

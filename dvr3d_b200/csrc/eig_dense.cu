@@ -3,13 +3,15 @@
 // Replaces diag3d -> diag -> dsyev('V','L') of the reference (:2661-2764, :2638-2659) for
 // the plain FP64 path. Same structure as the batched solver (Householder reduction,
 // bisection, inverse iteration, back-transformation) but spread over the whole GPU:
-//   - the reduction is one cooperative kernel: every CTA owns a slice of rows of the
-//     trailing matrix; per column three bounded grid barriers separate the reflector
-//     formation, the fused (pending rank-2 update + symmetric product) pass and w;
+//   - the reduction is blocked like LAPACK's dsytrd/dlatrd: a cooperative kernel forms
+//     the 32 reflectors of a panel (one symmetric product over the lower triangle of the
+//     trailing matrix per column, in 64x64 tiles with deterministic partial sums and four
+//     bounded grid barriers per column), then a DMMA SYR2K updates the trailing matrix;
 //   - eigenvalues by multisection: one warp per wanted eigenvalue, 32 Sturm counts per
 //     pass, the interval shrinks 33x per pass;
 //   - inverse iteration one thread per cluster of close eigenvalues;
 //   - back-transformation by the stored reflectors, one warp per 4 eigenvectors.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 
@@ -21,164 +23,352 @@ namespace dvr3d {
 
 namespace {
 
-constexpr int kDtThreads = 256;  // 8 warps: lanes = rows, warps = column groups
-constexpr int kDtRmax = 8;       // row sub-chunks of 32 per CTA -> trailing size <= G*256
+constexpr int TB = 64;          // symmetric tile edge
+constexpr int TS = TB + 1;      // shared-memory column stride (conflict-free transposed reads)
+constexpr int kPnThreads = 256;
+constexpr int kMaxNb = 64;
 
-__global__ void __launch_bounds__(kDtThreads) dense_tridiag_kernel(DenseTri t) {
-    const int n = t.n;
+constexpr int kChunk = 256;     // rows owned by one owner CTA (one row per thread)
+
+// Optional phase timers: CTA 0 accumulates SM clock cycles spent in each phase
+// (prof[0..5]: column update, reflector, symmetric product, reduction, w, exit).
+#define PROF_MARK(ph)                                                   \
+    do {                                                                \
+        if (t.prof && cta == 0 && tid == 0) {                          \
+            const long long now_ = clock64();                           \
+            if (prof_last_ >= 0) t.prof[prof_ph_] += now_ - prof_last_; \
+            prof_last_ = now_;                                          \
+            prof_ph_ = (ph);                                            \
+        }                                                               \
+    } while (0)
+
+// One panel of the blocked Householder reduction (the dlatrd scheme: columns are formed
+// from the panel-start matrix plus the rank-2 corrections V W^T + W V^T of the panel's
+// earlier columns; the trailing matrix itself is updated once per panel by syr2k).
+// Work split: every CTA takes 64x64 lower tiles of the symmetric product; the first
+// NO = ceil(n/256) CTAs also own 256 rows each for the vector work (column update,
+// reductions, w), so cross-CTA sums are over NO partials only.
+// Per column four bounded grid barriers separate: column update + norm | symmetric
+// product (deterministic per-tile partial sums) | reduction of the partials | w.
+__global__ void __launch_bounds__(kPnThreads, 3) dense_panel_kernel(DenseTri t) {
+    const int n = t.n, NT = t.NT;
     const long long ld = t.lda;
     double *A = t.A;
-    const int G = gridDim.x, cta = blockIdx.x;
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int G = gridDim.x, cta = blockIdx.x, tid = threadIdx.x;
+    const int lane = tid & 31, warp = tid >> 5;
+    const int NO = (n + kChunk - 1) / kChunk;
+    const bool owner = cta < NO;
+    const int r_own = cta * kChunk + tid;  // the row this thread owns (if owner)
+    __shared__ double S[TB * TS];
+    __shared__ double vI[TB], vJ[TB];
     __shared__ double red[32];
-    __shared__ double s_part[kDtRmax * 32 * 8];
-    __shared__ double s_tau, s_scal, s_beta;
-    bool pending = false;
-    for (int k = 0; k + 2 < n; ++k) {
-        const int m = n - k - 1;                    // trailing rows k+1 .. n-1
-        int chunk = (m + G - 1) / G;
-        chunk = ((chunk + 31) / 32) * 32;
-        const int r0 = k + 1 + cta * chunk;
-        const int r1 = min(n, r0 + chunk);
-        // (a) finish column k on own rows, partial norm of rows >= k+2
-        double ss = 0.0;
-        {
-            const double vk = pending ? t.vp[k] : 0.0, wk = pending ? t.wp[k] : 0.0;
-            if (cta == 0 && tid == 0 && pending) A[(size_t)k * ld + k] -= 2.0 * vk * wk;
-            for (int i = r0 + tid; i < r1; i += blockDim.x) {
-                double x = A[(size_t)k * ld + i];
-                if (pending) {
-                    x -= t.vp[i] * wk + t.wp[i] * vk;
-                    A[(size_t)k * ld + i] = x;
-                }
-                if (i >= k + 2) ss += x * x;
+    __shared__ double rsum[4][TB];
+    __shared__ double s_corr[2 * kMaxNb];
+    __shared__ double s_tau, s_scal, s_a2;
+    const int nbmax = t.nbmax;
+    double *part_n = t.part;                  // [NO] norms / dots
+    double *part_q = t.part + G;              // [NO][2 nbmax] V^T v, W^T v
+    long long prof_last_ = -1;
+    int prof_ph_ = 0;
+    for (int i = 0; i < t.nb; ++i) {
+        const int k = t.j0 + i;
+        if (k + 2 >= n) break;
+        // ---- phase A: column k of the current matrix on owned rows, partial norm
+        PROF_MARK(0);
+        if (owner) {
+            double ss = 0.0;
+            const int r = r_own;
+            if (r >= k && r < n) {
+                double a = A[(size_t)k * ld + r];
+                for (int q = 0; q < i; ++q)
+                    a -= t.V[(size_t)q * n + r] * t.W[(size_t)q * n + k] + t.W[(size_t)q * n + r] * t.V[(size_t)q * n + k];
+                t.acol[r] = a;
+                if (r >= k + 2) ss = a * a;
             }
+            ss = block_sum(ss, red);
+            if (tid == 0) part_n[cta] = ss;
         }
-        ss = block_sum(ss, red);
-        if (tid == 0) t.part[cta] = ss;
         if (!grid_sync(t.bar, t.err)) return;
-        // (b) reflector (redundantly in every CTA), fused pass over own rows
+        // ---- phase B: reflector (redundantly in every CTA)
+        PROF_MARK(1);
         if (tid < 32) {
             double s = 0.0;
-            for (int c = tid; c < G; c += 32) s += t.part[c];
+            for (int c = tid; c < NO; c += 32) s += part_n[c];
             s = warp_sum(s);
             if (tid == 0) {
-                const double alpha = A[(size_t)k * ld + k + 1];
+                const double alpha = t.acol[k + 1];
+                double beta, tk, sc;
                 if (s == 0.0) {
-                    s_tau = 0.0;
-                    s_beta = alpha;
-                    s_scal = 0.0;
+                    tk = 0.0;
+                    beta = alpha;
+                    sc = 0.0;
                 } else {
-                    const double beta = -copysign(sqrt(alpha * alpha + s), alpha);
-                    s_tau = (beta - alpha) / beta;
-                    s_beta = beta;
-                    s_scal = 1.0 / (alpha - beta);
+                    beta = -copysign(sqrt(alpha * alpha + s), alpha);
+                    tk = (beta - alpha) / beta;
+                    sc = 1.0 / (alpha - beta);
                 }
+                s_tau = tk;
+                s_scal = sc;
                 if (cta == 0) {
-                    t.d[k] = A[(size_t)k * ld + k];
-                    t.e[k] = s_beta;
-                    t.tau[k] = s_tau;
-                    t.scal[k] = s_scal;
+                    t.d[k] = t.acol[k];
+                    t.e[k] = beta;
+                    t.tau[k] = tk;
                 }
             }
         }
         __syncthreads();
         const double tk = s_tau, scal = s_scal;
-        const int nsub = (r1 > r0) ? (r1 - r0 + 31) / 32 : 0;
-        double acc[kDtRmax];
-        double vpi[kDtRmax], wpi[kDtRmax];
+        auto vval = [&](int r) -> double {
+            if (r <= k || r >= n) return 0.0;
+            return (r == k + 1) ? 1.0 : t.acol[r] * scal;
+        };
+        // ---- phase C: s = A22 v over lower tiles of rows/cols >= k+1
+        PROF_MARK(2);
+        const int t0 = (k + 1) / TB;
+        const int ntr = NT - t0;
+        const long long ntiles = (long long)ntr * (ntr + 1) / 2;
+        if (tk != 0.0 && cta < ntiles) {
+            // the next tile (and its two v slices) is loaded into registers while the
+            // current one is reduced from shared memory; warp w reads columns w, w+8, ..
+            // with one 512-byte coalesced row segment per instruction
+            double pre[16];
+            double pv_pre = 0.0;
+            int I = 0, J = 0;
+            auto decode = [&](long long tt, int &Io, int &Jo) {
+                int li = (int)((sqrt(8.0 * (double)tt + 1.0) - 1.0) * 0.5);
+                while ((long long)li * (li + 1) / 2 > tt) --li;
+                while ((long long)(li + 1) * (li + 2) / 2 <= tt) ++li;
+                Io = t0 + li;
+                Jo = t0 + (int)(tt - (long long)li * (li + 1) / 2);
+            };
+            auto fetch = [&](int Io, int Jo) {
+                const int r0 = Io * TB, c0 = Jo * TB;
+                const int rr = r0 + 2 * lane;
 #pragma unroll
-        for (int r = 0; r < kDtRmax; ++r) {
-            acc[r] = 0.0;
-            const int i = r0 + r * 32 + lane;
-            vpi[r] = (pending && r < nsub && i < r1) ? t.vp[i] : 0.0;
-            wpi[r] = (pending && r < nsub && i < r1) ? t.wp[i] : 0.0;
-        }
-        if (nsub > 0 && (tk != 0.0 || pending)) {
-            for (int j = k + 1 + warp; j < n; j += 8) {
-                const double vj = (j == k + 1) ? 1.0 : A[(size_t)k * ld + j] * scal;
-                const double vpj = pending ? t.vp[j] : 0.0, wpj = pending ? t.wp[j] : 0.0;
-                double *col = A + (size_t)j * ld;
-#pragma unroll
-                for (int r = 0; r < kDtRmax; ++r) {
-                    if (r < nsub) {
-                        const int i = r0 + r * 32 + lane;
-                        if (i < r1) {
-                            double x = col[i];
-                            if (pending) {
-                                x -= vpi[r] * wpj + wpi[r] * vpj;
-                                col[i] = x;
-                            }
-                            acc[r] += x * vj;
-                        }
+                for (int m = 0; m < 8; ++m) {
+                    const int gc = c0 + warp + 8 * m;
+                    const double *src = A + (size_t)gc * ld + rr;
+                    if (gc < n && rr + 1 < n) {
+                        const double2 x = __ldcg(reinterpret_cast<const double2 *>(src));
+                        pre[2 * m] = x.x;
+                        pre[2 * m + 1] = x.y;
+                    } else {
+                        pre[2 * m] = (gc < n && rr < n) ? src[0] : 0.0;
+                        pre[2 * m + 1] = 0.0;
                     }
+                }
+                pv_pre = (tid < TB) ? vval(r0 + tid) : (tid < 2 * TB ? vval(c0 + tid - TB) : 0.0);
+            };
+            decode(cta, I, J);
+            fetch(I, J);
+            for (long long tt = cta; tt < ntiles; tt += G) {
+                const int cI = I, cJ = J;
+#pragma unroll
+                for (int m = 0; m < 8; ++m) {
+                    S[(warp + 8 * m) * TS + 2 * lane] = pre[2 * m];
+                    S[(warp + 8 * m) * TS + 2 * lane + 1] = pre[2 * m + 1];
+                }
+                if (tid < TB) vI[tid] = pv_pre;
+                else if (tid < 2 * TB) vJ[tid - TB] = pv_pre;
+                if (tt + G < ntiles) {
+                    decode(tt + G, I, J);
+                    fetch(I, J);
+                }
+                __syncthreads();
+                if (cI == cJ) {
+                    // mirror the lower triangle into the upper one
+                    for (int q = tid; q < TB * TB; q += kPnThreads) {
+                        const int c = q / TB, r = q % TB;
+                        if (r < c) S[c * TS + r] = S[r * TS + c];
+                    }
+                    __syncthreads();
+                }
+                const int r = tid & 63, g = tid >> 6;
+                {   // row products y_I[r] = sum_c S[c][r] vJ[c]
+                    double acc = 0.0;
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) acc += S[(g * 16 + u) * TS + r] * vJ[g * 16 + u];
+                    rsum[g][r] = acc;
+                }
+                double acc2 = 0.0;
+                if (cI != cJ) {  // column products y_J[c] = sum_r S[c][r] vI[r]
+#pragma unroll
+                    for (int u = 0; u < 16; ++u) acc2 += S[r * TS + g * 16 + u] * vI[g * 16 + u];
+                }
+                __syncthreads();
+                if (tid < TB)
+                    t.P[((size_t)cI * NT + cJ) * TB + tid] = rsum[0][tid] + rsum[1][tid] + rsum[2][tid] + rsum[3][tid];
+                __syncthreads();
+                if (cI != cJ) {
+                    rsum[g][r] = acc2;
+                    __syncthreads();
+                    if (tid < TB)
+                        t.P[((size_t)cJ * NT + cI) * TB + tid] = rsum[0][tid] + rsum[1][tid] + rsum[2][tid] + rsum[3][tid];
+                    __syncthreads();
                 }
             }
         }
-        // reduce the 8 column groups
+        // owners: store v (panel column i and reflector storage); partial V^T v, W^T v
+        if (owner) {
+            const int r = r_own;
+            if (r > k && r < n) {
+                const double v = vval(r);
+                t.V[(size_t)i * n + r] = v;
+                if (r >= k + 2) A[(size_t)k * ld + r] = v;
+            }
+            const int rb = cta * kChunk;
+            for (int q = warp; q < 2 * i; q += kPnThreads / 32) {
+                const double *x = (q < i) ? t.V + (size_t)q * n : t.W + (size_t)(q - i) * n;
+                double s = 0.0;
 #pragma unroll
-        for (int r = 0; r < kDtRmax; ++r)
-            if (r < nsub) s_part[(warp * kDtRmax + r) * 32 + lane] = acc[r];
-        __syncthreads();
-        double pv = 0.0;
-        for (int q = tid; q < nsub * 32; q += blockDim.x) {
-            const int r = q >> 5, l = q & 31;
-            const int i = r0 + q;
-            double s = 0.0;
-            for (int w = 0; w < 8; ++w) s += s_part[(w * kDtRmax + r) * 32 + l];
-            if (i < r1) {
-                const double vi = (i == k + 1) ? 1.0 : A[(size_t)k * ld + i] * scal;
-                const double p = tk * s;
-                t.pbuf[i] = p;
-                pv += p * vi;
+                for (int m = 0; m < kChunk / 32; ++m) {
+                    const int rr = rb + lane + 32 * m;
+                    if (rr > k && rr < n) s += x[rr] * vval(rr);
+                }
+                s = warp_sum(s);
+                if (lane == 0) part_q[(size_t)cta * 2 * nbmax + ((q < i) ? q : nbmax + (q - i))] = s;
             }
         }
-        pv = block_sum(pv, red);
-        if (tid == 0) t.part[G + cta] = pv;
         if (!grid_sync(t.bar, t.err)) return;
-        // (c) w = p - (tau/2)(p.v) v on own rows; becomes the pending update
-        __shared__ double s_pv;
-        if (tid < 32) {
-            double s = 0.0;
-            for (int c = tid; c < G; c += 32) s += t.part[G + c];
-            s = warp_sum(s);
-            if (tid == 0) s_pv = s;
+        // ---- phase D (owners): y = partial sums - V (W^T v) - W (V^T v); p = tau y
+        PROF_MARK(3);
+        if (owner) {
+            for (int q = warp; q < 2 * i; q += kPnThreads / 32) {
+                const int off = (q < i) ? q : nbmax + (q - i);
+                double s = 0.0;
+                for (int c = lane; c < NO; c += 32) s += part_q[(size_t)c * 2 * nbmax + off];
+                s = warp_sum(s);
+                if (lane == 0) s_corr[q] = s;  // [0,i): V^T v ; [i,2i): W^T v
+            }
+            __syncthreads();
+            double pv = 0.0;
+            const int r = r_own;
+            if (r > k && r < n) {
+                double y0 = 0.0, y1 = 0.0, y2 = 0.0, y3 = 0.0;
+                if (tk != 0.0) {
+                    const double *Pr = t.P + ((size_t)(r / TB) * NT) * TB + (r % TB);
+                    int c = t0;
+                    for (; c + 3 < NT; c += 4) {
+                        y0 += Pr[(size_t)c * TB];
+                        y1 += Pr[(size_t)(c + 1) * TB];
+                        y2 += Pr[(size_t)(c + 2) * TB];
+                        y3 += Pr[(size_t)(c + 3) * TB];
+                    }
+                    for (; c < NT; ++c) y0 += Pr[(size_t)c * TB];
+                }
+                double y = (y0 + y1) + (y2 + y3);
+                for (int q = 0; q < i; ++q)
+                    y -= t.V[(size_t)q * n + r] * s_corr[i + q] + t.W[(size_t)q * n + r] * s_corr[q];
+                const double p = tk * y;
+                t.ybuf[r] = p;
+                pv = p * vval(r);
+            }
+            pv = block_sum(pv, red);
+            if (tid == 0) part_n[cta] = pv;
+        }
+        if (!grid_sync(t.bar, t.err)) return;
+        // ---- phase E (owners): w = p - (tau/2)(p.v) v -> W[:, i]
+        PROF_MARK(4);
+        if (owner) {
+            if (tid < 32) {
+                double s = 0.0;
+                for (int c = tid; c < NO; c += 32) s += part_n[c];
+                s = warp_sum(s);
+                if (tid == 0) s_a2 = -0.5 * tk * s;
+            }
+            __syncthreads();
+            const int r = r_own;
+            if (r > k && r < n) t.W[(size_t)i * n + r] = t.ybuf[r] + s_a2 * vval(r);
+        }
+        if (!grid_sync(t.bar, t.err)) return;
+    }
+    PROF_MARK(5);
+}
+
+// Trailing update A[j1:, j1:] (lower) -= V W^T + W V^T with DMMA, K = 2 nb.
+__device__ __forceinline__ void dmma884d(double &c0, double &c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+__global__ void __launch_bounds__(128) syr2k_lower_kernel(double *A, long long ld, int n, int j1, const double *V,
+                                                          const double *W, int nb) {
+    const long long tt = blockIdx.x;
+    int li = (int)((sqrt(8.0 * (double)tt + 1.0) - 1.0) * 0.5);
+    while ((long long)li * (li + 1) / 2 > tt) --li;
+    while ((long long)(li + 1) * (li + 2) / 2 <= tt) ++li;
+    const int lj = (int)(tt - (long long)li * (li + 1) / 2);
+    const int i0 = j1 + li * 64, jj0 = j1 + lj * 64;
+    __shared__ double Xs[64][20];
+    __shared__ double Ys[64][20];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    double acc[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    const int K = 2 * nb;
+    for (int k0 = 0; k0 < K; k0 += 16) {
+#pragma unroll
+        for (int q = 0; q < 8; ++q) {
+            const int e = tid + q * 128;
+            const int kk = e / 64, m = e % 64;
+            const int gk = k0 + kk;
+            double x = 0.0, y = 0.0;
+            if (gk < K) {
+                const int gi = i0 + m, gj = jj0 + m;
+                const double *Xc = (gk < nb) ? V + (size_t)gk * n : W + (size_t)(gk - nb) * n;
+                const double *Yc = (gk < nb) ? W + (size_t)gk * n : V + (size_t)(gk - nb) * n;
+                if (gi < n) x = Xc[gi];
+                if (gj < n) y = Yc[gj];
+            }
+            Xs[m][kk] = x;
+            Ys[m][kk] = y;
         }
         __syncthreads();
-        const double alpha2 = -0.5 * tk * s_pv;
-        for (int i = r0 + tid; i < r1; i += blockDim.x) {
-            const double vi = (i == k + 1) ? 1.0 : A[(size_t)k * ld + i] * scal;
-            t.vp[i] = vi;
-            t.wp[i] = t.pbuf[i] + alpha2 * vi;
+        const int r = lane >> 2, c = lane & 3;
+#pragma unroll
+        for (int kk = 0; kk < 16; kk += 4) {
+            double af[4], bf[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) af[q] = Xs[wm + q * 8 + r][kk + c];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) bf[q] = Ys[wn + q * 8 + r][kk + c];
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < 4; ++b) dmma884d(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
         }
-        pending = (tk != 0.0);
-        if (!grid_sync(t.bar, t.err)) return;
+        __syncthreads();
     }
-    if (cta == 0 && tid == 0) {
-        if (n == 1) {
-            t.d[0] = A[0];
-            t.e[0] = 0.0;
-            t.tau[0] = 0.0;
-            t.scal[0] = 0.0;
-            return;
-        }
-        double a00 = A[(size_t)(n - 2) * ld + (n - 2)];
-        double a10 = A[(size_t)(n - 2) * ld + (n - 1)];
-        double a11 = A[(size_t)(n - 1) * ld + (n - 1)];
-        if (pending) {
-            a00 -= 2.0 * t.vp[n - 2] * t.wp[n - 2];
-            a10 -= t.vp[n - 1] * t.wp[n - 2] + t.wp[n - 1] * t.vp[n - 2];
-            a11 -= 2.0 * t.vp[n - 1] * t.wp[n - 1];
-        }
-        t.d[n - 2] = a00;
-        t.d[n - 1] = a11;
-        t.e[n - 2] = a10;
-        t.e[n - 1] = 0.0;
-        t.tau[n - 2] = 0.0;
-        t.tau[n - 1] = 0.0;
-        t.scal[n - 2] = 0.0;
-        t.scal[n - 1] = 0.0;
+    const int r = lane >> 2, c2 = (lane & 3) * 2;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i = i0 + wm + a * 8 + r, j = jj0 + wn + b * 8 + c2 + h;
+                if (i < n && j < n && i >= j) A[(size_t)j * ld + i] -= acc[a][b][h];
+            }
+}
+
+__global__ void dense_finish_kernel(const double *A, long long ld, int n, double *d, double *e, double *tau) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    if (n == 1) {
+        d[0] = A[0];
+        e[0] = 0.0;
+        tau[0] = 0.0;
+        return;
     }
+    d[n - 2] = A[(size_t)(n - 2) * ld + (n - 2)];
+    d[n - 1] = A[(size_t)(n - 1) * ld + (n - 1)];
+    e[n - 2] = A[(size_t)(n - 2) * ld + (n - 1)];
+    e[n - 1] = 0.0;
+    tau[n - 2] = 0.0;
+    tau[n - 1] = 0.0;
 }
 
 // Gershgorin bounds, pivmin, e^2 and ||T||_1 (one CTA).
@@ -275,7 +465,7 @@ __global__ void untangle_kernel(const double *X, int n, int nev, double *Z, long
 
 constexpr int kBtCols = 4;
 __global__ void backtransform_kernel(const double *A, long long lda, int n, const double *tau,
-                                     const double *scal, double *Z, long long ldz, int nev) {
+                                     double *Z, long long ldz, int nev) {
     const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const int lane = threadIdx.x & 31;
     const int c0 = gw * kBtCols;
@@ -284,11 +474,10 @@ __global__ void backtransform_kernel(const double *A, long long lda, int n, cons
     for (int k = n - 3; k >= 0; --k) {
         const double tk = tau[k];
         if (tk == 0.0) continue;
-        const double sk = scal[k];
         const double *col = A + (size_t)k * lda;
         double s[kBtCols] = {0.0, 0.0, 0.0, 0.0};
         for (int i = k + 1 + lane; i < n; i += 32) {
-            const double vi = (i == k + 1) ? 1.0 : col[i] * sk;
+            const double vi = (i == k + 1) ? 1.0 : col[i];
 #pragma unroll
             for (int c = 0; c < kBtCols; ++c)
                 if (c < nc) s[c] += vi * Z[(size_t)(c0 + c) * ldz + i];
@@ -296,7 +485,7 @@ __global__ void backtransform_kernel(const double *A, long long lda, int n, cons
 #pragma unroll
         for (int c = 0; c < kBtCols; ++c) s[c] = warp_sum(s[c]) * tk;
         for (int i = k + 1 + lane; i < n; i += 32) {
-            const double vi = (i == k + 1) ? 1.0 : col[i] * sk;
+            const double vi = (i == k + 1) ? 1.0 : col[i];
 #pragma unroll
             for (int c = 0; c < kBtCols; ++c)
                 if (c < nc) Z[(size_t)(c0 + c) * ldz + i] -= s[c] * vi;
@@ -309,18 +498,45 @@ __global__ void backtransform_kernel(const double *A, long long lda, int n, cons
 int dense_tridiag_grid(int device) {
     int nsm = 0, per = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dense_tridiag_kernel, kDtThreads, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dense_panel_kernel, kPnThreads, 0);
     if (per < 1) per = 1;
-    return nsm;  // one CTA per SM (co-resident by construction)
+    return nsm * std::min(per, 3);
 }
 
+int dense_panel_width() { return 32; }
+
 cudaError_t launch_dense_tridiag(DenseTri &t, int grid, cudaStream_t st) {
-    void *args[] = {&t};
-    return cudaLaunchCooperativeKernel((void *)dense_tridiag_kernel, dim3(grid), dim3(kDtThreads), args, 0, st);
+    const int n = t.n;
+    const int nb = t.nbmax;
+    int npanel = 0;
+    for (int j0 = 0; j0 + 2 < n; j0 += nb) {
+        t.j0 = j0;
+        t.nb = std::min(nb, n - 2 - j0);
+        void *args[] = {&t};
+        if (t.ev && 2 * npanel + 1 < t.nev) cudaEventRecord(t.ev[2 * npanel], st);
+        DVR3D_COUNT_LAUNCH(1);
+        cudaError_t e = cudaLaunchCooperativeKernel((void *)dense_panel_kernel, dim3(grid), dim3(kPnThreads), args, 0, st);
+        if (t.ev && 2 * npanel + 1 < t.nev) cudaEventRecord(t.ev[2 * npanel + 1], st);
+        ++npanel;
+        if (e != cudaSuccess) return e;
+        const int j1 = j0 + t.nb;
+        if (j1 < n) {
+            const long long nt = (n - j1 + 63) / 64;
+            DVR3D_COUNT_LAUNCH(1);
+            syr2k_lower_kernel<<<(unsigned)(nt * (nt + 1) / 2), 128, 0, st>>>(t.A, t.lda, n, j1, t.V, t.W, t.nb);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return e;
+        }
+    }
+    DVR3D_COUNT_LAUNCH(1);
+    dense_finish_kernel<<<1, 32, 0, st>>>(t.A, t.lda, n, t.d, t.e, t.tau);
+    t.npanel = npanel;
+    return cudaGetLastError();
 }
 
 void launch_dense_eigvals(const double *d, const double *e, int n, int nev, double *e2, double *info,
                           double *w, cudaStream_t st) {
+    DVR3D_COUNT_LAUNCH(2);
     tri_bounds_kernel<<<1, 256, 0, st>>>(d, e, n, e2, info);
     const int warps_per_block = 4;
     multisect_kernel<<<(nev + warps_per_block - 1) / warps_per_block, 32 * warps_per_block, 0, st>>>(
@@ -328,15 +544,16 @@ void launch_dense_eigvals(const double *d, const double *e, int n, int nev, doub
 }
 
 void launch_dense_eigvecs(const double *A, long long lda, int n, const double *d, const double *e,
-                          const double *tau, const double *scal, const double *w, int nev,
+                          const double *tau, const double *w, int nev,
                           const double *info, int *cstart, int *ncl, double *fac, int T, double *X,
                           double *Z, long long ldz, cudaStream_t st) {
+    DVR3D_COUNT_LAUNCH(4);
     clusters_kernel<<<1, 32, 0, st>>>(w, nev, info, cstart, ncl);
     invit_dense_kernel<<<(T + 63) / 64, 64, 0, st>>>(d, e, n, w, nev, cstart, ncl, info, fac, T, X);
     const long long tot = (long long)n * nev;
     untangle_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(X, n, nev, Z, ldz);
     const int nwarps = (nev + kBtCols - 1) / kBtCols;
-    backtransform_kernel<<<(nwarps + 3) / 4, 128, 0, st>>>(A, lda, n, tau, scal, Z, ldz, nev);
+    backtransform_kernel<<<(nwarps + 3) / 4, 128, 0, st>>>(A, lda, n, tau, Z, ldz, nev);
 }
 
 }  // namespace dvr3d

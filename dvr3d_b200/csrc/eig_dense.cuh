@@ -8,23 +8,32 @@
 namespace dvr3d {
 
 struct DenseTri {
-    double *A;          // n x n full symmetric (overwritten: reflectors below the subdiagonal)
-    long long lda;
+    double *A;          // n x n (lower triangle used), ld = lda (multiple of 8); reflector k
+    long long lda;      // is left in A[k+2:, k] (v_{k+1} = 1 implied)
     int n;
-    double *d, *e, *tau, *scal;   // [n]
-    double *vp, *wp, *pbuf;       // [n] pending rank-2 vectors and p
-    double *part;                 // [2 * grid] partial sums
+    double *d, *e, *tau;          // [n]
+    double *V, *W;                // n x nbmax panels (ld = n)
+    double *acol, *ybuf;          // [n]
+    double *P;                    // symmetric-product partial sums, NT * NT * 64
+    double *part;                 // [grid * (1 + 2 nbmax)]
+    int NT;                       // number of 64-row blocks covering n
+    int j0, nb, nbmax;            // current panel
     GridBarrier *bar;             // zeroed before launch
     int *err;
+    long long *prof;              // optional [6] phase clock accumulators (CTA 0), or null
+    cudaEvent_t *ev;              // optional event pool timing each panel launch (2 per panel)
+    int nev;
+    int npanel;                   // out: panel launches made
 };
 
 int dense_tridiag_grid(int device);
+int dense_panel_width();
 cudaError_t launch_dense_tridiag(DenseTri &t, int grid, cudaStream_t st);
 // info[0..3] = lower bound, upper bound, pivmin, ||T||
 void launch_dense_eigvals(const double *d, const double *e, int n, int nev, double *e2, double *info,
                           double *w, cudaStream_t st);
 void launch_dense_eigvecs(const double *A, long long lda, int n, const double *d, const double *e,
-                          const double *tau, const double *scal, const double *w, int nev,
+                          const double *tau, const double *w, int nev,
                           const double *info, int *cstart, int *ncl, double *fac, int T, double *X,
                           double *Z, long long ldz, cudaStream_t st);
 

@@ -190,6 +190,7 @@ void launch_assemble_h3(const AsmParams &p, cudaStream_t st) {
     const long long tiles = (long long)((p.n + BM - 1) / BM);
     const long long nblk = tiles * (tiles + 1) / 2;
     if (nblk == 0) return;
+    DVR3D_COUNT_LAUNCH(1);
     assemble_h3_kernel<<<(unsigned)nblk, kThreads, 0, st>>>(p);
 }
 
@@ -197,6 +198,7 @@ void launch_dgemm(bool ta, bool tb, int M, int N, int K, double alpha, const dou
                   const double *B, long long ldb, double beta, double *C, long long ldc, cudaStream_t st) {
     if (M <= 0 || N <= 0) return;
     dim3 grid((N + BN - 1) / BN, (M + BM - 1) / BM);
+    DVR3D_COUNT_LAUNCH(1);
     if (!ta && !tb) dgemm_kernel<false, false><<<grid, kThreads, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
     else if (ta && !tb) dgemm_kernel<true, false><<<grid, kThreads, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);
     else if (!ta && tb) dgemm_kernel<false, true><<<grid, kThreads, 0, st>>>(M, N, K, alpha, A, lda, B, ldb, beta, C, ldc);

@@ -7,6 +7,8 @@
 #include <algorithm>
 #include <chrono>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <numeric>
 
@@ -23,6 +25,12 @@
     } while (0)
 
 namespace dvr3d {
+
+long long g_kernel_launches = 0;
+
+namespace {
+thread_local long long t_h2d = 0, t_d2h = 0;
+}
 
 // ---------------------------------------------------------------- arena
 DeviceArena::~DeviceArena() { release_all(); }
@@ -64,6 +72,7 @@ template <class T>
 T *upload(dvr3d_ctx *ctx, const std::string &name, const std::vector<T> &v) {
     T *p = ctx->arena.get_t<T>(name, std::max<size_t>(v.size(), 1));
     if (!v.empty()) CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, ctx->stream));
+    t_h2d += (long long)(v.size() * sizeof(T));
     return p;
 }
 
@@ -71,6 +80,7 @@ template <class T>
 std::vector<T> download(dvr3d_ctx *ctx, const T *p, size_t n) {
     std::vector<T> v(n);
     if (n) CK(cudaMemcpyAsync(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
+    t_d2h += (long long)(n * sizeof(T));
     CK(cudaStreamSynchronize(ctx->stream));
     return v;
 }
@@ -80,6 +90,7 @@ inline long long round_up(long long x, long long m) { return (x + m - 1) / m * m
 void check_dev_err(dvr3d_ctx *ctx, const int *err_dev, const char *stage) {
     int e = 0;
     CK(cudaMemcpyAsync(&e, err_dev, sizeof(int), cudaMemcpyDeviceToHost, ctx->stream));
+    t_d2h += sizeof(int);
     CK(cudaStreamSynchronize(ctx->stream));
     if (e == kDevBarrierTimeout) throw HostError{DVR3D_ERR_NOCONV, std::string(stage) + ": grid barrier wait exceeded its limit"};
     if (e != 0) throw HostError{DVR3D_ERR_NOCONV, std::string(stage) + ": device error flag " + std::to_string(e)};
@@ -550,6 +561,12 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
     BlockPlan p;
     plan_block(deck, kk, p);
     auto th1 = std::chrono::steady_clock::now();
+    const long long launches0 = g_kernel_launches;
+    t_h2d = 0;
+    t_d2h = 0;
+    res.dom_ms = res.dom_bytes = res.dom_flops = 0.0;
+    res.dom_launches = 0;
+    std::memset(res.dom_kernel, 0, sizeof(res.dom_kernel));
     cudaStream_t st = ctx->stream;
     CK(cudaEventRecord(ctx->ev[0], st));
     Contracted C;
@@ -590,30 +607,57 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
     if (opt.want_h3 && res.h3) {
         if (res.h3_cap < (size_t)N * N) throw HostError{DVR3D_ERR_BUFFER, "h3 buffer too small"};
         CK(cudaMemcpyAsync(res.h3, H3, sizeof(double) * N * N, cudaMemcpyDeviceToHost, st));
+        t_d2h += (long long)sizeof(double) * N * N;
     }
     // ---- final eigensolve (diag3d), plain FP64 path
-    double *Hw = ctx->arena.get_t<double>("h3w", (size_t)N * N);
-    CK(cudaMemcpyAsync(Hw, H3, sizeof(double) * N * N, cudaMemcpyDeviceToDevice, st));
+    const long long ldw = round_up(N, 8);
+    double *Hw = ctx->arena.get_t<double>("h3w", (size_t)ldw * N);
+    CK(cudaMemcpy2DAsync(Hw, ldw * sizeof(double), H3, (size_t)N * sizeof(double), (size_t)N * sizeof(double), N,
+                         cudaMemcpyDeviceToDevice, st));
     DenseTri dt{};
     dt.A = Hw;
-    dt.lda = N;
+    dt.lda = ldw;
     dt.n = N;
     dt.d = ctx->arena.get_t<double>("dt_d", N);
     dt.e = ctx->arena.get_t<double>("dt_e", N);
     dt.tau = ctx->arena.get_t<double>("dt_tau", N);
-    dt.scal = ctx->arena.get_t<double>("dt_scal", N);
-    dt.vp = ctx->arena.get_t<double>("dt_vp", N);
-    dt.wp = ctx->arena.get_t<double>("dt_wp", N);
-    dt.pbuf = ctx->arena.get_t<double>("dt_p", N);
     const int G = ctx->dense_grid;
-    if ((long long)N > (long long)G * 256)
-        throw HostError{DVR3D_ERR_UNSUPPORTED, "final Hamiltonian larger than 256 rows per SM"};
-    dt.part = ctx->arena.get_t<double>("dt_part", 2 * (size_t)G);
+    if ((long long)N > 256LL * G) throw HostError{DVR3D_ERR_UNSUPPORTED, "final Hamiltonian too large for the dense path"};
+    dt.nbmax = dense_panel_width();
+    dt.NT = (N + 63) / 64;
+    dt.V = ctx->arena.get_t<double>("dt_V", (size_t)N * dt.nbmax);
+    dt.W = ctx->arena.get_t<double>("dt_W", (size_t)N * dt.nbmax);
+    dt.acol = ctx->arena.get_t<double>("dt_acol", N);
+    dt.ybuf = ctx->arena.get_t<double>("dt_y", N);
+    dt.P = ctx->arena.get_t<double>("dt_P", (size_t)dt.NT * dt.NT * 64);
+    dt.part = ctx->arena.get_t<double>("dt_part", (size_t)G * (1 + 2 * dt.nbmax));
     dt.bar = ctx->arena.get_t<GridBarrier>("dt_bar", 1);
     dt.err = ctx->arena.get_t<int>("dt_err", 1);
     CK(cudaMemsetAsync(dt.bar, 0, sizeof(GridBarrier), st));
     CK(cudaMemsetAsync(dt.err, 0, sizeof(int), st));
+    const char *prof_env = std::getenv("DVR3D_PROF");
+    const bool prof = prof_env && prof_env[0] == '1';
+    if (prof) {
+        dt.prof = ctx->arena.get_t<long long>("dt_prof", 8);
+        CK(cudaMemsetAsync(dt.prof, 0, 8 * sizeof(long long), st));
+    }
+    const int npan = (N + dt.nbmax - 1) / dt.nbmax + 1;
+    if ((int)ctx->panel_ev.size() < 2 * npan) {
+        const size_t old = ctx->panel_ev.size();
+        ctx->panel_ev.resize(2 * npan);
+        for (size_t q = old; q < ctx->panel_ev.size(); ++q) CK(cudaEventCreate(&ctx->panel_ev[q]));
+    }
+    dt.ev = ctx->panel_ev.data();
+    dt.nev = (int)ctx->panel_ev.size();
     CK(launch_dense_tridiag(dt, G, st));
+    if (prof) {
+        std::vector<long long> pc = download(ctx, dt.prof, 6);
+        int khz = 0;
+        cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, ctx->device);
+        std::fprintf(stderr, "dense reduction N=%d grid=%d phase ms (at %d MHz):", N, G, khz / 1000);
+        for (int q = 0; q < 6; ++q) std::fprintf(stderr, " %.2f", (double)pc[q] / (double)khz);
+        std::fprintf(stderr, "\n");
+    }
     double *e2s = ctx->arena.get_t<double>("dt_e2", N);
     double *info = ctx->arena.get_t<double>("dt_info", 4);
     double *wv = ctx->arena.get_t<double>("dt_w", meval);
@@ -628,17 +672,21 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
         Z = ctx->arena.get_t<double>("dv_z", (size_t)N * meval);
         int *cs = ctx->arena.get_t<int>("dv_cs", meval + 1);
         int *ncl = ctx->arena.get_t<int>("dv_ncl", 1);
-        launch_dense_eigvecs(Hw, N, N, dt.d, dt.e, dt.tau, dt.scal, wv, meval, info, cs, ncl, fac, T, X, Z, N, st);
+        launch_dense_eigvecs(Hw, ldw, N, dt.d, dt.e, dt.tau, wv, meval, info, cs, ncl, fac, T, X, Z, N, st);
         CK(cudaGetLastError());
     }
     CK(cudaEventRecord(ctx->ev[3], st));
     check_dev_err(ctx, dt.err, "final tridiagonal reduction");
-    if (res.eval) CK(cudaMemcpyAsync(res.eval, wv, sizeof(double) * meval, cudaMemcpyDeviceToHost, st));
+    if (res.eval) {
+        CK(cudaMemcpyAsync(res.eval, wv, sizeof(double) * meval, cudaMemcpyDeviceToHost, st));
+        t_d2h += (long long)sizeof(double) * meval;
+    }
     res.max_resid = -1.0;
     if (vecs && (res.resid || opt.want_vectors)) {
         double *R = ctx->arena.get_t<double>("dv_r", (size_t)N * meval);
         double *rn = ctx->arena.get_t<double>("dv_rn", meval);
         launch_dgemm(false, false, N, meval, N, 1.0, H3, N, Z, N, 0.0, R, N, st);
+        DVR3D_COUNT_LAUNCH(1);
         resid_kernel<<<meval, 256, 0, st>>>(R, Z, wv, N, N, meval, rn);
         CK(cudaGetLastError());
         std::vector<double> rv = download(ctx, rn, meval);
@@ -650,6 +698,7 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
     if (res.evec && Z) {
         if (res.evec_cap < (size_t)N * meval) throw HostError{DVR3D_ERR_BUFFER, "evec buffer too small"};
         CK(cudaMemcpyAsync(res.evec, Z, sizeof(double) * N * meval, cudaMemcpyDeviceToHost, st));
+        t_d2h += (long long)sizeof(double) * N * meval;
     }
     CK(cudaStreamSynchronize(st));
     float ms1 = 0, ms2 = 0, ms3 = 0;
@@ -662,6 +711,27 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
     res.stage_ms[3] = ms3;
     res.stage_ms[4] = ms1 + ms2 + ms3;
     res.stage_ms[5] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - th0).count();
+    // dominant kernel: the panel kernel of the Householder reduction; its algorithmic
+    // traffic is one read of the trailing lower triangle per column
+    double pms = 0.0;
+    for (int q = 0; q < dt.npanel && 2 * q + 1 < dt.nev; ++q) {
+        float m = 0.f;
+        CK(cudaEventElapsedTime(&m, ctx->panel_ev[2 * q], ctx->panel_ev[2 * q + 1]));
+        pms += m;
+    }
+    double bytes = 0.0;
+    for (int k = 0; k + 2 < N; ++k) {
+        const double m = (double)(N - k - 1);
+        bytes += 8.0 * m * (m + 1.0) * 0.5;
+    }
+    res.dom_ms = pms;
+    res.dom_bytes = bytes;
+    res.dom_flops = 0.0;
+    res.dom_launches = dt.npanel;
+    std::snprintf(res.dom_kernel, sizeof(res.dom_kernel), "dense_panel_kernel");
+    res.launches = (int)(g_kernel_launches - launches0);
+    res.h2d_bytes = t_h2d;
+    res.d2h_bytes = t_d2h;
 }
 
 }  // namespace dvr3d

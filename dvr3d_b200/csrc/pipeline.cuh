@@ -43,8 +43,8 @@ struct CudaFail {
 
 struct dvr3d_ctx {
     int device = 0;
-    cudaStream_t stream = nullptr;
-    bool own_stream = false;
+    cudaStream_t stream = nullptr;     // stream all work of this context is issued on
+    cudaStream_t own_stream = nullptr; // the stream the context created (destroyed with it)
     std::string last_error;
     dvr3d::PesParams pes{};
     std::vector<double> pes_grid;  // host copy of a tabulated PES
@@ -52,6 +52,7 @@ struct dvr3d_ctx {
     cudaEvent_t ev[8] = {};
     int sm_count = 0;
     int dense_grid = 0;
+    std::vector<cudaEvent_t> panel_ev;  // timing pool for the reduction panels
 };
 
 namespace dvr3d {

@@ -119,6 +119,15 @@ typedef struct dvr3d_result {
     double stage_ms[6];     /* device time: 0 set-up, 1 block builds+eigensolves+selection,
                                2 assembly, 3 final eigensolve, 4 total, 5 host set-up       */
     double max_resid;       /* max FP64 residual ||H x - e x|| over returned levels (Eh)    */
+    /* measurement counters of this solve (CUDA events on the context's stream) */
+    double dom_ms;          /* device time of the dominant kernel's launches                */
+    double dom_bytes;       /* algorithmic bytes those launches must move (or flops, below) */
+    double dom_flops;       /* algorithmic flops of those launches (0 if bandwidth-bound)   */
+    int dom_launches;       /* number of launches of the dominant kernel                    */
+    int launches;           /* kernels launched by the library for this solve               */
+    long long h2d_bytes;    /* host -> device bytes copied by this solve                    */
+    long long d2h_bytes;    /* device -> host bytes copied by this solve                    */
+    char dom_kernel[48];    /* name of the dominant kernel                                  */
     /* caller-provided buffers (may be NULL / 0) */
     double *eval;   int eval_cap;     /* levels (Eh), ascending                               */
     int *iv2;       int iv2_cap;      /* per-block selection counts (blocks in solve order)   */

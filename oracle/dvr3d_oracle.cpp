@@ -901,6 +901,17 @@ void nfmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     }
     int nham3 = iv2a[nalf - 1] + iv2b[nalf - 1] - 1;  // :3092
     auto t1 = std::chrono::steady_clock::now();
+    if (final_mode == 3) {
+        if (tr) {
+            tr->nblocks = nalf;
+            tr->nham3 = nham3;
+            if (tr->iv2 && tr->iv2_cap >= nalf)
+                for (int i = 0; i < nalf; ++i) tr->iv2[i] = iv2b[i];
+            tr->stage_s[0] = std::chrono::duration<double>(t1 - t0).count();
+        }
+        if (res) res->nham3 = nham3;
+        return;
+    }
     // bloc3d :3455-3505
     std::vector<double> ham3((size_t)nham3 * nham3, 0.0);
     auto V = [&](int col) { return &vecs2d[(size_t)col * nham2]; };
@@ -1171,6 +1182,21 @@ void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     }
     int nham3 = low3d;
     auto t1 = std::chrono::steady_clock::now();
+    if (final_mode == 3) {
+        if (tr) {
+            tr->nblocks = npntc;
+            tr->nham3 = nham3;
+            if (tr->iv1 && tr->iv1_cap >= npntc * npntb)
+                std::memcpy(tr->iv1, iv1.data(), sizeof(int) * npntc * npntb);
+            if (tr->iv2 && tr->iv2_cap >= npntc)
+                for (int i = 0; i < npntc; ++i) tr->iv2[i] = iv2[i];
+            if (tr->n2d && tr->n2d_cap >= npntc)
+                for (int i = 0; i < npntc; ++i) tr->n2d[i] = ndim2d[i];
+            tr->stage_s[0] = std::chrono::duration<double>(t1 - t0).count();
+        }
+        if (res) res->nham3 = nham3;
+        return;
+    }
     // mkham3 :2301-2552, first part: cint per block (P x iv2), P = npnta*npntb
     int ncint = npnta * npntb;
     std::vector<std::vector<double>> cint(npntc);

@@ -52,7 +52,8 @@ typedef struct oracle_trace {
 
 /* final_mode: 0 = dsyev('V','L') with lwork = 3*N as diag() does (:2650-2654);
  *             1 = dsyevd (the divide-and-conquer variant kept commented in :2612-2636);
- *             2 = stop after assembly (no final diagonalisation). */
+ *             2 = stop after assembly (no final diagonalisation);
+ *             3 = stop after the 2D selection (sizes and counts only). */
 int oracle_solve_block(const dvr3d_deck *deck, int kk, int pes_kind, const double *pes,
                        int npes, const double *vgrid, size_t nvgrid, int final_mode,
                        oracle_trace *trace, dvr3d_result *res);
