@@ -31,6 +31,8 @@ DVR3D_ERR_PES = -10
 DVR3D_ERR_DECK = -11
 DVR3D_ERR_NO_DEVICE = -12
 DVR3D_ERR_BUFFER = -13
+DVR3D_ERR_SCRATCH = -14
+DVR3D_NOALLOC_SCRATCH_BYTES = 64 * 1024 * 1024
 
 DVR3D_PES_NONE = 0
 DVR3D_PES_MORSE_SUM = 1
@@ -127,6 +129,8 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
                                           P(C.c_size_t)]),
         "dvr3d_b200_diag_batched": (C.c_int, [vp, C.c_int, P(C.c_int), P(C.c_longlong),
                                               P(C.c_longlong), vp, vp, C.c_int]),
+        "dvr3d_b200_diag_batched_noalloc": (C.c_int, [vp, C.c_int, P(C.c_int), P(C.c_longlong),
+                                                      P(C.c_longlong), vp, vp, C.c_int]),
     }
     for name, (res, args) in sig.items():
         if hasattr(lib, name):

@@ -99,6 +99,7 @@ const char *dvr3d_b200_strerror(int code) {
     case DVR3D_ERR_DECK: return "job deck could not be parsed";
     case DVR3D_ERR_NO_DEVICE: return "no usable CUDA device";
     case DVR3D_ERR_BUFFER: return "caller buffer too small";
+    case DVR3D_ERR_SCRATCH: return "request exceeds the 64 MiB fixed scratch of dvr3d_b200_diag_batched_noalloc";
     default: return "unknown error";
     }
 }
@@ -281,8 +282,7 @@ int dvr3d_b200_diag_batched(dvr3d_ctx *ctx, int nblk, const int *n_host, const l
         std::vector<int> dummy;
         (void)dummy;
         dvr3d::BatchDesc bdc{nblk, bd.n, up("dg_asz", asz), bd.voff};
-        extern void dvr3d_symmetrize_lower(const dvr3d::BatchDesc &, double *, int, cudaStream_t);
-        dvr3d_symmetrize_lower(bdc, ac, nmax, st);
+        dvr3d::launch_symmetrize_lower(bdc, ac, nmax, st);
         dvr3d::launch_tridiag_batched(bdc, ac, d, e, tau, nmax, st);
         dvr3d::launch_eigvals_batched(bdc, d, e, w, cnt, 0, 0.0, st);
         for (int b = 0; b < nblk; ++b)
@@ -388,21 +388,3 @@ int dvr3d_b200_run_deck(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_optio
 }
 
 }  // extern "C"
-
-// mirror the lower triangle of each block into the upper one (dsyev('V','L') semantics)
-namespace {
-__global__ void symmetrize_lower_kernel(dvr3d::BatchDesc bd, double *A) {
-    const int b = blockIdx.y;
-    const int n = bd.n[b];
-    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= (long long)n * n) return;
-    const int i = (int)(idx % n), j = (int)(idx / n);
-    if (j > i) A[bd.aoff[b] + idx] = A[bd.aoff[b] + (long long)i * n + j];
-}
-}  // namespace
-
-void dvr3d_symmetrize_lower(const dvr3d::BatchDesc &bd, double *A, int nmax, cudaStream_t st) {
-    dim3 grid((unsigned)(((long long)nmax * nmax + 255) / 256), bd.nblk);
-    DVR3D_COUNT_LAUNCH(1);
-    symmetrize_lower_kernel<<<grid, 256, 0, st>>>(bd, A);
-}

@@ -293,7 +293,22 @@ __global__ void __launch_bounds__(kVecThreads) eigvecs_kernel(BatchDesc bd, cons
     (void)err;
 }
 
+__global__ void symmetrize_lower_kernel(BatchDesc bd, double *A) {
+    const int b = blockIdx.y;
+    const int n = bd.n[b];
+    const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= (long long)n * n) return;
+    const int i = (int)(idx % n), j = (int)(idx / n);
+    if (j > i) A[bd.aoff[b] + idx] = A[bd.aoff[b] + (long long)i * n + j];
+}
+
 }  // namespace
+
+void launch_symmetrize_lower(const BatchDesc &bd, double *A, int nmax, cudaStream_t st) {
+    dim3 grid((unsigned)(((long long)nmax * nmax + 255) / 256), bd.nblk);
+    DVR3D_COUNT_LAUNCH(1);
+    symmetrize_lower_kernel<<<grid, 256, 0, st>>>(bd, A);
+}
 
 void launch_tridiag_batched(const BatchDesc &bd, double *A, double *d, double *e, double *tau,
                             int nmax, cudaStream_t st) {

@@ -22,6 +22,10 @@ struct BatchDesc {
     const long long *voff;   // [nblk] offset of block b in the n-length arrays d, e, tau, w
 };
 
+// Mirror the lower triangle of every block into its upper triangle (the reference's
+// dsyev('V','L') reads only the lower triangle; the kernels here use full storage).
+void launch_symmetrize_lower(const BatchDesc &bd, double *A, int nmax, cudaStream_t st);
+
 // Tridiagonalise all blocks (A overwritten by the reflectors, lower part). Full symmetric
 // storage is required on input.
 void launch_tridiag_batched(const BatchDesc &bd, double *A, double *d, double *e, double *tau,

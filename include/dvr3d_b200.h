@@ -43,7 +43,9 @@ enum dvr3d_status {
     DVR3D_ERR_PES = -10,         /* potential returned a non-finite value                 */
     DVR3D_ERR_DECK = -11,        /* job deck could not be parsed                          */
     DVR3D_ERR_NO_DEVICE = -12,   /* no CUDA device / extension not usable                 */
-    DVR3D_ERR_BUFFER = -13       /* caller buffer too small                               */
+    DVR3D_ERR_BUFFER = -13,      /* caller buffer too small                               */
+    DVR3D_ERR_SCRATCH = -14      /* request larger than the fixed scratch of the
+                                    allocation-free entry point                          */
 };
 
 typedef struct dvr3d_ctx dvr3d_ctx;
@@ -194,6 +196,24 @@ int dvr3d_b200_run_deck(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_optio
 int dvr3d_b200_diag_batched(dvr3d_ctx *ctx, int nblk, const int *n_host,
                             const long long *off_host, const long long *woff_host,
                             double *a_dev, double *w_dev, int vecs);
+
+/* ---- allocation-free variant ---------------------------------------------------------- */
+/* No counterpart in the reference. Same computation and arguments as
+ * dvr3d_b200_diag_batched, for callers that must not allocate device memory (a host whose
+ * framework's memory pool owns the GPU memory and forbids outside cudaMalloc, or a latency-
+ * critical loop where cudaMalloc/cudaFree and their device-wide synchronisation must not
+ * happen). No context is needed: the work runs on `stream` (a cudaStream_t, 0 = default
+ * stream) of the current device, and all scratch comes from one array of
+ * DVR3D_NOALLOC_SCRATCH_BYTES compiled into the library, held by every GPU that loads it.
+ * Limit: requests needing more scratch than that -- about 8*(4n + 2n^2 + 5n*min(n,128)) bytes
+ * summed over the blocks with vecs != 0 -- return DVR3D_ERR_SCRATCH; split them into several
+ * calls. The first call on a device looks the array up (do it before any stream capture on
+ * that device). All calls share the array: calls that may overlap on the GPU race and must
+ * be serialised by the caller. Synchronises `stream` before returning. */
+#define DVR3D_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)
+int dvr3d_b200_diag_batched_noalloc(void *stream, int nblk, const int *n_host,
+                                    const long long *off_host, const long long *woff_host,
+                                    double *a_dev, double *w_dev, int vecs);
 
 #ifdef __cplusplus
 }
