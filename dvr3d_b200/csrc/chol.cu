@@ -1,0 +1,262 @@
+// chol.cu -- FP64 Cholesky factorisation fused with the triangular inverse, recursive, on
+// the DMMA GEMM (gemm_pipe.cu).
+//
+// For A = [[A11, .], [A21, A22]] (n1 + n2 rows, n1 a multiple of 64):
+//   (1) recurse on A11                      -> inv(L11) in place
+//   (2) L21 = A21 inv(L11)^T                 (GEMM, triangular second operand) -> scratch
+//   (3) A22 <- A22 - L21 L21^T               (GEMM, lower tiles only)
+//   (4) recurse on A22                      -> inv(L22) in place
+//   (5) A21 <- -inv(L22) L21 inv(L11)        (two triangular GEMMs)
+// so that on exit the lower triangle holds inv(L) with L L^T = A (the factor itself is never
+// needed by the shift-invert solver). Leaves (<= 64) are factored and inverted by one CTA in
+// shared memory. Work: n^3/3 (factorisation) + n^3/3 (inverse) flop, the top levels as a few
+// large GEMMs instead of one thin GEMM per 64-column panel.
+#include <cmath>
+
+#include "chol.cuh"
+#include "common.cuh"
+#include "gemm64.cuh"
+
+namespace dvr3d {
+
+namespace {
+
+constexpr int NB = kCholNb;
+constexpr int kLeafThreads = 256;
+constexpr size_t kLeafSmem = 2 * NB * (NB + 1) * sizeof(double);
+
+__global__ void shift_copy_lower_kernel(const double *H, long long ldh, int n, double sigma, double *A,
+                                        long long lda) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)n * lda) return;
+    const int j = (int)(t / lda), i = (int)(t % lda);
+    if (i >= n) return;
+    double v = 0.0;
+    if (i >= j) v = H[(size_t)j * ldh + i] - (i == j ? sigma : 0.0);
+    A[(size_t)j * lda + i] = v;
+}
+
+// Cholesky of the nb x nb block at (j0, j0) (nb <= 64, lower triangle read) and inverse of
+// its factor. inv_out null: the factor goes back into A and its inverse into... nowhere;
+// inv_out given: inverse written there (ld 64, zeros above); in_place_inv: the inverse
+// replaces the block's lower triangle in A.
+__global__ void __launch_bounds__(kLeafThreads) potrf_leaf_kernel(double *A, long long lda, int j0, int nb,
+                                                                  double *inv_out, int in_place_inv, double rel_tol,
+                                                                  int *err) {
+    if (*(volatile int *)err != 0) return;
+    extern __shared__ double sm[];
+    double(*L)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
+    double(*X)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm + NB * (NB + 1));
+    __shared__ int s_bad;
+    __shared__ double s_thr;
+    const int tid = threadIdx.x;
+    const int ti = tid & (NB - 1), tj0 = tid >> 6;  // this thread owns rows ti, columns tj0 + 4u
+    for (int u = 0; u < NB / 4; ++u) {
+        const int j = tj0 + 4 * u;
+        double v = 0.0;
+        if (ti < nb && j < nb && ti >= j) v = A[(size_t)(j0 + j) * lda + j0 + ti];
+        L[ti][j] = v;
+        X[ti][j] = (ti == j) ? 1.0 : 0.0;
+    }
+    if (tid == 0) {
+        s_bad = 0;
+        double mx = 0.0;
+        for (int i = 0; i < nb; ++i) mx = fmax(mx, A[(size_t)(j0 + i) * lda + j0 + i]);
+        s_thr = rel_tol * mx;
+    }
+    __syncthreads();
+    // right-looking factorisation
+    for (int k = 0; k < nb; ++k) {
+        if (tid == 0) {
+            const double d = L[k][k];
+            if (!(d > s_thr) || !isfinite(d)) s_bad = 1;
+            else L[k][k] = sqrt(d);
+        }
+        __syncthreads();
+        if (s_bad) break;
+        if (tid > k && tid < nb) L[tid][k] /= L[k][k];
+        __syncthreads();
+        const double lik = L[ti][k];
+        for (int u = 0; u < NB / 4; ++u) {
+            const int j = tj0 + 4 * u;
+            if (j > k && ti >= j && ti < nb) L[ti][j] -= lik * L[j][k];
+        }
+        __syncthreads();
+    }
+    if (s_bad) {
+        if (tid == 0) atomicExch(err, (int)kDevNotPosDef);
+        return;
+    }
+    // X = inv(L), right-looking forward substitution on the identity
+    for (int k = 0; k < nb; ++k) {
+        const double dk = L[k][k];
+        if (tid <= k) X[k][tid] /= dk;
+        __syncthreads();
+        const double lik = (ti > k && ti < nb) ? L[ti][k] : 0.0;
+        for (int u = 0; u < NB / 4; ++u) {
+            const int c = tj0 + 4 * u;
+            if (lik != 0.0 && c <= k) X[ti][c] -= lik * X[k][c];
+        }
+        __syncthreads();
+    }
+    for (int u = 0; u < NB / 4; ++u) {
+        const int j = tj0 + 4 * u;
+        if (ti < nb && j < nb && ti >= j) A[(size_t)(j0 + j) * lda + j0 + ti] = in_place_inv ? X[ti][j] : L[ti][j];
+        if (inv_out) inv_out[(size_t)j * NB + ti] = (ti < nb && j < nb && ti >= j) ? X[ti][j] : 0.0;
+    }
+}
+
+cudaError_t leaf(double *A, long long lda, int j0, int nb, double *inv_out, int in_place, double rel_tol, int *err,
+                 cudaStream_t st) {
+    static bool attr = false;
+    if (!attr) {
+        const cudaError_t e =
+            cudaFuncSetAttribute(potrf_leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLeafSmem);
+        if (e != cudaSuccess) return e;
+        attr = true;
+    }
+    DVR3D_COUNT_LAUNCH(1);
+    potrf_leaf_kernel<<<1, kLeafThreads, kLeafSmem, st>>>(A, lda, j0, nb, inv_out, in_place, rel_tol, err);
+    return cudaGetLastError();
+}
+
+__global__ void copy_block_kernel(const double *S, long long lds, double *D, long long ldd, int m, int n) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)m * n) return;
+    const int j = (int)(t / m), i = (int)(t % m);
+    D[(size_t)j * ldd + i] = S[(size_t)j * lds + i];
+}
+
+constexpr size_t kSplitWork = (size_t)4 << 20;  // doubles of split-K scratch
+
+int split_of(int M, int N, int K, bool lower) {
+    const long long tm = (M + 63) / 64, tn = (N + 63) / 64;
+    const long long tiles = lower ? tm * (tm + 1) / 2 : tm * tn;
+    if (tiles >= 296) return 1;
+    long long s = (600 + tiles - 1) / tiles;
+    s = std::min<long long>(s, 16);
+    s = std::min<long long>(s, (K + 63) / 64);
+    s = std::min<long long>(s, (long long)(kSplitWork / ((size_t)M * N + 1)));
+    return (int)std::max<long long>(s, 1);
+}
+
+struct Rec {
+    double *A;
+    long long lda;
+    double *stack;     // scratch for L21 blocks, used depth-first
+    double *work;      // split-K scratch
+    int *err;
+    cudaStream_t st;
+
+    cudaError_t gemm(GemmOp g) {
+        g.splitk = split_of(g.M, g.N, g.K, g.lower_out != 0);
+        g.work = work;
+        return launch_gemm(g, st);
+    }
+
+    cudaError_t run(int off, int n, double *sp) {
+        cudaError_t e;
+        if (n <= NB) return leaf(A, lda, off, n, nullptr, 1, 0.0, err, st);
+        int n1 = ((n / 2 + NB - 1) / NB) * NB;
+        if (n1 >= n) n1 = n - NB;
+        const int n2 = n - n1;
+        double *A11 = A + (size_t)off * lda + off;
+        double *A21 = A11 + n1;
+        double *A22 = A + (size_t)(off + n1) * lda + off + n1;
+        const long long ldt = (n2 + 7) / 8 * 8;
+        double *L21 = sp;
+        if ((e = run(off, n1, sp)) != cudaSuccess) return e;
+        GemmOp a;  // L21 = A21 inv(L11)^T
+        a.M = n2;
+        a.N = n1;
+        a.K = n1;
+        a.A = A21;
+        a.lda = lda;
+        a.B = A11;
+        a.ldb = lda;
+        a.tb = true;
+        a.tri_b = 2;
+        a.C = L21;
+        a.ldc = ldt;
+        if ((e = gemm(a)) != cudaSuccess) return e;
+        GemmOp s;  // A22 -= L21 L21^T
+        s.M = n2;
+        s.N = n2;
+        s.K = n1;
+        s.alpha = -1.0;
+        s.beta = 1.0;
+        s.A = L21;
+        s.lda = ldt;
+        s.B = L21;
+        s.ldb = ldt;
+        s.tb = true;
+        s.C = A22;
+        s.ldc = lda;
+        s.lower_out = 1;
+        if ((e = gemm(s)) != cudaSuccess) return e;
+        if ((e = run(off + n1, n2, sp + (size_t)ldt * n1)) != cudaSuccess) return e;
+        GemmOp z;  // A21 <- inv(L22) L21
+        z.M = n2;
+        z.N = n1;
+        z.K = n2;
+        z.A = A22;
+        z.lda = lda;
+        z.tri = 1;
+        z.B = L21;
+        z.ldb = ldt;
+        z.C = A21;
+        z.ldc = lda;
+        if ((e = gemm(z)) != cudaSuccess) return e;
+        GemmOp c;  // L21 <- -A21 inv(L11), then back into A21
+        c.M = n2;
+        c.N = n1;
+        c.K = n1;
+        c.alpha = -1.0;
+        c.A = A21;
+        c.lda = lda;
+        c.B = A11;
+        c.ldb = lda;
+        c.tri_b = 1;
+        c.C = L21;
+        c.ldc = ldt;
+        if ((e = gemm(c)) != cudaSuccess) return e;
+        DVR3D_COUNT_LAUNCH(1);
+        copy_block_kernel<<<(unsigned)(((long long)n2 * n1 + 255) / 256), 256, 0, st>>>(L21, ldt, A21, lda, n2, n1);
+        return cudaGetLastError();
+    }
+};
+
+size_t stack_need(int n) {
+    if (n <= NB) return 0;
+    int n1 = ((n / 2 + NB - 1) / NB) * NB;
+    if (n1 >= n) n1 = n - NB;
+    const int n2 = n - n1;
+    const size_t mine = (size_t)((n2 + 7) / 8 * 8) * n1;
+    return std::max(stack_need(n1), mine + stack_need(n2));
+}
+
+}  // namespace
+
+size_t chol_work_doubles(int n) { return stack_need(n) + kSplitWork + 64; }
+
+cudaError_t launch_shift_copy_lower(const double *H, long long ldh, int n, double sigma, double *A, long long lda,
+                                    cudaStream_t st) {
+    const long long tot = (long long)n * lda;
+    DVR3D_COUNT_LAUNCH(1);
+    shift_copy_lower_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(H, ldh, n, sigma, A, lda);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_potrf_inv_lower(double *A, long long lda, int n, double *work, int *err, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    if (lda & 1) return cudaErrorInvalidValue;
+    Rec r{A, lda, work + kSplitWork + 64, work, err, st};
+    return r.run(0, n, r.stack);
+}
+
+cudaError_t launch_chol_small(double *G, int b, double *ginv, double rel_tol, int *err, cudaStream_t st) {
+    if (b > NB) return cudaErrorInvalidValue;
+    return leaf(G, b, 0, b, ginv, 0, rel_tol, err, st);
+}
+
+}  // namespace dvr3d

@@ -18,7 +18,8 @@ enum DeviceErr : int {
     kDevBarrierTimeout = 1,   // a grid barrier wait ran past its iteration limit
     kDevNoConv = 2,           // an iterative device solver hit its iteration limit
     kDevBadPes = 3,           // non-finite potential value
-    kDevOverflow = 4          // a selection exceeded the caller's MAX2D / MAX3D
+    kDevOverflow = 4,         // a selection exceeded the caller's MAX2D / MAX3D
+    kDevNotPosDef = 5         // a Cholesky pivot was not positive
 };
 
 __device__ __forceinline__ double warp_sum(double v) {

@@ -17,6 +17,7 @@
 
 #include "common.cuh"
 #include "eig_dense.cuh"
+#include "gemm64.cuh"
 #include "tridiag_dev.cuh"
 
 namespace dvr3d {
@@ -493,7 +494,243 @@ __global__ void backtransform_kernel(const double *A, long long lda, int n, cons
     }
 }
 
+// ---- eigenvectors of T by inverse iteration with the factors in shared memory
+// One warp per cluster (1 warp per CTA). The recurrences (LU with partial pivoting of
+// T - lambda I, forward and backward solves) run on lane 0 from shared memory; scaling,
+// Gram-Schmidt inside the cluster and normalisation use the whole warp. Same steps as
+// invit_cluster (dstein manner), written straight into column-major Z.
+__global__ void __launch_bounds__(32) invit_smem_kernel(const double *d, const double *e, int n, const double *w,
+                                                        const int *cstart, const int *ncl, const double *info,
+                                                        double *Z, long long ldz) {
+    extern __shared__ double sm[];
+    double *D = sm, *E1 = D + n, *E2 = E1 + n, *Lm = E2 + n, *x = Lm + n;
+    unsigned char *P = reinterpret_cast<unsigned char *>(x + n);
+    const int lane = threadIdx.x;
+    const int nc = *ncl;
+    const double onenrm = info[3];
+    const double eps = DBL_EPSILON, tiny = eps * onenrm, pertol = 10.0 * eps * onenrm;
+    for (int c = blockIdx.x; c < nc; c += gridDim.x) {
+        const int j0 = cstart[c], j1 = cstart[c + 1];
+        double lamprev = 0.0;
+        for (int j = j0; j < j1; ++j) {
+            double lam = w[j];
+            if (j > j0 && lam - lamprev < pertol) lam = lamprev + pertol;
+            lamprev = lam;
+            if (lane == 0) {
+                double av = d[0] - lam, bv = (n > 1) ? e[0] : 0.0;
+                for (int i = 0; i < n - 1; ++i) {
+                    const double cc = e[i];
+                    const double an = d[i + 1] - lam, bn = (i + 2 < n) ? e[i + 1] : 0.0;
+                    if (fabs(av) >= fabs(cc)) {
+                        if (av == 0.0) av = tiny;
+                        const double mlt = cc / av;
+                        P[i] = 0;
+                        Lm[i] = mlt;
+                        D[i] = av;
+                        E1[i] = bv;
+                        E2[i] = 0.0;
+                        av = an - mlt * bv;
+                        bv = bn;
+                    } else {
+                        const double mlt = av / cc;
+                        P[i] = 1;
+                        Lm[i] = mlt;
+                        D[i] = cc;
+                        E1[i] = an;
+                        E2[i] = bn;
+                        av = bv - mlt * an;
+                        bv = -mlt * bn;
+                    }
+                }
+                if (fabs(av) < tiny) av = (av < 0.0) ? -tiny : tiny;
+                D[n - 1] = av;
+            }
+            __syncwarp();
+            for (int i = lane; i < n - 1; i += 32)
+                if (fabs(D[i]) < tiny) D[i] = (D[i] < 0.0) ? -tiny : tiny;
+            for (int i = lane; i < n; i += 32) {
+                const unsigned h = hash32((unsigned)(i * 2654435761u) ^ (unsigned)(j * 40503u + 17u));
+                x[i] = ((double)(h & 0xffffff) / 8388608.0) - 1.0;
+            }
+            __syncwarp();
+            for (int it = 0; it < 4; ++it) {
+                double s1 = 0.0;
+                for (int i = lane; i < n; i += 32) s1 += fabs(x[i]);
+                s1 = warp_sum(s1);
+                const double sc = (double)n * onenrm * fmax(eps, fabs(D[n - 1])) / fmax(s1, DBL_MIN);
+                for (int i = lane; i < n; i += 32) x[i] *= sc;
+                __syncwarp();
+                if (lane == 0) {
+                    for (int i = 0; i < n - 1; ++i) {
+                        double yi = x[i], yn = x[i + 1];
+                        if (P[i]) {
+                            const double tmp = yi;
+                            yi = yn;
+                            yn = tmp;
+                            x[i] = yi;
+                        }
+                        x[i + 1] = yn - Lm[i] * yi;
+                    }
+                    double x1 = 0.0, x2 = 0.0;
+                    for (int i = n - 1; i >= 0; --i) {
+                        const double xi = (x[i] - E1[i] * x1 - E2[i] * x2) / D[i];
+                        x[i] = xi;
+                        x2 = x1;
+                        x1 = xi;
+                    }
+                }
+                __syncwarp();
+                for (int jj = j0; jj < j; ++jj) {
+                    const double *zc = Z + (size_t)jj * ldz;
+                    double dot = 0.0;
+                    for (int i = lane; i < n; i += 32) dot += x[i] * zc[i];
+                    dot = warp_sum(dot);
+                    for (int i = lane; i < n; i += 32) x[i] -= dot * zc[i];
+                }
+                double nrm = 0.0;
+                for (int i = lane; i < n; i += 32) nrm += x[i] * x[i];
+                nrm = sqrt(warp_sum(nrm));
+                const double inv = (nrm > 0.0) ? 1.0 / nrm : 0.0;
+                for (int i = lane; i < n; i += 32) x[i] *= inv;
+                __syncwarp();
+            }
+            // sign convention: the first largest component positive
+            double big = 0.0;
+            int bi = n;
+            for (int i = lane; i < n; i += 32)
+                if (fabs(x[i]) > fabs(big)) {
+                    big = x[i];
+                    bi = i;
+                }
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ob = __shfl_xor_sync(0xffffffffu, big, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (fabs(ob) > fabs(big) || (fabs(ob) == fabs(big) && oi < bi)) {
+                    big = ob;
+                    bi = oi;
+                }
+            }
+            const double sg = (big < 0.0) ? -1.0 : 1.0;
+            double *zc = Z + (size_t)j * ldz;
+            for (int i = lane; i < n; i += 32) zc[i] = sg * x[i];
+            __syncwarp();
+        }
+    }
+}
+
+// ---- blocked back-transformation Z <- H_0 H_1 ... H_{n-3} Z (compact WY, as dormtr)
+// V panel (rows p0..n-1, nbk columns): column c is reflector p0+c, zero above row p0+c+1,
+// one at row p0+c+1, A[r, p0+c] below.
+__global__ void build_v_kernel(const double *A, long long lda, int n, int p0, int nbk, double *V, long long ldv) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const int R = n - p0;
+    if (t >= (long long)R * nbk) return;
+    const int c = (int)(t / R), i = (int)(t % R);
+    const int r = p0 + i, top = p0 + c + 1;
+    V[(size_t)c * ldv + i] = (r < top) ? 0.0 : (r == top ? 1.0 : A[(size_t)(p0 + c) * lda + r]);
+}
+
+// Tm (upper, ld 32) of the block reflector I - V Tm V^T from S = V^T V (ld 32) and tau (dlarft,
+// forward, columnwise).
+__global__ void larft_kernel(const double *S, const double *tau, int nbk, double *Tm) {
+    __shared__ double t[32][33];
+    const int r = threadIdx.x;
+    for (int c = 0; c < 32; ++c) t[r][c] = 0.0;
+    __syncwarp();
+    for (int i = 0; i < nbk; ++i) {
+        const double ti = tau[i];
+        if (r < i) {
+            double s = 0.0;
+            for (int c = r; c < i; ++c) s += t[r][c] * S[i * 32 + c];
+            t[r][i] = -ti * s;
+        } else if (r == i) {
+            t[i][i] = ti;
+        }
+        __syncwarp();
+    }
+    for (int c = 0; c < 32; ++c) Tm[c * 32 + r] = t[r][c];
+}
+
 }  // namespace
+
+size_t dense_bt_work_doubles(int n, int nev) {
+    const long long ldv = (n + 7) / 8 * 8;
+    return (size_t)ldv * 32 + 2 * 32 * 32 + 2 * (size_t)32 * nev + (size_t)64 * 32 * nev + 64;
+}
+
+cudaError_t launch_dense_backtransform(const double *A, long long lda, int n, const double *tau, double *Z,
+                                       long long ldz, int nev, double *work, cudaStream_t st) {
+    if (n < 3 || nev <= 0) return cudaSuccess;
+    if (ldz & 1) return cudaErrorInvalidValue;
+    const long long ldv = (n + 7) / 8 * 8;
+    double *V = work, *S = V + ldv * 32, *Tm = S + 32 * 32, *W = Tm + 32 * 32, *W2 = W + (size_t)32 * nev;
+    double *sk = W2 + (size_t)32 * nev;
+    cudaError_t e;
+    const int nref = n - 2;
+    const int npan = (nref + 31) / 32;
+    for (int q = npan - 1; q >= 0; --q) {
+        const int p0 = q * 32, nbk = std::min(32, nref - p0), R = n - p0;
+        DVR3D_COUNT_LAUNCH(1);
+        build_v_kernel<<<(unsigned)(((long long)R * nbk + 255) / 256), 256, 0, st>>>(A, lda, n, p0, nbk, V, ldv);
+        GemmOp g;  // S = V^T V
+        g.M = nbk;
+        g.N = nbk;
+        g.K = R;
+        g.A = V;
+        g.lda = ldv;
+        g.ta = true;
+        g.B = V;
+        g.ldb = ldv;
+        g.C = S;
+        g.ldc = 32;
+        g.splitk = std::max(1, std::min(64, (R + 15) / 16 / 8));
+        g.work = sk;
+        if ((e = launch_gemm(g, st)) != cudaSuccess) return e;
+        DVR3D_COUNT_LAUNCH(1);
+        larft_kernel<<<1, 32, 0, st>>>(S, tau + p0, nbk, Tm);
+        GemmOp a;  // W = V^T Z[p0:, :]
+        a.M = nbk;
+        a.N = nev;
+        a.K = R;
+        a.A = V;
+        a.lda = ldv;
+        a.ta = true;
+        a.B = Z + p0;
+        a.ldb = ldz;
+        a.C = W;
+        a.ldc = 32;
+        const int tiles = (nev + 63) / 64;
+        a.splitk = std::max(1, std::min(64, std::min((600 + tiles - 1) / tiles, (R + 15) / 16)));
+        a.work = sk;
+        if ((e = launch_gemm(a, st)) != cudaSuccess) return e;
+        GemmOp b;  // W2 = Tm W
+        b.M = nbk;
+        b.N = nev;
+        b.K = nbk;
+        b.A = Tm;
+        b.lda = 32;
+        b.B = W;
+        b.ldb = 32;
+        b.C = W2;
+        b.ldc = 32;
+        if ((e = launch_gemm(b, st)) != cudaSuccess) return e;
+        GemmOp c;  // Z[p0:, :] -= V W2
+        c.M = R;
+        c.N = nev;
+        c.K = nbk;
+        c.alpha = -1.0;
+        c.beta = 1.0;
+        c.A = V;
+        c.lda = ldv;
+        c.B = W2;
+        c.ldb = 32;
+        c.C = Z + p0;
+        c.ldc = ldz;
+        if ((e = launch_gemm(c, st)) != cudaSuccess) return e;
+    }
+    return cudaGetLastError();
+}
 
 int dense_tridiag_grid(int device) {
     int nsm = 0, per = 0;
@@ -546,14 +783,33 @@ void launch_dense_eigvals(const double *d, const double *e, int n, int nev, doub
 void launch_dense_eigvecs(const double *A, long long lda, int n, const double *d, const double *e,
                           const double *tau, const double *w, int nev,
                           const double *info, int *cstart, int *ncl, double *fac, int T, double *X,
-                          double *Z, long long ldz, cudaStream_t st) {
-    DVR3D_COUNT_LAUNCH(4);
+                          double *Z, long long ldz, double *bt_work, cudaStream_t st) {
+    DVR3D_COUNT_LAUNCH(1);
     clusters_kernel<<<1, 32, 0, st>>>(w, nev, info, cstart, ncl);
-    invit_dense_kernel<<<(T + 63) / 64, 64, 0, st>>>(d, e, n, w, nev, cstart, ncl, info, fac, T, X);
-    const long long tot = (long long)n * nev;
-    untangle_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(X, n, nev, Z, ldz);
-    const int nwarps = (nev + kBtCols - 1) / kBtCols;
-    backtransform_kernel<<<(nwarps + 3) / 4, 128, 0, st>>>(A, lda, n, tau, Z, ldz, nev);
+    const size_t smem = invit_smem_bytes(n);
+    if (smem <= (size_t)kInvitSmemMax) {
+        static bool attr = false;
+        if (!attr) {
+            cudaFuncSetAttribute(invit_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kInvitSmemMax);
+            attr = true;
+        }
+        DVR3D_COUNT_LAUNCH(1);
+        invit_smem_kernel<<<nev, 32, smem, st>>>(d, e, n, w, cstart, ncl, info, Z, ldz);
+    } else {
+        DVR3D_COUNT_LAUNCH(2);
+        invit_dense_kernel<<<(T + 63) / 64, 64, 0, st>>>(d, e, n, w, nev, cstart, ncl, info, fac, T, X);
+        const long long tot = (long long)n * nev;
+        untangle_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(X, n, nev, Z, ldz);
+    }
+    if (bt_work && !(ldz & 1)) {
+        launch_dense_backtransform(A, lda, n, tau, Z, ldz, nev, bt_work, st);
+    } else {
+        DVR3D_COUNT_LAUNCH(1);
+        const int nwarps = (nev + kBtCols - 1) / kBtCols;
+        backtransform_kernel<<<(nwarps + 3) / 4, 128, 0, st>>>(A, lda, n, tau, Z, ldz, nev);
+    }
 }
+
+size_t invit_smem_bytes(int n) { return (size_t)n * (5 * sizeof(double) + 1) + 16; }
 
 }  // namespace dvr3d

@@ -32,9 +32,18 @@ cudaError_t launch_dense_tridiag(DenseTri &t, int grid, cudaStream_t st);
 // info[0..3] = lower bound, upper bound, pivmin, ||T||
 void launch_dense_eigvals(const double *d, const double *e, int n, int nev, double *e2, double *info,
                           double *w, cudaStream_t st);
+// Eigenvectors of the reduced matrix for the nev eigenvalues w, back-transformed into Z.
+// Inverse iteration runs with its factors in shared memory when invit_smem_bytes(n) <=
+// kInvitSmemMax (else from fac, 5 n T doubles, and X, n nev doubles); the back-transform is
+// blocked (GEMM) when bt_work (dense_bt_work_doubles(n, nev)) is given and ldz is even.
+constexpr int kInvitSmemMax = 200 * 1024;
+size_t invit_smem_bytes(int n);
+size_t dense_bt_work_doubles(int n, int nev);
 void launch_dense_eigvecs(const double *A, long long lda, int n, const double *d, const double *e,
                           const double *tau, const double *w, int nev,
                           const double *info, int *cstart, int *ncl, double *fac, int T, double *X,
-                          double *Z, long long ldz, cudaStream_t st);
+                          double *Z, long long ldz, double *bt_work, cudaStream_t st);
+cudaError_t launch_dense_backtransform(const double *A, long long lda, int n, const double *tau, double *Z,
+                                       long long ldz, int nev, double *work, cudaStream_t st);
 
 }  // namespace dvr3d

@@ -184,7 +184,81 @@ __global__ void __launch_bounds__(kThreads) dgemm_kernel(int M, int N, int K, do
             }
 }
 
+// ---------------------------------------------------------------- grouped DGEMM
+template <bool TA>
+__global__ void __launch_bounds__(kThreads) grouped_dgemm_kernel(GroupedGemm gg) {
+    const int t = blockIdx.x;
+    int g = 0;
+    while (g + 1 < gg.ngroups && gg.tile_start[g + 1] <= t) ++g;
+    const int M = gg.M[g], K = gg.K[g], N = gg.N;
+    const int tm = (M + BM - 1) / BM;
+    const int local = t - gg.tile_start[g];
+    const int i0 = (local % tm) * BM, j0 = (local / tm) * BN;
+    const double *A = gg.A + gg.aoff[g];
+    const double *B = gg.B + gg.boff[g];
+    double *C = gg.C + gg.coff[g];
+    const long long lda = gg.lda, ldb = gg.ldb, ldc = gg.ldc;
+    __shared__ __align__(16) double As[BM][LDS];
+    __shared__ __align__(16) double Bs[BN][LDS];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * 32;
+    double acc[4][4][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    for (int k0 = 0; k0 < K; k0 += BK) {
+#pragma unroll
+        for (int q = 0; q < (BM * BK) / kThreads; ++q) {
+            const int e = tid + q * kThreads;
+            int m, k;
+            if (TA) {
+                m = e / BK;
+                k = e % BK;
+            } else {
+                k = e / BM;
+                m = e % BM;
+            }
+            const int gi = i0 + m, gk = k0 + k;
+            double v = 0.0;
+            if (gi < M && gk < K) v = TA ? A[(size_t)gi * lda + gk] : A[(size_t)gk * lda + gi];
+            As[m][k] = v;
+        }
+#pragma unroll
+        for (int q = 0; q < (BN * BK) / kThreads; ++q) {
+            const int e = tid + q * kThreads;
+            const int n = e / BK, k = e % BK;
+            const int gj = j0 + n, gk = k0 + k;
+            Bs[n][k] = (gj < N && gk < K) ? B[(size_t)gj * ldb + gk] : 0.0;
+        }
+        __syncthreads();
+        warp_tile_mma(As, Bs, wm, wn, lane, acc);
+        __syncthreads();
+    }
+    const int r = lane >> 2, c2 = (lane & 3) * 2;
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i = i0 + wm + a * 8 + r, j = j0 + wn + b * 8 + c2 + h;
+                if (i < M && j < N) {
+                    double *cp = C + (size_t)j * ldc + i;
+                    const double old = (gg.beta != 0.0) ? *cp : 0.0;
+                    *cp = gg.alpha * acc[a][b][h] + gg.beta * old;
+                }
+            }
+}
+
 }  // namespace
+
+void launch_grouped_dgemm(const GroupedGemm &g, bool transA, int total_tiles, cudaStream_t st) {
+    if (total_tiles <= 0) return;
+    DVR3D_COUNT_LAUNCH(1);
+    if (transA) grouped_dgemm_kernel<true><<<total_tiles, kThreads, 0, st>>>(g);
+    else grouped_dgemm_kernel<false><<<total_tiles, kThreads, 0, st>>>(g);
+}
 
 void launch_assemble_h3(const AsmParams &p, cudaStream_t st) {
     const long long tiles = (long long)((p.n + BM - 1) / BM);

@@ -1,0 +1,213 @@
+// gemm_pipe.cu -- pipelined FP64 tensor-core GEMM (DMMA mma.sync m8n8k4 .f64, cp.async
+// double buffering) with the options the shift-invert Krylov solver needs:
+//   * either operand stored column-major or transposed (no copies),
+//   * a triangular first operand (K range limited per output row tile),
+//   * lower-triangle output only (SYRK-style updates of a symmetric matrix),
+//   * split-K over gridDim.y with a deterministic second-pass reduction.
+//
+// Tiles are BM x BN = 64 x 64 (or 64 x 32 for thin right-hand sides), BK = 16; four warps,
+// 2 x 2, each a 32 x (BN/2) sub-tile. Shared-memory layouts follow the contiguous direction
+// of the source so that every cp.async moves 16 bytes: [m][k] (stride 20 doubles) for
+// k-contiguous operands, [k][m] (stride BM+4) for m-contiguous ones; both strides make the
+// DMMA fragment reads bank-conflict free.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+
+#include "common.cuh"
+#include "gemm64.cuh"
+
+namespace dvr3d {
+
+namespace {
+
+constexpr int kBM = 64, kBK = 16, kThr = 128;
+constexpr int kSK = kBK + 4;  // stride of [m][k] tiles
+
+__device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
+                 : "+d"(c0), "+d"(c1)
+                 : "d"(a), "d"(b));
+}
+
+__device__ __forceinline__ void cp16(void *smem, const void *gmem, int bytes) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(bytes));
+}
+
+// Tile of ROWS x kBK elements, element (r, k) of the operand at src(r, k).
+//   KC = true : source contiguous in k   -> smem [ROWS][kSK]
+//   KC = false: source contiguous in r   -> smem [kBK][ROWS + 4]
+template <int ROWS, bool KC>
+struct TileLoader {
+    static constexpr int kStride = KC ? kSK : ROWS + 4;
+    static constexpr int kElems = KC ? ROWS * kSK : kBK * (ROWS + 4);
+    // base points at element (r0, k0); ld is the stride between consecutive k (r-contiguous)
+    // or consecutive r (k-contiguous); rmax / kmax: valid extents from (r0, k0)
+    __device__ static void load(double *sm, const double *base, long long ld, int rmax, int kmax, int tid) {
+        constexpr int kChunks = ROWS * kBK / 2;
+#pragma unroll
+        for (int q = 0; q < (kChunks + kThr - 1) / kThr; ++q) {
+            const int e = tid + q * kThr;
+            if (kChunks % kThr != 0 && e >= kChunks) break;
+            int r, k, valid;
+            if (KC) {
+                r = e >> 3;
+                k = (e & 7) * 2;
+                valid = (r < rmax) ? min(max(kmax - k, 0), 2) : 0;
+            } else {
+                k = e / (ROWS / 2);
+                r = (e % (ROWS / 2)) * 2;
+                valid = (k < kmax) ? min(max(rmax - r, 0), 2) : 0;
+            }
+            double *dst = KC ? sm + r * kSK + k : sm + k * kStride + r;
+            const double *src = valid ? (KC ? base + (size_t)r * ld + k : base + (size_t)k * ld + r) : base;
+            cp16(dst, src, valid * 8);
+        }
+    }
+    __device__ static double at(const double *sm, int r, int k) { return KC ? sm[r * kSK + k] : sm[k * kStride + r]; }
+};
+
+// op(A)(i, k): TA ? A[i * lda + k] : A[k * lda + i]   (k-contiguous when TA)
+// op(B)(k, j): TB ? B[k * ldb + j] : B[j * ldb + k]   (k-contiguous when !TB)
+template <bool TA, bool TB, int BN>
+__global__ void __launch_bounds__(kThr) gemm_pipe_kernel(GemmOp p, int tiles_m) {
+    using LA = TileLoader<kBM, TA>;
+    using LB = TileLoader<BN, !TB>;
+    constexpr int WN = BN / 2, FN = WN / 8;
+    __shared__ __align__(16) double As[2][LA::kElems];
+    __shared__ __align__(16) double Bs[2][LB::kElems];
+    int tm, tn;
+    if (p.lower_out) {
+        const long long t = blockIdx.x;
+        int ti = (int)((sqrt(8.0 * (double)t + 1.0) - 1.0) * 0.5);
+        while ((long long)ti * (ti + 1) / 2 > t) --ti;
+        while ((long long)(ti + 1) * (ti + 2) / 2 <= t) ++ti;
+        tm = ti;
+        tn = (int)(t - (long long)ti * (ti + 1) / 2);
+    } else {
+        tm = blockIdx.x % tiles_m;
+        tn = blockIdx.x / tiles_m;
+    }
+    const int i0 = tm * kBM, j0 = tn * BN;
+    // K range of this tile (triangular op(A)) and of this split
+    int kb = 0, ke = p.K;
+    if (p.tri == 1) ke = min(ke, i0 + kBM);
+    else if (p.tri == 2) kb = (i0 / kBK) * kBK;
+    if (p.tri_b == 1) kb = max(kb, (j0 / kBK) * kBK);
+    else if (p.tri_b == 2) ke = min(ke, j0 + BN);
+    const int ntk = ke > kb ? (ke - kb + kBK - 1) / kBK : 0;
+    const int S = gridDim.y, z = blockIdx.y;
+    const int t0 = (int)((long long)ntk * z / S), t1 = (int)((long long)ntk * (z + 1) / S);
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int wm = (warp >> 1) * 32, wn = (warp & 1) * WN;
+    double acc[4][FN][2];
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < FN; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+    auto load = [&](int st, int kt) {
+        const int k0 = kb + kt * kBK;
+        const int kmax = ke - k0;
+        const double *a = TA ? p.A + (size_t)i0 * p.lda + k0 : p.A + (size_t)k0 * p.lda + i0;
+        LA::load(As[st], a, p.lda, p.M - i0, kmax, tid);
+        const double *b = TB ? p.B + (size_t)k0 * p.ldb + j0 : p.B + (size_t)j0 * p.ldb + k0;
+        LB::load(Bs[st], b, p.ldb, p.N - j0, kmax, tid);
+        asm volatile("cp.async.commit_group;\n" ::);
+    };
+    const int r = lane >> 2, c = lane & 3;
+    if (t0 < t1) load(0, t0);
+    for (int kt = t0; kt < t1; ++kt) {
+        const int st = (kt - t0) & 1;
+        if (kt + 1 < t1) {
+            load(st ^ 1, kt + 1);
+            asm volatile("cp.async.wait_group 1;\n" ::);
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::);
+        }
+        __syncthreads();
+#pragma unroll
+        for (int kk = 0; kk < kBK; kk += 4) {
+            double af[4], bf[FN];
+#pragma unroll
+            for (int t = 0; t < 4; ++t) af[t] = LA::at(As[st], wm + t * 8 + r, kk + c);
+#pragma unroll
+            for (int t = 0; t < FN; ++t) bf[t] = LB::at(Bs[st], wn + t * 8 + r, kk + c);
+#pragma unroll
+            for (int a = 0; a < 4; ++a)
+#pragma unroll
+                for (int b = 0; b < FN; ++b) dmma(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+        }
+        __syncthreads();
+    }
+    const int c2 = c * 2;
+    const bool split = (S > 1);
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < FN; ++b)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const int i = i0 + wm + a * 8 + r, j = j0 + wn + b * 8 + c2 + h;
+                if (i >= p.M || j >= p.N) continue;
+                if (p.lower_out && j > i) continue;
+                if (split) {
+                    p.work[((size_t)z * p.N + j) * p.M + i] = acc[a][b][h];
+                } else {
+                    double *cp = p.C + (size_t)j * p.ldc + i;
+                    const double old = (p.beta != 0.0) ? *cp : 0.0;
+                    *cp = p.alpha * acc[a][b][h] + p.beta * old;
+                }
+            }
+}
+
+__global__ void splitk_reduce_kernel(GemmOp p, int S) {
+    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (long long)p.M * p.N) return;
+    const int i = (int)(t % p.M), j = (int)(t / p.M);
+    if (p.lower_out && j > i) return;
+    double s = 0.0;
+    for (int z = 0; z < S; ++z) s += p.work[((size_t)z * p.N + j) * p.M + i];
+    double *cp = p.C + (size_t)j * p.ldc + i;
+    const double old = (p.beta != 0.0) ? *cp : 0.0;
+    *cp = p.alpha * s + p.beta * old;
+}
+
+template <int BN>
+cudaError_t launch_bn(const GemmOp &p, int S, cudaStream_t st) {
+    const int tiles_m = (p.M + kBM - 1) / kBM, tiles_n = (p.N + BN - 1) / BN;
+    const long long nt = p.lower_out ? (long long)tiles_m * (tiles_m + 1) / 2 : (long long)tiles_m * tiles_n;
+    dim3 grid((unsigned)nt, (unsigned)S);
+    DVR3D_COUNT_LAUNCH(1);
+    if (!p.ta && !p.tb) gemm_pipe_kernel<false, false, BN><<<grid, kThr, 0, st>>>(p, tiles_m);
+    else if (p.ta && !p.tb) gemm_pipe_kernel<true, false, BN><<<grid, kThr, 0, st>>>(p, tiles_m);
+    else if (!p.ta && p.tb) gemm_pipe_kernel<false, true, BN><<<grid, kThr, 0, st>>>(p, tiles_m);
+    else gemm_pipe_kernel<true, true, BN><<<grid, kThr, 0, st>>>(p, tiles_m);
+    return cudaGetLastError();
+}
+
+}  // namespace
+
+size_t gemm_splitk_work(int M, int N, int S) { return S > 1 ? (size_t)S * M * N : 0; }
+
+cudaError_t launch_gemm(const GemmOp &p0, cudaStream_t st) {
+    GemmOp p = p0;
+    if (p.M <= 0 || p.N <= 0) return cudaSuccess;
+    if (p.lower_out && p.M != p.N) return cudaErrorInvalidValue;
+    // 16-byte cp.async: every operand base and leading dimension must be even in doubles
+    if ((p.lda & 1) || (p.ldb & 1) || (reinterpret_cast<uintptr_t>(p.A) & 15) ||
+        (reinterpret_cast<uintptr_t>(p.B) & 15))
+        return cudaErrorInvalidValue;
+    int S = std::max(1, p.splitk);
+    if (p.K <= 0) S = 1;
+    if (S > 1 && !p.work) return cudaErrorInvalidValue;
+    const int bn = (p.N <= 32 && !p.lower_out) ? 32 : 64;
+    cudaError_t e = (bn == 32) ? launch_bn<32>(p, S, st) : launch_bn<64>(p, S, st);
+    if (e != cudaSuccess || S == 1) return e;
+    const long long tot = (long long)p.M * p.N;
+    DVR3D_COUNT_LAUNCH(1);
+    splitk_reduce_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(p, S);
+    return cudaGetLastError();
+}
+
+}  // namespace dvr3d

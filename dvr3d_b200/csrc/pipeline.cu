@@ -32,6 +32,9 @@ namespace {
 thread_local long long t_h2d = 0, t_d2h = 0;
 }
 
+void note_h2d(long long bytes) { t_h2d += bytes; }
+void note_d2h(long long bytes) { t_d2h += bytes; }
+
 // ---------------------------------------------------------------- arena
 DeviceArena::~DeviceArena() { release_all(); }
 
@@ -95,19 +98,6 @@ void check_dev_err(dvr3d_ctx *ctx, const int *err_dev, const char *stage) {
     if (e == kDevBarrierTimeout) throw HostError{DVR3D_ERR_NOCONV, std::string(stage) + ": grid barrier wait exceeded its limit"};
     if (e != 0) throw HostError{DVR3D_ERR_NOCONV, std::string(stage) + ": device error flag " + std::to_string(e)};
 }
-
-// Output of the 2D stage: the contracted basis, ready for assembly.
-struct Contracted {
-    double *Vt = nullptr;   // ldv x ncol (zero padded)
-    long long ldv = 0;
-    int P = 0, N = 0;
-    int *g = nullptr;       // [N] block of each column
-    double *e2 = nullptr;   // [N] 2D eigenvalues
-    const double *T = nullptr;
-    int ldt = 0;
-    std::vector<int> iv2;   // per block selected counts
-    int nblocks = 0;
-};
 
 void eigvecs_work(const std::vector<int> &n, const std::vector<int> &sel, std::vector<long long> &off,
                   long long &total) {
@@ -552,6 +542,84 @@ __global__ void resid_kernel(const double *R, const double *Z, const double *w, 
 
 }  // namespace
 
+// ---------------------------------------------------------------- dense eigensolver
+void dense_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int nev, bool vecs, double *w, double *Z,
+                  long long ldz, const char *tag, bool time_panels, DenseOut *out) {
+    cudaStream_t st = ctx->stream;
+    const std::string t(tag);
+    DenseTri dt{};
+    dt.A = A;
+    dt.lda = lda;
+    dt.n = n;
+    dt.d = ctx->arena.get_t<double>(t + "d", n);
+    dt.e = ctx->arena.get_t<double>(t + "e", n);
+    dt.tau = ctx->arena.get_t<double>(t + "tau", n);
+    const int G = ctx->dense_grid;
+    if ((long long)n > 256LL * G) throw HostError{DVR3D_ERR_UNSUPPORTED, "matrix too large for the dense eigensolver"};
+    dt.nbmax = dense_panel_width();
+    dt.NT = (n + 63) / 64;
+    dt.V = ctx->arena.get_t<double>(t + "V", (size_t)n * dt.nbmax);
+    dt.W = ctx->arena.get_t<double>(t + "W", (size_t)n * dt.nbmax);
+    dt.acol = ctx->arena.get_t<double>(t + "acol", n);
+    dt.ybuf = ctx->arena.get_t<double>(t + "y", n);
+    dt.P = ctx->arena.get_t<double>(t + "P", (size_t)dt.NT * dt.NT * 64);
+    dt.part = ctx->arena.get_t<double>(t + "part", (size_t)G * (1 + 2 * dt.nbmax));
+    dt.bar = ctx->arena.get_t<GridBarrier>(t + "bar", 1);
+    dt.err = ctx->arena.get_t<int>(t + "err", 1);
+    CK(cudaMemsetAsync(dt.bar, 0, sizeof(GridBarrier), st));
+    CK(cudaMemsetAsync(dt.err, 0, sizeof(int), st));
+    const char *prof_env = std::getenv("DVR3D_PROF");
+    const bool prof = prof_env && prof_env[0] == '1';
+    if (prof) {
+        dt.prof = ctx->arena.get_t<long long>(t + "prof", 8);
+        CK(cudaMemsetAsync(dt.prof, 0, 8 * sizeof(long long), st));
+    }
+    if (time_panels) {
+        const int npan = (n + dt.nbmax - 1) / dt.nbmax + 1;
+        if ((int)ctx->panel_ev.size() < 2 * npan) {
+            const size_t old = ctx->panel_ev.size();
+            ctx->panel_ev.resize(2 * npan);
+            for (size_t q = old; q < ctx->panel_ev.size(); ++q) CK(cudaEventCreate(&ctx->panel_ev[q]));
+        }
+        dt.ev = ctx->panel_ev.data();
+        dt.nev = (int)ctx->panel_ev.size();
+    }
+    CK(launch_dense_tridiag(dt, G, st));
+    if (prof) {
+        std::vector<long long> pc = download(ctx, dt.prof, 6);
+        int khz = 0;
+        cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, ctx->device);
+        std::fprintf(stderr, "dense reduction N=%d grid=%d phase ms (at %d MHz):", n, G, khz / 1000);
+        for (int q = 0; q < 6; ++q) std::fprintf(stderr, " %.2f", (double)pc[q] / (double)khz);
+        std::fprintf(stderr, "\n");
+    }
+    double *e2s = ctx->arena.get_t<double>(t + "e2", n);
+    double *info = ctx->arena.get_t<double>(t + "info", 4);
+    launch_dense_eigvals(dt.d, dt.e, n, nev, e2s, info, w, st);
+    CK(cudaGetLastError());
+    if (vecs) {
+        const int T = std::min(nev, 1024);
+        const bool smem = invit_smem_bytes(n) <= (size_t)kInvitSmemMax;
+        double *fac = smem ? nullptr : ctx->arena.get_t<double>(t + "fac", (size_t)5 * n * T);
+        double *X = smem ? nullptr : ctx->arena.get_t<double>(t + "x", (size_t)n * nev);
+        int *cs = ctx->arena.get_t<int>(t + "cs", nev + 1);
+        int *ncl = ctx->arena.get_t<int>(t + "ncl", 1);
+        double *bt = ctx->arena.get_t<double>(t + "bt", dense_bt_work_doubles(n, nev));
+        launch_dense_eigvecs(A, lda, n, dt.d, dt.e, dt.tau, w, nev, info, cs, ncl, fac, T, X, Z, ldz, bt, st);
+        CK(cudaGetLastError());
+    }
+    check_dev_err(ctx, dt.err, "dense tridiagonal reduction");
+    if (out && time_panels) {
+        out->npanel = dt.npanel;
+        out->panel_ms = 0.0;
+        for (int q = 0; q < dt.npanel && 2 * q + 1 < dt.nev; ++q) {
+            float m = 0.f;
+            CK(cudaEventElapsedTime(&m, ctx->panel_ev[2 * q], ctx->panel_ev[2 * q + 1]));
+            out->panel_ms += m;
+        }
+    }
+}
+
 // ---------------------------------------------------------------- one k block
 void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_options &opt,
                  dvr3d_result &res) {
@@ -589,8 +657,37 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
         return;
     }
     if (res.eval && res.eval_cap < meval) throw HostError{DVR3D_ERR_BUFFER, "eval buffer smaller than min(neval, N)"};
+    const bool mixed = (opt.precision == DVR3D_PREC_MIXED_DAVIDSON);
+    auto finish_times = [&](double &ms1, double &ms2, double &ms3) {
+        CK(cudaStreamSynchronize(st));
+        float a = 0, b = 0, c = 0;
+        CK(cudaEventElapsedTime(&a, ctx->ev[0], ctx->ev[1]));
+        CK(cudaEventElapsedTime(&b, ctx->ev[1], ctx->ev[2]));
+        CK(cudaEventElapsedTime(&c, ctx->ev[2], ctx->ev[3]));
+        ms1 = a;
+        ms2 = b;
+        ms3 = c;
+        res.stage_ms[0] = std::chrono::duration<double, std::milli>(th1 - th0).count();
+        res.stage_ms[1] = ms1;
+        res.stage_ms[2] = ms2;
+        res.stage_ms[3] = ms3;
+        res.stage_ms[4] = ms1 + ms2 + ms3;
+        res.stage_ms[5] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - th0).count();
+    };
+    auto put_levels = [&](const double *wv, const double *Z) {
+        if (res.eval) {
+            CK(cudaMemcpyAsync(res.eval, wv, sizeof(double) * meval, cudaMemcpyDeviceToHost, st));
+            t_d2h += (long long)sizeof(double) * meval;
+        }
+        if (res.evec && Z) {
+            if (res.evec_cap < (size_t)N * meval) throw HostError{DVR3D_ERR_BUFFER, "evec buffer too small"};
+            CK(cudaMemcpyAsync(res.evec, Z, sizeof(double) * N * meval, cudaMemcpyDeviceToHost, st));
+            t_d2h += (long long)sizeof(double) * N * meval;
+        }
+    };
     // ---- assembly (bloc3d / mkham3+loadh)
-    double *H3 = ctx->arena.get_t<double>("h3", (size_t)N * N);
+    const long long ldh = mixed ? round_up(N, 8) : N;
+    double *H3 = ctx->arena.get_t<double>("h3", (size_t)ldh * N);
     AsmParams ap{};
     ap.Vt = C.Vt;
     ap.ldv = C.ldv;
@@ -600,94 +697,65 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
     ap.ldt = C.ldt;
     ap.e2 = C.e2;
     ap.H = H3;
-    ap.ldh = N;
+    ap.ldh = ldh;
     launch_assemble_h3(ap, st);
     CK(cudaGetLastError());
     CK(cudaEventRecord(ctx->ev[2], st));
     if (opt.want_h3 && res.h3) {
         if (res.h3_cap < (size_t)N * N) throw HostError{DVR3D_ERR_BUFFER, "h3 buffer too small"};
-        CK(cudaMemcpyAsync(res.h3, H3, sizeof(double) * N * N, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpy2DAsync(res.h3, (size_t)N * sizeof(double), H3, (size_t)ldh * sizeof(double),
+                             (size_t)N * sizeof(double), N, cudaMemcpyDeviceToHost, st));
         t_d2h += (long long)sizeof(double) * N * N;
     }
-    // ---- final eigensolve (diag3d), plain FP64 path
+    if (mixed) {
+        // ---- shift-invert block Krylov for the lowest levels; dense FP64 fallback below
+        std::vector<double> e2h = download(ctx, C.e2, N);
+        const double emin = *std::min_element(e2h.begin(), e2h.end());
+        double *wv = ctx->arena.get_t<double>("dt_w", meval);
+        double *Z = res.evec ? ctx->arena.get_t<double>("dv_z", (size_t)N * meval) : nullptr;
+        std::vector<double> rn;
+        KrylovStats ks;
+        const bool ok = si_krylov_solve(ctx, H3, ldh, N, emin, opt, meval, wv, rn, Z, ks);
+        if (ok) {
+            CK(cudaEventRecord(ctx->ev[3], st));
+            put_levels(wv, Z);
+            if (res.resid)
+                for (int j = 0; j < std::min(meval, res.resid_cap); ++j) res.resid[j] = rn[j];
+            res.max_resid = ks.max_resid;
+            res.iterations = ks.blocks;
+            double ms1, ms2, ms3;
+            finish_times(ms1, ms2, ms3);
+            // dominant kernel: the DMMA GEMM of the factorisation and Krylov steps
+            res.dom_ms = ks.factor_ms + ks.krylov_ms;
+            res.dom_bytes = 0.0;
+            res.dom_flops = ks.flops;
+            res.dom_launches = 0;
+            std::snprintf(res.dom_kernel, sizeof(res.dom_kernel), "gemm_pipe_kernel");
+            res.launches = (int)(g_kernel_launches - launches0);
+            res.h2d_bytes = t_h2d;
+            res.d2h_bytes = t_d2h;
+            return;
+        }
+        res.fallback = 1;
+    }
+    // ---- final eigensolve (diag3d), dense FP64
     const long long ldw = round_up(N, 8);
     double *Hw = ctx->arena.get_t<double>("h3w", (size_t)ldw * N);
-    CK(cudaMemcpy2DAsync(Hw, ldw * sizeof(double), H3, (size_t)N * sizeof(double), (size_t)N * sizeof(double), N,
+    CK(cudaMemcpy2DAsync(Hw, ldw * sizeof(double), H3, (size_t)ldh * sizeof(double), (size_t)N * sizeof(double), N,
                          cudaMemcpyDeviceToDevice, st));
-    DenseTri dt{};
-    dt.A = Hw;
-    dt.lda = ldw;
-    dt.n = N;
-    dt.d = ctx->arena.get_t<double>("dt_d", N);
-    dt.e = ctx->arena.get_t<double>("dt_e", N);
-    dt.tau = ctx->arena.get_t<double>("dt_tau", N);
-    const int G = ctx->dense_grid;
-    if ((long long)N > 256LL * G) throw HostError{DVR3D_ERR_UNSUPPORTED, "final Hamiltonian too large for the dense path"};
-    dt.nbmax = dense_panel_width();
-    dt.NT = (N + 63) / 64;
-    dt.V = ctx->arena.get_t<double>("dt_V", (size_t)N * dt.nbmax);
-    dt.W = ctx->arena.get_t<double>("dt_W", (size_t)N * dt.nbmax);
-    dt.acol = ctx->arena.get_t<double>("dt_acol", N);
-    dt.ybuf = ctx->arena.get_t<double>("dt_y", N);
-    dt.P = ctx->arena.get_t<double>("dt_P", (size_t)dt.NT * dt.NT * 64);
-    dt.part = ctx->arena.get_t<double>("dt_part", (size_t)G * (1 + 2 * dt.nbmax));
-    dt.bar = ctx->arena.get_t<GridBarrier>("dt_bar", 1);
-    dt.err = ctx->arena.get_t<int>("dt_err", 1);
-    CK(cudaMemsetAsync(dt.bar, 0, sizeof(GridBarrier), st));
-    CK(cudaMemsetAsync(dt.err, 0, sizeof(int), st));
-    const char *prof_env = std::getenv("DVR3D_PROF");
-    const bool prof = prof_env && prof_env[0] == '1';
-    if (prof) {
-        dt.prof = ctx->arena.get_t<long long>("dt_prof", 8);
-        CK(cudaMemsetAsync(dt.prof, 0, 8 * sizeof(long long), st));
-    }
-    const int npan = (N + dt.nbmax - 1) / dt.nbmax + 1;
-    if ((int)ctx->panel_ev.size() < 2 * npan) {
-        const size_t old = ctx->panel_ev.size();
-        ctx->panel_ev.resize(2 * npan);
-        for (size_t q = old; q < ctx->panel_ev.size(); ++q) CK(cudaEventCreate(&ctx->panel_ev[q]));
-    }
-    dt.ev = ctx->panel_ev.data();
-    dt.nev = (int)ctx->panel_ev.size();
-    CK(launch_dense_tridiag(dt, G, st));
-    if (prof) {
-        std::vector<long long> pc = download(ctx, dt.prof, 6);
-        int khz = 0;
-        cudaDeviceGetAttribute(&khz, cudaDevAttrClockRate, ctx->device);
-        std::fprintf(stderr, "dense reduction N=%d grid=%d phase ms (at %d MHz):", N, G, khz / 1000);
-        for (int q = 0; q < 6; ++q) std::fprintf(stderr, " %.2f", (double)pc[q] / (double)khz);
-        std::fprintf(stderr, "\n");
-    }
-    double *e2s = ctx->arena.get_t<double>("dt_e2", N);
-    double *info = ctx->arena.get_t<double>("dt_info", 4);
     double *wv = ctx->arena.get_t<double>("dt_w", meval);
-    launch_dense_eigvals(dt.d, dt.e, N, meval, e2s, info, wv, st);
-    CK(cudaGetLastError());
     const bool vecs = opt.want_vectors || res.evec || res.resid;
-    double *Z = nullptr;
-    if (vecs) {
-        const int T = std::min(meval, 1024);
-        double *fac = ctx->arena.get_t<double>("dv_fac", (size_t)5 * N * T);
-        double *X = ctx->arena.get_t<double>("dv_x", (size_t)N * meval);
-        Z = ctx->arena.get_t<double>("dv_z", (size_t)N * meval);
-        int *cs = ctx->arena.get_t<int>("dv_cs", meval + 1);
-        int *ncl = ctx->arena.get_t<int>("dv_ncl", 1);
-        launch_dense_eigvecs(Hw, ldw, N, dt.d, dt.e, dt.tau, wv, meval, info, cs, ncl, fac, T, X, Z, N, st);
-        CK(cudaGetLastError());
-    }
+    double *Z = vecs ? ctx->arena.get_t<double>("dv_z", (size_t)N * meval) : nullptr;
+    DenseOut dout;
+    dense_lowest(ctx, Hw, ldw, N, meval, vecs, wv, Z, N, "dt_", true, &dout);
     CK(cudaEventRecord(ctx->ev[3], st));
-    check_dev_err(ctx, dt.err, "final tridiagonal reduction");
-    if (res.eval) {
-        CK(cudaMemcpyAsync(res.eval, wv, sizeof(double) * meval, cudaMemcpyDeviceToHost, st));
-        t_d2h += (long long)sizeof(double) * meval;
-    }
     res.max_resid = -1.0;
     if (vecs && (res.resid || opt.want_vectors)) {
         double *R = ctx->arena.get_t<double>("dv_r", (size_t)N * meval);
         double *rn = ctx->arena.get_t<double>("dv_rn", meval);
-        launch_dgemm(false, false, N, meval, N, 1.0, H3, N, Z, N, 0.0, R, N, st);
-        DVR3D_COUNT_LAUNCH(1);
+        launch_dgemm(false, false, N, meval, N, 1.0, H3, ldh, Z, N, 0.0, R, N, st);
         resid_kernel<<<meval, 256, 0, st>>>(R, Z, wv, N, N, meval, rn);
+        DVR3D_COUNT_LAUNCH(1);
         CK(cudaGetLastError());
         std::vector<double> rv = download(ctx, rn, meval);
         res.max_resid = 0.0;
@@ -695,39 +763,20 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
         if (res.resid)
             for (int j = 0; j < std::min(meval, res.resid_cap); ++j) res.resid[j] = rv[j];
     }
-    if (res.evec && Z) {
-        if (res.evec_cap < (size_t)N * meval) throw HostError{DVR3D_ERR_BUFFER, "evec buffer too small"};
-        CK(cudaMemcpyAsync(res.evec, Z, sizeof(double) * N * meval, cudaMemcpyDeviceToHost, st));
-        t_d2h += (long long)sizeof(double) * N * meval;
-    }
-    CK(cudaStreamSynchronize(st));
-    float ms1 = 0, ms2 = 0, ms3 = 0;
-    CK(cudaEventElapsedTime(&ms1, ctx->ev[0], ctx->ev[1]));
-    CK(cudaEventElapsedTime(&ms2, ctx->ev[1], ctx->ev[2]));
-    CK(cudaEventElapsedTime(&ms3, ctx->ev[2], ctx->ev[3]));
-    res.stage_ms[0] = std::chrono::duration<double, std::milli>(th1 - th0).count();
-    res.stage_ms[1] = ms1;
-    res.stage_ms[2] = ms2;
-    res.stage_ms[3] = ms3;
-    res.stage_ms[4] = ms1 + ms2 + ms3;
-    res.stage_ms[5] = std::chrono::duration<double, std::milli>(std::chrono::steady_clock::now() - th0).count();
+    put_levels(wv, Z);
+    double ms1, ms2, ms3;
+    finish_times(ms1, ms2, ms3);
     // dominant kernel: the panel kernel of the Householder reduction; its algorithmic
     // traffic is one read of the trailing lower triangle per column
-    double pms = 0.0;
-    for (int q = 0; q < dt.npanel && 2 * q + 1 < dt.nev; ++q) {
-        float m = 0.f;
-        CK(cudaEventElapsedTime(&m, ctx->panel_ev[2 * q], ctx->panel_ev[2 * q + 1]));
-        pms += m;
-    }
     double bytes = 0.0;
     for (int k = 0; k + 2 < N; ++k) {
         const double m = (double)(N - k - 1);
         bytes += 8.0 * m * (m + 1.0) * 0.5;
     }
-    res.dom_ms = pms;
+    res.dom_ms = dout.panel_ms;
     res.dom_bytes = bytes;
     res.dom_flops = 0.0;
-    res.dom_launches = dt.npanel;
+    res.dom_launches = dout.npanel;
     std::snprintf(res.dom_kernel, sizeof(res.dom_kernel), "dense_panel_kernel");
     res.launches = (int)(g_kernel_launches - launches0);
     res.h2d_bytes = t_h2d;

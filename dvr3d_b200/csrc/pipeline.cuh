@@ -57,6 +57,72 @@ struct dvr3d_ctx {
 
 namespace dvr3d {
 
+// Output of the 1D/2D stages: the contracted basis, ready for assembly or for the
+// matrix-free operator H3 = blockdiag(C_g^T) (T x I_P) blockdiag(C_g) + diag(e2).
+struct Contracted {
+    double *Vt = nullptr;   // ldv x ncol (zero padded), column i = sqrt(w)-scaled basis function
+    long long ldv = 0;
+    int P = 0, N = 0;
+    int *g = nullptr;       // [N] block of each column (device)
+    double *e2 = nullptr;   // [N] 2D eigenvalues (device)
+    const double *T = nullptr;  // block coupling matrix (device), T[g' * ldt + g]
+    int ldt = 0;
+    std::vector<int> iv2;   // per block selected counts (host)
+    int nblocks = 0;
+};
+
+// Block-Davidson for the lowest `nwant` levels of the contracted Hamiltonian (matrix-free).
+// Writes the levels (ascending) to wv_dev, FP64 residual norms to rn_host, and, when
+// evec_dev is not null, the eigenvectors (N x nwant). Returns the iteration count.
+struct DavidsonStats {
+    int iterations = 0;
+    int matvecs = 0;
+    double max_resid = 0.0;
+    double hv_ms = 0.0;        // device time of the operator applications
+    double hv_flops = 0.0;     // algorithmic flops of those applications
+    int hv_launches = 0;
+};
+void davidson_solve(dvr3d_ctx *ctx, const Contracted &C, const dvr3d_options &opt, int nwant,
+                    double *wv_dev, std::vector<double> &rn_host, double *evec_dev,
+                    DavidsonStats &stats);
+
+// Host<->device byte counters of the current solve (reported in dvr3d_result).
+void note_h2d(long long bytes);
+void note_d2h(long long bytes);
+
+// Lowest nev eigenvalues (ascending, device w) and optionally eigenvectors (device Z, ldz)
+// of the symmetric n x n matrix A (lower triangle read, lda a multiple of 8; overwritten by
+// the reduction). Device scratch is taken from the arena under names starting with `tag`.
+// When time_panels is set, the reduction's panel launches are timed into *out.
+struct DenseOut {
+    double panel_ms = 0.0;
+    int npanel = 0;
+};
+void dense_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int nev, bool vecs, double *w, double *Z,
+                  long long ldz, const char *tag, bool time_panels, DenseOut *out);
+
+// Shift-invert block Krylov solve for the lowest `nwant` levels of the assembled H3
+// (full symmetric storage, ldh even). emin_bound: a lower bound of the spectrum (min e2).
+// Returns false when it gives up (Krylov space limit, breakdown, no SPD shift found); the
+// caller then uses the dense eigensolver.
+struct KrylovStats {
+    double sigma = 0.0;
+    int retries = 0;       // shifts that failed the Cholesky pivot test
+    int block = 0;
+    int blocks = 0;        // Krylov blocks built
+    int m = 0;             // final subspace size
+    int checks = 0;        // Rayleigh-Ritz checks
+    int nconv = 0;
+    double worst_bound = 0.0;
+    double factor_ms = 0.0, krylov_ms = 0.0, rr_ms = 0.0;
+    double flops = 0.0;    // algorithmic flops of the factorisation, Krylov steps and checks
+    double max_resid = 0.0;
+};
+int si_krylov_first_size(int nwant, int block);
+bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, double emin_bound,
+                     const dvr3d_options &opt, int nwant, double *wv_dev, std::vector<double> &rn_host,
+                     double *evec_dev, KrylovStats &ks);
+
 // Solve one k block. Throws HostError / CudaFail.
 void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_options &opt,
                  dvr3d_result &res);

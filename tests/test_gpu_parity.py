@@ -144,3 +144,41 @@ def test_errors_are_codes_not_exits(ctx):
     # context still usable afterwards
     ok = configs.radau_water_like(10, 12, 30000.0, 20, title="after error")
     ctx.solve(parse_deck(ok.deck), 0)
+
+
+# ---------------------------------------------------------------- iterative (shift-invert Krylov) path
+TOL_MIXED_CM = 1e-3  # bar of the iterative path against the plain FP64 GPU path
+
+
+def _mixed_vs_dense(ctx, w, expect_fallback=False):
+    d = parse_deck(w.deck)
+    ctx.set_pes(w.pes)
+    a = ctx.solve(d, 0)
+    b = ctx.solve(d, 0, precision=dvr3d_b200.DVR3D_PREC_MIXED_DAVIDSON, want_resid=True)
+    assert b.nham3 == a.nham3 and len(b.eval) == len(a.eval)
+    assert b.fallback == int(expect_fallback)
+    err = np.abs(b.eval - a.eval) * AUTOCM
+    assert err.max() <= TOL_MIXED_CM, f"max level error {err.max():.3e} cm-1"
+    assert b.max_resid < 1e-5
+    if not expect_fallback:
+        assert b.iterations > 0
+    return a, b, err
+
+
+def test_mixed_small_basis_falls_back_to_dense(ctx):
+    """config 1 (N=924, 200 levels): the Krylov space would exceed the basis -> dense FP64."""
+    _mixed_vs_dense(ctx, configs.config1(), expect_fallback=True)
+
+
+def test_mixed_jacobi_medium_many_levels(ctx):
+    _, b, err = _mixed_vs_dense(ctx, configs.jacobi_h3p_like(20, 20, 32, 50000.0, 45000.0, 300, title="jacobi medium"))
+    assert b.nham3 > 4000
+
+
+def test_mixed_radau_config2(ctx):
+    _mixed_vs_dense(ctx, configs.config2())
+
+
+def test_mixed_config4_500_levels(ctx):
+    a, b, err = _mixed_vs_dense(ctx, configs.config4())
+    assert b.nham3 > 12000 and len(b.eval) == 500
