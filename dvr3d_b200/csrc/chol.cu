@@ -23,7 +23,7 @@ namespace {
 
 constexpr int NB = kCholNb;
 constexpr int kLeafThreads = 256;
-constexpr size_t kLeafSmem = 2 * NB * (NB + 1) * sizeof(double);
+constexpr size_t kLeafSmem = (NB * (NB + 1) + 2 * NB) * sizeof(double);
 
 __global__ void shift_copy_lower_kernel(const double *H, long long ldh, int n, double sigma, double *A,
                                         long long lda) {
@@ -37,72 +37,109 @@ __global__ void shift_copy_lower_kernel(const double *H, long long ldh, int n, d
 }
 
 // Cholesky of the nb x nb block at (j0, j0) (nb <= 64, lower triangle read) and inverse of
-// its factor. inv_out null: the factor goes back into A and its inverse into... nowhere;
-// inv_out given: inverse written there (ld 64, zeros above); in_place_inv: the inverse
-// replaces the block's lower triangle in A.
+// its factor. in_place_inv = 0: the factor goes back into A; 1: the inverse replaces the
+// block's lower triangle. inv_out (optional): the inverse (ld 64, zeros above).
+// Each thread keeps its 16 elements (row ti, columns tj0 + 4u) in registers; per column
+// step only the pivot column (or, in the inverse, the pivot row) goes through shared memory
+// (double-buffered), so one barrier per step suffices.
 __global__ void __launch_bounds__(kLeafThreads) potrf_leaf_kernel(double *A, long long lda, int j0, int nb,
                                                                   double *inv_out, int in_place_inv, double rel_tol,
                                                                   int *err) {
     if (*(volatile int *)err != 0) return;
     extern __shared__ double sm[];
-    double(*L)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);
-    double(*X)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm + NB * (NB + 1));
-    __shared__ int s_bad;
+    double(*L)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);  // final factor
+    double(*buf)[NB] = reinterpret_cast<double(*)[NB]>(sm + NB * (NB + 1));  // [2][64] pivot column / row
     __shared__ double s_thr;
     const int tid = threadIdx.x;
-    const int ti = tid & (NB - 1), tj0 = tid >> 6;  // this thread owns rows ti, columns tj0 + 4u
-    for (int u = 0; u < NB / 4; ++u) {
+    const int ti = tid & (NB - 1), tj0 = tid >> 6;  // this thread owns row ti, columns tj0 + 4u
+    constexpr int U = NB / 4;
+    double own[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
         const int j = tj0 + 4 * u;
-        double v = 0.0;
-        if (ti < nb && j < nb && ti >= j) v = A[(size_t)(j0 + j) * lda + j0 + ti];
-        L[ti][j] = v;
-        X[ti][j] = (ti == j) ? 1.0 : 0.0;
-    }
-    if (tid == 0) {
-        s_bad = 0;
-        double mx = 0.0;
-        for (int i = 0; i < nb; ++i) mx = fmax(mx, A[(size_t)(j0 + i) * lda + j0 + i]);
-        s_thr = rel_tol * mx;
+        own[u] = (ti < nb && j < nb && ti >= j) ? A[(size_t)(j0 + j) * lda + j0 + ti] : 0.0;
+        if (ti == j) buf[0][ti] = own[u];  // diagonal, for the pivot threshold
     }
     __syncthreads();
-    // right-looking factorisation
-    for (int k = 0; k < nb; ++k) {
-        if (tid == 0) {
-            const double d = L[k][k];
-            if (!(d > s_thr) || !isfinite(d)) s_bad = 1;
-            else L[k][k] = sqrt(d);
-        }
-        __syncthreads();
-        if (s_bad) break;
-        if (tid > k && tid < nb) L[tid][k] /= L[k][k];
-        __syncthreads();
-        const double lik = L[ti][k];
-        for (int u = 0; u < NB / 4; ++u) {
-            const int j = tj0 + 4 * u;
-            if (j > k && ti >= j && ti < nb) L[ti][j] -= lik * L[j][k];
-        }
-        __syncthreads();
+    if (tid < 32) {  // threshold relative to the largest diagonal entry
+        double mx = 0.0;
+        for (int i = tid; i < nb; i += 32) mx = fmax(mx, buf[0][i]);
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
+        if (tid == 0) s_thr = rel_tol * mx;
     }
-    if (s_bad) {
+    __syncthreads();
+    // right-looking factorisation in L D L^T form (column k published unscaled)
+    bool bad = false;
+    if (tj0 == 0) buf[0][ti] = own[0];  // column 0
+    for (int k = 0; k < nb; ++k) {
+        double *col = buf[k & 1], *nxt = buf[(k + 1) & 1];
+        __syncthreads();
+        const double d = col[k];
+        if (!(d > s_thr) || !isfinite(d)) {  // uniform: every thread reads the same d
+            bad = true;
+            break;
+        }
+        const double lik = (ti > k && ti < nb) ? col[ti] * (1.0 / d) : 0.0;
+#pragma unroll
+        for (int u = 0; u < U; ++u) {
+            const int j = tj0 + 4 * u;
+            if (j > k && ti >= j) own[u] -= lik * col[j];
+            if (j == k + 1) nxt[ti] = own[u];  // column k+1 is final after this step
+        }
+    }
+    if (bad) {
         if (tid == 0) atomicExch(err, (int)kDevNotPosDef);
         return;
     }
-    // X = inv(L), right-looking forward substitution on the identity
+    // L = (unit factor) D^{1/2}: column j scaled by 1/sqrt(d_j), diagonal sqrt(d_j)
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int j = tj0 + 4 * u;
+        if (ti == j) buf[0][j] = own[u];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
+        const int j = tj0 + 4 * u;
+        double v = 0.0;
+        if (ti < nb && j < nb && ti >= j) v = (ti == j) ? sqrt(own[u]) : own[u] / sqrt(buf[0][j]);
+        own[u] = v;
+        L[ti][j] = v;
+    }
+    __syncthreads();
+    // X = inv(L): row k of X is final once divided by L[k][k]; its owners publish it
+    // (divided), then the rows below subtract L[i][k] times it
+    double x[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) x[u] = (ti == tj0 + 4 * u) ? 1.0 : 0.0;
     for (int k = 0; k < nb; ++k) {
-        const double dk = L[k][k];
-        if (tid <= k) X[k][tid] /= dk;
-        __syncthreads();
-        const double lik = (ti > k && ti < nb) ? L[ti][k] : 0.0;
-        for (int u = 0; u < NB / 4; ++u) {
-            const int c = tj0 + 4 * u;
-            if (lik != 0.0 && c <= k) X[ti][c] -= lik * X[k][c];
+        double *row = buf[k & 1];
+        if (ti == k) {
+            const double r = 1.0 / L[k][k];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                x[u] *= r;
+                row[tj0 + 4 * u] = x[u];
+            }
         }
         __syncthreads();
+        const double lik = (ti > k && ti < nb) ? L[ti][k] : 0.0;
+        if (lik != 0.0) {
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = tj0 + 4 * u;
+                if (c <= k) x[u] -= lik * row[c];
+            }
+        }
     }
-    for (int u = 0; u < NB / 4; ++u) {
+#pragma unroll
+    for (int u = 0; u < U; ++u) {
         const int j = tj0 + 4 * u;
-        if (ti < nb && j < nb && ti >= j) A[(size_t)(j0 + j) * lda + j0 + ti] = in_place_inv ? X[ti][j] : L[ti][j];
-        if (inv_out) inv_out[(size_t)j * NB + ti] = (ti < nb && j < nb && ti >= j) ? X[ti][j] : 0.0;
+        const bool in = (ti < nb && j < nb && ti >= j);
+        if (in) A[(size_t)(j0 + j) * lda + j0 + ti] = in_place_inv ? x[u] : own[u];
+        if (inv_out) inv_out[(size_t)j * NB + ti] = in ? x[u] : 0.0;
     }
 }
 

@@ -634,15 +634,19 @@ __global__ void build_v_kernel(const double *A, long long lda, int n, int p0, in
 // Tm (upper, ld 32) of the block reflector I - V Tm V^T from S = V^T V (ld 32) and tau (dlarft,
 // forward, columnwise).
 __global__ void larft_kernel(const double *S, const double *tau, int nbk, double *Tm) {
-    __shared__ double t[32][33];
+    __shared__ double t[32][33], sv[32][33], ts[32];
     const int r = threadIdx.x;
-    for (int c = 0; c < 32; ++c) t[r][c] = 0.0;
+    for (int c = 0; c < 32; ++c) {
+        t[r][c] = 0.0;
+        sv[c][r] = (r < nbk && c < nbk) ? S[c * 32 + r] : 0.0;  // sv[i][c] = S(c, i)
+    }
+    ts[r] = (r < nbk) ? tau[r] : 0.0;
     __syncwarp();
     for (int i = 0; i < nbk; ++i) {
-        const double ti = tau[i];
+        const double ti = ts[i];
         if (r < i) {
             double s = 0.0;
-            for (int c = r; c < i; ++c) s += t[r][c] * S[i * 32 + c];
+            for (int c = r; c < i; ++c) s += t[r][c] * sv[i][c];
             t[r][i] = -ti * s;
         } else if (r == i) {
             t[i][i] = ti;
