@@ -14,14 +14,16 @@ from dataclasses import dataclass, field
 import numpy as np
 
 from . import _abi
-from ._abi import (DVR3D_PES_GRID, DVR3D_PES_MORSE_SUM, DVR3D_PES_MORSE_SUM_NPARAM,
-                   DVR3D_PREC_FP64, DVR3D_PREC_MIXED_DAVIDSON, Deck, Options, Result)
+from ._abi import (DVR3D_LP_NPARAM, DVR3D_PATH_DAVIDSON, DVR3D_PATH_DENSE, DVR3D_PATH_SHIFT_INVERT,
+                   DVR3D_PES_GRID, DVR3D_PES_MORSE_SUM, DVR3D_PES_MORSE_SUM_NPARAM, DVR3D_PREC_FP64,
+                   DVR3D_PREC_MIXED_DAVIDSON, Deck, Options, Result)
 
 AUTOCM = 2.19474624e5  # hartree -> cm-1, as diag3d (:2681)
 
 __all__ = ["Context", "Deck", "DVR3DError", "SolveResult", "parse_deck", "AUTOCM",
            "DVR3D_PES_MORSE_SUM", "DVR3D_PES_GRID", "DVR3D_PREC_FP64",
-           "DVR3D_PREC_MIXED_DAVIDSON", "k_blocks", "host_grid"]
+           "DVR3D_PREC_MIXED_DAVIDSON", "DVR3D_LP_NPARAM", "DVR3D_PATH_DENSE", "DVR3D_PATH_SHIFT_INVERT",
+           "DVR3D_PATH_DAVIDSON", "k_blocks", "host_grid"]
 
 
 class DVR3DError(RuntimeError):
@@ -103,7 +105,9 @@ class SolveResult:
 def _counters(r: Result) -> dict:
     return {"dom_ms": r.dom_ms, "dom_bytes": r.dom_bytes, "dom_flops": r.dom_flops,
             "dom_launches": r.dom_launches, "launches": r.launches, "h2d_bytes": r.h2d_bytes,
-            "d2h_bytes": r.d2h_bytes, "dom_kernel": r.dom_kernel.decode()}
+            "d2h_bytes": r.d2h_bytes, "dom_kernel": r.dom_kernel.decode(), "path": r.path,
+            "matvecs": r.matvecs, "lp_pairs": r.lp_pairs, "lp_loss_first": r.lp_loss_first,
+            "lp_loss_last": r.lp_loss_last}
 
 
 class Context:
@@ -168,7 +172,7 @@ class Context:
 
     def solve(self, deck: Deck, kk: int | None = None, *, precision: int = DVR3D_PREC_FP64,
               nlevels: int = 0, tol_cm: float = 0.0, max_iter: int = 0, block: int = 0,
-              learned_precond: bool = False, want_vectors: bool = False, want_h3: bool = False,
+              learned_precond: int = 0, want_vectors: bool = False, want_h3: bool = False,
               want_resid: bool = False) -> SolveResult:
         """Solve one k block (dvr3d_b200_solve_block)."""
         if kk is None:
@@ -212,6 +216,41 @@ class Context:
                            iterations=r.iterations, fallback=r.fallback,
                            resid=None if rs is None else rs[:m].copy(),
                            evec=None if evec is None else evec[:, :m], h3=h3, extra=_counters(r))
+
+    # ---- learned Davidson preconditioner
+    def lp_get_weights(self) -> np.ndarray:
+        w = np.zeros(DVR3D_LP_NPARAM)
+        rc = self._lib.dvr3d_b200_lp_get_weights(self._h, w.ctypes.data_as(C.POINTER(C.c_double)), w.size)
+        if rc < 0:
+            self._check(rc)
+        return w
+
+    def lp_set_weights(self, w) -> None:
+        w = np.ascontiguousarray(np.asarray(w, dtype=np.float64))
+        self._check(self._lib.dvr3d_b200_lp_set_weights(self._h, w.ctypes.data_as(C.POINTER(C.c_double)), w.size))
+
+    def lp_eval(self, w, lam, f1, f2, f3, scale, theta, delta) -> tuple[np.ndarray, np.ndarray]:
+        """Network outputs g (nmode x ncol) and sum(delta * dg/dw), by the device kernels."""
+        P = C.POINTER(C.c_double)
+        arr = [np.ascontiguousarray(np.asarray(x, dtype=np.float64)) for x in (w, lam, f1, f2, f3, theta)]
+        d = np.asfortranarray(np.asarray(delta, dtype=np.float64))
+        nmode, ncol = d.shape
+        g = np.zeros((nmode, ncol), order="F")
+        grad = np.zeros(DVR3D_LP_NPARAM)
+        self._check(self._lib.dvr3d_b200_lp_eval(
+            self._h, arr[0].ctypes.data_as(P), nmode, ncol, arr[1].ctypes.data_as(P), arr[2].ctypes.data_as(P),
+            arr[3].ctypes.data_as(P), arr[4].ctypes.data_as(P), float(scale), arr[5].ctypes.data_as(P),
+            d.ctypes.data_as(P), g.ctypes.data_as(P), grad.ctypes.data_as(P)))
+        return g, grad
+
+    def lp_train_loss(self, w, want_grad: bool = True) -> tuple[float, np.ndarray | None]:
+        P = C.POINTER(C.c_double)
+        w = np.ascontiguousarray(np.asarray(w, dtype=np.float64))
+        loss = np.zeros(1)
+        grad = np.zeros(DVR3D_LP_NPARAM) if want_grad else None
+        self._check(self._lib.dvr3d_b200_lp_train_loss(self._h, w.ctypes.data_as(P), loss.ctypes.data_as(P),
+                                                       grad.ctypes.data_as(P) if want_grad else None))
+        return float(loss[0]), grad
 
     def solve_batch(self, decks: list[Deck], pes_rows) -> list[SolveResult]:
         n = len(decks)

@@ -67,6 +67,10 @@ class Deck(C.Structure):
         return d
 
 
+DVR3D_LP_NPARAM = 369
+DVR3D_PATH_DENSE, DVR3D_PATH_SHIFT_INVERT, DVR3D_PATH_DAVIDSON = 0, 1, 2
+
+
 class Options(C.Structure):
     _fields_ = [("precision", C.c_int), ("nlevels", C.c_int), ("tol_cm", C.c_double),
                 ("max_iter", C.c_int), ("block", C.c_int), ("learned_precond", C.c_int),
@@ -85,7 +89,9 @@ class Result(C.Structure):
                 ("iv2", C.POINTER(C.c_int)), ("iv2_cap", C.c_int),
                 ("resid", C.POINTER(C.c_double)), ("resid_cap", C.c_int),
                 ("evec", C.POINTER(C.c_double)), ("evec_cap", C.c_size_t),
-                ("h3", C.POINTER(C.c_double)), ("h3_cap", C.c_size_t)]
+                ("h3", C.POINTER(C.c_double)), ("h3_cap", C.c_size_t),
+                ("path", C.c_int), ("matvecs", C.c_int), ("lp_pairs", C.c_int),
+                ("lp_loss_first", C.c_double), ("lp_loss_last", C.c_double)]
 
 
 def header_entry_points() -> list[str]:
@@ -131,6 +137,12 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
                                               P(C.c_longlong), vp, vp, C.c_int]),
         "dvr3d_b200_diag_batched_noalloc": (C.c_int, [vp, C.c_int, P(C.c_int), P(C.c_longlong),
                                                       P(C.c_longlong), vp, vp, C.c_int]),
+        "dvr3d_b200_lp_get_weights": (C.c_int, [vp, P(C.c_double), C.c_int]),
+        "dvr3d_b200_lp_set_weights": (C.c_int, [vp, P(C.c_double), C.c_int]),
+        "dvr3d_b200_lp_eval": (C.c_int, [vp, P(C.c_double), C.c_int, C.c_int, P(C.c_double), P(C.c_double),
+                                         P(C.c_double), P(C.c_double), C.c_double, P(C.c_double),
+                                         P(C.c_double), P(C.c_double), P(C.c_double)]),
+        "dvr3d_b200_lp_train_loss": (C.c_int, [vp, P(C.c_double), P(C.c_double), P(C.c_double)]),
     }
     for name, (res, args) in sig.items():
         if hasattr(lib, name):

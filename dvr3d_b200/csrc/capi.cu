@@ -9,6 +9,7 @@
 #include "../../include/dvr3d_b200.h"
 #include "eig_batched.cuh"
 #include "eig_dense.cuh"
+#include "learned_precond.cuh"
 #include "pipeline.cuh"
 
 using dvr3d::CudaFail;
@@ -383,6 +384,93 @@ int dvr3d_b200_run_deck(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_optio
         }
         copy_out(s, out, outcap, outlen);
         copy_out(lv, lev, levcap, levlen);
+        return DVR3D_OK;
+    });
+}
+
+int dvr3d_b200_lp_get_weights(dvr3d_ctx *ctx, double *w, int n) {
+    if (!ctx || !w) return DVR3D_ERR_ARG;
+    return guarded(ctx, [&]() -> int {
+        if (!ctx->lp_trained) throw HostError{DVR3D_ERR_ARG, "no trained preconditioner in this context"};
+        if (n < dvr3d::kLpParams) throw HostError{DVR3D_ERR_BUFFER, "weight buffer smaller than DVR3D_LP_NPARAM"};
+        cudaSetDevice(ctx->device);
+        const double *d = ctx->arena.get_t<double>("lp_w", dvr3d::kLpParams);
+        cudaError_t e = cudaMemcpyAsync(w, d, sizeof(double) * dvr3d::kLpParams, cudaMemcpyDeviceToHost, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) throw CudaFail{e, "lp_get_weights"};
+        return dvr3d::kLpParams;
+    });
+}
+
+int dvr3d_b200_lp_set_weights(dvr3d_ctx *ctx, const double *w, int n) {
+    if (!ctx || !w) return DVR3D_ERR_ARG;
+    return guarded(ctx, [&]() -> int {
+        if (n != dvr3d::kLpParams) throw HostError{DVR3D_ERR_ARG, "expected DVR3D_LP_NPARAM parameters"};
+        for (int p = 0; p < n; ++p)
+            if (!std::isfinite(w[p])) throw HostError{DVR3D_ERR_ARG, "non-finite preconditioner parameter"};
+        cudaSetDevice(ctx->device);
+        double *d = ctx->arena.get_t<double>("lp_w", dvr3d::kLpParams);
+        cudaError_t e = cudaMemcpyAsync(d, w, sizeof(double) * n, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) throw CudaFail{e, "lp_set_weights"};
+        ctx->lp_trained = true;
+        return DVR3D_OK;
+    });
+}
+
+int dvr3d_b200_lp_eval(dvr3d_ctx *ctx, const double *w, int nmode, int ncol, const double *lam,
+                       const double *f1, const double *f2, const double *f3, double scale,
+                       const double *theta, const double *delta, double *gout, double *grad) {
+    if (!ctx || !w || !lam || !f1 || !f2 || !f3 || !theta || !delta || !gout || !grad || nmode <= 0 || ncol <= 0 ||
+        !(scale > 0.0))
+        return DVR3D_ERR_ARG;
+    return guarded(ctx, [&]() -> int {
+        cudaSetDevice(ctx->device);
+        cudaStream_t st = ctx->stream;
+        auto up = [&](const char *nm, const double *src, size_t cnt) {
+            double *d = ctx->arena.get_t<double>(nm, cnt);
+            const cudaError_t e = cudaMemcpyAsync(d, src, sizeof(double) * cnt, cudaMemcpyHostToDevice, st);
+            if (e != cudaSuccess) throw CudaFail{e, "lp_eval upload"};
+            return d;
+        };
+        dvr3d::LpModes m;
+        m.lam = up("lpe_lam", lam, nmode);
+        m.f1 = up("lpe_f1", f1, nmode);
+        m.f2 = up("lpe_f2", f2, nmode);
+        m.f3 = up("lpe_f3", f3, nmode);
+        m.n = nmode;
+        m.scale = scale;
+        const double *dth = up("lpe_th", theta, ncol);
+        const double *dd = up("lpe_delta", delta, (size_t)nmode * ncol);
+        const double *dw = up("lpe_w", w, dvr3d::kLpParams);
+        double *dg = ctx->arena.get_t<double>("lpe_g", (size_t)nmode * ncol);
+        double *dgr = ctx->arena.get_t<double>("lpe_grad", dvr3d::kLpParams);
+        double *work = ctx->arena.get_t<double>("lpe_work", dvr3d::lp_grad_work_doubles());
+        cudaError_t e = dvr3d::launch_lp_forward(m, dw, dth, ncol, dg, st);
+        if (e == cudaSuccess) e = dvr3d::lp_mlp_grad(m, dw, dth, ncol, dd, dgr, work, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(gout, dg, sizeof(double) * nmode * ncol, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaMemcpyAsync(grad, dgr, sizeof(double) * dvr3d::kLpParams, cudaMemcpyDeviceToHost, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) throw CudaFail{e, "lp_eval"};
+        return DVR3D_OK;
+    });
+}
+
+int dvr3d_b200_lp_train_loss(dvr3d_ctx *ctx, const double *w, double *loss, double *grad) {
+    if (!ctx || !w || !loss) return DVR3D_ERR_ARG;
+    return guarded(ctx, [&]() -> int {
+        cudaSetDevice(ctx->device);
+        cudaStream_t st = ctx->stream;
+        double *dw = ctx->arena.get_t<double>("lpt_w", dvr3d::kLpParams);
+        double *dg = ctx->arena.get_t<double>("lpt_g", dvr3d::kLpParams);
+        cudaError_t e = cudaMemcpyAsync(dw, w, sizeof(double) * dvr3d::kLpParams, cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) throw CudaFail{e, "lp_train_loss upload"};
+        *loss = dvr3d::lp_train_loss(ctx, dw, grad ? dg : nullptr);
+        if (grad) {
+            e = cudaMemcpyAsync(grad, dg, sizeof(double) * dvr3d::kLpParams, cudaMemcpyDeviceToHost, st);
+            if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) throw CudaFail{e, "lp_train_loss"};
+        }
         return DVR3D_OK;
     });
 }

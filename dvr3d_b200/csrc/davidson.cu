@@ -1,29 +1,30 @@
-// davidson.cu -- block-Davidson solver for the lowest levels of the contracted Hamiltonian.
+// davidson.cu -- block-Davidson for a few lowest levels of the assembled contracted
+// Hamiltonian, preconditioned by its channel blocks (optionally with the learned correction),
+// judged by FP64 residuals; and the trainer of the learned correction.
 //
-// The reference diagonalises the assembled final Hamiltonian completely (diag3d -> dsyev,
-// :2661-2764) although only NEVAL levels are kept. Here the lowest levels are found
-// iteratively, and the Hamiltonian is never formed: with C_g the sqrt(w)-scaled contracted
-// basis functions of block g (columns of Vt, P rows each),
-//     H3 v = blockdiag(C_g^T) (T (x) I_P) blockdiag(C_g) v + e2 o v,
-// i.e. per block of vectors: Y_g = C_g V_g (grouped GEMM), Z = Y T (GEMM over blocks),
-// (HV)_g = C_g^T Z_g (grouped GEMM). That is ~(4 P N + 2 P nblk^2) flop per vector instead
-// of 2 N^2, and only Vt (P x N) is read instead of an N x N matrix.
-//
-// Iteration (thick-restarted block Davidson with locking):
-//   Rayleigh-Ritz on the current basis S (G = S^T H S, m <= 160, solved in shared memory)
-//   -> Ritz pairs and FP64 residuals -> leading converged pairs are locked (removed from
-//   the search space, later corrections are orthogonalised against them) -> corrections for
-//   the next `block` unconverged pairs from the preconditioner -> orthogonalised against the
-//   locked vectors and the Ritz vectors (classical Gram-Schmidt, twice), orthonormalised
-//   through the eigen-decomposition of their Gram matrix (near-dependent directions dropped)
-//   -> appended with their H images.
+// The reference diagonalises the final Hamiltonian completely (diag3d -> dsyev,
+// :2661-2764) even when NEVAL is small. For a few levels no factorisation is needed:
+//   basis V (orthonormal, m <= 3 b columns), HV = H3 V (DMMA GEMM with the assembled H3)
+//   -> Rayleigh-Ritz (G = V^T HV, shared-memory eigensolver) -> Ritz pairs, FP64 residuals
+//   -> converged when every wanted pair satisfies rho^2 / gap <= tol
+//   -> corrections t = P(r, theta) from the channel blocks (learned_precond.cuh)
+//   -> classical Gram-Schmidt against V twice, Cholesky-QR twice, appended; thick restart
+//      to the 2 b leading Ritz vectors when the basis is full.
+// In training mode the solver records (residual, theta, basis) snapshots of the wanted pairs;
+// after convergence the ideal corrections e = (x_final - x) outside the basis of that moment
+// are formed and the network is fitted to them on the device (Adam, full batch).
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <numeric>
+#include <string>
 #include <vector>
 
+#include "chol.cuh"
 #include "common.cuh"
 #include "gemm64.cuh"
+#include "learned_precond.cuh"
 #include "pipeline.cuh"
 #include "small_syev.cuh"
 
@@ -36,36 +37,6 @@
 namespace dvr3d {
 
 namespace {
-
-constexpr int kMaxSub = kSmallSyevMax;  // largest Rayleigh-Ritz problem (shared memory)
-
-// diag(H3)_i = e2_i + T[g_i, g_i] ||Vt[:, i]||^2 ; one warp per column
-__global__ void hdiag_kernel(const double *Vt, long long ldv, int P, int N, const int *g, const double *T,
-                             int ldt, const double *e2, double *hd) {
-    const int w = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
-    if (w >= N) return;
-    const double *c = Vt + (size_t)w * ldv;
-    double s = 0.0;
-    for (int p = lane; p < P; p += 32) s += c[p] * c[p];
-    s = warp_sum(s);
-    if (lane == 0) hd[w] = e2[w] + T[(size_t)g[w] * ldt + g[w]] * s;
-}
-
-__global__ void unit_columns_kernel(double *S, long long ld, int N, const int *idx, int m) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)N * m) return;
-    const int j = (int)(t / N), i = (int)(t % N);
-    S[(size_t)j * ld + i] = (i == idx[j]) ? 1.0 : 0.0;
-}
-
-// HV += e2 o V
-__global__ void add_diag_kernel(const double *e2, const double *V, long long ldv, double *HV, long long ldh, int N,
-                                int b) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)N * b) return;
-    const int j = (int)(t / N), i = (int)(t % N);
-    HV[(size_t)j * ldh + i] += e2[i] * V[(size_t)j * ldv + i];
-}
 
 // R[:, j] = HX[:, j] - w_j X[:, j], rn[j] = ||R[:, j]||; one CTA per column
 __global__ void residual_kernel(const double *X, const double *HX, long long ld, const double *w, int N, double *R,
@@ -83,329 +54,476 @@ __global__ void residual_kernel(const double *X, const double *HX, long long ld,
     if (threadIdx.x == 0) rn[j] = sqrt(s);
 }
 
-// Davidson (diagonal) preconditioner: t_i = r_i / (theta - d_i), safeguarded
-__global__ void precond_diag_kernel(const double *R, long long ldr, const double *w, const double *hd, int N, int nb,
-                                    double *Tc, long long ldt) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)N * nb) return;
-    const int j = (int)(t / N), i = (int)(t % N);
-    double den = w[j] - hd[i];
-    const double eps = 1.0e-6;
-    if (fabs(den) < eps) den = (den < 0.0) ? -eps : eps;
-    Tc[(size_t)j * ldt + i] = R[(size_t)j * ldr + i] / den;
+// E[:, j] = sign(xf_j . xs_j) xf_j - xs_j; one CTA per column
+__global__ void ideal_correction_kernel(const double *XF, const double *XS, long long ld, int N, double *E) {
+    const int j = blockIdx.x;
+    const double *xf = XF + (size_t)j * ld, *xs = XS + (size_t)j * ld;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) s += xf[i] * xs[i];
+    __shared__ double red[32];
+    s = block_sum(s, red);
+    const double sg = (s < 0.0) ? -1.0 : 1.0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) E[(size_t)j * ld + i] = sg * xf[i] - xs[i];
 }
 
-// dst[:, j] = src[:, j] for j < ncol (contiguous columns, same leading dimension)
-__global__ void copy_cols_kernel(const double *src, double *dst, long long ld, int N, int ncol) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)N * ncol) return;
-    const int j = (int)(t / N), i = (int)(t % N);
-    dst[(size_t)j * ld + i] = src[(size_t)j * ld + i];
+// Column norms of T (one CTA per column); columns whose norm is below rel * max(norm_ref)
+// are replaced by a deterministic pseudo-random vector, the others scaled to unit norm.
+__global__ void colnorm_kernel(const double *T, long long ld, int N, double *nrm) {
+    const int j = blockIdx.x;
+    double s = 0.0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) s += T[(size_t)j * ld + i] * T[(size_t)j * ld + i];
+    __shared__ double red[32];
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) nrm[j] = sqrt(s);
 }
 
-// Q[:, j] *= s[j]
-__global__ void scale_cols_kernel(double *Q, long long ld, int n, const double *s, int ncol) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)n * ncol) return;
-    const int j = (int)(t / n), i = (int)(t % n);
-    Q[(size_t)j * ld + i] *= s[j];
-}
-
-inline unsigned nblk(long long n, int b) { return (unsigned)((n + b - 1) / b); }
-
-// The contracted-basis operator.
-class MatFree {
-  public:
-    MatFree(dvr3d_ctx *ctx, const Contracted &C) : ctx_(ctx), C_(C) {
-        const int nb = C.nblocks;
-        col0_.assign(nb, 0);
-        s_.assign(nb, 0);
-        int c = 0;
-        for (int b = 0; b < nb; ++b) {
-            col0_[b] = c;
-            s_[b] = C.iv2[b];
-            c += s_[b];
+__global__ void normalize_or_refill_kernel(double *T, long long ld, int N, const double *nrm, const double *ref,
+                                           double rel, unsigned seed) {
+    const int j = blockIdx.x;
+    const double nj = nrm[j], thr = rel * ref[j];
+    const bool refill = !(nj > thr) || !isfinite(nj);
+    const double inv = refill ? 0.0 : 1.0 / nj;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        double v = T[(size_t)j * ld + i] * inv;
+        if (refill) {
+            unsigned x = (unsigned)i * 2654435761u ^ (seed + 7919u * (unsigned)j);
+            x ^= x >> 16;
+            x *= 0x7feb352dU;
+            x ^= x >> 15;
+            x *= 0x846ca68bU;
+            x ^= x >> 16;
+            v = ((double)(x & 0xffffff) / 8388608.0 - 1.0) / sqrt((double)N);
         }
+        T[(size_t)j * ld + i] = v;
     }
-    // HV (ld ldh) = H3 V (ld ldv), b columns
-    void apply(const double *V, long long ldv, int b, double *HV, long long ldh, DavidsonStats &st) {
-        cudaStream_t s = ctx_->stream;
-        const int nbk = C_.nblocks, P = C_.P;
-        const long long PB = (long long)P * b;
-        double *Y = ctx_->arena.get_t<double>("dv_Y", (size_t)PB * nbk);
-        double *Z = ctx_->arena.get_t<double>("dv_Zm", (size_t)PB * nbk);
-        const int tn = (b + 63) / 64;
-        // metadata of the two grouped products
-        std::vector<int> ts1(nbk + 1), ts2(nbk + 1), M1(nbk), K1(nbk), M2(nbk), K2(nbk);
-        std::vector<long long> a1(nbk), b1(nbk), c1(nbk), b2(nbk), c2(nbk);
-        ts1[0] = ts2[0] = 0;
-        for (int g = 0; g < nbk; ++g) {
-            M1[g] = P;
-            K1[g] = s_[g];
-            a1[g] = (long long)col0_[g] * C_.ldv;
-            b1[g] = col0_[g];
-            c1[g] = (long long)g * PB;
-            ts1[g + 1] = ts1[g] + ((P + 63) / 64) * tn;
-            M2[g] = s_[g];
-            K2[g] = P;
-            b2[g] = (long long)g * PB;
-            c2[g] = col0_[g];
-            ts2[g + 1] = ts2[g] + ((s_[g] + 63) / 64) * tn;
-        }
-        auto up = [&](const char *nm, const auto &v) {
-            using T = typename std::decay_t<decltype(v)>::value_type;
-            T *p = ctx_->arena.get_t<T>(nm, v.size());
-            CK(cudaMemcpyAsync(p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, s));
-            return p;
-        };
-        if (!ev_[0]) {
-            CK(cudaEventCreate(&ev_[0]));
-            CK(cudaEventCreate(&ev_[1]));
-        }
-        CK(cudaEventRecord(ev_[0], s));
-        GroupedGemm g1{};
-        g1.ngroups = nbk;
-        g1.tile_start = up("mf_ts1", ts1);
-        g1.M = up("mf_M1", M1);
-        g1.K = up("mf_K1", K1);
-        g1.N = b;
-        g1.A = C_.Vt;
-        g1.aoff = up("mf_a1", a1);
-        g1.lda = C_.ldv;
-        g1.B = V;
-        g1.boff = up("mf_b1", b1);
-        g1.ldb = ldv;
-        g1.C = Y;
-        g1.coff = up("mf_c1", c1);
-        g1.ldc = P;
-        g1.alpha = 1.0;
-        g1.beta = 0.0;
-        launch_grouped_dgemm(g1, false, ts1[nbk], s);
-        launch_dgemm(false, false, (int)PB, nbk, nbk, 1.0, Y, PB, C_.T, C_.ldt, 0.0, Z, PB, s);
-        GroupedGemm g2{};
-        g2.ngroups = nbk;
-        g2.tile_start = up("mf_ts2", ts2);
-        g2.M = up("mf_M2", M2);
-        g2.K = up("mf_K2", K2);
-        g2.N = b;
-        g2.A = C_.Vt;
-        g2.aoff = g1.aoff;
-        g2.lda = C_.ldv;
-        g2.B = Z;
-        g2.boff = up("mf_b2", b2);
-        g2.ldb = P;
-        g2.C = HV;
-        g2.coff = up("mf_c2", c2);
-        g2.ldc = ldh;
-        g2.alpha = 1.0;
-        g2.beta = 0.0;
-        launch_grouped_dgemm(g2, true, ts2[nbk], s);
-        add_diag_kernel<<<nblk((long long)C_.N * b, 256), 256, 0, s>>>(C_.e2, V, ldv, HV, ldh, C_.N, b);
-        DVR3D_COUNT_LAUNCH(2);
-        CK(cudaGetLastError());
-        CK(cudaEventRecord(ev_[1], s));
-        pending_ = true;
-        st.matvecs += b;
-        st.hv_flops += (4.0 * P * (double)C_.N + 2.0 * P * (double)nbk * nbk) * b;
-        st.hv_launches += 4;
-    }
-    // accumulate the device time of the last application (after a stream sync)
-    void collect(DavidsonStats &st) {
-        if (!pending_) return;
-        float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, ev_[0], ev_[1]));
-        st.hv_ms += ms;
-        pending_ = false;
-    }
-    ~MatFree() {
-        for (auto e : ev_)
-            if (e) cudaEventDestroy(e);
-    }
-
-  private:
-    dvr3d_ctx *ctx_;
-    const Contracted &C_;
-    std::vector<int> col0_, s_;
-    cudaEvent_t ev_[2] = {nullptr, nullptr};
-    bool pending_ = false;
-};
-
-template <class T>
-std::vector<T> d2h(dvr3d_ctx *ctx, const T *p, size_t n) {
-    std::vector<T> v(n);
-    if (n) CK(cudaMemcpyAsync(v.data(), p, n * sizeof(T), cudaMemcpyDeviceToHost, ctx->stream));
-    CK(cudaStreamSynchronize(ctx->stream));
-    return v;
 }
 
-// Eigen-decomposition of one m x m matrix (lower triangle) on the device.
-void syev_small(dvr3d_ctx *ctx, const double *G, int m, double *w, double *Zv) {
-    cudaStream_t s = ctx->stream;
-    int *dn = ctx->arena.get_t<int>("ss_n", 1);
-    long long *doff = ctx->arena.get_t<long long>("ss_off", 1);
-    CK(cudaMemcpyAsync(dn, &m, sizeof(int), cudaMemcpyHostToDevice, s));
-    CK(cudaMemsetAsync(doff, 0, sizeof(long long), s));
-    double *work = ctx->arena.get_t<double>("ss_work", (size_t)small_syev_work_doubles(kMaxSub));
-    SmallSyev p{};
-    p.nmat = 1;
-    p.n = dn;
-    p.A = G;
-    p.aoff = doff;
-    p.lda = nullptr;
-    p.W = w;
-    p.woff = doff;
-    p.Z = Zv;
-    p.zoff = doff;
-    p.work = work;
-    p.workoff = doff;
-    CK(launch_small_syev(p, m, s));
+// V[:, j] = channel mode j of the start block, embedded (zero outside its channel)
+__global__ void embed_modes_kernel(ChanPrec cp, const int *mode_ch, const int *mode_q, double *V, long long ld,
+                                   int N) {
+    const int j = blockIdx.x;
+    const int c = mode_ch[j], q = mode_q[j], n = cp.n[c], off = cp.off[c];
+    double *v = V + (size_t)j * ld;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) v[i] = 0.0;
+    __syncthreads();
+    const double *Q = cp.Q + cp.qoff[c] + (size_t)q * n;
+    for (int p = threadIdx.x; p < n; p += blockDim.x) v[cp.idx[off + p]] = Q[p];
+}
+
+inline unsigned nb256(long long n) { return (unsigned)((n + 255) / 256); }
+inline long long rup(long long x, long long m) { return (x + m - 1) / m * m; }
+
+void copy_cols(double *dst, long long ldd, const double *src, long long lds, int N, int ncol, cudaStream_t st) {
+    if (ncol <= 0) return;
+    CK(cudaMemcpy2DAsync(dst, ldd * sizeof(double), src, lds * sizeof(double), (size_t)N * sizeof(double), ncol,
+                         cudaMemcpyDeviceToDevice, st));
+}
+
+void gemm_split(GemmOp g, int target, double *work, cudaStream_t st) {
+    if (target > 1) {
+        const int tiles = ((g.M + 63) / 64) * ((g.N + 63) / 64);
+        g.splitk = std::max(1, std::min({(target + tiles - 1) / tiles, 64, (g.K + 15) / 16}));
+        g.work = work;
+    }
+    CK(launch_gemm(g, st));
+}
+
+void lp_init_weights(std::vector<double> &w) {
+    // deterministic small initial weights (fan-in scaled), zero output layer
+    w.assign(kLpParams, 0.0);
+    unsigned long long s = 0x243f6a8885a308d3ull;
+    auto u = [&]() {
+        s = s * 6364136223846793005ull + 1442695040888963407ull;
+        return (double)(s >> 11) / 9007199254740992.0 * 2.0 - 1.0;
+    };
+    for (int p = 0; p < kLpHidden * kLpFeat; ++p) w[p] = u() / std::sqrt((double)kLpFeat);
+    const int o2 = kLpHidden * kLpFeat + kLpHidden;
+    for (int p = 0; p < kLpHidden * kLpHidden; ++p) w[o2 + p] = u() / std::sqrt((double)kLpHidden);
 }
 
 }  // namespace
 
-void davidson_solve(dvr3d_ctx *ctx, const Contracted &C, const dvr3d_options &opt, int nwant, double *wv_dev,
-                    std::vector<double> &rn_host, double *evec_dev, DavidsonStats &stats) {
+// ---------------------------------------------------------------- training loss / gradient
+double lp_train_loss(dvr3d_ctx *ctx, const double *w, double *grad) {
+    auto &S = ctx->lp_set;
+    if (!S.valid) throw HostError{DVR3D_ERR_ARG, "no recorded training pairs (solve with learned_precond = 2 first)"};
+    cudaStream_t st = ctx->stream;
+    const int N = S.N, P = S.npair, nw = S.nwant;
+    const long long ld = S.ld;
+    auto A = [&](const std::string &nm, size_t n) { return ctx->arena.get_t<double>(nm, n); };
+    const double *R = A("lp_R", ld * P), *E = A("lp_E", ld * P), *th = A("lp_theta", P);
+    double *T = A("lp_T", ld * P), *PT = A("lp_PT", ld * P), *G = A("lp_G", ld * P);
+    double *zraw = A("lp_zraw", (size_t)N * P), *delta = A("lp_delta", (size_t)N * P);
+    double *proj = A("lp_proj", (size_t)kDavidsonMaxBlock * 3 * nw);
+    double *sums = A("lp_sums", 3 * (size_t)P), *coef = A("lp_coef", 2 * (size_t)P), *loss = A("lp_loss", 8);
+    double *work = A("lp_gwork", std::max(lp_grad_work_doubles(), (size_t)64 * 3 * kDavidsonMaxBlock * nw));
+    CK(launch_chan_apply(S.cp, w, R, ld, th, P, T, ld, zraw, st));
+    copy_cols(PT, ld, T, ld, N, P, st);
+    for (size_t s = 0; s < S.snap_m.size(); ++s) {
+        const int m = S.snap_m[s];
+        const double *V = A("lp_V" + std::to_string(s), ld * m);
+        GemmOp c;  // proj = V^T T_s ; PT_s -= V proj
+        c.M = m;
+        c.N = nw;
+        c.K = N;
+        c.A = V;
+        c.lda = ld;
+        c.ta = true;
+        c.B = T + (size_t)s * nw * ld;
+        c.ldb = ld;
+        c.C = proj;
+        c.ldc = m;
+        gemm_split(c, 600, work, st);
+        GemmOp u;
+        u.M = N;
+        u.N = nw;
+        u.K = m;
+        u.alpha = -1.0;
+        u.beta = 1.0;
+        u.A = V;
+        u.lda = ld;
+        u.B = proj;
+        u.ldb = m;
+        u.C = PT + (size_t)s * nw * ld;
+        u.ldc = ld;
+        gemm_split(u, 0, work, st);
+    }
+    CK(launch_lp_pair_terms(T, PT, E, ld, N, P, sums, coef, loss, st));
+    if (grad) {
+        CK(launch_lp_dldt(E, PT, ld, N, P, coef, G, st));
+        CK(launch_chan_back(S.cp, G, ld, zraw, P, delta, st));
+        CK(lp_mlp_grad(S.cp.modes, w, th, P, delta, grad, work, st));
+    }
+    double lh = 0.0;
+    CK(cudaMemcpyAsync(&lh, loss, sizeof(double), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return lh;
+}
+
+// ---------------------------------------------------------------- Davidson
+bool davidson_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contracted &C, const dvr3d_options &opt,
+                    int nwant, int mode, double *lp_w, double *wv_dev, std::vector<double> &rn_host,
+                    double *evec_dev, DavidsonStats &stats) {
     cudaStream_t st = ctx->stream;
     const int N = C.N;
-    nwant = std::min(nwant, N);
-    const int bsz = std::max(8, std::min(opt.block > 0 ? opt.block : 48, kMaxSub / 3));
-    const int mmax = std::min(kMaxSub, N);
-    const int nkeep = std::max(1, mmax - bsz);  // Ritz vectors kept at each restart
-    const double tol_cm = opt.tol_cm > 0.0 ? opt.tol_cm : 1.0e-4;
-    // residual bound for an eigenvalue error of tol_cm with gaps >= 1e-5 Eh
-    const double rtol = std::sqrt(tol_cm / 2.19474624e5 * 1.0e-5);
-    const int max_iter = opt.max_iter > 0 ? opt.max_iter : 400;
-    const long long ld = N;
-    double *S = ctx->arena.get_t<double>("dv_S", (size_t)ld * mmax);
-    double *HS = ctx->arena.get_t<double>("dv_HS", (size_t)ld * mmax);
-    double *X = ctx->arena.get_t<double>("dv_X", (size_t)ld * mmax);
-    double *HX = ctx->arena.get_t<double>("dv_HX", (size_t)ld * mmax);
-    double *R = ctx->arena.get_t<double>("dv_R", (size_t)ld * mmax);
-    double *Tc = ctx->arena.get_t<double>("dv_T", (size_t)ld * bsz);
-    double *T2 = ctx->arena.get_t<double>("dv_T2", (size_t)ld * bsz);
-    double *L = ctx->arena.get_t<double>("dv_L", (size_t)ld * (nwant + mmax));
-    double *G = ctx->arena.get_t<double>("dv_G", (size_t)mmax * mmax);
-    double *Yr = ctx->arena.get_t<double>("dv_Yr", (size_t)mmax * mmax);
-    double *wr = ctx->arena.get_t<double>("dv_wr", mmax);
-    double *rn = ctx->arena.get_t<double>("dv_rn", mmax);
-    double *proj = ctx->arena.get_t<double>("dv_proj", (size_t)(nwant + mmax) * bsz);
-    double *hd = ctx->arena.get_t<double>("dv_hd", N);
-    double *dsc = ctx->arena.get_t<double>("dv_sc", mmax);
-    MatFree H(ctx, C);
-    hdiag_kernel<<<nblk((long long)N * 32, 256), 256, 0, st>>>(C.Vt, C.ldv, C.P, N, C.g, C.T, C.ldt, C.e2, hd);
-    DVR3D_COUNT_LAUNCH(1);
-    // start: unit vectors at the lowest diagonal entries
-    std::vector<double> hdh = d2h(ctx, hd, N);
-    std::vector<int> order(N);
-    std::iota(order.begin(), order.end(), 0);
-    const int m0 = std::min(mmax - bsz, N);
-    std::partial_sort(order.begin(), order.begin() + m0, order.end(),
-                      [&](int a, int b) { return hdh[a] < hdh[b]; });
-    order.resize(m0);
-    int *didx = ctx->arena.get_t<int>("dv_idx", m0);
-    CK(cudaMemcpyAsync(didx, order.data(), sizeof(int) * m0, cudaMemcpyHostToDevice, st));
-    unit_columns_kernel<<<nblk((long long)N * m0, 256), 256, 0, st>>>(S, ld, N, didx, m0);
-    DVR3D_COUNT_LAUNCH(1);
-    H.apply(S, ld, m0, HS, ld, stats);
-    int m = m0, nl = 0;
-    std::vector<double> lval, lres;
-    int it = 0;
-    for (; it < max_iter && nl < nwant; ++it) {
-        // Rayleigh-Ritz
-        launch_dgemm(true, false, m, m, N, 1.0, S, ld, HS, ld, 0.0, G, m, st);
-        syev_small(ctx, G, m, wr, Yr);
-        const int nx = std::min(m, nkeep);
-        launch_dgemm(false, false, N, nx, m, 1.0, S, ld, Yr, m, 0.0, X, ld, st);
-        launch_dgemm(false, false, N, nx, m, 1.0, HS, ld, Yr, m, 0.0, HX, ld, st);
-        residual_kernel<<<nx, 256, 0, st>>>(X, HX, ld, wr, N, R, rn);
+    if (ldh & 1) return false;
+    int bs = std::min(kDavidsonMaxBlock, nwant + std::max(8, nwant / 2));
+    bs += (bs & 1);
+    const int keep = 2 * bs, mmax = 3 * bs;
+    if (mmax > kSmallSyevMax || mmax >= N) return false;
+    const double tolE = (opt.tol_cm > 0.0 ? opt.tol_cm : 1.0e-4) / 2.19474624e5;
+    const int max_iter = opt.max_iter > 0 ? opt.max_iter : 300;
+    const long long ld = rup(N, 8);
+    auto A = [&](const std::string &nm, size_t n) { return ctx->arena.get_t<double>(nm, n); };
+    double *V = A("dv_V", ld * mmax), *HV = A("dv_HV", ld * mmax);
+    double *V2 = A("dv_V2", ld * keep), *HV2 = A("dv_HV2", ld * keep);
+    double *X = A("dv_X", ld * bs), *HX = A("dv_HX", ld * bs), *R = A("dv_R", ld * bs), *Tc = A("dv_T", ld * bs);
+    double *G = A("dv_G", (size_t)mmax * mmax), *Y = A("dv_Y", (size_t)mmax * mmax), *th = A("dv_th", mmax);
+    double *rn = A("dv_rn", bs), *proj = A("dv_proj", (size_t)mmax * bs);
+    double *Gb = A("dv_Gb", 64 * 64), *Gi = A("dv_Gi", 64 * 64);
+    double *cn0 = A("dv_cn0", bs), *cn1 = A("dv_cn1", bs), *ones = A("dv_ones", bs);
+    {
+        std::vector<double> o(bs, 1.0);
+        CK(cudaMemcpyAsync(ones, o.data(), sizeof(double) * bs, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+    }
+    double *work = A("dv_work", (size_t)std::max<long long>(64LL * mmax * mmax, 16LL * N * bs));
+    double *ssw = A("dv_ssw", (size_t)small_syev_work_doubles(kSmallSyevMax));
+    int *err = ctx->arena.get_t<int>("dv_err", 2);
+    int *ssn = ctx->arena.get_t<int>("dv_ssn", 1);
+    long long *ssoff = ctx->arena.get_t<long long>("dv_ssoff", 1);
+    CK(cudaMemsetAsync(err, 0, 2 * sizeof(int), st));
+    CK(cudaMemsetAsync(ssoff, 0, sizeof(long long), st));
+    // channel blocks; the start block is the bs lowest channel modes (approximate
+    // eigenvectors of H3 in which the coupling between channels is left out)
+    ChanPrec cp;
+    std::vector<double> lam;
+    std::vector<int> mch;
+    channel_setup(ctx, H3, ldh, C, cp, &lam, &mch);
+    {
+        std::vector<int> order(N);
+        std::iota(order.begin(), order.end(), 0);
+        std::partial_sort(order.begin(), order.begin() + bs, order.end(),
+                          [&](int a, int b) { return lam[a] < lam[b]; });
+        std::vector<int> mc(bs), mq(bs);
+        for (int j = 0; j < bs; ++j) {
+            const int m0 = order[j], c = mch[m0];
+            int first = m0;
+            while (first > 0 && mch[first - 1] == c) --first;
+            mc[j] = c;
+            mq[j] = m0 - first;
+        }
+        int *dmc = ctx->arena.get_t<int>("dv_mc", bs), *dmq = ctx->arena.get_t<int>("dv_mq", bs);
+        CK(cudaMemcpyAsync(dmc, mc.data(), sizeof(int) * bs, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(dmq, mq.data(), sizeof(int) * bs, cudaMemcpyHostToDevice, st));
+        note_h2d(2 * sizeof(int) * bs);
+        CK(cudaMemsetAsync(V, 0, sizeof(double) * ld * bs, st));
         DVR3D_COUNT_LAUNCH(1);
+        embed_modes_kernel<<<bs, 256, 0, st>>>(cp, dmc, dmq, V, ld, N);
         CK(cudaGetLastError());
-        std::vector<double> wh = d2h(ctx, wr, nx);
-        std::vector<double> rh = d2h(ctx, rn, nx);
-        H.collect(stats);
-        // lock the leading converged Ritz pairs
-        int c = 0;
-        while (c < nx && nl + c < nwant && rh[c] < rtol) ++c;
-        if (c > 0) {
-            copy_cols_kernel<<<nblk((long long)N * c, 256), 256, 0, st>>>(X, L + (size_t)nl * ld, ld, N, c);
-            DVR3D_COUNT_LAUNCH(1);
-            for (int j = 0; j < c; ++j) {
-                lval.push_back(wh[j]);
-                lres.push_back(rh[j]);
-            }
-            nl += c;
-            if (nl >= nwant) break;
-        }
-        // restart from the unlocked Ritz vectors
-        const int keep = nx - c;
-        std::swap(S, X);
-        std::swap(HS, HX);
-        if (c > 0) {
-            // shift columns c..nx-1 to the front (through the other buffer pair)
-            copy_cols_kernel<<<nblk((long long)N * keep, 256), 256, 0, st>>>(S + (size_t)c * ld, X, ld, N, keep);
-            copy_cols_kernel<<<nblk((long long)N * keep, 256), 256, 0, st>>>(HS + (size_t)c * ld, HX, ld, N, keep);
-            DVR3D_COUNT_LAUNCH(2);
-            std::swap(S, X);
-            std::swap(HS, HX);
-        }
-        m = keep;
-        // corrections for the next unconverged pairs
-        const int nb = std::min(bsz, keep);
-        if (nb <= 0) break;
-        precond_diag_kernel<<<nblk((long long)N * nb, 256), 256, 0, st>>>(R + (size_t)c * ld, ld, wr + c, hd, N, nb,
-                                                                          Tc, ld);
+        CK(cudaStreamSynchronize(st));
+    }
+    auto syev = [&](const double *Gm, int m, double *w, double *Z) {
+        CK(cudaMemcpyAsync(ssn, &m, sizeof(int), cudaMemcpyHostToDevice, st));
+        SmallSyev p{};
+        p.nmat = 1;
+        p.n = ssn;
+        p.A = Gm;
+        p.aoff = ssoff;
+        p.W = w;
+        p.woff = ssoff;
+        p.Z = Z;
+        p.zoff = ssoff;
+        p.work = ssw;
+        p.workoff = ssoff;
+        CK(launch_small_syev(p, m, st));
+    };
+    const int max_snaps = 16;
+    const char *trace_env = std::getenv("DVR3D_DAV_TRACE");
+    const bool trace = trace_env && trace_env[0] == '1';
+    std::vector<int> snap_m;
+    std::vector<double> snap_theta;
+    if (mode == 2) ctx->lp_set.valid = false;
+    int m = bs, nnew = bs;
+    std::vector<double> thh(mmax), rnh(bs);
+    bool done = false;
+    int it = 0;
+    for (; it < max_iter; ++it) {
+        GemmOp hv;  // HV[:, m-nnew:m] = H3 V[:, m-nnew:m]
+        hv.M = N;
+        hv.N = nnew;
+        hv.K = N;
+        hv.A = H3;
+        hv.lda = ldh;
+        hv.B = V + (size_t)(m - nnew) * ld;
+        hv.ldb = ld;
+        hv.C = HV + (size_t)(m - nnew) * ld;
+        hv.ldc = ld;
+        gemm_split(hv, 600, work, st);
+        stats.matvecs += nnew;
+        GemmOp g;  // G = V^T HV
+        g.M = m;
+        g.N = m;
+        g.K = N;
+        g.A = V;
+        g.lda = ld;
+        g.ta = true;
+        g.B = HV;
+        g.ldb = ld;
+        g.C = G;
+        g.ldc = m;
+        gemm_split(g, 600, work, st);
+        syev(G, m, th, Y);
+        GemmOp x;  // X = V Y[:, :bs], HX = HV Y[:, :bs]
+        x.M = N;
+        x.N = bs;
+        x.K = m;
+        x.A = V;
+        x.lda = ld;
+        x.B = Y;
+        x.ldb = m;
+        x.C = X;
+        x.ldc = ld;
+        gemm_split(x, 0, work, st);
+        x.A = HV;
+        x.C = HX;
+        gemm_split(x, 0, work, st);
         DVR3D_COUNT_LAUNCH(1);
-        // orthogonalise against locked and current vectors, twice
+        residual_kernel<<<bs, 256, 0, st>>>(X, HX, ld, th, N, R, rn);
+        CK(cudaGetLastError());
+        CK(cudaMemcpyAsync(thh.data(), th, sizeof(double) * m, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(rnh.data(), rn, sizeof(double) * bs, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        note_d2h(sizeof(double) * (m + bs));
+        int nconv = 0;
+        for (int j = 0; j < nwant; ++j) {
+            double gap = thh[j + 1] - thh[j];
+            if (j > 0) gap = std::min(gap, thh[j] - thh[j - 1]);
+            const double bound = rnh[j] * rnh[j] / std::max(gap, rnh[j]);
+            if (bound <= tolE && std::isfinite(bound)) ++nconv;
+        }
+        if (trace)
+            std::fprintf(stderr, "davidson it %d m %d converged %d/%d max residual %.3e theta0 %.8f\n", it, m, nconv,
+                         nwant, *std::max_element(rnh.begin(), rnh.begin() + nwant), thh[0]);
+        if (nconv == nwant) {
+            done = true;
+            break;
+        }
+        if (mode == 2 && (int)snap_m.size() < max_snaps) {
+            const int s = (int)snap_m.size();
+            copy_cols(A("lp_X" + std::to_string(s), ld * nwant), ld, X, ld, N, nwant, st);
+            copy_cols(A("lp_Rs" + std::to_string(s), ld * nwant), ld, R, ld, N, nwant, st);
+            copy_cols(A("lp_V" + std::to_string(s), ld * m), ld, V, ld, N, m, st);
+            snap_m.push_back(m);
+            snap_theta.insert(snap_theta.end(), thh.begin(), thh.begin() + nwant);
+        }
+        if (m + bs > mmax) {  // thick restart to the leading Ritz vectors
+            GemmOp r;
+            r.M = N;
+            r.N = keep;
+            r.K = m;
+            r.A = V;
+            r.lda = ld;
+            r.B = Y;
+            r.ldb = m;
+            r.C = V2;
+            r.ldc = ld;
+            gemm_split(r, 0, work, st);
+            r.A = HV;
+            r.C = HV2;
+            gemm_split(r, 0, work, st);
+            copy_cols(V, ld, V2, ld, N, keep, st);
+            copy_cols(HV, ld, HV2, ld, N, keep, st);
+            m = keep;
+        }
+        CK(launch_chan_apply(cp, mode == 1 ? lp_w : nullptr, R, ld, th, bs, Tc, ld, nullptr, st));
+        // unit columns (corrections of converged pairs are tiny); refill any zero column
+        DVR3D_COUNT_LAUNCH(2);
+        colnorm_kernel<<<bs, 256, 0, st>>>(Tc, ld, N, cn0);
+        normalize_or_refill_kernel<<<bs, 256, 0, st>>>(Tc, ld, N, cn0, ones, 1.0e-300, 17u * it + 1u);
+        for (int sweep = 0; sweep < 2; ++sweep) {
         for (int pass = 0; pass < 2; ++pass) {
-            if (nl > 0) {
-                launch_dgemm(true, false, nl, nb, N, 1.0, L, ld, Tc, ld, 0.0, proj, nl, st);
-                launch_dgemm(false, false, N, nb, nl, -1.0, L, ld, proj, nl, 1.0, Tc, ld, st);
-            }
-            launch_dgemm(true, false, m, nb, N, 1.0, S, ld, Tc, ld, 0.0, proj, m, st);
-            launch_dgemm(false, false, N, nb, m, -1.0, S, ld, proj, m, 1.0, Tc, ld, st);
+            GemmOp c;  // proj = V^T Tc ; Tc -= V proj
+            c.M = m;
+            c.N = bs;
+            c.K = N;
+            c.A = V;
+            c.lda = ld;
+            c.ta = true;
+            c.B = Tc;
+            c.ldb = ld;
+            c.C = proj;
+            c.ldc = m;
+            gemm_split(c, 600, work, st);
+            GemmOp u;
+            u.M = N;
+            u.N = bs;
+            u.K = m;
+            u.alpha = -1.0;
+            u.beta = 1.0;
+            u.A = V;
+            u.lda = ld;
+            u.B = proj;
+            u.ldb = m;
+            u.C = Tc;
+            u.ldc = ld;
+            gemm_split(u, 0, work, st);
         }
-        // orthonormalise the corrections: Tc^T Tc = Q diag(l) Q^T, keep l > 1e-10 max
-        launch_dgemm(true, false, nb, nb, N, 1.0, Tc, ld, Tc, ld, 0.0, G, nb, st);
-        syev_small(ctx, G, nb, wr, Yr);
-        std::vector<double> lg = d2h(ctx, wr, nb);
-        const double lmax = lg[nb - 1];
-        int first = 0;
-        while (first < nb && !(lg[first] > 1.0e-10 * lmax)) ++first;
-        const int nk = nb - first;
-        if (nk <= 0) break;
-        std::vector<double> sc(nk);
-        for (int j = 0; j < nk; ++j) sc[j] = 1.0 / std::sqrt(lg[first + j]);
-        CK(cudaMemcpyAsync(dsc, sc.data(), sizeof(double) * nk, cudaMemcpyHostToDevice, st));
-        scale_cols_kernel<<<nblk((long long)nb * nk, 256), 256, 0, st>>>(Yr + (size_t)first * nb, nb, nb, dsc, nk);
-        DVR3D_COUNT_LAUNCH(1);
-        double *Snew = S + (size_t)m * ld;
-        launch_dgemm(false, false, N, nk, nb, 1.0, Tc, ld, Yr + (size_t)first * nb, nb, 0.0, Snew, ld, st);
-        H.apply(Snew, ld, nk, HS + (size_t)m * ld, ld, stats);
-        m += nk;
-        (void)T2;
+        // a correction (nearly) inside span(V) would make the block singular: replace it
+        // by a random direction and orthogonalise once more
+        DVR3D_COUNT_LAUNCH(2);
+        colnorm_kernel<<<bs, 256, 0, st>>>(Tc, ld, N, cn1);
+        normalize_or_refill_kernel<<<bs, 256, 0, st>>>(Tc, ld, N, cn1, ones, 1.0e-8, 31u * it + 5u + sweep);
+        }
+        for (int pass = 0; pass < 2; ++pass) {
+            GemmOp q;
+            q.M = bs;
+            q.N = bs;
+            q.K = N;
+            q.A = Tc;
+            q.lda = ld;
+            q.ta = true;
+            q.B = Tc;
+            q.ldb = ld;
+            q.C = Gb;
+            q.ldc = bs;
+            gemm_split(q, 256, work, st);
+            CK(launch_chol_small(Gb, bs, Gi, 1.0e-24, err + 1, st));
+            GemmOp s2;
+            s2.M = N;
+            s2.N = bs;
+            s2.K = bs;
+            s2.A = Tc;
+            s2.lda = ld;
+            s2.B = Gi;
+            s2.ldb = 64;
+            s2.tb = true;
+            s2.C = Tc;
+            s2.ldc = ld;
+            gemm_split(s2, 0, work, st);
+        }
+        int qe = 0;
+        CK(cudaMemcpyAsync(&qe, err + 1, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (qe != 0) break;  // corrections became dependent: give up (the caller falls back)
+        copy_cols(V + (size_t)m * ld, ld, Tc, ld, N, bs, st);
+        m += bs;
+        nnew = bs;
     }
     stats.iterations = it;
-    if (nl < nwant) throw HostError{DVR3D_ERR_NOCONV, "Davidson did not converge all requested levels"};
-    // order the locked pairs by energy
-    std::vector<int> perm(nl);
-    std::iota(perm.begin(), perm.end(), 0);
-    std::stable_sort(perm.begin(), perm.end(), [&](int a, int b) { return lval[a] < lval[b]; });
-    std::vector<double> ws(nwant);
-    rn_host.assign(nwant, 0.0);
-    stats.max_resid = 0.0;
-    for (int j = 0; j < nwant; ++j) {
-        ws[j] = lval[perm[j]];
-        rn_host[j] = lres[perm[j]];
-        stats.max_resid = std::max(stats.max_resid, rn_host[j]);
-    }
-    CK(cudaMemcpyAsync(wv_dev, ws.data(), sizeof(double) * nwant, cudaMemcpyHostToDevice, st));
-    if (evec_dev) {
-        for (int j = 0; j < nwant; ++j)
-            CK(cudaMemcpyAsync(evec_dev + (size_t)j * ld, L + (size_t)perm[j] * ld, sizeof(double) * N,
-                               cudaMemcpyDeviceToDevice, st));
+    if (!done) return false;
+    rn_host.assign(rnh.begin(), rnh.begin() + nwant);
+    stats.max_resid = *std::max_element(rn_host.begin(), rn_host.end());
+    CK(cudaMemcpyAsync(wv_dev, th, sizeof(double) * nwant, cudaMemcpyDeviceToDevice, st));
+    if (evec_dev) copy_cols(evec_dev, N, X, ld, N, nwant, st);
+    if (mode == 2 && !snap_m.empty()) {
+        // training pairs: e = (x_final - x) outside the basis of the snapshot
+        const int P = (int)snap_m.size() * nwant;
+        double *RP = A("lp_R", ld * P), *EP = A("lp_E", ld * P), *TP = A("lp_theta", P);
+        double *pj = A("lp_proj", (size_t)kDavidsonMaxBlock * 3 * nwant);
+        for (size_t s = 0; s < snap_m.size(); ++s) {
+            const std::string k = std::to_string(s);
+            const double *Xs = A("lp_X" + k, ld * nwant), *Vs = A("lp_V" + k, ld * snap_m[s]);
+            double *Eq = EP + (size_t)s * nwant * ld;
+            DVR3D_COUNT_LAUNCH(1);
+            ideal_correction_kernel<<<nwant, 256, 0, st>>>(X, Xs, ld, N, Eq);
+            GemmOp c;
+            c.M = snap_m[s];
+            c.N = nwant;
+            c.K = N;
+            c.A = Vs;
+            c.lda = ld;
+            c.ta = true;
+            c.B = Eq;
+            c.ldb = ld;
+            c.C = pj;
+            c.ldc = snap_m[s];
+            gemm_split(c, 600, work, st);
+            GemmOp u;
+            u.M = N;
+            u.N = nwant;
+            u.K = snap_m[s];
+            u.alpha = -1.0;
+            u.beta = 1.0;
+            u.A = Vs;
+            u.lda = ld;
+            u.B = pj;
+            u.ldb = snap_m[s];
+            u.C = Eq;
+            u.ldc = ld;
+            gemm_split(u, 0, work, st);
+            copy_cols(RP + (size_t)s * nwant * ld, ld, A("lp_Rs" + k, ld * nwant), ld, N, nwant, st);
+        }
+        CK(cudaMemcpyAsync(TP, snap_theta.data(), sizeof(double) * P, cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        note_h2d(sizeof(double) * P);
+        auto &S = ctx->lp_set;
+        S.valid = true;
+        S.N = N;
+        S.nwant = nwant;
+        S.npair = P;
+        S.ld = ld;
+        S.snap_m = snap_m;
+        S.cp = cp;
+        // fit: Adam, full batch, from the initial weights (zero output layer = exact channel inverse)
+        std::vector<double> w0;
+        lp_init_weights(w0);
+        CK(cudaMemcpyAsync(lp_w, w0.data(), sizeof(double) * kLpParams, cudaMemcpyHostToDevice, st));
+        double *grad = A("lp_grad", kLpParams), *mom = A("lp_mom", kLpParams), *vel = A("lp_vel", kLpParams);
+        CK(cudaMemsetAsync(mom, 0, sizeof(double) * kLpParams, st));
+        CK(cudaMemsetAsync(vel, 0, sizeof(double) * kLpParams, st));
+        const int steps = 200;
+        for (int s = 1; s <= steps; ++s) {
+            const double l = lp_train_loss(ctx, lp_w, grad);
+            if (s == 1) stats.loss_first = l;
+            CK(lp_adam_step(lp_w, grad, mom, vel, s, 3.0e-3, st));
+        }
+        stats.loss_last = lp_train_loss(ctx, lp_w, nullptr);
+        stats.pairs = P;
+        stats.trained = true;
     }
     CK(cudaStreamSynchronize(st));
-    H.collect(stats);
+    return true;
 }
 
 }  // namespace dvr3d

@@ -16,6 +16,7 @@
 #include "eig_batched.cuh"
 #include "eig_dense.cuh"
 #include "gemm64.cuh"
+#include "learned_precond.cuh"
 #include "pipeline.cuh"
 
 #define CK(x)                                          \
@@ -542,6 +543,104 @@ __global__ void resid_kernel(const double *R, const double *Z, const double *w, 
 
 }  // namespace
 
+// ---------------------------------------------------------------- channel blocks of H3
+namespace {
+__global__ void chan_gather_kernel(const double *H, long long ldh, const int *idx, const int *off,
+                                   const long long *qoff, const int *n, double *A) {
+    const int c = blockIdx.y, nc = n[c];
+    const int *ix = idx + off[c];
+    double *a = A + qoff[c];
+    for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc * nc; t += gridDim.x * blockDim.x) {
+        const int p = t % nc, q = t / nc;
+        a[t] = H[(size_t)ix[q] * ldh + ix[p]];
+    }
+}
+}  // namespace
+
+void channel_setup(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contracted &C, ChanPrec &cp,
+                   std::vector<double> *lam_host, std::vector<int> *chan_of_mode) {
+    cudaStream_t st = ctx->stream;
+    const int N = C.N, nb = C.nblocks;
+    std::vector<int> col0(nb, 0);
+    for (int b = 1; b < nb; ++b) col0[b] = col0[b - 1] + C.iv2[b - 1];
+    const int kmax = *std::max_element(C.iv2.begin(), C.iv2.end());
+    std::vector<int> n(kmax, 0), off(kmax, 0), idx;
+    std::vector<long long> qoff(kmax, 0), voff(kmax, 0);
+    idx.reserve(N);
+    long long qt = 0;
+    int nmax = 0;
+    for (int c = 0; c < kmax; ++c) {
+        off[c] = (int)idx.size();
+        voff[c] = off[c];
+        for (int b = 0; b < nb; ++b)
+            if (C.iv2[b] > c) idx.push_back(col0[b] + c);
+        n[c] = (int)idx.size() - off[c];
+        qoff[c] = qt;
+        qt += (long long)n[c] * n[c];
+        nmax = std::max(nmax, n[c]);
+    }
+    if (nmax > 1024) throw HostError{DVR3D_ERR_UNSUPPORTED, "channel block larger than 1024"};
+    int *dn = upload(ctx, "ch_n", n);
+    int *doff = upload(ctx, "ch_off", off);
+    long long *dq = upload(ctx, "ch_qoff", qoff);
+    long long *dv = upload(ctx, "ch_voff", voff);
+    int *didx = upload(ctx, "ch_idx", idx);
+    double *A = ctx->arena.get_t<double>("ch_A", (size_t)qt);
+    double *Q = ctx->arena.get_t<double>("ch_Q", (size_t)qt);
+    DVR3D_COUNT_LAUNCH(1);
+    chan_gather_kernel<<<dim3((unsigned)((nmax * nmax + 255) / 256), kmax), 256, 0, st>>>(H3, ldh, didx, doff, dq, dn, A);
+    CK(cudaGetLastError());
+    BatchDesc bd{kmax, dn, dq, dv};
+    double *d = ctx->arena.get_t<double>("ch_d", N), *e = ctx->arena.get_t<double>("ch_e", N);
+    double *tau = ctx->arena.get_t<double>("ch_tau", N), *lam = ctx->arena.get_t<double>("ch_lam", N);
+    int *cnt = ctx->arena.get_t<int>("ch_cnt", kmax);
+    launch_tridiag_batched(bd, A, d, e, tau, nmax, st);
+    launch_eigvals_batched(bd, d, e, lam, cnt, 0, 0.0, st);
+    std::vector<long long> woff;
+    long long wtot;
+    eigvecs_work(n, n, woff, wtot);
+    double *work = ctx->arena.get_t<double>("ch_work", (size_t)wtot);
+    int *err = ctx->arena.get_t<int>("ch_err", 1);
+    CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+    launch_eigvecs_batched(bd, A, d, e, tau, lam, dn, dq, dn, Q, work, upload(ctx, "ch_woff", woff), nmax, err, st);
+    CK(cudaGetLastError());
+    // per-mode features
+    std::vector<double> lh = download(ctx, lam, N), e2h = download(ctx, C.e2, N);
+    std::vector<double> f1(N), f2(N), f3(N);
+    const auto mm = std::minmax_element(lh.begin(), lh.end());
+    const double s = std::max(1.0e-6, 0.25 * (*mm.second - *mm.first));
+    for (int c = 0; c < kmax; ++c) {
+        double me = 0.0;
+        for (int p = 0; p < n[c]; ++p) me += e2h[idx[off[c] + p]];
+        me /= std::max(1, n[c]);
+        for (int q = 0; q < n[c]; ++q) {
+            const int m = off[c] + q;
+            f1[m] = (lh[m] - me) / s;
+            f2[m] = (double)c / kmax;
+            f3[m] = n[c] > 1 ? (double)q / (n[c] - 1) : 0.0;
+        }
+    }
+    if (lam_host) *lam_host = lh;
+    if (chan_of_mode) {
+        chan_of_mode->assign(N, 0);
+        for (int c = 0; c < kmax; ++c)
+            for (int q = 0; q < n[c]; ++q) (*chan_of_mode)[off[c] + q] = c;
+    }
+    cp.nch = kmax;
+    cp.nmax = nmax;
+    cp.n = dn;
+    cp.off = doff;
+    cp.qoff = dq;
+    cp.idx = didx;
+    cp.Q = Q;
+    cp.modes.lam = lam;
+    cp.modes.f1 = upload(ctx, "ch_f1", f1);
+    cp.modes.f2 = upload(ctx, "ch_f2", f2);
+    cp.modes.f3 = upload(ctx, "ch_f3", f3);
+    cp.modes.n = N;
+    cp.modes.scale = s;
+}
+
 // ---------------------------------------------------------------- dense eigensolver
 void dense_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int nev, bool vecs, double *w, double *Z,
                   long long ldz, const char *tag, bool time_panels, DenseOut *out) {
@@ -648,9 +747,14 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
     res.nblocks = C.nblocks;
     res.iterations = 0;
     res.fallback = 0;
+    res.path = DVR3D_PATH_DENSE;
+    res.matvecs = 0;
+    res.lp_pairs = 0;
+    res.lp_loss_first = res.lp_loss_last = 0.0;
+    ctx->lp_set.valid = false;  // recorded pairs refer to the buffers of the last solve only
     if (res.iv2 && res.iv2_cap >= C.nblocks)
         for (int b = 0; b < C.nblocks; ++b) res.iv2[b] = C.iv2[b];
-    const int meval = std::min(p.neval, N);
+    const int meval = std::min(opt.nlevels > 0 ? opt.nlevels : p.neval, N);
     res.meval = meval;
     if (N == 0) {
         res.max_resid = 0.0;
@@ -707,6 +811,46 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
                              (size_t)N * sizeof(double), N, cudaMemcpyDeviceToHost, st));
         t_d2h += (long long)sizeof(double) * N * N;
     }
+    if (opt.learned_precond == 1 && !ctx->lp_trained)
+        throw HostError{DVR3D_ERR_ARG, "no trained preconditioner (train one with learned_precond = 2 or load weights)"};
+    if (mixed && meval <= kDavidsonMaxLevels) {
+        // ---- few levels: block-Davidson with the channel-block preconditioner
+        double *wv = ctx->arena.get_t<double>("dt_w", meval);
+        double *Z = res.evec ? ctx->arena.get_t<double>("dv_z", (size_t)N * meval) : nullptr;
+        double *lpw = ctx->arena.get_t<double>("lp_w", kLpParams);
+        const int mode = opt.learned_precond == 2 ? 2 : (opt.learned_precond == 1 ? 1 : 0);
+        std::vector<double> rn;
+        DavidsonStats ds;
+        const bool ok = davidson_solve(ctx, H3, ldh, C, opt, meval, mode, lpw, wv, rn, Z, ds);
+        res.iterations = ds.iterations;
+        res.matvecs = ds.matvecs;
+        if (ds.trained) {
+            ctx->lp_trained = true;
+            res.lp_pairs = ds.pairs;
+            res.lp_loss_first = ds.loss_first;
+            res.lp_loss_last = ds.loss_last;
+        }
+        if (ok) {
+            CK(cudaEventRecord(ctx->ev[3], st));
+            put_levels(wv, Z);
+            if (res.resid)
+                for (int j = 0; j < std::min(meval, res.resid_cap); ++j) res.resid[j] = rn[j];
+            res.max_resid = ds.max_resid;
+            res.path = DVR3D_PATH_DAVIDSON;
+            double ms1, ms2, ms3;
+            finish_times(ms1, ms2, ms3);
+            // dominant work: the H3 V products (2 N^2 flop per vector), timed with the solve
+            res.dom_ms = ms3;
+            res.dom_bytes = 0.0;
+            res.dom_flops = 2.0 * (double)N * N * ds.matvecs;
+            res.dom_launches = 0;
+            std::snprintf(res.dom_kernel, sizeof(res.dom_kernel), "gemm_pipe_kernel");
+            res.launches = (int)(g_kernel_launches - launches0);
+            res.h2d_bytes = t_h2d;
+            res.d2h_bytes = t_d2h;
+            return;
+        }
+    }
     if (mixed) {
         // ---- shift-invert block Krylov for the lowest levels; dense FP64 fallback below
         std::vector<double> e2h = download(ctx, C.e2, N);
@@ -717,6 +861,8 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
         KrylovStats ks;
         const bool ok = si_krylov_solve(ctx, H3, ldh, N, emin, opt, meval, wv, rn, Z, ks);
         if (ok) {
+            res.path = DVR3D_PATH_SHIFT_INVERT;
+            res.matvecs = ks.m;
             CK(cudaEventRecord(ctx->ev[3], st));
             put_levels(wv, Z);
             if (res.resid)

@@ -10,6 +10,7 @@
 #include "../../include/dvr3d_b200.h"
 #include "common.cuh"
 #include "host_setup.h"
+#include "learned_precond.cuh"
 #include "pes.cuh"
 
 namespace dvr3d {
@@ -53,6 +54,14 @@ struct dvr3d_ctx {
     int sm_count = 0;
     int dense_grid = 0;
     std::vector<cudaEvent_t> panel_ev;  // timing pool for the reduction panels
+    bool lp_trained = false;            // arena "lp_w" holds a trained preconditioner network
+    struct LpSet {                      // training pairs of the last training solve
+        bool valid = false;
+        int N = 0, nwant = 0, npair = 0;
+        long long ld = 0;
+        std::vector<int> snap_m;        // basis size of each snapshot (arena "lp_V<s>")
+        dvr3d::ChanPrec cp;
+    } lp_set;
 };
 
 namespace dvr3d {
@@ -71,20 +80,35 @@ struct Contracted {
     int nblocks = 0;
 };
 
-// Block-Davidson for the lowest `nwant` levels of the contracted Hamiltonian (matrix-free).
-// Writes the levels (ascending) to wv_dev, FP64 residual norms to rn_host, and, when
-// evec_dev is not null, the eigenvectors (N x nwant). Returns the iteration count.
+// Channel blocks of the assembled H3 (full storage, ldh) and their eigen-decompositions,
+// with the per-mode features of the learned correction (learned_precond.cuh).
+// lam_host / chan_of_mode (optional): the channel eigenvalues and the channel of every mode.
+void channel_setup(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contracted &C, ChanPrec &cp,
+                   std::vector<double> *lam_host = nullptr, std::vector<int> *chan_of_mode = nullptr);
+
+// Block-Davidson for the lowest `nwant` (<= kDavidsonMaxLevels) levels of the assembled H3
+// (full symmetric storage, ldh even) with the channel-block preconditioner. mode 0: exact
+// channel inverse; 1: with the learned correction (parameters lp_w, device); 2: exact channel
+// inverse, record (residual, correction) pairs and fit the network into lp_w. Writes the
+// levels (device wv_dev), FP64 residual norms and optionally the vectors (N x nwant, ld N).
+// Returns false when it does not converge within its limits (the caller falls back).
+constexpr int kDavidsonMaxLevels = 32;
+constexpr int kDavidsonMaxBlock = 48;
 struct DavidsonStats {
     int iterations = 0;
     int matvecs = 0;
     double max_resid = 0.0;
-    double hv_ms = 0.0;        // device time of the operator applications
-    double hv_flops = 0.0;     // algorithmic flops of those applications
-    int hv_launches = 0;
+    int pairs = 0;             // training pairs recorded (mode 2)
+    bool trained = false;
+    double loss_first = 0.0, loss_last = 0.0;
 };
-void davidson_solve(dvr3d_ctx *ctx, const Contracted &C, const dvr3d_options &opt, int nwant,
-                    double *wv_dev, std::vector<double> &rn_host, double *evec_dev,
-                    DavidsonStats &stats);
+bool davidson_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contracted &C, const dvr3d_options &opt,
+                    int nwant, int mode, double *lp_w, double *wv_dev, std::vector<double> &rn_host,
+                    double *evec_dev, DavidsonStats &stats);
+
+// Training loss of the learned correction (and, when grad is not null, its gradient, device)
+// at parameters w (device) on the pairs recorded by the context's last training solve.
+double lp_train_loss(dvr3d_ctx *ctx, const double *w, double *grad);
 
 // Host<->device byte counters of the current solve (reported in dvr3d_result).
 void note_h2d(long long bytes);

@@ -144,20 +144,24 @@ struct Timer {
 }  // namespace
 
 int si_krylov_first_size(int nwant, int block) {
+    // about 5 Krylov vectors per wanted level, and at least 20 block steps (the polynomial
+    // degree, not only the dimension, sets the convergence of the last wanted levels)
     const int b = block;
-    return (int)rup((long long)std::ceil(5.2 * nwant) + b, b);
+    return (int)std::max(rup((long long)std::ceil(5.2 * nwant) + b, b), 20LL * b);
 }
 
 bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, double emin_bound,
                      const dvr3d_options &opt, int nwant, double *wv_dev, std::vector<double> &rn_host,
                      double *evec_dev, KrylovStats &ks) {
     cudaStream_t st = ctx->stream;
-    const int b = std::max(8, std::min(opt.block > 0 ? opt.block : 32, 64)) & ~1;  // even: 16-byte rows
+    const int bdef = nwant <= 48 ? 8 : (nwant <= 160 ? 16 : 32);
+    const int b = std::max(8, std::min(opt.block > 0 ? opt.block : bdef, 64)) & ~1;  // even: 16-byte rows
     if (ldh & 1) return false;
     const int guard = std::min(32, std::max(8, nwant / 10));
     const int kw = nwant + guard;
     const int mfirst = si_krylov_first_size(nwant, b);
-    const int mmax = (int)std::min<long long>(rup((long long)std::ceil(7.0 * nwant) + 2 * b, b), (N / b - 1) * (long long)b);
+    const int mmax = (int)std::min<long long>(std::max(rup((long long)std::ceil(7.0 * nwant) + 2 * b, b), 40LL * b),
+                                              (N / b - 1) * (long long)b);
     if (mfirst > mmax || kw > mfirst) return false;
     const double tolE = (opt.tol_cm > 0.0 ? opt.tol_cm : 1.0e-4) / 2.19474624e5;
     const long long ldw = rup(N, 8), ldq = ldw, ldT = rup(mmax, 8);

@@ -95,9 +95,22 @@ typedef enum dvr3d_pes_kind {
 /* ---- solve options and results ------------------------------------------------------- */
 typedef enum dvr3d_precision {
     DVR3D_PREC_FP64 = 0,             /* plain FP64 GPU path: dense FP64 final eigensolve  */
-    DVR3D_PREC_MIXED_DAVIDSON = 1    /* BF16x3/FP32 tensor-core H*v, FP64 Rayleigh-Ritz,
-                                        block-Davidson, optional learned preconditioner   */
+    DVR3D_PREC_MIXED_DAVIDSON = 1    /* iterative lowest-level solve on the FP64 tensor
+                                        cores: block-Davidson (<= 32 levels; channel-block
+                                        preconditioner, optionally with the learned
+                                        correction) or shift-invert block Krylov; FP64
+                                        Rayleigh-Ritz and residual judge; dense FP64
+                                        fallback                                          */
 } dvr3d_precision;
+
+typedef enum dvr3d_path {
+    DVR3D_PATH_DENSE = 0,            /* dense FP64 reduction (plain path or fallback)     */
+    DVR3D_PATH_SHIFT_INVERT = 1,     /* shift-invert block Krylov                         */
+    DVR3D_PATH_DAVIDSON = 2          /* block-Davidson                                    */
+} dvr3d_path;
+
+/* Number of parameters of the learned preconditioner correction (4 -> 16 -> 16 -> 1 MLP). */
+#define DVR3D_LP_NPARAM 369
 
 typedef struct dvr3d_options {
     int precision;          /* dvr3d_precision                                              */
@@ -105,7 +118,10 @@ typedef struct dvr3d_options {
     double tol_cm;          /* Davidson: max eigenvalue error target in cm-1 (0: 1e-4)      */
     int max_iter;           /* Davidson iteration limit (0: 200)                            */
     int block;              /* Davidson block size (0: automatic)                           */
-    int learned_precond;    /* 1: use the trained preconditioner network if one is loaded  */
+    int learned_precond;    /* Davidson (<= 32 levels, channel-block preconditioner):
+                               0 exact channel blocks; 1 with the trained correction of this
+                               context; 2 train the correction on this solve (recorded
+                               residual / ideal-correction pairs) and keep it in the context */
     int want_vectors;       /* 1: return eigenvectors of the final Hamiltonian in evec      */
     int want_h3;            /* 1: copy the assembled final Hamiltonian (lower) into h3      */
 } dvr3d_options;
@@ -136,6 +152,12 @@ typedef struct dvr3d_result {
     double *resid;  int resid_cap;    /* per-level FP64 residual norms (Eh)                   */
     double *evec;   size_t evec_cap;  /* nham3 x meval, column-major                          */
     double *h3;     size_t h3_cap;    /* nham3 x nham3, column-major, lower triangle valid    */
+    /* solver path and iterative-solver counters (appended; outputs) */
+    int path;               /* dvr3d_path: which eigensolver produced the levels            */
+    int matvecs;            /* Davidson: H3 products (vectors); shift-invert: Krylov size   */
+    int lp_pairs;           /* training pairs recorded when learned_precond = 2              */
+    double lp_loss_first;   /* learned preconditioner loss before / after training          */
+    double lp_loss_last;
 } dvr3d_result;
 
 /* ---- entry points ----------------------------------------------------------------- */
@@ -198,6 +220,28 @@ int dvr3d_b200_diag_batched(dvr3d_ctx *ctx, int nblk, const int *n_host,
                             double *a_dev, double *w_dev, int vecs);
 
 /* ---- allocation-free variant ---------------------------------------------------------- */
+/* ---- learned Davidson preconditioner (no counterpart in the reference) ----
+ * A solve with options.learned_precond = 2 records (residual, ideal correction) pairs and
+ * trains the context's network; later solves with learned_precond = 1 use it (for example
+ * trained on k = 0 and reused for the other k blocks, or on one surface of a fit and reused
+ * for the next). Its parameters can be read out and loaded into another context. */
+/* Copies the trained parameters into w (n >= DVR3D_LP_NPARAM); returns DVR3D_LP_NPARAM, or
+ * DVR3D_ERR_ARG when the context holds no trained network. */
+int dvr3d_b200_lp_get_weights(dvr3d_ctx *ctx, double *w, int n);
+/* Loads parameters (n == DVR3D_LP_NPARAM) as the context's trained network. */
+int dvr3d_b200_lp_set_weights(dvr3d_ctx *ctx, const double *w, int n);
+/* The network on its own, by the device kernels the solver and trainer use: for nmode modes
+ * (channel eigenvalue lam, features f1, f2, f3, energy scale) and ncol Ritz values theta,
+ * gout[m + j nmode] = 1 + f(phi(m, theta_j)) and grad = sum_mj delta[m + j nmode] dg/dw
+ * (DVR3D_LP_NPARAM entries). Host arrays. */
+int dvr3d_b200_lp_eval(dvr3d_ctx *ctx, const double *w, int nmode, int ncol, const double *lam,
+                       const double *f1, const double *f2, const double *f3, double scale,
+                       const double *theta, const double *delta, double *gout, double *grad);
+/* Training loss (and its gradient when grad is not NULL) at parameters w (host) on the pairs
+ * recorded by this context's last solve, which must have been a training solve
+ * (learned_precond = 2). */
+int dvr3d_b200_lp_train_loss(dvr3d_ctx *ctx, const double *w, double *loss, double *grad);
+
 /* No counterpart in the reference. Same computation and arguments as
  * dvr3d_b200_diag_batched, for callers that must not allocate device memory (a host whose
  * framework's memory pool owns the GPU memory and forbids outside cudaMalloc, or a latency-
