@@ -401,9 +401,11 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
             break;
         }
         if (breakdown) break;
-        const int inc = std::max(2, (int)std::ceil(0.4 * nwant / b));
-        if ((s + inc) * b > mmax) break;
-        next = s + inc;
+        // grow by about ten vectors per level still outside the tolerance (the levels near
+        // the top of the wanted window converge last, at a roughly steady rate per block)
+        const int inc = std::max(2, (int)((10LL * (nwant - nconv) + b - 1) / b));
+        if (s * b >= mmax) break;
+        next = std::min(s + inc, mmax / b);
     }
     ks.factor_ms = tf.ms();
     ks.krylov_ms = tk_ms;
