@@ -1,5 +1,6 @@
 // eig_batched.cu -- batched FP64 symmetric eigensolver kernels (one CTA per block).
 // See eig_batched.cuh for the role of each stage and the reference routines replaced.
+#include <algorithm>
 #include <cfloat>
 #include <cmath>
 
@@ -11,8 +12,7 @@ namespace dvr3d {
 
 namespace {
 
-constexpr int kTriThreads = 256;
-constexpr int kTriRows = 4;  // rows per thread -> n <= 1024
+constexpr int kTriMaxThreads = 1024;  // one row per thread -> n <= 1024
 
 // ------------------------------------------------------------------ tridiagonalisation
 // Lower Householder reduction as dsytd2('L'): for k = 0..n-3 the reflector
@@ -20,7 +20,7 @@ constexpr int kTriRows = 4;  // rows per thread -> n <= 1024
 // The rank-2 update of step k-1 is applied lazily: to column k first (so the reflector
 // of step k can be formed), then fused with the symmetric product A22 v_k of step k, so
 // the trailing block is read and written once per step.
-__global__ void __launch_bounds__(kTriThreads) tridiag_kernel(BatchDesc bd, double *A, double *dg,
+__global__ void __launch_bounds__(kTriMaxThreads) tridiag_kernel(BatchDesc bd, double *A, double *dg,
                                                                double *eo, double *tauo) {
     const int b = blockIdx.x;
     if (b >= bd.nblk) return;
@@ -83,55 +83,50 @@ __global__ void __launch_bounds__(kTriThreads) tridiag_kernel(BatchDesc bd, doub
             v[i] = vi;
         }
         __syncthreads();
-        // (3) fused: apply pending update to A22 and accumulate s = A22 v
-        double s_acc[kTriRows];
-        double vpi[kTriRows], wpi[kTriRows];
-#pragma unroll
-        for (int r = 0; r < kTriRows; ++r) {
-            s_acc[r] = 0.0;
-            const int i = k + 1 + tid + r * blockDim.x;
-            vpi[r] = (pending && i < n) ? vp[i] : 0.0;
-            wpi[r] = (pending && i < n) ? wp[i] : 0.0;
-        }
-        if (tk != 0.0 || pending) {
-            for (int j = k + 1; j < n; ++j) {
-                double *col = a + (size_t)j * n;
-                const double vj = v[j];
-                const double vpj = pending ? vp[j] : 0.0, wpj = pending ? wp[j] : 0.0;
-#pragma unroll
-                for (int r = 0; r < kTriRows; ++r) {
-                    const int i = k + 1 + tid + r * blockDim.x;
-                    if (i < n) {
-                        double x = col[i];
-                        if (pending) {
-                            x -= vpi[r] * wpj + wpi[r] * vpj;
-                            col[i] = x;
-                        }
-                        s_acc[r] += x * vj;
-                    }
+        // (3) fused: apply pending update to A22 and accumulate s = A22 v. One row per thread;
+        // four columns per iteration keep several independent loads in flight per thread
+        const int i = k + 1 + tid;
+        const bool act = i < n;
+        const double vpi = (pending && act) ? vp[i] : 0.0, wpi = (pending && act) ? wp[i] : 0.0;
+        double s_acc = 0.0;
+        if (act && (tk != 0.0 || pending)) {
+            int j = k + 1;
+            for (; j + 3 < n; j += 4) {
+                double *c0 = a + (size_t)j * n + i;
+                double x0 = c0[0], x1 = c0[n], x2 = c0[2 * (size_t)n], x3 = c0[3 * (size_t)n];
+                if (pending) {
+                    x0 -= vpi * wp[j] + wpi * vp[j];
+                    x1 -= vpi * wp[j + 1] + wpi * vp[j + 1];
+                    x2 -= vpi * wp[j + 2] + wpi * vp[j + 2];
+                    x3 -= vpi * wp[j + 3] + wpi * vp[j + 3];
+                    c0[0] = x0;
+                    c0[n] = x1;
+                    c0[2 * (size_t)n] = x2;
+                    c0[3 * (size_t)n] = x3;
                 }
+                s_acc += (x0 * v[j] + x1 * v[j + 1]) + (x2 * v[j + 2] + x3 * v[j + 3]);
+            }
+            for (; j < n; ++j) {
+                double *cj = a + (size_t)j * n + i;
+                double x = *cj;
+                if (pending) {
+                    x -= vpi * wp[j] + wpi * vp[j];
+                    *cj = x;
+                }
+                s_acc += x * v[j];
             }
         }
         // p = tau s ; w = p - (tau/2)(p.v) v
-        double pv = 0.0;
-#pragma unroll
-        for (int r = 0; r < kTriRows; ++r) {
-            const int i = k + 1 + tid + r * blockDim.x;
-            if (i < n) pv += tk * s_acc[r] * v[i];
-        }
+        double pv = act ? tk * s_acc * v[i] : 0.0;
         pv = block_sum(pv, red);
         const double alpha2 = -0.5 * tk * pv;
         __syncthreads();
-        for (int i = tid; i < n; i += blockDim.x) {
-            vp[i] = v[i];
-            wp[i] = 0.0;
+        for (int q = tid; q < n; q += blockDim.x) {
+            vp[q] = v[q];
+            wp[q] = 0.0;
         }
         __syncthreads();
-#pragma unroll
-        for (int r = 0; r < kTriRows; ++r) {
-            const int i = k + 1 + tid + r * blockDim.x;
-            if (i < n) wp[i] = tk * s_acc[r] + alpha2 * v[i];
-        }
+        if (act) wp[i] = tk * s_acc + alpha2 * v[i];
         pending = (tk != 0.0);
         __syncthreads();
     }
@@ -293,6 +288,238 @@ __global__ void __launch_bounds__(kVecThreads) eigvecs_kernel(BatchDesc bd, cons
     (void)err;
 }
 
+// ------------------------------------------------------------------ eigenvectors, fast form
+// Same method as eigvecs_kernel (dstein-style inverse iteration, Gram-Schmidt inside clusters
+// closer than 1e-6 ||T||, back-transformation by the block's reflectors), organised for speed:
+//   * one warp per cluster, the LU factors of T - lambda I and the iterate in that warp's
+//     slice of shared memory (lane 0 runs the recurrences, the warp the vector operations);
+//   * the back-transformation in panels of 16 reflectors (compact WY, I - V Tm V^T): per
+//     panel V and Tm in shared memory, one thread per eigenvector column computing
+//     W = V^T z, W2 = Tm W and z -= V W2 in registers.
+constexpr int kFastPanel = 16;
+
+__global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double *dg, const double *eo,
+                                    const double *tauo, const double *wo, const int *sel, const long long *zoff,
+                                    const int *zld, double *Z) {
+    const int b = blockIdx.x;
+    if (b >= bd.nblk) return;
+    const int n = bd.n[b];
+    const int m = sel[b];
+    if (m <= 0) return;
+    const double *a = A + bd.aoff[b];
+    const double *d = dg + bd.voff[b], *e = eo + bd.voff[b], *tau = tauo + bd.voff[b];
+    const double *w = wo + bd.voff[b];
+    double *z = Z + zoff[b];
+    const int ldz = zld[b];
+    extern __shared__ double sm[];
+    __shared__ int cstart[1025];
+    __shared__ int s_ncl;
+    __shared__ double s_onenrm;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
+    if (tid == 0) {
+        double on = 0.0;
+        for (int i = 0; i < n; ++i) {
+            const double r = fabs(d[i]) + (i > 0 ? fabs(e[i - 1]) : 0.0) + (i < n - 1 ? fabs(e[i]) : 0.0);
+            on = fmax(on, r);
+        }
+        s_onenrm = fmax(on, DBL_MIN);
+        const double ortol = 1.0e-6 * s_onenrm;
+        int nc = 0;
+        cstart[nc++] = 0;
+        for (int j = 1; j < m; ++j)
+            if (w[j] - w[j - 1] > ortol) cstart[nc++] = j;
+        cstart[nc] = m;
+        s_ncl = nc;
+    }
+    __syncthreads();
+    // ---- inverse iteration, one warp per cluster
+    {
+        const size_t slice = (size_t)5 * n + (n + 7) / 8;  // doubles per warp
+        double *D = sm + warp * slice, *E1 = D + n, *E2 = E1 + n, *Lm = E2 + n, *x = Lm + n;
+        unsigned char *P = reinterpret_cast<unsigned char *>(x + n);
+        const double onenrm = s_onenrm;
+        const double eps = DBL_EPSILON, tiny = eps * onenrm, pertol = 10.0 * eps * onenrm;
+        for (int c = warp; c < s_ncl; c += nwarp) {
+            const int j0 = cstart[c], j1 = cstart[c + 1];
+            double lamprev = 0.0;
+            for (int j = j0; j < j1; ++j) {
+                double lam = w[j];
+                if (j > j0 && lam - lamprev < pertol) lam = lamprev + pertol;
+                lamprev = lam;
+                if (lane == 0) {
+                    double av = d[0] - lam, bv = (n > 1) ? e[0] : 0.0;
+                    for (int i = 0; i < n - 1; ++i) {
+                        const double cc = e[i];
+                        const double an = d[i + 1] - lam, bn = (i + 2 < n) ? e[i + 1] : 0.0;
+                        if (fabs(av) >= fabs(cc)) {
+                            if (av == 0.0) av = tiny;
+                            const double mlt = cc / av;
+                            P[i] = 0;
+                            Lm[i] = mlt;
+                            D[i] = av;
+                            E1[i] = bv;
+                            E2[i] = 0.0;
+                            av = an - mlt * bv;
+                            bv = bn;
+                        } else {
+                            const double mlt = av / cc;
+                            P[i] = 1;
+                            Lm[i] = mlt;
+                            D[i] = cc;
+                            E1[i] = an;
+                            E2[i] = bn;
+                            av = bv - mlt * an;
+                            bv = -mlt * bn;
+                        }
+                    }
+                    if (fabs(av) < tiny) av = (av < 0.0) ? -tiny : tiny;
+                    D[n - 1] = av;
+                }
+                __syncwarp();
+                for (int i = lane; i < n - 1; i += 32)
+                    if (fabs(D[i]) < tiny) D[i] = (D[i] < 0.0) ? -tiny : tiny;
+                for (int i = lane; i < n; i += 32) {
+                    const unsigned h = hash32((unsigned)(i * 2654435761u) ^ (unsigned)(j * 40503u + 17u));
+                    x[i] = ((double)(h & 0xffffff) / 8388608.0) - 1.0;
+                }
+                __syncwarp();
+                for (int it = 0; it < 4; ++it) {
+                    double s1 = 0.0;
+                    for (int i = lane; i < n; i += 32) s1 += fabs(x[i]);
+                    s1 = warp_sum(s1);
+                    const double sc = (double)n * onenrm * fmax(eps, fabs(D[n - 1])) / fmax(s1, DBL_MIN);
+                    for (int i = lane; i < n; i += 32) x[i] *= sc;
+                    __syncwarp();
+                    if (lane == 0) {
+                        for (int i = 0; i < n - 1; ++i) {
+                            double yi = x[i], yn = x[i + 1];
+                            if (P[i]) {
+                                const double tmp = yi;
+                                yi = yn;
+                                yn = tmp;
+                                x[i] = yi;
+                            }
+                            x[i + 1] = yn - Lm[i] * yi;
+                        }
+                        double x1 = 0.0, x2 = 0.0;
+                        for (int i = n - 1; i >= 0; --i) {
+                            const double xi = (x[i] - E1[i] * x1 - E2[i] * x2) / D[i];
+                            x[i] = xi;
+                            x2 = x1;
+                            x1 = xi;
+                        }
+                    }
+                    __syncwarp();
+                    for (int jj = j0; jj < j; ++jj) {
+                        const double *zc = z + (size_t)jj * ldz;
+                        double dot = 0.0;
+                        for (int i = lane; i < n; i += 32) dot += x[i] * zc[i];
+                        dot = warp_sum(dot);
+                        for (int i = lane; i < n; i += 32) x[i] -= dot * zc[i];
+                    }
+                    double nrm = 0.0;
+                    for (int i = lane; i < n; i += 32) nrm += x[i] * x[i];
+                    nrm = sqrt(warp_sum(nrm));
+                    const double inv = (nrm > 0.0) ? 1.0 / nrm : 0.0;
+                    for (int i = lane; i < n; i += 32) x[i] *= inv;
+                    __syncwarp();
+                }
+                // sign convention: the first largest component positive
+                double big = 0.0;
+                int bi = n;
+                for (int i = lane; i < n; i += 32)
+                    if (fabs(x[i]) > fabs(big)) {
+                        big = x[i];
+                        bi = i;
+                    }
+#pragma unroll
+                for (int o = 16; o > 0; o >>= 1) {
+                    const double ob = __shfl_xor_sync(0xffffffffu, big, o);
+                    const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                    if (fabs(ob) > fabs(big) || (fabs(ob) == fabs(big) && oi < bi)) {
+                        big = ob;
+                        bi = oi;
+                    }
+                }
+                const double sg = (big < 0.0) ? -1.0 : 1.0;
+                double *zc = z + (size_t)j * ldz;
+                for (int i = lane; i < n; i += 32) zc[i] = sg * x[i];
+                __syncwarp();
+            }
+        }
+    }
+    __syncthreads();
+    // ---- back-transformation z <- H_0 H_1 ... H_{n-3} z, panels of 16 reflectors
+    const int nref = n - 2;
+    if (nref <= 0) return;
+    double *Vs = sm;                                   // [kFastPanel][n]
+    double *Sg = Vs + (size_t)kFastPanel * n;          // [16][16] Gram, then
+    double *Tm = Sg + kFastPanel * kFastPanel;         // [16][16] upper triangular factor
+    for (int p0 = ((nref - 1) / kFastPanel) * kFastPanel; p0 >= 0; p0 -= kFastPanel) {
+        const int nbk = min(kFastPanel, nref - p0);
+        for (int q = tid; q < kFastPanel * n; q += blockDim.x) {
+            const int c = q / n, i = q % n, top = p0 + c + 1;
+            double v = 0.0;
+            if (c < nbk && i >= top) v = (i == top) ? 1.0 : a[(size_t)(p0 + c) * n + i];
+            Vs[q] = v;
+        }
+        __syncthreads();
+        for (int q = tid; q < kFastPanel * kFastPanel; q += blockDim.x) {
+            const int c1 = q / kFastPanel, c2 = q % kFastPanel;
+            double s = 0.0;
+            if (c1 < nbk && c2 < nbk)
+                for (int i = p0 + 1; i < n; ++i) s += Vs[c1 * n + i] * Vs[c2 * n + i];
+            Sg[q] = s;
+        }
+        __syncthreads();
+        if (tid < kFastPanel) {  // dlarft (forward, columnwise), one thread per row of Tm
+            const int r = tid;
+            for (int c = 0; c < kFastPanel; ++c) Tm[r * kFastPanel + c] = 0.0;
+        }
+        __syncthreads();
+        for (int i = 0; i < nbk; ++i) {
+            if (tid < kFastPanel) {
+                const int r = tid;
+                const double ti = tau[p0 + i];
+                if (r < i) {
+                    double s = 0.0;
+                    for (int c = r; c < i; ++c) s += Tm[r * kFastPanel + c] * Sg[c * kFastPanel + i];
+                    Tm[r * kFastPanel + i] = -ti * s;
+                } else if (r == i) {
+                    Tm[i * kFastPanel + i] = ti;
+                }
+            }
+            __syncthreads();
+        }
+        for (int col = tid; col < m; col += blockDim.x) {
+            double *zc = z + (size_t)col * ldz;
+            double wv[kFastPanel];
+#pragma unroll
+            for (int c = 0; c < kFastPanel; ++c) wv[c] = 0.0;
+            for (int i = p0 + 1; i < n; ++i) {
+                const double zi = zc[i];
+#pragma unroll
+                for (int c = 0; c < kFastPanel; ++c) wv[c] += Vs[c * n + i] * zi;
+            }
+            double w2[kFastPanel];
+#pragma unroll
+            for (int r = 0; r < kFastPanel; ++r) {
+                double s = 0.0;
+#pragma unroll
+                for (int c = 0; c < kFastPanel; ++c) s += Tm[r * kFastPanel + c] * wv[c];
+                w2[r] = s;
+            }
+            for (int i = p0 + 1; i < n; ++i) {
+                double s = 0.0;
+#pragma unroll
+                for (int c = 0; c < kFastPanel; ++c) s += Vs[c * n + i] * w2[c];
+                zc[i] -= s;
+            }
+        }
+        __syncthreads();
+    }
+}
+
 __global__ void symmetrize_lower_kernel(BatchDesc bd, double *A) {
     const int b = blockIdx.y;
     const int n = bd.n[b];
@@ -315,7 +542,8 @@ void launch_tridiag_batched(const BatchDesc &bd, double *A, double *d, double *e
     if (bd.nblk <= 0) return;
     const size_t smem = (size_t)3 * nmax * sizeof(double);
     DVR3D_COUNT_LAUNCH(1);
-    tridiag_kernel<<<bd.nblk, kTriThreads, smem, st>>>(bd, A, d, e, tau);
+    const int threads = std::min(kTriMaxThreads, std::max(64, (nmax + 31) / 32 * 32));
+    tridiag_kernel<<<bd.nblk, threads, smem, st>>>(bd, A, d, e, tau);
 }
 
 void launch_eigvals_batched(const BatchDesc &bd, const double *d, const double *e, double *w,
@@ -340,6 +568,29 @@ void launch_eigvecs_batched(const BatchDesc &bd, const double *A, const double *
     DVR3D_COUNT_LAUNCH(1);
     eigvecs_kernel<<<bd.nblk, kVecThreads, smem, st>>>(bd, A, d, e, tau, w, sel, zoff, zld, Z, work,
                                                        workoff, err);
+}
+
+size_t eigvecs_fast_smem(int nmax, int nwarp) {
+    const size_t inv = (size_t)nwarp * (5 * (size_t)nmax + (nmax + 7) / 8) * sizeof(double);
+    const size_t bt = ((size_t)kFastPanel * nmax + 2 * kFastPanel * kFastPanel) * sizeof(double);
+    return std::max(inv, bt);
+}
+
+void launch_eigvecs_batched_fast(const BatchDesc &bd, const double *A, const double *d, const double *e,
+                                 const double *tau, const double *w, const int *sel, const long long *zoff,
+                                 const int *zld, double *Z, int nmax, cudaStream_t st) {
+    if (bd.nblk <= 0) return;
+    const size_t cap = 200 * 1024;
+    int nwarp = 8;
+    while (nwarp > 1 && eigvecs_fast_smem(nmax, nwarp) > cap) --nwarp;
+    const size_t smem = eigvecs_fast_smem(nmax, nwarp);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(eigvecs_fast_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+        attr = true;
+    }
+    DVR3D_COUNT_LAUNCH(1);
+    eigvecs_fast_kernel<<<bd.nblk, 32 * nwarp, smem, st>>>(bd, A, d, e, tau, w, sel, zoff, zld, Z);
 }
 
 }  // namespace dvr3d

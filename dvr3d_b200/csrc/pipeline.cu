@@ -100,17 +100,6 @@ void check_dev_err(dvr3d_ctx *ctx, const int *err_dev, const char *stage) {
     if (e != 0) throw HostError{DVR3D_ERR_NOCONV, std::string(stage) + ": device error flag " + std::to_string(e)};
 }
 
-void eigvecs_work(const std::vector<int> &n, const std::vector<int> &sel, std::vector<long long> &off,
-                  long long &total) {
-    off.resize(n.size());
-    total = 0;
-    for (size_t b = 0; b < n.size(); ++b) {
-        off[b] = total;
-        const long long T = std::min(128, std::max(sel[b], 1));
-        total += 5LL * n[b] * T + (long long)n[b] * std::max(sel[b], 0);
-    }
-}
-
 // ---------------------------------------------------------------- Radau (nfmain)
 void radau_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
     cudaStream_t st = ctx->stream;
@@ -225,14 +214,8 @@ void radau_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
         }
         col += sel[b];
     }
-    std::vector<long long> woff;
-    long long wtot;
-    eigvecs_work(nv, sel, woff, wtot);
-    double *work = ctx->arena.get_t<double>("evwork", (size_t)wtot);
-    int *err = ctx->arena.get_t<int>("err", 1);
-    CK(cudaMemsetAsync(err, 0, sizeof(int), st));
-    launch_eigvecs_batched(bd, H, d, e, tau, w, upload(ctx, "sel", sel), upload(ctx, "zoff", zoff),
-                           upload(ctx, "zld", zld), out.Vt, work, upload(ctx, "woff", woff), n, err, st);
+    launch_eigvecs_batched_fast(bd, H, d, e, tau, w, upload(ctx, "sel", sel), upload(ctx, "zoff", zoff),
+                                upload(ctx, "zld", zld), out.Vt, n, st);
     CK(cudaGetLastError());
     // sqrt of the pair weight w_p = 1/(2 mu r_a^2) + 1/(2 mu r_b^2) (blc2d2 :3537-3539)
     std::vector<double> sw(out.ldv, 0.0);
@@ -329,15 +312,9 @@ void jacobi_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
     }
     double *U = ctx->arena.get_t<double>("u1", (size_t)std::max<long long>(ut, 1));
     {
-        std::vector<long long> woff;
-        long long wtot;
-        eigvecs_work(nv1, iv1, woff, wtot);
-        double *work = ctx->arena.get_t<double>("evwork", (size_t)wtot);
-        int *err = ctx->arena.get_t<int>("err", 1);
-        CK(cudaMemsetAsync(err, 0, sizeof(int), st));
         std::vector<int> zld1(nb1, na);
-        launch_eigvecs_batched(bd1, H1, d1, e1, t1, w1, upload(ctx, "sel1", iv1), upload(ctx, "zoff1", zoff1),
-                               upload(ctx, "zld1", zld1), U, work, upload(ctx, "woff1", woff), na, err, st);
+        launch_eigvecs_batched_fast(bd1, H1, d1, e1, t1, w1, upload(ctx, "sel1", iv1), upload(ctx, "zoff1", zoff1),
+                                    upload(ctx, "zld1", zld1), U, na, st);
         CK(cudaGetLastError());
     }
     // 1D eigenvalues and coordinate-b index of each 2D basis function
@@ -459,14 +436,8 @@ void jacobi_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
     }
     double *V2 = ctx->arena.get_t<double>("v2", (size_t)std::max<long long>(v2t, 1));
     {
-        std::vector<long long> woff;
-        long long wtot;
-        eigvecs_work(nv2, sel2, woff, wtot);
-        double *work = ctx->arena.get_t<double>("evwork", (size_t)wtot);
-        int *err = ctx->arena.get_t<int>("err", 1);
-        CK(cudaMemsetAsync(err, 0, sizeof(int), st));
-        launch_eigvecs_batched(bd2, H2, d2, e2d, t2, w2, upload(ctx, "sel2", sel2), upload(ctx, "zoff2", zoff2),
-                               upload(ctx, "zld2", zld2), V2, work, upload(ctx, "woff2", woff), n2max, err, st);
+        launch_eigvecs_batched_fast(bd2, H2, d2, e2d, t2, w2, upload(ctx, "sel2", sel2), upload(ctx, "zoff2", zoff2),
+                                    upload(ctx, "zld2", zld2), V2, n2max, st);
         CK(cudaGetLastError());
     }
     // contracted basis (mkham3 first part :2362-2411)
@@ -596,13 +567,7 @@ void channel_setup(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contra
     int *cnt = ctx->arena.get_t<int>("ch_cnt", kmax);
     launch_tridiag_batched(bd, A, d, e, tau, nmax, st);
     launch_eigvals_batched(bd, d, e, lam, cnt, 0, 0.0, st);
-    std::vector<long long> woff;
-    long long wtot;
-    eigvecs_work(n, n, woff, wtot);
-    double *work = ctx->arena.get_t<double>("ch_work", (size_t)wtot);
-    int *err = ctx->arena.get_t<int>("ch_err", 1);
-    CK(cudaMemsetAsync(err, 0, sizeof(int), st));
-    launch_eigvecs_batched(bd, A, d, e, tau, lam, dn, dq, dn, Q, work, upload(ctx, "ch_woff", woff), nmax, err, st);
+    launch_eigvecs_batched_fast(bd, A, d, e, tau, lam, dn, dq, dn, Q, nmax, st);
     CK(cudaGetLastError());
     // per-mode features
     std::vector<double> lh = download(ctx, lam, N), e2h = download(ctx, C.e2, N);
