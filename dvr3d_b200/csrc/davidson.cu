@@ -123,6 +123,7 @@ void gemm_split(GemmOp g, int target, double *work, cudaStream_t st) {
     if (target > 1) {
         const int tiles = ((g.M + 63) / 64) * ((g.N + 63) / 64);
         g.splitk = std::max(1, std::min({(target + tiles - 1) / tiles, 64, (g.K + 15) / 16}));
+        if (g.splitk > 8 && tiles * 8 >= 296) g.splitk = 8;
         g.work = work;
     }
     CK(launch_gemm(g, st));

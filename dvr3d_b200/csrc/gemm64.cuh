@@ -53,8 +53,10 @@ void launch_grouped_dgemm(const GroupedGemm &g, bool transA, int total_tiles, cu
 //   tri_b = 1: op(B) lower triangular (only k >= j contributes), 2: upper (only k <= j);
 //            the other triangle must hold zeros (only whole k tiles are skipped)
 //   lower_out: M == N, only C(i,j) with i >= j is computed and written
-//   splitk > 1: K split over that many CTAs per tile, partial sums in work
-//            (gemm_splitk_work(M, N, splitk) doubles), reduced in a second kernel
+//   splitk > 1: K split over that many CTAs per tile; up to 8 slices form a thread-block
+//            cluster and sum their partial tiles through distributed shared memory (work
+//            unused); more slices need work (gemm_splitk_work(M, N, splitk) doubles) and a
+//            second reduction kernel
 // A, B 16-byte aligned, lda and ldb even.
 struct GemmOp {
     int M = 0, N = 0, K = 0;

@@ -3,13 +3,16 @@
 //   * either operand stored column-major or transposed (no copies),
 //   * a triangular first operand (K range limited per output row tile),
 //   * lower-triangle output only (SYRK-style updates of a symmetric matrix),
-//   * split-K over gridDim.y with a deterministic second-pass reduction.
+//   * split-K over gridDim.y: up to 8 slices as one thread-block cluster whose partial tiles
+//     are summed through distributed shared memory (deterministic, no second kernel), more
+//     slices through a scratch buffer and a second-pass reduction.
 //
 // Tiles are BM x BN = 64 x 64 (or 64 x 32 for thin right-hand sides), BK = 16; four warps,
 // 2 x 2, each a 32 x (BN/2) sub-tile. Shared-memory layouts follow the contiguous direction
 // of the source so that every cp.async moves 16 bytes: [m][k] (stride 20 doubles) for
 // k-contiguous operands, [k][m] (stride BM+4) for m-contiguous ones; both strides make the
 // DMMA fragment reads bank-conflict free.
+#include <cooperative_groups.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -23,6 +26,7 @@ namespace {
 
 constexpr int kBM = 64, kBK = 16, kThr = 128;
 constexpr int kSK = kBK + 4;  // stride of [m][k] tiles
+constexpr int kMaxClusterSplit = 8;  // portable cluster size
 
 __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
@@ -70,13 +74,16 @@ struct TileLoader {
 
 // op(A)(i, k): TA ? A[i * lda + k] : A[k * lda + i]   (k-contiguous when TA)
 // op(B)(k, j): TB ? B[k * ldb + j] : B[j * ldb + k]   (k-contiguous when !TB)
-template <bool TA, bool TB, int BN>
+template <bool TA, bool TB, int BN, bool CL>
 __global__ void __launch_bounds__(kThr) gemm_pipe_kernel(GemmOp p, int tiles_m) {
     using LA = TileLoader<kBM, TA>;
     using LB = TileLoader<BN, !TB>;
     constexpr int WN = BN / 2, FN = WN / 8;
-    __shared__ __align__(16) double As[2][LA::kElems];
-    __shared__ __align__(16) double Bs[2][LB::kElems];
+    constexpr int kSmem = 2 * LA::kElems + 2 * LB::kElems;
+    static_assert(kSmem >= kBM * BN, "staging of the cluster reduction fits the operand buffers");
+    __shared__ __align__(16) double smem_all[kSmem];
+    double(*As)[LA::kElems] = reinterpret_cast<double(*)[LA::kElems]>(smem_all);
+    double(*Bs)[LB::kElems] = reinterpret_cast<double(*)[LB::kElems]>(smem_all + 2 * LA::kElems);
     int tm, tn;
     if (p.lower_out) {
         const long long t = blockIdx.x;
@@ -141,6 +148,36 @@ __global__ void __launch_bounds__(kThr) gemm_pipe_kernel(GemmOp p, int tiles_m) 
         __syncthreads();
     }
     const int c2 = c * 2;
+    if constexpr (CL) {
+        // cluster split-K: stage this slice's tile, sum the S slices through distributed
+        // shared memory, each CTA of the cluster finishing 64/S rows of the tile
+        namespace cg = cooperative_groups;
+        cg::cluster_group cluster = cg::this_cluster();
+        __syncthreads();
+        double *stage = smem_all;
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < FN; ++b)
+#pragma unroll
+                for (int h = 0; h < 2; ++h) stage[(wm + a * 8 + r) * BN + wn + b * 8 + c2 + h] = acc[a][b][h];
+        cluster.sync();
+        const int rank = (int)cluster.block_rank();
+        const int r0 = rank * kBM / S, r1 = (rank + 1) * kBM / S;
+        for (int q = threadIdx.x; q < (r1 - r0) * BN; q += kThr) {
+            const int rr = r0 + q / BN, cc = q % BN;
+            const int i = i0 + rr, j = j0 + cc;
+            double sum = 0.0;
+            for (int u = 0; u < S; ++u) sum += cluster.map_shared_rank(stage, u)[rr * BN + cc];
+            if (i < p.M && j < p.N && !(p.lower_out && j > i)) {
+                double *cp = p.C + (size_t)j * p.ldc + i;
+                const double old = (p.beta != 0.0) ? *cp : 0.0;
+                *cp = p.alpha * sum + p.beta * old;
+            }
+        }
+        cluster.sync();
+        return;
+    }
     const bool split = (S > 1);
 #pragma unroll
     for (int a = 0; a < 4; ++a)
@@ -173,22 +210,42 @@ __global__ void splitk_reduce_kernel(GemmOp p, int S) {
     *cp = p.alpha * s + p.beta * old;
 }
 
-template <int BN>
+template <bool TA, bool TB, int BN, bool CL>
+cudaError_t launch_one(const GemmOp &p, dim3 grid, int S, int tiles_m, cudaStream_t st) {
+    if (!CL) {
+        gemm_pipe_kernel<TA, TB, BN, false><<<grid, kThr, 0, st>>>(p, tiles_m);
+        return cudaGetLastError();
+    }
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = dim3(kThr);
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeClusterDimension;
+    attr[0].val.clusterDim.x = 1;
+    attr[0].val.clusterDim.y = S;
+    attr[0].val.clusterDim.z = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, gemm_pipe_kernel<TA, TB, BN, true>, p, tiles_m);
+}
+
+template <int BN, bool CL>
 cudaError_t launch_bn(const GemmOp &p, int S, cudaStream_t st) {
     const int tiles_m = (p.M + kBM - 1) / kBM, tiles_n = (p.N + BN - 1) / BN;
     const long long nt = p.lower_out ? (long long)tiles_m * (tiles_m + 1) / 2 : (long long)tiles_m * tiles_n;
     dim3 grid((unsigned)nt, (unsigned)S);
     DVR3D_COUNT_LAUNCH(1);
-    if (!p.ta && !p.tb) gemm_pipe_kernel<false, false, BN><<<grid, kThr, 0, st>>>(p, tiles_m);
-    else if (p.ta && !p.tb) gemm_pipe_kernel<true, false, BN><<<grid, kThr, 0, st>>>(p, tiles_m);
-    else if (!p.ta && p.tb) gemm_pipe_kernel<false, true, BN><<<grid, kThr, 0, st>>>(p, tiles_m);
-    else gemm_pipe_kernel<true, true, BN><<<grid, kThr, 0, st>>>(p, tiles_m);
-    return cudaGetLastError();
+    if (!p.ta && !p.tb) return launch_one<false, false, BN, CL>(p, grid, S, tiles_m, st);
+    if (p.ta && !p.tb) return launch_one<true, false, BN, CL>(p, grid, S, tiles_m, st);
+    if (!p.ta && p.tb) return launch_one<false, true, BN, CL>(p, grid, S, tiles_m, st);
+    return launch_one<true, true, BN, CL>(p, grid, S, tiles_m, st);
 }
 
 }  // namespace
 
-size_t gemm_splitk_work(int M, int N, int S) { return S > 1 ? (size_t)S * M * N : 0; }
+size_t gemm_splitk_work(int M, int N, int S) { return S > kMaxClusterSplit ? (size_t)S * M * N : 0; }
 
 cudaError_t launch_gemm(const GemmOp &p0, cudaStream_t st) {
     GemmOp p = p0;
@@ -200,10 +257,13 @@ cudaError_t launch_gemm(const GemmOp &p0, cudaStream_t st) {
         return cudaErrorInvalidValue;
     int S = std::max(1, p.splitk);
     if (p.K <= 0) S = 1;
-    if (S > 1 && !p.work) return cudaErrorInvalidValue;
+    const bool cl = (S > 1 && S <= kMaxClusterSplit);
+    if (S > 1 && !cl && !p.work) return cudaErrorInvalidValue;
     const int bn = (p.N <= 32 && !p.lower_out) ? 32 : 64;
-    cudaError_t e = (bn == 32) ? launch_bn<32>(p, S, st) : launch_bn<64>(p, S, st);
-    if (e != cudaSuccess || S == 1) return e;
+    cudaError_t e;
+    if (cl) e = (bn == 32) ? launch_bn<32, true>(p, S, st) : launch_bn<64, true>(p, S, st);
+    else e = (bn == 32) ? launch_bn<32, false>(p, S, st) : launch_bn<64, false>(p, S, st);
+    if (e != cudaSuccess || S == 1 || cl) return e;
     const long long tot = (long long)p.M * p.N;
     DVR3D_COUNT_LAUNCH(1);
     splitk_reduce_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(p, S);

@@ -115,9 +115,12 @@ __global__ void gather_norm_kernel(const double *X, long long ldx, const int *pe
 inline unsigned nb256(long long n) { return (unsigned)((n + 255) / 256); }
 inline long long rup(long long x, long long m) { return (x + m - 1) / m * m; }
 
+// split-K factor for about `target` CTAs; at most 8 (one thread-block cluster, no second
+// reduction kernel) once that already gives two waves of CTAs
 int splits(int tiles, int ktiles, int target, int smax) {
     int s = (target + tiles - 1) / std::max(tiles, 1);
     s = std::max(1, std::min({s, smax, ktiles}));
+    if (s > 8 && tiles * 8 >= 296) s = 8;
     return s;
 }
 
