@@ -23,7 +23,6 @@ namespace {
 
 constexpr int NB = kCholNb;
 constexpr int kLeafThreads = 256;
-constexpr size_t kLeafSmem = (NB * (NB + 1) + 2 * NB) * sizeof(double);
 
 __global__ void shift_copy_lower_kernel(const double *H, long long ldh, int n, double sigma, double *A,
                                         long long lda) {
@@ -39,121 +38,132 @@ __global__ void shift_copy_lower_kernel(const double *H, long long ldh, int n, d
 // Cholesky of the nb x nb block at (j0, j0) (nb <= 64, lower triangle read) and inverse of
 // its factor. in_place_inv = 0: the factor goes back into A; 1: the inverse replaces the
 // block's lower triangle. inv_out (optional): the inverse (ld 64, zeros above).
-// Each thread keeps its 16 elements (row ti, columns tj0 + 4u) in registers; per column
-// step only the pivot column (or, in the inverse, the pivot row) goes through shared memory
-// (double-buffered), so one barrier per step suffices.
-__global__ void __launch_bounds__(kLeafThreads) potrf_leaf_kernel(double *A, long long lda, int j0, int nb,
-                                                                  double *inv_out, int in_place_inv, double rel_tol,
-                                                                  int *err) {
+// One right-looking sweep forms A = U D U^T (U unit lower) and, in the same steps, the
+// forward substitution X = inv(U) (row k of X is final when step k starts; step k
+// subtracts U[i][k] X[k] from the rows below); then L = U D^{1/2}, inv(L) = D^{-1/2} X.
+// Thread (row ti, group tg) keeps columns 16 tg .. 16 tg + 15 of the matrix and of X in
+// registers. The pivot column is published with zeros on and above the diagonal and row k
+// of X has zeros right of its diagonal, so every step is the same 32 unmasked FMAs per
+// thread (finished columns and the upper triangle take zero updates); one barrier per step.
+__global__ void __launch_bounds__(kLeafThreads, 1) potrf_leaf_kernel(double *A, long long lda, int j0, int nb,
+                                                                     double *inv_out, int in_place_inv,
+                                                                     double rel_tol, int *err) {
     if (*(volatile int *)err != 0) return;
-    extern __shared__ double sm[];
-    double(*L)[NB + 1] = reinterpret_cast<double(*)[NB + 1]>(sm);  // final factor
-    double(*buf)[NB] = reinterpret_cast<double(*)[NB]>(sm + NB * (NB + 1));  // [2][64] pivot column / row
+    __shared__ __align__(16) double colb[2][NB];
+    __shared__ __align__(16) double rowb[2][NB];
+    __shared__ double piv[2], rdb[2];
+    __shared__ double sq[NB], rsq[NB];
     __shared__ double s_thr;
     const int tid = threadIdx.x;
-    const int ti = tid & (NB - 1), tj0 = tid >> 6;  // this thread owns row ti, columns tj0 + 4u
+    const int ti = tid & (NB - 1), tg = tid >> 6;
     constexpr int U = NB / 4;
-    double own[U];
+    const int jb = tg * U;
+    double own[U], x[U];
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-        const int j = tj0 + 4 * u;
+        const int j = jb + u;
         own[u] = (ti < nb && j < nb && ti >= j) ? A[(size_t)(j0 + j) * lda + j0 + ti] : 0.0;
-        if (ti == j) buf[0][ti] = own[u];  // diagonal, for the pivot threshold
+        x[u] = (ti == j) ? 1.0 : 0.0;
+        if (ti == j) sq[ti] = own[u];  // diagonal, for the pivot threshold
+        if (ti == 0) rowb[0][j] = x[u];
+    }
+    if (tg == 0) {
+        colb[0][ti] = (ti > 0) ? own[0] : 0.0;
+        if (ti == 0) {
+            piv[0] = own[0];
+            rdb[0] = 1.0 / own[0];
+        }
     }
     __syncthreads();
     if (tid < 32) {  // threshold relative to the largest diagonal entry
         double mx = 0.0;
-        for (int i = tid; i < nb; i += 32) mx = fmax(mx, buf[0][i]);
+        for (int i = tid; i < nb; i += 32) mx = fmax(mx, sq[i]);
 #pragma unroll
         for (int o = 16; o > 0; o >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, o));
         if (tid == 0) s_thr = rel_tol * mx;
     }
-    __syncthreads();
-    // right-looking factorisation in L D L^T form (column k published unscaled)
     bool bad = false;
-    if (tj0 == 0) buf[0][ti] = own[0];  // column 0
     for (int k = 0; k < nb; ++k) {
-        double *col = buf[k & 1], *nxt = buf[(k + 1) & 1];
+        const int cb = k & 1, nbuf = cb ^ 1;
         __syncthreads();
-        const double d = col[k];
+        const double d = piv[cb];
         if (!(d > s_thr) || !isfinite(d)) {  // uniform: every thread reads the same d
             bad = true;
             break;
         }
-        const double lik = (ti > k && ti < nb) ? col[ti] * (1.0 / d) : 0.0;
+        const double lik = colb[cb][ti] * rdb[cb];  // zero on and above the pivot
+        double cv[U], rv[U];
+#pragma unroll
+        for (int u = 0; u < U; u += 2) {
+            const double2 c2 = *reinterpret_cast<const double2 *>(&colb[cb][jb + u]);
+            const double2 r2 = *reinterpret_cast<const double2 *>(&rowb[cb][jb + u]);
+            cv[u] = c2.x;
+            cv[u + 1] = c2.y;
+            rv[u] = r2.x;
+            rv[u + 1] = r2.y;
+        }
 #pragma unroll
         for (int u = 0; u < U; ++u) {
-            const int j = tj0 + 4 * u;
-            if (j > k && ti >= j) own[u] -= lik * col[j];
-            if (j == k + 1) nxt[ti] = own[u];  // column k+1 is final after this step
+            own[u] = fma(-lik, cv[u], own[u]);
+            x[u] = fma(-lik, rv[u], x[u]);
+        }
+        const int kn = k + 1;
+        if (tg == (kn >> 4) && kn < NB) {  // column k+1 is final after this step
+            double v = 0.0;
+            switch (kn & 15) {
+#define DVR3D_PICK(c) \
+    case c:           \
+        v = own[c];   \
+        break;
+                DVR3D_PICK(0) DVR3D_PICK(1) DVR3D_PICK(2) DVR3D_PICK(3) DVR3D_PICK(4) DVR3D_PICK(5) DVR3D_PICK(6)
+                DVR3D_PICK(7) DVR3D_PICK(8) DVR3D_PICK(9) DVR3D_PICK(10) DVR3D_PICK(11) DVR3D_PICK(12)
+                DVR3D_PICK(13) DVR3D_PICK(14) DVR3D_PICK(15)
+#undef DVR3D_PICK
+            }
+            colb[nbuf][ti] = (ti > kn) ? v : 0.0;
+            if (ti == kn) {
+                piv[nbuf] = v;
+                rdb[nbuf] = 1.0 / v;
+            }
+        }
+        if (ti == kn) {  // so is row k+1 of X
+#pragma unroll
+            for (int u = 0; u < U; ++u) rowb[nbuf][jb + u] = x[u];
         }
     }
     if (bad) {
         if (tid == 0) atomicExch(err, (int)kDevNotPosDef);
         return;
     }
-    // L = (unit factor) D^{1/2}: column j scaled by 1/sqrt(d_j), diagonal sqrt(d_j)
+    // L = U D^{1/2} (column j of the unscaled factor times 1/sqrt(d_j), diagonal sqrt(d_j));
+    // inv(L) = D^{-1/2} X
     __syncthreads();
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-        const int j = tj0 + 4 * u;
-        if (ti == j) buf[0][j] = own[u];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int u = 0; u < U; ++u) {
-        const int j = tj0 + 4 * u;
-        double v = 0.0;
-        if (ti < nb && j < nb && ti >= j) v = (ti == j) ? sqrt(own[u]) : own[u] / sqrt(buf[0][j]);
-        own[u] = v;
-        L[ti][j] = v;
-    }
-    __syncthreads();
-    // X = inv(L): row k of X is final once divided by L[k][k]; its owners publish it
-    // (divided), then the rows below subtract L[i][k] times it
-    double x[U];
-#pragma unroll
-    for (int u = 0; u < U; ++u) x[u] = (ti == tj0 + 4 * u) ? 1.0 : 0.0;
-    for (int k = 0; k < nb; ++k) {
-        double *row = buf[k & 1];
-        if (ti == k) {
-            const double r = 1.0 / L[k][k];
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                x[u] *= r;
-                row[tj0 + 4 * u] = x[u];
-            }
-        }
-        __syncthreads();
-        const double lik = (ti > k && ti < nb) ? L[ti][k] : 0.0;
-        if (lik != 0.0) {
-#pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int c = tj0 + 4 * u;
-                if (c <= k) x[u] -= lik * row[c];
-            }
+        const int j = jb + u;
+        if (ti == j && ti < nb) {
+            const double r = sqrt(own[u]);
+            sq[j] = r;
+            rsq[j] = 1.0 / r;
         }
     }
+    __syncthreads();
+    const double rrow = (ti < nb) ? rsq[ti] : 0.0;
 #pragma unroll
     for (int u = 0; u < U; ++u) {
-        const int j = tj0 + 4 * u;
+        const int j = jb + u;
         const bool in = (ti < nb && j < nb && ti >= j);
-        if (in) A[(size_t)(j0 + j) * lda + j0 + ti] = in_place_inv ? x[u] : own[u];
-        if (inv_out) inv_out[(size_t)j * NB + ti] = in ? x[u] : 0.0;
+        const double l = (ti == j) ? sq[j] : own[u] * rsq[j];
+        const double xi = x[u] * rrow;
+        if (in) A[(size_t)(j0 + j) * lda + j0 + ti] = in_place_inv ? xi : l;
+        if (inv_out) inv_out[(size_t)j * NB + ti] = in ? xi : 0.0;
     }
 }
 
 cudaError_t leaf(double *A, long long lda, int j0, int nb, double *inv_out, int in_place, double rel_tol, int *err,
                  cudaStream_t st) {
-    static bool attr = false;
-    if (!attr) {
-        const cudaError_t e =
-            cudaFuncSetAttribute(potrf_leaf_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kLeafSmem);
-        if (e != cudaSuccess) return e;
-        attr = true;
-    }
     DVR3D_COUNT_LAUNCH(1);
-    potrf_leaf_kernel<<<1, kLeafThreads, kLeafSmem, st>>>(A, lda, j0, nb, inv_out, in_place, rel_tol, err);
+    potrf_leaf_kernel<<<1, kLeafThreads, 0, st>>>(A, lda, j0, nb, inv_out, in_place, rel_tol, err);
     return cudaGetLastError();
 }
 

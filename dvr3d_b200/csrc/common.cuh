@@ -90,4 +90,40 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, int *err, unsigned lon
     return s_ok != 0;
 }
 
+// Grid barrier on a counter that only grows: barrier number e of a sequence completes when
+// the counter reaches (e + 1) * gridDim; `target` carries the running count (start it at the
+// arrivals made by earlier launches on the same counter, which is zeroed once before them).
+// No reset step, so the last arrival releases everybody at once. Bounded like grid_sync; a
+// CTA that sees another's error flag while waiting returns false as well.
+__device__ __forceinline__ bool grid_sync_counted(unsigned int *count, unsigned int &target, int *err,
+                                                  unsigned long long limit = (1ull << 26)) {
+    __syncthreads();
+    __shared__ int s_okc;
+    target += gridDim.x * gridDim.y * gridDim.z;
+    if (threadIdx.x == 0) {
+        __threadfence();
+        atomicAdd(count, 1u);
+        volatile unsigned int *vc = count;
+        unsigned long long spins = 0;
+        int ok = 1;
+        while (*vc < target) {
+            ++spins;
+            if ((spins & 1023ull) == 0 && *(volatile int *)err != 0) {
+                ok = 0;
+                break;
+            }
+            if (spins > limit) {
+                atomicExch(err, (int)kDevBarrierTimeout);
+                ok = 0;
+                break;
+            }
+            if (spins > 4096) __nanosleep(32);
+        }
+        __threadfence();
+        s_okc = ok;
+    }
+    __syncthreads();
+    return s_okc != 0;
+}
+
 }  // namespace dvr3d

@@ -28,6 +28,7 @@ constexpr int TB = 64;          // symmetric tile edge
 constexpr int TS = TB + 1;      // shared-memory column stride (conflict-free transposed reads)
 constexpr int kPnThreads = 256;
 constexpr int kMaxNb = 64;
+constexpr int kPw = 32;         // panel width of the reduction (columns per panel)
 
 constexpr int kChunk = 256;     // rows owned by one owner CTA (one row per thread)
 
@@ -46,11 +47,12 @@ constexpr int kChunk = 256;     // rows owned by one owner CTA (one row per thre
 // One panel of the blocked Householder reduction (the dlatrd scheme: columns are formed
 // from the panel-start matrix plus the rank-2 corrections V W^T + W V^T of the panel's
 // earlier columns; the trailing matrix itself is updated once per panel by syr2k).
-// Work split: every CTA takes 64x64 lower tiles of the symmetric product; the first
-// NO = ceil(n/256) CTAs also own 256 rows each for the vector work (column update,
-// reductions, w), so cross-CTA sums are over NO partials only.
-// Per column four bounded grid barriers separate: column update + norm | symmetric
-// product (deterministic per-tile partial sums) | reduction of the partials | w.
+// Work split: every CTA takes 64x64 lower tiles of the symmetric product, the V/W dot
+// products and rows of the reduction; the first NO = ceil(n/256) CTAs also own 256 rows
+// each for the column update, so the norm is a sum over NO partials only.
+// Per column three bounded grid barriers separate: column update (with the previous
+// column's w) + norm | reflector, symmetric product (deterministic per-tile partial sums),
+// V^T v and W^T v | reduction of the partials into p = tau y and p.v.
 __global__ void __launch_bounds__(kPnThreads, 3) dense_panel_kernel(DenseTri t) {
     const int n = t.n, NT = t.NT;
     const long long ld = t.lda;
@@ -60,41 +62,123 @@ __global__ void __launch_bounds__(kPnThreads, 3) dense_panel_kernel(DenseTri t) 
     const int NO = (n + kChunk - 1) / kChunk;
     const bool owner = cta < NO;
     const int r_own = cta * kChunk + tid;  // the row this thread owns (if owner)
-    __shared__ double S[TB * TS];
+    extern __shared__ double dsm[];
+    double *cache = dsm;                              // t.cache_tiles resident tiles (panel-start values)
+    double *S = dsm + (size_t)t.cache_tiles * TB * TS;  // scratch tile for the streamed path
     __shared__ double vI[TB], vJ[TB];
     __shared__ double red[32];
     __shared__ double rsum[4][TB];
+    __shared__ double rsJ[4][TB];
     __shared__ double s_corr[2 * kMaxNb];
+    __shared__ double s_red4[4][2 * kPw];
     __shared__ double s_tau, s_scal, s_a2;
     const int nbmax = t.nbmax;
-    double *part_n = t.part;                  // [NO] norms / dots
-    double *part_q = t.part + G;              // [NO][2 nbmax] V^T v, W^T v
+    double *part_n = t.part;                  // [NO] partial norms of the column
+    double *part_d = t.part + G;              // [G] partial p.v
+    double *part_q = t.part + 2 * G;          // [NO][2 nbmax] V^T v, W^T v
     long long prof_last_ = -1;
     int prof_ph_ = 0;
+    // resident mode: this CTA's lower tiles of the trailing matrix (fixed for the panel: the
+    // reduction forms columns from the panel-start matrix) are read once into shared memory;
+    // tiles beyond the cache are streamed from global memory per column as below
+    const int t0s = (t.j0 + 1) / TB;
+    const long long ntiles_s = (long long)(NT - t0s) * (NT - t0s + 1) / 2;
+    auto decode_rel = [&](long long tt, int base, int &Io, int &Jo) {
+        int li = (int)((sqrt(8.0 * (double)tt + 1.0) - 1.0) * 0.5);
+        while ((long long)li * (li + 1) / 2 > tt) --li;
+        while ((long long)(li + 1) * (li + 2) / 2 <= tt) ++li;
+        Io = base + li;
+        Jo = base + (int)(tt - (long long)li * (li + 1) / 2);
+    };
+    if (t.cache_tiles > 0) {
+        int slot = 0;
+        for (long long tt = cta; tt < ntiles_s && slot < t.cache_tiles; tt += G, ++slot) {
+            int I, J;
+            decode_rel(tt, t0s, I, J);
+            double *Sc = cache + (size_t)slot * TB * TS;
+            const int r0 = I * TB, c0 = J * TB;
+            for (int q = tid; q < TB * TB; q += kPnThreads) {
+                const int c = q / TB, r = q % TB;
+                const int gr = r0 + r, gc = c0 + c;
+                Sc[c * TS + r] = (gr < n && gc < n) ? __ldcg(A + (size_t)gc * ld + gr) : 0.0;
+            }
+            if (I == J) {
+                __syncthreads();
+                for (int q = tid; q < TB * TB; q += kPnThreads) {
+                    const int c = q / TB, r = q % TB;
+                    if (r < c) Sc[c * TS + r] = Sc[r * TS + c];
+                }
+            }
+        }
+        __syncthreads();
+    }
+    // w of the previous column: w = p - (tau/2)(p.v) v, with p (ybuf) and the partial p.v of
+    // every CTA (part_d) from its reduction phase
+    auto prev_scale = [&](double tprev) {
+        if (tid < 32) {
+            double s = 0.0;
+            for (int c0 = 0; c0 < G; c0 += 256) {
+#pragma unroll
+                for (int u = 0; u < 8; ++u) {
+                    const int c = c0 + tid + 32 * u;
+                    s += (c < G) ? part_d[c] : 0.0;
+                }
+            }
+            s = warp_sum(s);
+            if (tid == 0) s_a2 = -0.5 * tprev * s;
+        }
+        __syncthreads();
+        return s_a2;
+    };
+    unsigned int bar_target = t.bar_base;
+    double tprev = 0.0;
     for (int i = 0; i < t.nb; ++i) {
         const int k = t.j0 + i;
-        if (k + 2 >= n) break;
-        // ---- phase A: column k of the current matrix on owned rows, partial norm
+        // ---- phase A: column k of the current matrix on owned rows (the previous column's
+        // rank-2 term is formed here from its p and v), partial norm; W of the previous column
         PROF_MARK(0);
+        const double a2 = (i > 0) ? prev_scale(tprev) : 0.0;
         if (owner) {
             double ss = 0.0;
             const int r = r_own;
             if (r >= k && r < n) {
                 double a = A[(size_t)k * ld + r];
-                for (int q = 0; q < i; ++q)
-                    a -= t.V[(size_t)q * n + r] * t.W[(size_t)q * n + k] + t.W[(size_t)q * n + r] * t.V[(size_t)q * n + k];
+                // all panel columns at once (independent loads; the buffers are zeroed before
+                // the first panel, and columns not yet finished get a zero factor)
+                double acc = 0.0;
+#pragma unroll
+                for (int q = 0; q < kPw; ++q) {
+                    const double f = (q + 1 < i) ? 1.0 : 0.0;
+                    acc += f * (t.V[(size_t)q * n + r] * t.W[(size_t)q * n + k] +
+                                t.W[(size_t)q * n + r] * t.V[(size_t)q * n + k]);
+                }
+                a -= acc;
+                if (i > 0) {
+                    const double *Vp = t.V + (size_t)(i - 1) * n;
+                    const double vr = Vp[r];
+                    const double wr = t.ybuf[r] + a2 * vr;
+                    const double wk = t.ybuf[k] + a2 * Vp[k];
+                    t.W[(size_t)(i - 1) * n + r] = wr;
+                    a -= vr * wk + wr * Vp[k];
+                }
                 t.acol[r] = a;
                 if (r >= k + 2) ss = a * a;
             }
             ss = block_sum(ss, red);
             if (tid == 0) part_n[cta] = ss;
         }
-        if (!grid_sync(t.bar, t.err)) return;
+        if (!grid_sync_counted(&t.bar->count, bar_target, t.err)) return;
         // ---- phase B: reflector (redundantly in every CTA)
         PROF_MARK(1);
         if (tid < 32) {
             double s = 0.0;
-            for (int c = tid; c < NO; c += 32) s += part_n[c];
+            for (int c0 = 0; c0 < NO; c0 += 128) {
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const int c = c0 + tid + 32 * u;
+                    s += (c < NO) ? part_n[c] : 0.0;
+                }
+            }
             s = warp_sum(s);
             if (tid == 0) {
                 const double alpha = t.acol[k + 1];
@@ -119,6 +203,7 @@ __global__ void __launch_bounds__(kPnThreads, 3) dense_panel_kernel(DenseTri t) 
         }
         __syncthreads();
         const double tk = s_tau, scal = s_scal;
+        tprev = tk;
         auto vval = [&](int r) -> double {
             if (r <= k || r >= n) return 0.0;
             return (r == k + 1) ? 1.0 : t.acol[r] * scal;
@@ -128,7 +213,97 @@ __global__ void __launch_bounds__(kPnThreads, 3) dense_panel_kernel(DenseTri t) 
         const int t0 = (k + 1) / TB;
         const int ntr = NT - t0;
         const long long ntiles = (long long)ntr * (ntr + 1) / 2;
-        if (tk != 0.0 && cta < ntiles) {
+        if (tk != 0.0 && t.cache_tiles > 0) {
+            // resident tiles: the v segments of all of them are fetched up front (independent
+            // loads), then two barriers per tile
+            const int nmine = ntiles_s > cta ? (int)((ntiles_s - 1 - cta) / G + 1) : 0;
+            constexpr int kPre = 6;
+            double prev[kPre];
+#pragma unroll
+            for (int u = 0; u < kPre; ++u) {
+                prev[u] = 0.0;
+                if (u < nmine && u < t.cache_tiles) {
+                    int cI, cJ;
+                    decode_rel(cta + (long long)u * G, t0s, cI, cJ);
+                    if (cJ >= t0) prev[u] = (tid < TB) ? vval(cI * TB + tid) : (tid < 2 * TB ? vval(cJ * TB + tid - TB) : 0.0);
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < kPre; ++u) {
+                if (u < nmine && u < t.cache_tiles) {
+                    int cI, cJ;
+                    decode_rel(cta + (long long)u * G, t0s, cI, cJ);
+                    if (cJ >= t0) {
+                        const double *Sc = cache + (size_t)u * TB * TS;
+                        if (tid < TB) vI[tid] = prev[u];
+                        else if (tid < 2 * TB) vJ[tid - TB] = prev[u];
+                        __syncthreads();
+                        const int r = tid & 63, g = tid >> 6;
+                        double acc = 0.0, acc2 = 0.0;
+#pragma unroll
+                        for (int q = 0; q < 16; ++q) acc += Sc[(g * 16 + q) * TS + r] * vJ[g * 16 + q];
+                        if (cI != cJ) {
+#pragma unroll
+                            for (int q = 0; q < 16; ++q) acc2 += Sc[r * TS + g * 16 + q] * vI[g * 16 + q];
+                        }
+                        rsum[g][r] = acc;
+                        rsJ[g][r] = acc2;
+                        __syncthreads();
+                        if (tid < TB)
+                            t.P[((size_t)cI * NT + cJ) * TB + tid] = rsum[0][tid] + rsum[1][tid] + rsum[2][tid] + rsum[3][tid];
+                        else if (cI != cJ && tid < 2 * TB)
+                            t.P[((size_t)cJ * NT + cI) * TB + tid - TB] =
+                                rsJ[0][tid - TB] + rsJ[1][tid - TB] + rsJ[2][tid - TB] + rsJ[3][tid - TB];
+                    }
+                }
+            }
+            // tiles beyond the preloaded ones (cache overflow: streamed from global memory)
+            const int ufirst = (t.cache_tiles < kPre) ? t.cache_tiles : kPre;
+            for (int u = ufirst; u < nmine; ++u) {
+                int cI, cJ;
+                decode_rel(cta + (long long)u * G, t0s, cI, cJ);
+                if (cJ < t0) continue;
+                const double *Sc;
+                if (u < t.cache_tiles) {
+                    Sc = cache + (size_t)u * TB * TS;
+                } else {
+                    __syncthreads();
+                    const int r0 = cI * TB, c0 = cJ * TB;
+                    for (int q = tid; q < TB * TB; q += kPnThreads) {
+                        const int c = q / TB, r = q % TB;
+                        const int gr = r0 + r, gc = c0 + c;
+                        S[c * TS + r] = (gr < n && gc < n) ? __ldcg(A + (size_t)gc * ld + gr) : 0.0;
+                    }
+                    if (cI == cJ) {
+                        __syncthreads();
+                        for (int q = tid; q < TB * TB; q += kPnThreads) {
+                            const int c = q / TB, r = q % TB;
+                            if (r < c) S[c * TS + r] = S[r * TS + c];
+                        }
+                    }
+                    Sc = S;
+                }
+                if (tid < TB) vI[tid] = vval(cI * TB + tid);
+                else if (tid < 2 * TB) vJ[tid - TB] = vval(cJ * TB + tid - TB);
+                __syncthreads();
+                const int r = tid & 63, g = tid >> 6;
+                double acc = 0.0, acc2 = 0.0;
+#pragma unroll
+                for (int q = 0; q < 16; ++q) acc += Sc[(g * 16 + q) * TS + r] * vJ[g * 16 + q];
+                if (cI != cJ) {
+#pragma unroll
+                    for (int q = 0; q < 16; ++q) acc2 += Sc[r * TS + g * 16 + q] * vI[g * 16 + q];
+                }
+                rsum[g][r] = acc;
+                rsJ[g][r] = acc2;
+                __syncthreads();
+                if (tid < TB)
+                    t.P[((size_t)cI * NT + cJ) * TB + tid] = rsum[0][tid] + rsum[1][tid] + rsum[2][tid] + rsum[3][tid];
+                else if (cI != cJ && tid < 2 * TB)
+                    t.P[((size_t)cJ * NT + cI) * TB + tid - TB] =
+                        rsJ[0][tid - TB] + rsJ[1][tid - TB] + rsJ[2][tid - TB] + rsJ[3][tid - TB];
+            }
+        } else if (tk != 0.0 && cta < ntiles) {
             // the next tile (and its two v slices) is loaded into registers while the
             // current one is reduced from shared memory; warp w reads columns w, w+8, ..
             // with one 512-byte coalesced row segment per instruction
@@ -209,7 +384,7 @@ __global__ void __launch_bounds__(kPnThreads, 3) dense_panel_kernel(DenseTri t) 
                 }
             }
         }
-        // owners: store v (panel column i and reflector storage); partial V^T v, W^T v
+        // owners: store v (panel column i and reflector storage)
         if (owner) {
             const int r = r_own;
             if (r > k && r < n) {
@@ -217,71 +392,97 @@ __global__ void __launch_bounds__(kPnThreads, 3) dense_panel_kernel(DenseTri t) 
                 t.V[(size_t)i * n + r] = v;
                 if (r >= k + 2) A[(size_t)k * ld + r] = v;
             }
-            const int rb = cta * kChunk;
-            for (int q = warp; q < 2 * i; q += kPnThreads / 32) {
+        }
+        // partial V^T v, W^T v: one warp per (panel column, 256-row chunk), over all CTAs
+        {
+            const int nw = G * (kPnThreads / 32);
+            for (int it = cta * (kPnThreads / 32) + warp; it < 2 * i * NO; it += nw) {
+                const int q = it / NO, c = it - q * NO;
                 const double *x = (q < i) ? t.V + (size_t)q * n : t.W + (size_t)(q - i) * n;
+                const int rb = c * kChunk;
                 double s = 0.0;
 #pragma unroll
                 for (int m = 0; m < kChunk / 32; ++m) {
                     const int rr = rb + lane + 32 * m;
-                    if (rr > k && rr < n) s += x[rr] * vval(rr);
+                    const int rc = rr < n ? rr : n - 1;
+                    const double xv = x[rc], av = t.acol[rc];
+                    const double vv = (rr <= k || rr >= n) ? 0.0 : ((rr == k + 1) ? 1.0 : av * scal);
+                    s += xv * vv;
                 }
                 s = warp_sum(s);
-                if (lane == 0) part_q[(size_t)cta * 2 * nbmax + ((q < i) ? q : nbmax + (q - i))] = s;
+                if (lane == 0) part_q[(size_t)c * 2 * nbmax + ((q < i) ? q : nbmax + (q - i))] = s;
             }
         }
-        if (!grid_sync(t.bar, t.err)) return;
-        // ---- phase D (owners): y = partial sums - V (W^T v) - W (V^T v); p = tau y
+        if (!grid_sync_counted(&t.bar->count, bar_target, t.err)) return;
+        // ---- phase D (all CTAs, eight lanes per row): y_r = sum of the partial products of
+        // row r - V (W^T v) - W (V^T v); p = tau y; partial p.v per CTA
         PROF_MARK(3);
-        if (owner) {
-            for (int q = warp; q < 2 * i; q += kPnThreads / 32) {
-                const int off = (q < i) ? q : nbmax + (q - i);
-                double s = 0.0;
-                for (int c = lane; c < NO; c += 32) s += part_q[(size_t)c * 2 * nbmax + off];
-                s = warp_sum(s);
-                if (lane == 0) s_corr[q] = s;  // [0,i): V^T v ; [i,2i): W^T v
-            }
-            __syncthreads();
-            double pv = 0.0;
-            const int r = r_own;
-            if (r > k && r < n) {
-                double y0 = 0.0, y1 = 0.0, y2 = 0.0, y3 = 0.0;
-                if (tk != 0.0) {
-                    const double *Pr = t.P + ((size_t)(r / TB) * NT) * TB + (r % TB);
-                    int c = t0;
-                    for (; c + 3 < NT; c += 4) {
-                        y0 += Pr[(size_t)c * TB];
-                        y1 += Pr[(size_t)(c + 1) * TB];
-                        y2 += Pr[(size_t)(c + 2) * TB];
-                        y3 += Pr[(size_t)(c + 3) * TB];
+        {   // s_corr[q] = (V^T v)_q, s_corr[kPw + q] = (W^T v)_q, zero for q >= i; four
+            // threads per value sum interleaved partials
+            const int qq = tid & (2 * kPw - 1), pt = tid >> 6;
+            const int q = qq & (kPw - 1);
+            const int off = (qq < kPw) ? q : nbmax + q;
+            double s = 0.0;
+            if (q < i) {
+                for (int c0 = pt; c0 < NO; c0 += 16) {
+#pragma unroll
+                    for (int u = 0; u < 4; ++u) {
+                        const int c = c0 + 4 * u;
+                        s += (c < NO) ? part_q[(size_t)c * 2 * nbmax + off] : 0.0;
                     }
-                    for (; c < NT; ++c) y0 += Pr[(size_t)c * TB];
                 }
-                double y = (y0 + y1) + (y2 + y3);
-                for (int q = 0; q < i; ++q)
-                    y -= t.V[(size_t)q * n + r] * s_corr[i + q] + t.W[(size_t)q * n + r] * s_corr[q];
-                const double p = tk * y;
-                t.ybuf[r] = p;
-                pv = p * vval(r);
             }
-            pv = block_sum(pv, red);
-            if (tid == 0) part_n[cta] = pv;
-        }
-        if (!grid_sync(t.bar, t.err)) return;
-        // ---- phase E (owners): w = p - (tau/2)(p.v) v -> W[:, i]
-        PROF_MARK(4);
-        if (owner) {
-            if (tid < 32) {
-                double s = 0.0;
-                for (int c = tid; c < NO; c += 32) s += part_n[c];
-                s = warp_sum(s);
-                if (tid == 0) s_a2 = -0.5 * tk * s;
-            }
+            s_red4[pt][qq] = s;
             __syncthreads();
-            const int r = r_own;
-            if (r > k && r < n) t.W[(size_t)i * n + r] = t.ybuf[r] + s_a2 * vval(r);
+            if (tid < 2 * kPw) s_corr[tid] = s_red4[0][tid] + s_red4[1][tid] + s_red4[2][tid] + s_red4[3][tid];
         }
-        if (!grid_sync(t.bar, t.err)) return;
+        __syncthreads();
+        {
+            double pvl = 0.0;
+            const int sub = lane >> 3, sl = lane & 7;
+            for (int rb = k + 1 + (cta * (kPnThreads / 32) + warp) * 4; rb < n; rb += G * (kPnThreads / 8)) {
+                const int r = rb + sub;
+                double y = 0.0;
+                if (r < n) {
+                    if (tk != 0.0) {
+                        const double *Pr = t.P + ((size_t)(r / TB) * NT) * TB + (r % TB);
+                        for (int c0 = t0; c0 < NT; c0 += 32) {
+#pragma unroll
+                            for (int u = 0; u < 4; ++u) {
+                                const int c = c0 + sl + 8 * u;
+                                y += (c < NT) ? Pr[(size_t)c * TB] : 0.0;
+                            }
+                        }
+                    }
+#pragma unroll
+                    for (int u = 0; u < kPw / 8; ++u) {
+                        const int q = sl + 8 * u;
+                        y -= t.V[(size_t)q * n + r] * s_corr[kPw + q] + t.W[(size_t)q * n + r] * s_corr[q];
+                    }
+                }
+                y += __shfl_xor_sync(0xffffffffu, y, 4);
+                y += __shfl_xor_sync(0xffffffffu, y, 2);
+                y += __shfl_xor_sync(0xffffffffu, y, 1);
+                if (r < n && sl == 0) {
+                    const double p = tk * y;
+                    t.ybuf[r] = p;
+                    pvl += p * vval(r);
+                }
+            }
+            pvl = block_sum(pvl, red);
+            if (tid == 0) part_d[cta] = pvl;
+        }
+        if (!grid_sync_counted(&t.bar->count, bar_target, t.err)) return;
+    }
+    // w of the panel's last column (the kernel boundary orders it before the trailing update)
+    PROF_MARK(4);
+    {
+        const int ip = t.nb - 1, kp = t.j0 + ip;
+        const double a2 = prev_scale(tprev);
+        if (owner) {
+            const int r = r_own;
+            if (r > kp && r < n) t.W[(size_t)ip * n + r] = t.ybuf[r] + a2 * t.V[(size_t)ip * n + r];
+        }
     }
     PROF_MARK(5);
 }
@@ -739,26 +940,55 @@ cudaError_t launch_dense_backtransform(const double *A, long long lda, int n, co
 int dense_tridiag_grid(int device) {
     int nsm = 0, per = 0;
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dense_panel_kernel, kPnThreads, 0);
+    cudaFuncSetAttribute(dense_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, 64 * 1024);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dense_panel_kernel, kPnThreads, (size_t)TB * TS * sizeof(double));
     if (per < 1) per = 1;
     return nsm * std::min(per, 3);
 }
 
-int dense_panel_width() { return 32; }
+int dense_panel_width() { return kPw; }
+
+int dense_resident_plan(int device, int n, int *grid) {
+    // one CTA per SM with as many 64 x 64 tiles as fit next to the scratch tile; used while
+    // most of the lower tiles of the matrix fit on chip (about n <= 2900 on B200)
+    int nsm = 0, smem_optin = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, device);
+    cudaDeviceGetAttribute(&smem_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, device);
+    const size_t tile = (size_t)TB * TS * sizeof(double);
+    const int slots = (int)((smem_optin - 8 * 1024) / tile) - 1;  // static shared memory kept aside
+    if (slots < 1) return 0;
+    const long long NT = (n + TB - 1) / TB, ntiles = NT * (NT + 1) / 2;
+    if (ntiles > (long long)nsm * slots * 5 / 4) return 0;
+    cudaError_t e = cudaFuncSetAttribute(dense_panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)(((size_t)slots + 1) * tile));
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    int per = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, dense_panel_kernel, kPnThreads, ((size_t)slots + 1) * tile);
+    if (per < 1) return 0;
+    *grid = nsm;
+    return slots;
+}
 
 cudaError_t launch_dense_tridiag(DenseTri &t, int grid, cudaStream_t st) {
     const int n = t.n;
     const int nb = t.nbmax;
+    if (nb != kPw) return cudaErrorInvalidValue;
     int npanel = 0;
+    t.bar_base = 0;
     for (int j0 = 0; j0 + 2 < n; j0 += nb) {
         t.j0 = j0;
         t.nb = std::min(nb, n - 2 - j0);
         void *args[] = {&t};
         if (t.ev && 2 * npanel + 1 < t.nev) cudaEventRecord(t.ev[2 * npanel], st);
         DVR3D_COUNT_LAUNCH(1);
-        cudaError_t e = cudaLaunchCooperativeKernel((void *)dense_panel_kernel, dim3(grid), dim3(kPnThreads), args, 0, st);
+        const size_t smem = ((size_t)t.cache_tiles + 1) * TB * TS * sizeof(double);
+        cudaError_t e = cudaLaunchCooperativeKernel((void *)dense_panel_kernel, dim3(grid), dim3(kPnThreads), args, smem, st);
         if (t.ev && 2 * npanel + 1 < t.nev) cudaEventRecord(t.ev[2 * npanel + 1], st);
         ++npanel;
+        t.bar_base += 3u * (unsigned)t.nb * (unsigned)grid;  // three barriers per column
         if (e != cudaSuccess) return e;
         const int j1 = j0 + t.nb;
         if (j1 < n) {

@@ -15,16 +15,22 @@ struct DenseTri {
     double *V, *W;                // n x nbmax panels (ld = n)
     double *acol, *ybuf;          // [n]
     double *P;                    // symmetric-product partial sums, NT * NT * 64
-    double *part;                 // [grid * (1 + 2 nbmax)]
+    double *part;                 // [grid * (2 + 2 nbmax)]
     int NT;                       // number of 64-row blocks covering n
     int j0, nb, nbmax;            // current panel
-    GridBarrier *bar;             // zeroed before launch
+    GridBarrier *bar;             // zeroed before the first panel
+    unsigned int bar_base;        // barrier arrivals made by earlier panels (set by the launcher)
     int *err;
     long long *prof;              // optional [6] phase clock accumulators (CTA 0), or null
     cudaEvent_t *ev;              // optional event pool timing each panel launch (2 per panel)
     int nev;
     int npanel;                   // out: panel launches made
+    int cache_tiles;              // > 0: resident mode, tiles kept in shared memory per CTA
 };
+
+// Resident mode for small matrices: returns the tiles per CTA (0: not applicable) and the
+// grid to launch with.
+int dense_resident_plan(int device, int n, int *grid);
 
 int dense_tridiag_grid(int device);
 int dense_panel_width();

@@ -198,16 +198,36 @@ __global__ void __launch_bounds__(kThr) gemm_pipe_kernel(GemmOp p, int tiles_m) 
             }
 }
 
-__global__ void splitk_reduce_kernel(GemmOp p, int S) {
-    const long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= (long long)p.M * p.N) return;
-    const int i = (int)(t % p.M), j = (int)(t / p.M);
-    if (p.lower_out && j > i) return;
+// Sum of the S partial tiles: a block covers 32 consecutive rows of one column; its eight
+// warps take every eighth slice (eight independent loads in flight per thread) and add
+// their sums through shared memory.
+__global__ void __launch_bounds__(256) splitk_reduce_kernel(GemmOp p, int S) {
+    __shared__ double part[8][33];
+    const int lane = threadIdx.x & 31, g = threadIdx.x >> 5;
+    const int i = blockIdx.x * 32 + lane, j = blockIdx.y;
+    const bool live = i < p.M && !(p.lower_out && j > i);
     double s = 0.0;
-    for (int z = 0; z < S; ++z) s += p.work[((size_t)z * p.N + j) * p.M + i];
-    double *cp = p.C + (size_t)j * p.ldc + i;
-    const double old = (p.beta != 0.0) ? *cp : 0.0;
-    *cp = p.alpha * s + p.beta * old;
+    if (live) {
+        const double *w = p.work + (size_t)j * p.M + i;
+        const size_t zs = (size_t)p.N * p.M;
+        for (int z0 = g; z0 < S; z0 += 64) {
+#pragma unroll
+            for (int u = 0; u < 8; ++u) {
+                const int z = z0 + 8 * u;
+                s += (z < S) ? w[(size_t)z * zs] : 0.0;
+            }
+        }
+    }
+    part[g][lane] = s;
+    __syncthreads();
+    if (g == 0 && live) {
+        double t = 0.0;
+#pragma unroll
+        for (int q = 0; q < 8; ++q) t += part[q][lane];
+        double *cp = p.C + (size_t)j * p.ldc + i;
+        const double old = (p.beta != 0.0) ? *cp : 0.0;
+        *cp = p.alpha * t + p.beta * old;
+    }
 }
 
 template <bool TA, bool TB, int BN, bool CL>
@@ -258,15 +278,14 @@ cudaError_t launch_gemm(const GemmOp &p0, cudaStream_t st) {
     int S = std::max(1, p.splitk);
     if (p.K <= 0) S = 1;
     const bool cl = (S > 1 && S <= kMaxClusterSplit);
-    if (S > 1 && !cl && !p.work) return cudaErrorInvalidValue;
+    if (S > 1 && !cl && (!p.work || p.N > 65535)) return cudaErrorInvalidValue;
     const int bn = (p.N <= 32 && !p.lower_out) ? 32 : 64;
     cudaError_t e;
     if (cl) e = (bn == 32) ? launch_bn<32, true>(p, S, st) : launch_bn<64, true>(p, S, st);
     else e = (bn == 32) ? launch_bn<32, false>(p, S, st) : launch_bn<64, false>(p, S, st);
     if (e != cudaSuccess || S == 1 || cl) return e;
-    const long long tot = (long long)p.M * p.N;
     DVR3D_COUNT_LAUNCH(1);
-    splitk_reduce_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(p, S);
+    splitk_reduce_kernel<<<dim3((unsigned)((p.M + 31) / 32), (unsigned)p.N), 256, 0, st>>>(p, S);
     return cudaGetLastError();
 }
 

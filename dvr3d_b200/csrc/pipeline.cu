@@ -618,16 +618,19 @@ void dense_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int nev, bool
     dt.d = ctx->arena.get_t<double>(t + "d", n);
     dt.e = ctx->arena.get_t<double>(t + "e", n);
     dt.tau = ctx->arena.get_t<double>(t + "tau", n);
-    const int G = ctx->dense_grid;
+    int G = ctx->dense_grid;
     if ((long long)n > 256LL * G) throw HostError{DVR3D_ERR_UNSUPPORTED, "matrix too large for the dense eigensolver"};
     dt.nbmax = dense_panel_width();
     dt.NT = (n + 63) / 64;
     dt.V = ctx->arena.get_t<double>(t + "V", (size_t)n * dt.nbmax);
     dt.W = ctx->arena.get_t<double>(t + "W", (size_t)n * dt.nbmax);
+    // the panel kernel reads all panel columns of V and W unconditionally: finite values
+    CK(cudaMemsetAsync(dt.V, 0, sizeof(double) * n * dt.nbmax, st));
+    CK(cudaMemsetAsync(dt.W, 0, sizeof(double) * n * dt.nbmax, st));
     dt.acol = ctx->arena.get_t<double>(t + "acol", n);
     dt.ybuf = ctx->arena.get_t<double>(t + "y", n);
     dt.P = ctx->arena.get_t<double>(t + "P", (size_t)dt.NT * dt.NT * 64);
-    dt.part = ctx->arena.get_t<double>(t + "part", (size_t)G * (1 + 2 * dt.nbmax));
+    dt.part = ctx->arena.get_t<double>(t + "part", (size_t)G * (2 + 2 * dt.nbmax));
     dt.bar = ctx->arena.get_t<GridBarrier>(t + "bar", 1);
     dt.err = ctx->arena.get_t<int>(t + "err", 1);
     CK(cudaMemsetAsync(dt.bar, 0, sizeof(GridBarrier), st));
@@ -647,6 +650,14 @@ void dense_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int nev, bool
         }
         dt.ev = ctx->panel_ev.data();
         dt.nev = (int)ctx->panel_ev.size();
+    }
+    {
+        int gres = 0;
+        const int slots = dense_resident_plan(ctx->device, n, &gres);
+        if (slots > 0 && gres <= G) {
+            dt.cache_tiles = slots;
+            G = gres;
+        }
     }
     CK(launch_dense_tridiag(dt, G, st));
     if (prof) {

@@ -176,7 +176,6 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
     double *Q = ctx->arena.get_t<double>("si_Q", (size_t)ldq * (mmax + b));
     double *T = ctx->arena.get_t<double>("si_T", (size_t)ldT * mmax);
     double *Y1 = ctx->arena.get_t<double>("si_Y1", (size_t)ldq * b);
-    double *W = ctx->arena.get_t<double>("si_W", (size_t)ldq * b);
     double *G = ctx->arena.get_t<double>("si_G", 64 * 64);
     double *Gi = ctx->arena.get_t<double>("si_Gi", 64 * 64);
     double *proj = ctx->arena.get_t<double>("si_P", (size_t)mmax * b);
@@ -270,6 +269,8 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
             y.splitk = trmm_s;
             y.work = work;
             CK(launch_gemm(y, st));
+            // the new block is formed in place in its slot of Q (not read by the projections)
+            double *W = Q + (size_t)(s + 1) * b * ldq;
             GemmOp w = y;
             w.ta = true;
             w.tri = 2;
@@ -314,10 +315,7 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
                     CK(cudaGetLastError());
                 }
             }
-            double *Qn = Q + (size_t)(s + 1) * b * ldq;
-            CK(cudaMemcpy2DAsync(Qn, ldq * sizeof(double), W, ldq * sizeof(double), (size_t)N * sizeof(double), b,
-                                 cudaMemcpyDeviceToDevice, st));
-            cholqr(Qn);
+            cholqr(W);
             flops += 2.0 * (double)N * N * b + 8.0 * (double)N * m * b + 8.0 * (double)N * b * b;
         }
         tk.stop(st);
