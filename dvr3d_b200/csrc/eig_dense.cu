@@ -1014,10 +1014,9 @@ void launch_dense_eigvals(const double *d, const double *e, int n, int nev, doub
         d, e2, n, nev, info, w);
 }
 
-void launch_dense_eigvecs(const double *A, long long lda, int n, const double *d, const double *e,
-                          const double *tau, const double *w, int nev,
-                          const double *info, int *cstart, int *ncl, double *fac, int T, double *X,
-                          double *Z, long long ldz, double *bt_work, cudaStream_t st) {
+void launch_tridiag_eigvecs(const double *d, const double *e, int n, const double *w, int nev, const double *info,
+                            int *cstart, int *ncl, double *fac, int T, double *X, double *Z, long long ldz,
+                            cudaStream_t st) {
     DVR3D_COUNT_LAUNCH(1);
     clusters_kernel<<<1, 32, 0, st>>>(w, nev, info, cstart, ncl);
     const size_t smem = invit_smem_bytes(n);
@@ -1035,6 +1034,13 @@ void launch_dense_eigvecs(const double *A, long long lda, int n, const double *d
         const long long tot = (long long)n * nev;
         untangle_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(X, n, nev, Z, ldz);
     }
+}
+
+void launch_dense_eigvecs(const double *A, long long lda, int n, const double *d, const double *e,
+                          const double *tau, const double *w, int nev,
+                          const double *info, int *cstart, int *ncl, double *fac, int T, double *X,
+                          double *Z, long long ldz, double *bt_work, cudaStream_t st) {
+    launch_tridiag_eigvecs(d, e, n, w, nev, info, cstart, ncl, fac, T, X, Z, ldz, st);
     if (bt_work && !(ldz & 1)) {
         launch_dense_backtransform(A, lda, n, tau, Z, ldz, nev, bt_work, st);
     } else {

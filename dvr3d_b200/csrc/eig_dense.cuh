@@ -45,6 +45,10 @@ void launch_dense_eigvals(const double *d, const double *e, int n, int nev, doub
 constexpr int kInvitSmemMax = 200 * 1024;
 size_t invit_smem_bytes(int n);
 size_t dense_bt_work_doubles(int n, int nev);
+// Eigenvectors of the tridiagonal (d, e) for the nev eigenvalues w into Z (no back-transform).
+void launch_tridiag_eigvecs(const double *d, const double *e, int n, const double *w, int nev, const double *info,
+                            int *cstart, int *ncl, double *fac, int T, double *X, double *Z, long long ldz,
+                            cudaStream_t st);
 void launch_dense_eigvecs(const double *A, long long lda, int n, const double *d, const double *e,
                           const double *tau, const double *w, int nev,
                           const double *info, int *cstart, int *ncl, double *fac, int T, double *X,

@@ -14,6 +14,7 @@
 
 #include "blocks.cuh"
 #include "eig_batched.cuh"
+#include "band_eig.cuh"
 #include "eig_dense.cuh"
 #include "gemm64.cuh"
 #include "learned_precond.cuh"
@@ -693,6 +694,53 @@ void dense_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int nev, bool
             out->panel_ms += m;
         }
     }
+}
+
+// ---------------------------------------------------------------- band eigensolver
+bool band_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int b, int nev, double *w, double *Z,
+                 long long ldz, double drop_rel, double *dropped_rel) {
+    cudaStream_t st = ctx->stream;
+    if (b < 1 || b > kBandMaxBw || n < 3 || nev > n) return false;
+    auto *mx = ctx->arena.get_t<unsigned long long>("bd_max", 2);
+    CK(launch_band_prepare(A, lda, n, b, mx, st));
+    unsigned long long hb[2] = {0, 0};
+    CK(cudaMemcpyAsync(hb, mx, sizeof(hb), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    note_d2h(sizeof(hb));
+    double dropped, inside;
+    std::memcpy(&dropped, &hb[0], sizeof(double));
+    std::memcpy(&inside, &hb[1], sizeof(double));
+    const double rel = inside > 0.0 ? dropped / inside : (dropped > 0.0 ? 1.0 : 0.0);
+    if (dropped_rel) *dropped_rel = rel;
+    if (!(rel <= drop_rel)) return false;
+    BandTri t{};
+    t.A = A;
+    t.lda = lda;
+    t.n = n;
+    t.b = b;
+    t.d = ctx->arena.get_t<double>("bd_d", n);
+    t.e = ctx->arena.get_t<double>("bd_e", n);
+    t.vs = ctx->arena.get_t<double>("bd_vs", band_reflector_doubles(n, b));
+    t.taus = ctx->arena.get_t<double>("bd_tau", band_tau_doubles(n, b));
+    t.progress = ctx->arena.get_t<unsigned int>("bd_prog", n);
+    t.err = ctx->arena.get_t<int>("bd_err", 1);
+    CK(cudaMemsetAsync(t.err, 0, sizeof(int), st));
+    CK(launch_band_chase(t, st));
+    check_dev_err(ctx, t.err, "band reduction");
+    double *e2s = ctx->arena.get_t<double>("bd_e2", n);
+    double *info = ctx->arena.get_t<double>("bd_info", 4);
+    launch_dense_eigvals(t.d, t.e, n, nev, e2s, info, w, st);
+    CK(cudaGetLastError());
+    const int T = std::min(nev, 1024);
+    const bool smem = invit_smem_bytes(n) <= (size_t)kInvitSmemMax;
+    double *fac = smem ? nullptr : ctx->arena.get_t<double>("bd_fac", (size_t)5 * n * T);
+    double *X = smem ? nullptr : ctx->arena.get_t<double>("bd_x", (size_t)n * nev);
+    int *cs = ctx->arena.get_t<int>("bd_cs", nev + 1);
+    int *ncl = ctx->arena.get_t<int>("bd_ncl", 1);
+    launch_tridiag_eigvecs(t.d, t.e, n, w, nev, info, cs, ncl, fac, T, X, Z, ldz, st);
+    CK(cudaGetLastError());
+    CK(launch_band_backtransform(t, Z, ldz, nev, st));
+    return true;
 }
 
 // ---------------------------------------------------------------- one k block

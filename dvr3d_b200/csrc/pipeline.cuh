@@ -124,6 +124,12 @@ struct DenseOut {
 };
 void dense_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int nev, bool vecs, double *w, double *Z,
                   long long ldz, const char *tag, bool time_panels, DenseOut *out);
+// Lowest nev eigenpairs of a symmetric matrix (lower triangle of A, lda) treated as a band
+// of half-bandwidth b (<= 32): bulge chasing, tridiagonal eigensolve, back-transform into Z.
+// Returns false (nothing computed) when the entries beyond the band exceed drop_rel times
+// the largest entry inside it; *dropped_rel receives that ratio.
+bool band_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int b, int nev, double *w, double *Z,
+                 long long ldz, double drop_rel, double *dropped_rel);
 
 // Shift-invert block Krylov solve for the lowest `nwant` levels of the assembled H3
 // (full symmetric storage, ldh even). emin_bound: a lower bound of the spectrum (min e2).

@@ -27,6 +27,7 @@
 #include <numeric>
 #include <vector>
 
+#include "band_eig.cuh"
 #include "chol.cuh"
 #include "common.cuh"
 #include "gemm64.cuh"
@@ -337,7 +338,16 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
         double *Yv = ctx->arena.get_t<double>("si_Yv", (size_t)m * kw);
         Timer td;
         td.start(st);
-        dense_lowest(ctx, A, lda, m, kw, true, lam, Yv, m, "si_", false, nullptr);
+        // T is block tridiagonal up to the rounding-level reorthogonalisation coefficients:
+        // chase its band unless those are not small (then the dense reduction)
+        double dropped = 0.0;
+        const bool banded = b <= kBandMaxBw && band_lowest(ctx, A, lda, m, b, kw, lam, Yv, m, 1.0e-11, &dropped);
+        if (!banded) {
+            DVR3D_COUNT_LAUNCH(1);
+            upper_sym_neg_kernel<<<nb256((long long)m * m), 256, 0, st>>>(T, ldT, m, A, lda);
+            CK(cudaGetLastError());
+            dense_lowest(ctx, A, lda, m, kw, true, lam, Yv, m, "si_", false, nullptr);
+        }
         td.stop(st);
         double *X = ctx->arena.get_t<double>("si_X", (size_t)ldq * kw);
         double *HX = ctx->arena.get_t<double>("si_HX", (size_t)ldq * kw);
@@ -396,7 +406,9 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
             std::fprintf(stderr, "si_krylov: N=%d b=%d sigma=%.6e retries=%d m=%d converged %d/%d worst bound %.3e Eh "
                                  "(krylov %.2f ms, rr %.2f ms so far)\n",
                          N, b, sigma, ks.retries, m, nconv, nwant, worst, tk_ms, tr_ms);
-        if (trace) std::fprintf(stderr, "si_krylov: dense eigensolve of T (m=%d, %d vectors) %.2f ms\n", m, kw, td.ms());
+        if (trace)
+            std::fprintf(stderr, "si_krylov: %s eigensolve of T (m=%d, %d vectors, entries beyond the band %.2e of max) %.2f ms\n",
+                         banded ? "band" : "dense", m, kw, dropped, td.ms());
         if (nconv == nwant) {
             done = true;
             break;
