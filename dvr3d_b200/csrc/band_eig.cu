@@ -34,7 +34,7 @@ namespace {
 
 constexpr int kBW = kBandMaxBw;
 constexpr int kTS = kBW + 1;            // shared-memory row stride of a block
-constexpr int kChaseThreads = 128;      // four warps per sweep in flight
+constexpr int kChaseThreads = 160;      // five warps per sweep in flight
 constexpr int kBlk = kBW * kTS;         // doubles of one 32 x 32 block in shared memory
 constexpr size_t kChaseSmem = ((size_t)6 * kBlk + 3 * kBW) * sizeof(double);
 constexpr unsigned long long kSpinLimit = 1ull << 24;
@@ -93,14 +93,17 @@ __device__ __forceinline__ void warp_house(double x, int lane, int L, double &v,
     }
 }
 
-// One CTA per sweep in flight, four warps with fixed roles per task s:
-//   warp 0: the reflector (from column j or the bulge's first column), then O_s <- H O_s,
-//           written back, and the task published to the next sweep;
+// One CTA per sweep in flight, five warps with fixed roles per task s:
+//   warp 0: the reflector (from column j or the bulge's first column); its beta is written
+//           and the task published to the next sweep at once (the next sweep's task s-2,
+//           which this publication releases, shares only that entry with task s); then
+//           O_s <- H O_s, written back;
 //   warp 1: D_s <- H D_s H, written back (lower triangle);
 //   warp 2: O_{s+1} <- O_{s+1} H, kept in shared memory for task s+1;
-//   warp 3: waits for the previous sweep and loads task s+1's blocks (prefetch).
-// Warps 0-2 start after the reflector is in shared memory; all four meet at the end of the
-// task. The last task of a sweep is published only when all its parts are written.
+//   warps 3, 4: wait for the previous sweep and load task s+1's O_{s+2} and D_{s+1}.
+// Warps 0-2 start after the reflector is in shared memory; all five meet at the end of the
+// task, so a publication also covers everything of the earlier tasks. The last task of a
+// sweep is published only when all its parts are written.
 __global__ void __launch_bounds__(kChaseThreads) band_chase_kernel(BandTri t) {
     extern __shared__ double sm[];
     double *Ob = sm;                   // [2] O_s (held from the previous task) / O_{s+1}
@@ -127,8 +130,9 @@ __global__ void __launch_bounds__(kChaseThreads) band_chase_kernel(BandTri t) {
             tlast = now;
         }
     };
-    // warp 3: wait until sweep j-1 has published `need` tasks, then load task s's blocks
-    auto load_task = [&](int j, int s, int buf, int need) {
+    // warps 3 (which = 0: O_{s+1}, and column j for task 0) and 4 (which = 1: D_s): wait
+    // until sweep j-1 has published `need` tasks, then load task s's block
+    auto load_task = [&](int j, int s, int buf, int need, int which) {
         if (j > 0) {
             int ok = 1;
             if (lane == 0) {
@@ -156,30 +160,35 @@ __global__ void __launch_bounds__(kChaseThreads) band_chase_kernel(BandTri t) {
         const int r0 = j + 1 + s * b, L = min(b, n - r0);
         const int r1 = r0 + b, L1 = (r1 < n) ? min(b, n - r1) : 0;
         const int rl = min(r0 + lane, n - 1), rl1 = min(r1 + lane, n - 1);
-        double dv[kBW], ov[kBW];
+        double val[kBW];
+        if (which == 1) {
 #pragma unroll
-        for (int c = 0; c < kBW; ++c) {
-            const size_t col = (size_t)min(r0 + c, n - 1) * ld;
-            const double a0 = __ldcg(A + col + rl);
-            const double a1 = __ldcg(A + col + rl1);
-            dv[c] = (c < L && lane >= c && lane < L) ? a0 : 0.0;
-            ov[c] = (c < b && lane < L1) ? a1 : 0.0;
-        }
-        if (s == 0) {
-            const double xv = __ldcg(A + (size_t)j * ld + rl);
-            Xr[lane] = (lane < L) ? xv : 0.0;
-        }
-        double *D = Dr + buf * kBlk, *O = Orw + buf * kBlk;
+            for (int c = 0; c < kBW; ++c) {
+                const double a0 = __ldcg(A + (size_t)min(r0 + c, n - 1) * ld + rl);
+                val[c] = (c < L && lane >= c && lane < L) ? a0 : 0.0;
+            }
+            double *D = Dr + buf * kBlk;
 #pragma unroll
-        for (int c = 0; c < kBW; ++c) {
-            D[lane * kTS + c] = dv[c];
-            O[lane * kTS + c] = ov[c];
+            for (int c = 0; c < kBW; ++c) D[lane * kTS + c] = val[c];
+        } else {
+#pragma unroll
+            for (int c = 0; c < kBW; ++c) {
+                const double a1 = __ldcg(A + (size_t)min(r0 + c, n - 1) * ld + rl1);
+                val[c] = (c < b && lane < L1) ? a1 : 0.0;
+            }
+            if (s == 0) {
+                const double xv = __ldcg(A + (size_t)j * ld + rl);
+                Xr[lane] = (lane < L) ? xv : 0.0;
+            }
+            double *O = Orw + buf * kBlk;
+#pragma unroll
+            for (int c = 0; c < kBW; ++c) O[lane * kTS + c] = val[c];
         }
     };
     for (int j = blockIdx.x; j <= n - 3; j += gridDim.x) {
         const int nt = band_ntask(n, b, j);
         const int ntp = (j > 0) ? band_ntask(n, b, j - 1) : 0;
-        if (warp == 3) load_task(j, 0, 0, min(3, ntp));
+        if (warp >= 3) load_task(j, 0, 0, min(3, ntp), warp - 3);
         __syncthreads();
         if (s_abort) return;
         mark(0);
@@ -200,6 +209,18 @@ __global__ void __launch_bounds__(kChaseThreads) band_chase_kernel(BandTri t) {
                     t.taus[(size_t)j * t.ntmax + s] = tau;
                 }
                 t.vs[((size_t)j * t.ntmax + s) * kBW + lane] = v;
+                // beta at once, then the publication (the rest of O_s follows below)
+                if (lane == 0) {
+                    if (s == 0) A[(size_t)j * ld + r0] = beta;
+                    else A[(size_t)(r0 - b) * ld + r0] = beta;
+                }
+                if (s + 1 < nt) {
+                    __syncwarp();
+                    if (lane == 0) {
+                        __threadfence();
+                        st_release_u32(t.progress + j, (unsigned)(s + 1));
+                    }
+                }
             }
             __syncthreads();
             mark(1);
@@ -227,13 +248,6 @@ __global__ void __launch_bounds__(kChaseThreads) band_chase_kernel(BandTri t) {
                     if (lane < L) {
                         double *dst = A + (size_t)(r0 - b) * ld + r0 + lane;
                         for (int c = 0; c < b; ++c) dst[(size_t)c * ld] = Oc[lane * kTS + c];
-                    }
-                }
-                if (s + 1 < nt) {
-                    __syncwarp();
-                    if (lane == 0) {
-                        __threadfence();
-                        st_release_u32(t.progress + j, (unsigned)(s + 1));
                     }
                 }
             } else if (warp == 1) {
@@ -274,7 +288,7 @@ __global__ void __launch_bounds__(kChaseThreads) band_chase_kernel(BandTri t) {
                     for (int c = 0; c < kBW; ++c) On[lane * kTS + c] = Oraw[lane * kTS + c] - u * vsm[c];
                 }
             } else {
-                if (s + 1 < nt) load_task(j, s + 1, cur ^ 1, min(s + 4, ntp));
+                if (s + 1 < nt) load_task(j, s + 1, cur ^ 1, min(s + 4, ntp), warp - 3);
             }
             mark(2);
             __syncthreads();
@@ -300,95 +314,97 @@ __global__ void band_diag_kernel(const double *A, long long lda, int n, double *
 }
 
 // Back-transformation, COLS eigenvector columns per CTA held in shared memory (column c at
-// zs + c n). Sweeps are applied last first; the tasks of one sweep act on disjoint rows and
-// are split over the 8 warps, item k of warp w being task w + 8 k of a chunk of 8 kItems
-// tasks. A warp applies its reflector to all COLS columns at once (independent dot products
-// in flight); the reflectors of the next chunk are loaded while the current one is applied.
-constexpr int kItems = 12;
+// zs + c ldzs, ldzs = 1 mod 16 so the lanes' rows and columns spread over the banks).
+// Sweeps are applied last first; the tasks of one sweep act on disjoint rows and are split
+// over the 8 warps (task w + 8 k of a chunk of kChunkTasks). In a warp, lane (rg, c) takes
+// column c and rows COLS rg .. COLS rg + COLS - 1 of the reflector's window: COLS products,
+// a shuffle sum over the 32 / COLS row groups, COLS updates. The reflectors of the next
+// chunk are copied into shared memory (cp.async) while the current chunk is applied.
+constexpr int kChunkTasks = 96;
+
+__device__ __forceinline__ void cp_async8(double *dst, const double *src) {
+    const unsigned d = (unsigned)__cvta_generic_to_shared(dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(d), "l"(src) : "memory");
+}
 
 template <int COLS>
-__global__ void __launch_bounds__(256) band_bt_kernel(BandTri t, double *Z, long long ldz, int nev) {
-    extern __shared__ double zs[];
+__global__ void __launch_bounds__(256) band_bt_kernel(BandTri t, double *Z, long long ldz, int nev, int ldzs) {
+    extern __shared__ double sm[];
+    double *zs = sm;
+    double *vb = sm + (size_t)COLS * ldzs;       // [2][kChunkTasks][kBW]
+    double *tb = vb + 2 * kChunkTasks * kBW;     // [2][kChunkTasks]
     const int n = t.n, b = t.b;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int cc = lane % COLS, rg = lane / COLS;
     const int c0 = blockIdx.x * COLS;
     const int ncol = min(COLS, nev - c0);
-    for (int q = threadIdx.x; q < COLS * n; q += blockDim.x) {
+    for (int q = tid; q < COLS * n; q += blockDim.x) {
         const int c = q / n, r = q - c * n;
-        zs[q] = (c < ncol) ? Z[(size_t)(c0 + c) * ldz + r] : 0.0;
+        zs[(size_t)c * ldzs + r] = (c < ncol) ? Z[(size_t)(c0 + c) * ldz + r] : 0.0;
     }
-    constexpr int kChunkTasks = 8 * kItems;
-    double vc[kItems], tc[kItems], vn[kItems], tn[kItems];
-    auto load = [&](int j, int base, double *vv, double *tt) {
-        const int nt = band_ntask(n, b, j);
-#pragma unroll
-        for (int k = 0; k < kItems; ++k) {
-            const int s = base + warp + 8 * k;
-            const bool ok = s < nt;
-            vv[k] = ok ? __ldg(t.vs + ((size_t)j * t.ntmax + s) * kBW + lane) : 0.0;
-            tt[k] = ok ? __ldg(t.taus + (size_t)j * t.ntmax + s) : 0.0;
-        }
+    auto stage = [&](int j, int base, int buf) {
+        const int cnt = min(kChunkTasks, band_ntask(n, b, j) - base);
+        const double *vsrc = t.vs + ((size_t)j * t.ntmax + base) * kBW;
+        double *vd = vb + (size_t)buf * kChunkTasks * kBW;
+        for (int q = tid; q < cnt * kBW; q += blockDim.x) cp_async8(vd + q, vsrc + q);
+        const double *tsrc = t.taus + (size_t)j * t.ntmax + base;
+        double *td = tb + buf * kChunkTasks;
+        for (int q = tid; q < cnt; q += blockDim.x) cp_async8(td + q, tsrc + q);
+        asm volatile("cp.async.commit_group;" ::: "memory");
     };
-    int j = n - 3, base = 0;
-    if (j >= 0) load(j, base, vn, tn);
-    __syncthreads();
+    int j = n - 3, base = 0, buf = 0;
+    if (j >= 0) stage(j, base, buf);
     while (j >= 0) {
-#pragma unroll
-        for (int k = 0; k < kItems; ++k) {
-            vc[k] = vn[k];
-            tc[k] = tn[k];
-        }
-        const int cj = j, cbase = base;
-        // next chunk: the rest of this sweep, else the next sweep (last first)
+        asm volatile("cp.async.wait_group 0;" ::: "memory");
+        __syncthreads();  // chunk (j, base) staged; the previous chunk's updates are done
+        const int cj = j, cbase = base, cbuf = buf;
         base += kChunkTasks;
         if (base >= band_ntask(n, b, j)) {
             --j;
             base = 0;
         }
-        if (j >= 0) load(j, base, vn, tn);
-        const int nit = (band_ntask(n, b, cj) - cbase - warp + 7) / 8;  // this warp's tasks in the chunk
-#pragma unroll
-        for (int k = 0; k < kItems; ++k) {
-            if (k >= nit) break;
-            const int s = cbase + warp + 8 * k;
+        buf ^= 1;
+        if (j >= 0) stage(j, base, buf);
+        const double *vd = vb + (size_t)cbuf * kChunkTasks * kBW;
+        const double *td = tb + cbuf * kChunkTasks;
+        const int nt = band_ntask(n, b, cj);
+        for (int s = cbase + warp; s < nt && s < cbase + kChunkTasks; s += 8) {
+            const double tau = td[s - cbase];
+            if (tau == 0.0) continue;
             const int r0 = cj + 1 + s * b;
-            const int L = min(b, n - r0);
-            const bool in = lane < L;
-            const double v = vc[k];
-            const int ri = in ? r0 + lane : 0;
-            double z[COLS], dot[COLS];
+            const double *v = vd + (size_t)(s - cbase) * kBW + rg * COLS;
+            double vv[COLS], zz[COLS];
+            double part = 0.0;
 #pragma unroll
-            for (int c = 0; c < COLS; ++c) {
-                z[c] = zs[c * n + ri];
-                dot[c] = in ? v * z[c] : 0.0;
+            for (int i = 0; i < COLS; ++i) {
+                const int r = min(r0 + rg * COLS + i, n - 1);
+                vv[i] = v[i];
+                zz[i] = zs[(size_t)cc * ldzs + r];
+                part += vv[i] * zz[i];
             }
 #pragma unroll
-            for (int o = 16; o > 0; o >>= 1) {
+            for (int o = COLS; o < 32; o <<= 1) part += __shfl_xor_sync(kFull, part, o);
+            const double f = tau * part;
 #pragma unroll
-                for (int c = 0; c < COLS; ++c) dot[c] += __shfl_xor_sync(kFull, dot[c], o);
+            for (int i = 0; i < COLS; ++i) {
+                const int r = r0 + rg * COLS + i;
+                if (vv[i] != 0.0 && r < n) zs[(size_t)cc * ldzs + r] = zz[i] - f * vv[i];
             }
-#pragma unroll
-            for (int c = 0; c < COLS; ++c)
-                if (in) zs[c * n + ri] = z[c] - tc[k] * dot[c] * v;
         }
-        // tasks of one chunk are independent; successive chunks of a sweep too, but the
-        // next sweep overlaps this one
-        if (base == 0) __syncthreads();
     }
     __syncthreads();
-    for (int q = threadIdx.x; q < COLS * n; q += blockDim.x) {
+    for (int q = tid; q < COLS * n; q += blockDim.x) {
         const int c = q / n, r = q - c * n;
-        if (c < ncol) Z[(size_t)(c0 + c) * ldz + r] = zs[q];
+        if (c < ncol) Z[(size_t)(c0 + c) * ldz + r] = zs[(size_t)c * ldzs + r];
     }
 }
 
 template <int COLS>
-cudaError_t launch_bt(const BandTri &t, double *Z, long long ldz, int nev, cudaStream_t st) {
-    const size_t smem = (size_t)COLS * t.n * sizeof(double);
+cudaError_t launch_bt(const BandTri &t, double *Z, long long ldz, int nev, int ldzs, size_t smem, cudaStream_t st) {
     cudaError_t e = cudaFuncSetAttribute(band_bt_kernel<COLS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     DVR3D_COUNT_LAUNCH(1);
-    band_bt_kernel<COLS><<<(unsigned)((nev + COLS - 1) / COLS), 256, smem, st>>>(t, Z, ldz, nev);
+    band_bt_kernel<COLS><<<(unsigned)((nev + COLS - 1) / COLS), 256, smem, st>>>(t, Z, ldz, nev, ldzs);
     return cudaGetLastError();
 }
 
@@ -440,15 +456,23 @@ cudaError_t launch_band_chase(BandTri &t, cudaStream_t st) {
 
 cudaError_t launch_band_backtransform(const BandTri &t, double *Z, long long ldz, int nev, cudaStream_t st) {
     if (nev <= 0 || t.n < 3) return cudaSuccess;
-    int optin = 0, dev = 0;
+    int optin = 0, dev = 0, nsm = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const size_t per_col = (size_t)t.n * sizeof(double);
-    if (8 * per_col <= (size_t)optin) return launch_bt<8>(t, Z, ldz, nev, st);
-    if (4 * per_col <= (size_t)optin) return launch_bt<4>(t, Z, ldz, nev, st);
-    if (2 * per_col <= (size_t)optin) return launch_bt<2>(t, Z, ldz, nev, st);
-    if (per_col <= (size_t)optin) return launch_bt<1>(t, Z, ldz, nev, st);
-    return cudaErrorInvalidValue;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int ldzs = (t.n + 15) / 16 * 16 + 1;
+    const size_t fixed = (size_t)2 * kChunkTasks * (kBW + 1) * sizeof(double);
+    auto need = [&](int cols) { return fixed + (size_t)cols * ldzs * sizeof(double); };
+    // widest slab that fits, but no wider than keeps every SM busy
+    int cols = 8;
+    while (cols > 1 && (need(cols) > (size_t)optin || (nev + cols - 1) / cols < nsm)) cols /= 2;
+    if (need(cols) > (size_t)optin) return cudaErrorInvalidValue;
+    switch (cols) {
+        case 8: return launch_bt<8>(t, Z, ldz, nev, ldzs, need(8), st);
+        case 4: return launch_bt<4>(t, Z, ldz, nev, ldzs, need(4), st);
+        case 2: return launch_bt<2>(t, Z, ldz, nev, ldzs, need(2), st);
+        default: return launch_bt<1>(t, Z, ldz, nev, ldzs, need(1), st);
+    }
 }
 
 }  // namespace dvr3d
