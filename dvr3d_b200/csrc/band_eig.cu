@@ -203,24 +203,18 @@ __global__ void __launch_bounds__(kChaseThreads) band_chase_kernel(BandTri t) {
                 double v, tau, beta;
                 warp_house(x, lane, L, v, tau, beta);
                 vsm[lane] = v;
+                // beta at once, then the publication (the rest of O_s follows below). The
+                // release store is cumulative over the earlier tasks' writes of every warp,
+                // which the end-of-task barrier ordered before it.
                 if (lane == 0) {
                     s_tau = tau;
                     s_beta = beta;
+                    if (s == 0) A[(size_t)j * ld + r0] = beta;
+                    else A[(size_t)(r0 - b) * ld + r0] = beta;
+                    if (s + 1 < nt) st_release_u32(t.progress + j, (unsigned)(s + 1));
                     t.taus[(size_t)j * t.ntmax + s] = tau;
                 }
                 t.vs[((size_t)j * t.ntmax + s) * kBW + lane] = v;
-                // beta at once, then the publication (the rest of O_s follows below)
-                if (lane == 0) {
-                    if (s == 0) A[(size_t)j * ld + r0] = beta;
-                    else A[(size_t)(r0 - b) * ld + r0] = beta;
-                }
-                if (s + 1 < nt) {
-                    __syncwarp();
-                    if (lane == 0) {
-                        __threadfence();
-                        st_release_u32(t.progress + j, (unsigned)(s + 1));
-                    }
-                }
             }
             __syncthreads();
             mark(1);

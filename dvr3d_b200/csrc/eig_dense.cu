@@ -636,9 +636,12 @@ __global__ void multisect_kernel(const double *d, const double *e2, int n, int n
 }
 
 // Cluster starts for inverse iteration (single thread; nev is at most a few thousand).
-__global__ void clusters_kernel(const double *w, int nev, const double *info, int *cstart, int *ncl) {
+// Eigenvalues closer than ortol_rel ||T|| form a cluster whose vectors are computed in turn
+// and orthogonalised against each other; apart, inverse iteration's own accuracy
+// (eps ||T|| / gap) is their orthogonality.
+__global__ void clusters_kernel(const double *w, int nev, const double *info, double ortol_rel, int *cstart, int *ncl) {
     if (threadIdx.x != 0 || blockIdx.x != 0) return;
-    const double ortol = 1.0e-6 * info[3];
+    const double ortol = ortol_rel * info[3];
     int nc = 0;
     cstart[nc++] = 0;
     for (int j = 1; j < nev; ++j)
@@ -1016,9 +1019,9 @@ void launch_dense_eigvals(const double *d, const double *e, int n, int nev, doub
 
 void launch_tridiag_eigvecs(const double *d, const double *e, int n, const double *w, int nev, const double *info,
                             int *cstart, int *ncl, double *fac, int T, double *X, double *Z, long long ldz,
-                            cudaStream_t st) {
+                            double ortol_rel, cudaStream_t st) {
     DVR3D_COUNT_LAUNCH(1);
-    clusters_kernel<<<1, 32, 0, st>>>(w, nev, info, cstart, ncl);
+    clusters_kernel<<<1, 32, 0, st>>>(w, nev, info, ortol_rel, cstart, ncl);
     const size_t smem = invit_smem_bytes(n);
     if (smem <= (size_t)kInvitSmemMax) {
         static bool attr = false;
@@ -1040,7 +1043,7 @@ void launch_dense_eigvecs(const double *A, long long lda, int n, const double *d
                           const double *tau, const double *w, int nev,
                           const double *info, int *cstart, int *ncl, double *fac, int T, double *X,
                           double *Z, long long ldz, double *bt_work, cudaStream_t st) {
-    launch_tridiag_eigvecs(d, e, n, w, nev, info, cstart, ncl, fac, T, X, Z, ldz, st);
+    launch_tridiag_eigvecs(d, e, n, w, nev, info, cstart, ncl, fac, T, X, Z, ldz, 1.0e-6, st);
     if (bt_work && !(ldz & 1)) {
         launch_dense_backtransform(A, lda, n, tau, Z, ldz, nev, bt_work, st);
     } else {

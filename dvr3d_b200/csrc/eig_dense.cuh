@@ -45,10 +45,13 @@ void launch_dense_eigvals(const double *d, const double *e, int n, int nev, doub
 constexpr int kInvitSmemMax = 200 * 1024;
 size_t invit_smem_bytes(int n);
 size_t dense_bt_work_doubles(int n, int nev);
-// Eigenvectors of the tridiagonal (d, e) for the nev eigenvalues w into Z (no back-transform).
+// Eigenvectors of the tridiagonal (d, e) for the nev eigenvalues w into Z (no back-transform);
+// eigenvalues closer than ortol_rel ||T|| are orthogonalised as a cluster (1e-6 for the dense
+// path; the projected Krylov matrix, whose wanted eigenvalues are graded over orders of
+// magnitude, uses a far smaller one so they are not all one cluster).
 void launch_tridiag_eigvecs(const double *d, const double *e, int n, const double *w, int nev, const double *info,
                             int *cstart, int *ncl, double *fac, int T, double *X, double *Z, long long ldz,
-                            cudaStream_t st);
+                            double ortol_rel, cudaStream_t st);
 void launch_dense_eigvecs(const double *A, long long lda, int n, const double *d, const double *e,
                           const double *tau, const double *w, int nev,
                           const double *info, int *cstart, int *ncl, double *fac, int T, double *X,

@@ -79,11 +79,14 @@ __global__ void __launch_bounds__(kThr) gemm_pipe_kernel(GemmOp p, int tiles_m) 
     using LA = TileLoader<kBM, TA>;
     using LB = TileLoader<BN, !TB>;
     constexpr int WN = BN / 2, FN = WN / 8;
-    constexpr int kSmem = 2 * LA::kElems + 2 * LB::kElems;
+    // stages in flight: three for thin right-hand sides (two loads outstanding while one
+    // stage is multiplied), two for 64-wide tiles (static shared memory limit)
+    constexpr int NS = (BN == 32) ? 3 : 2;
+    constexpr int kSmem = NS * LA::kElems + NS * LB::kElems;
     static_assert(kSmem >= kBM * BN, "staging of the cluster reduction fits the operand buffers");
     __shared__ __align__(16) double smem_all[kSmem];
     double(*As)[LA::kElems] = reinterpret_cast<double(*)[LA::kElems]>(smem_all);
-    double(*Bs)[LB::kElems] = reinterpret_cast<double(*)[LB::kElems]>(smem_all + 2 * LA::kElems);
+    double(*Bs)[LB::kElems] = reinterpret_cast<double(*)[LB::kElems]>(smem_all + NS * LA::kElems);
     int tm, tn;
     if (p.lower_out) {
         const long long t = blockIdx.x;
@@ -123,11 +126,17 @@ __global__ void __launch_bounds__(kThr) gemm_pipe_kernel(GemmOp p, int tiles_m) 
         asm volatile("cp.async.commit_group;\n" ::);
     };
     const int r = lane >> 2, c = lane & 3;
-    if (t0 < t1) load(0, t0);
+#pragma unroll
+    for (int q = 0; q < NS - 1; ++q)
+        if (t0 + q < t1) load(q, t0 + q);
     for (int kt = t0; kt < t1; ++kt) {
-        const int st = (kt - t0) & 1;
-        if (kt + 1 < t1) {
-            load(st ^ 1, kt + 1);
+        const int st = (kt - t0) % NS;
+        // tile kt + NS - 1 goes into the stage freed by tile kt - 1 (the barrier at the end
+        // of the previous iteration); then wait until tile kt has landed
+        if (kt + NS - 1 < t1) {
+            load((kt - t0 + NS - 1) % NS, kt + NS - 1);
+            asm volatile("cp.async.wait_group %0;\n" ::"n"(NS - 1));
+        } else if (NS == 3 && kt + 1 < t1) {
             asm volatile("cp.async.wait_group 1;\n" ::);
         } else {
             asm volatile("cp.async.wait_group 0;\n" ::);

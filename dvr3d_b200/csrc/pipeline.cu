@@ -737,7 +737,7 @@ bool band_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int b, int nev
     double *X = smem ? nullptr : ctx->arena.get_t<double>("bd_x", (size_t)n * nev);
     int *cs = ctx->arena.get_t<int>("bd_cs", nev + 1);
     int *ncl = ctx->arena.get_t<int>("bd_ncl", 1);
-    launch_tridiag_eigvecs(t.d, t.e, n, w, nev, info, cs, ncl, fac, T, X, Z, ldz, st);
+    launch_tridiag_eigvecs(t.d, t.e, n, w, nev, info, cs, ncl, fac, T, X, Z, ldz, 1.0e-10, st);
     CK(cudaGetLastError());
     CK(launch_band_backtransform(t, Z, ldz, nev, st));
     return true;
