@@ -160,6 +160,69 @@ __global__ void __launch_bounds__(kLeafThreads, 1) potrf_leaf_kernel(double *A, 
     }
 }
 
+// Cholesky and inverse of a b x b block (b <= 32) in one warp: lane i keeps row i of the
+// matrix and of X = inv(U) in registers; step k broadcasts the pivot and column k / row k
+// by shuffles (no barriers). Same results as the leaf kernel: G's lower triangle receives
+// L, inv_out (ld 64) the inverse with zeros above the diagonal.
+__global__ void __launch_bounds__(32) chol_warp_kernel(double *G, int b, double *inv_out, double rel_tol, int *err) {
+    if (*(volatile int *)err != 0) return;
+    const int i = threadIdx.x;
+    constexpr unsigned kAll = 0xffffffffu;
+    double own[32], x[32];
+#pragma unroll
+    for (int c = 0; c < 32; ++c) {
+        own[c] = (i < b && c < b && c <= i) ? G[(size_t)c * b + i] : 0.0;
+        x[c] = (c == i) ? 1.0 : 0.0;
+    }
+    double dmax = 0.0;
+#pragma unroll
+    for (int c = 0; c < 32; ++c)
+        if (c == i) dmax = own[c];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(kAll, dmax, o));
+    const double thr = rel_tol * dmax;
+    bool bad = false;
+#pragma unroll
+    for (int k = 0; k < 32; ++k) {
+        if (k < b && !bad) {  // uniform
+            const double d = __shfl_sync(kAll, own[k], k);
+            if (!(d > thr) || !isfinite(d)) {
+                bad = true;
+            } else {
+                const double lik = (i > k && i < b) ? own[k] * (1.0 / d) : 0.0;
+#pragma unroll
+                for (int c = k + 1; c < 32; ++c) own[c] -= lik * __shfl_sync(kAll, own[k], c);
+#pragma unroll
+                for (int c = 0; c <= k; ++c) x[c] -= lik * __shfl_sync(kAll, x[c], k);
+            }
+        }
+    }
+    if (bad) {
+        if (i == 0) atomicExch(err, (int)kDevNotPosDef);
+        return;
+    }
+    double di = 0.0;
+#pragma unroll
+    for (int c = 0; c < 32; ++c)
+        if (c == i) di = own[c];
+    const double sq = (i < b) ? sqrt(di) : 1.0;
+    const double rs = 1.0 / sq;
+#pragma unroll
+    for (int c = 0; c < 32; ++c) {
+        const double rsc = __shfl_sync(kAll, rs, c);
+        const double sqc = __shfl_sync(kAll, sq, c);
+        const bool in = (i < b && c < b && c <= i);
+        if (in) G[(size_t)c * b + i] = (c == i) ? sqc : own[c] * rsc;
+        if (inv_out && c < 64) inv_out[(size_t)c * NB + i] = in ? x[c] * rs : 0.0;
+    }
+    if (inv_out) {  // rows b..63 of the 64-row inverse block stay zero
+        for (int q = i; q < NB * NB; q += 32) {
+            const int c = q / NB, r = q % NB;
+            if (r >= 32 || c >= 32) inv_out[q] = 0.0;
+        }
+    }
+}
+
 cudaError_t leaf(double *A, long long lda, int j0, int nb, double *inv_out, int in_place, double rel_tol, int *err,
                  cudaStream_t st) {
     DVR3D_COUNT_LAUNCH(1);
@@ -303,6 +366,11 @@ cudaError_t launch_potrf_inv_lower(double *A, long long lda, int n, double *work
 
 cudaError_t launch_chol_small(double *G, int b, double *ginv, double rel_tol, int *err, cudaStream_t st) {
     if (b > NB) return cudaErrorInvalidValue;
+    if (b <= 32) {
+        DVR3D_COUNT_LAUNCH(1);
+        chol_warp_kernel<<<1, 32, 0, st>>>(G, b, ginv, rel_tol, err);
+        return cudaGetLastError();
+    }
     return leaf(G, b, 0, b, ginv, 0, rel_tol, err, st);
 }
 

@@ -98,6 +98,10 @@ __global__ void __launch_bounds__(kThr) gemm_pipe_kernel(GemmOp p, int tiles_m) 
     } else {
         tm = blockIdx.x % tiles_m;
         tn = blockIdx.x / tiles_m;
+        // triangular operands: the tiles with the longest K ranges first (lower op(A): the
+        // bottom row tiles; upper op(B): the right column tiles), so they do not form the tail
+        if (p.tri == 1) tm = tiles_m - 1 - tm;
+        if (p.tri_b == 2) tn = (int)((gridDim.x / tiles_m) - 1) - tn;
     }
     const int i0 = tm * kBM, j0 = tn * BN;
     // K range of this tile (triangular op(A)) and of this split
