@@ -181,20 +181,25 @@ __global__ void __launch_bounds__(32) chol_warp_kernel(double *G, int b, double 
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) dmax = fmax(dmax, __shfl_xor_sync(kAll, dmax, o));
     const double thr = rel_tol * dmax;
+    // the step loop stays a loop (a fully unrolled one is too long for the instruction cache);
+    // column k of this lane's row is picked by selects, the other rows' entries by shuffles
     bool bad = false;
+#pragma unroll 1
+    for (int k = 0; k < b; ++k) {
+        double colk = 0.0;
 #pragma unroll
-    for (int k = 0; k < 32; ++k) {
-        if (k < b && !bad) {  // uniform
-            const double d = __shfl_sync(kAll, own[k], k);
-            if (!(d > thr) || !isfinite(d)) {
-                bad = true;
-            } else {
-                const double lik = (i > k && i < b) ? own[k] * (1.0 / d) : 0.0;
+        for (int c = 0; c < 32; ++c) colk = (c == k) ? own[c] : colk;
+        const double d = __shfl_sync(kAll, colk, k);
+        if (!(d > thr) || !isfinite(d)) {  // uniform: every lane holds the same d
+            bad = true;
+            break;
+        }
+        const double lik = (i > k && i < b) ? colk * (1.0 / d) : 0.0;
 #pragma unroll
-                for (int c = k + 1; c < 32; ++c) own[c] -= lik * __shfl_sync(kAll, own[k], c);
-#pragma unroll
-                for (int c = 0; c <= k; ++c) x[c] -= lik * __shfl_sync(kAll, x[c], k);
-            }
+        for (int c = 0; c < 32; ++c) {
+            const double ack = __shfl_sync(kAll, colk, c);  // row c's entry of column k
+            own[c] -= (c > k) ? lik * ack : 0.0;
+            x[c] -= lik * __shfl_sync(kAll, x[c], k);      // row k of X (zero right of k)
         }
     }
     if (bad) {
