@@ -83,30 +83,33 @@ __global__ void __launch_bounds__(kTriMaxThreads) tridiag_kernel(BatchDesc bd, d
             v[i] = vi;
         }
         __syncthreads();
-        // (3) fused: apply pending update to A22 and accumulate s = A22 v. One row per thread;
-        // four columns per iteration keep several independent loads in flight per thread
-        const int i = k + 1 + tid;
+        // (3) fused: apply pending update to A22 and accumulate s = A22 v. One row per thread,
+        // or per pair of adjacent threads (the two take alternate columns) when the block has
+        // threads to spare: twice the loads in flight per row. Four columns per iteration.
+        const int R = (blockDim.x >= 2u * (unsigned)n) ? 2 : 1;
+        const int i = k + 1 + tid / R, h = tid % R;
         const bool act = i < n;
         const double vpi = (pending && act) ? vp[i] : 0.0, wpi = (pending && act) ? wp[i] : 0.0;
         double s_acc = 0.0;
         if (act && (tk != 0.0 || pending)) {
-            int j = k + 1;
-            for (; j + 3 < n; j += 4) {
+            const size_t sn = (size_t)R * n;  // stride between this thread's columns
+            int j = k + 1 + h;
+            for (; j + 3 * R < n; j += 4 * R) {
                 double *c0 = a + (size_t)j * n + i;
-                double x0 = c0[0], x1 = c0[n], x2 = c0[2 * (size_t)n], x3 = c0[3 * (size_t)n];
+                double x0 = c0[0], x1 = c0[sn], x2 = c0[2 * sn], x3 = c0[3 * sn];
                 if (pending) {
                     x0 -= vpi * wp[j] + wpi * vp[j];
-                    x1 -= vpi * wp[j + 1] + wpi * vp[j + 1];
-                    x2 -= vpi * wp[j + 2] + wpi * vp[j + 2];
-                    x3 -= vpi * wp[j + 3] + wpi * vp[j + 3];
+                    x1 -= vpi * wp[j + R] + wpi * vp[j + R];
+                    x2 -= vpi * wp[j + 2 * R] + wpi * vp[j + 2 * R];
+                    x3 -= vpi * wp[j + 3 * R] + wpi * vp[j + 3 * R];
                     c0[0] = x0;
-                    c0[n] = x1;
-                    c0[2 * (size_t)n] = x2;
-                    c0[3 * (size_t)n] = x3;
+                    c0[sn] = x1;
+                    c0[2 * sn] = x2;
+                    c0[3 * sn] = x3;
                 }
-                s_acc += (x0 * v[j] + x1 * v[j + 1]) + (x2 * v[j + 2] + x3 * v[j + 3]);
+                s_acc += (x0 * v[j] + x1 * v[j + R]) + (x2 * v[j + 2 * R] + x3 * v[j + 3 * R]);
             }
-            for (; j < n; ++j) {
+            for (; j < n; j += R) {
                 double *cj = a + (size_t)j * n + i;
                 double x = *cj;
                 if (pending) {
@@ -116,8 +119,9 @@ __global__ void __launch_bounds__(kTriMaxThreads) tridiag_kernel(BatchDesc bd, d
                 s_acc += x * v[j];
             }
         }
+        if (R == 2) s_acc += __shfl_xor_sync(0xffffffffu, s_acc, 1);  // partner thread, same warp
         // p = tau s ; w = p - (tau/2)(p.v) v
-        double pv = act ? tk * s_acc * v[i] : 0.0;
+        double pv = (act && h == 0) ? tk * s_acc * v[i] : 0.0;
         pv = block_sum(pv, red);
         const double alpha2 = -0.5 * tk * pv;
         __syncthreads();
@@ -126,7 +130,7 @@ __global__ void __launch_bounds__(kTriMaxThreads) tridiag_kernel(BatchDesc bd, d
             wp[q] = 0.0;
         }
         __syncthreads();
-        if (act) wp[i] = tk * s_acc + alpha2 * v[i];
+        if (act && h == 0) wp[i] = tk * s_acc + alpha2 * v[i];
         pending = (tk != 0.0);
         __syncthreads();
     }
@@ -542,7 +546,9 @@ void launch_tridiag_batched(const BatchDesc &bd, double *A, double *d, double *e
     if (bd.nblk <= 0) return;
     const size_t smem = (size_t)3 * nmax * sizeof(double);
     DVR3D_COUNT_LAUNCH(1);
-    const int threads = std::min(kTriMaxThreads, std::max(64, (nmax + 31) / 32 * 32));
+    // two threads per row while 2 nmax fits in one block (see the fused loop)
+    const int rows_thr = (2 * nmax <= kTriMaxThreads) ? 2 * nmax : nmax;
+    const int threads = std::min(kTriMaxThreads, std::max(64, (rows_thr + 31) / 32 * 32));
     tridiag_kernel<<<bd.nblk, threads, smem, st>>>(bd, A, d, e, tau);
 }
 
