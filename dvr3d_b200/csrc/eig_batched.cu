@@ -305,7 +305,9 @@ constexpr int kFastPanel = 16;
 __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double *dg, const double *eo,
                                     const double *tauo, const double *wo, const int *sel, const long long *zoff,
                                     const int *zld, double *Z) {
-    const int b = blockIdx.x;
+    // gridDim.y CTAs share a block: CTA y takes the eigenvalue clusters c = y (mod gridDim.y)
+    // and back-transforms their columns
+    const int b = blockIdx.x, part = blockIdx.y, nparts = gridDim.y;
     if (b >= bd.nblk) return;
     const int n = bd.n[b];
     const int m = sel[b];
@@ -317,7 +319,8 @@ __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double 
     const int ldz = zld[b];
     extern __shared__ double sm[];
     __shared__ int cstart[1025];
-    __shared__ int s_ncl;
+    __shared__ int mycols[1024];  // columns of this CTA's clusters
+    __shared__ int s_ncl, s_nmine;
     __shared__ double s_onenrm;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarp = blockDim.x >> 5;
     if (tid == 0) {
@@ -334,6 +337,10 @@ __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double 
             if (w[j] - w[j - 1] > ortol) cstart[nc++] = j;
         cstart[nc] = m;
         s_ncl = nc;
+        int nm = 0;
+        for (int c = part; c < nc; c += nparts)
+            for (int j = cstart[c]; j < cstart[c + 1]; ++j) mycols[nm++] = j;
+        s_nmine = nm;
     }
     __syncthreads();
     // ---- inverse iteration, one warp per cluster
@@ -343,7 +350,7 @@ __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double 
         unsigned char *P = reinterpret_cast<unsigned char *>(x + n);
         const double onenrm = s_onenrm;
         const double eps = DBL_EPSILON, tiny = eps * onenrm, pertol = 10.0 * eps * onenrm;
-        for (int c = warp; c < s_ncl; c += nwarp) {
+        for (int c = part + nparts * warp; c < s_ncl; c += nparts * nwarp) {
             const int j0 = cstart[c], j1 = cstart[c + 1];
             double lamprev = 0.0;
             for (int j = j0; j < j1; ++j) {
@@ -495,8 +502,8 @@ __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double 
             }
             __syncthreads();
         }
-        for (int col = tid; col < m; col += blockDim.x) {
-            double *zc = z + (size_t)col * ldz;
+        for (int q = tid; q < s_nmine; q += blockDim.x) {
+            double *zc = z + (size_t)mycols[q] * ldz;
             double wv[kFastPanel];
 #pragma unroll
             for (int c = 0; c < kFastPanel; ++c) wv[c] = 0.0;
@@ -595,8 +602,13 @@ void launch_eigvecs_batched_fast(const BatchDesc &bd, const double *A, const dou
         cudaFuncSetAttribute(eigvecs_fast_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
         attr = true;
     }
+    // fewer blocks than SMs: two CTAs per block (their clusters split between them)
+    int dev = 0, nsm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const int parts = (bd.nblk < nsm) ? 2 : 1;
     DVR3D_COUNT_LAUNCH(1);
-    eigvecs_fast_kernel<<<bd.nblk, 32 * nwarp, smem, st>>>(bd, A, d, e, tau, w, sel, zoff, zld, Z);
+    eigvecs_fast_kernel<<<dim3(bd.nblk, parts), 32 * nwarp, smem, st>>>(bd, A, d, e, tau, w, sel, zoff, zld, Z);
 }
 
 }  // namespace dvr3d
