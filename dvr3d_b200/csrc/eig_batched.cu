@@ -389,6 +389,12 @@ __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double 
                 __syncwarp();
                 for (int i = lane; i < n - 1; i += 32)
                     if (fabs(D[i]) < tiny) D[i] = (D[i] < 0.0) ? -tiny : tiny;
+                __syncwarp();
+                // the solves below multiply by the pivots' reciprocals (one division per pivot
+                // here instead of one per pivot and iteration on the sequential path)
+                const double dlast = D[n - 1];
+                __syncwarp();
+                for (int i = lane; i < n; i += 32) D[i] = 1.0 / D[i];
                 for (int i = lane; i < n; i += 32) {
                     const unsigned h = hash32((unsigned)(i * 2654435761u) ^ (unsigned)(j * 40503u + 17u));
                     x[i] = ((double)(h & 0xffffff) / 8388608.0) - 1.0;
@@ -398,7 +404,7 @@ __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double 
                     double s1 = 0.0;
                     for (int i = lane; i < n; i += 32) s1 += fabs(x[i]);
                     s1 = warp_sum(s1);
-                    const double sc = (double)n * onenrm * fmax(eps, fabs(D[n - 1])) / fmax(s1, DBL_MIN);
+                    const double sc = (double)n * onenrm * fmax(eps, fabs(dlast)) / fmax(s1, DBL_MIN);
                     for (int i = lane; i < n; i += 32) x[i] *= sc;
                     __syncwarp();
                     if (lane == 0) {
@@ -414,7 +420,7 @@ __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double 
                         }
                         double x1 = 0.0, x2 = 0.0;
                         for (int i = n - 1; i >= 0; --i) {
-                            const double xi = (x[i] - E1[i] * x1 - E2[i] * x2) / D[i];
+                            const double xi = (x[i] - E1[i] * x1 - E2[i] * x2) * D[i];
                             x[i] = xi;
                             x2 = x1;
                             x1 = xi;
@@ -504,10 +510,20 @@ __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double 
         }
         for (int q = tid; q < s_nmine; q += blockDim.x) {
             double *zc = z + (size_t)mycols[q] * ldz;
+            // the column is walked four rows at a time so that four loads are in flight
             double wv[kFastPanel];
 #pragma unroll
             for (int c = 0; c < kFastPanel; ++c) wv[c] = 0.0;
-            for (int i = p0 + 1; i < n; ++i) {
+            int i = p0 + 1;
+            for (; i + 3 < n; i += 4) {
+                const double z0 = zc[i], z1 = zc[i + 1], z2 = zc[i + 2], z3 = zc[i + 3];
+#pragma unroll
+                for (int c = 0; c < kFastPanel; ++c) {
+                    const double *vc = Vs + c * n + i;
+                    wv[c] += (vc[0] * z0 + vc[1] * z1) + (vc[2] * z2 + vc[3] * z3);
+                }
+            }
+            for (; i < n; ++i) {
                 const double zi = zc[i];
 #pragma unroll
                 for (int c = 0; c < kFastPanel; ++c) wv[c] += Vs[c * n + i] * zi;
@@ -520,7 +536,24 @@ __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double 
                 for (int c = 0; c < kFastPanel; ++c) s += Tm[r * kFastPanel + c] * wv[c];
                 w2[r] = s;
             }
-            for (int i = p0 + 1; i < n; ++i) {
+            i = p0 + 1;
+            for (; i + 3 < n; i += 4) {
+                const double z0 = zc[i], z1 = zc[i + 1], z2 = zc[i + 2], z3 = zc[i + 3];
+                double s0 = 0.0, s1 = 0.0, s2 = 0.0, s3 = 0.0;
+#pragma unroll
+                for (int c = 0; c < kFastPanel; ++c) {
+                    const double *vc = Vs + c * n + i;
+                    s0 += vc[0] * w2[c];
+                    s1 += vc[1] * w2[c];
+                    s2 += vc[2] * w2[c];
+                    s3 += vc[3] * w2[c];
+                }
+                zc[i] = z0 - s0;
+                zc[i + 1] = z1 - s1;
+                zc[i + 2] = z2 - s2;
+                zc[i + 3] = z3 - s3;
+            }
+            for (; i < n; ++i) {
                 double s = 0.0;
 #pragma unroll
                 for (int c = 0; c < kFastPanel; ++c) s += Vs[c * n + i] * w2[c];
