@@ -752,6 +752,12 @@ __global__ void __launch_bounds__(32) invit_smem_kernel(const double *d, const d
             __syncwarp();
             for (int i = lane; i < n - 1; i += 32)
                 if (fabs(D[i]) < tiny) D[i] = (D[i] < 0.0) ? -tiny : tiny;
+            __syncwarp();
+            // the solves below multiply by the pivots' reciprocals (one division per pivot here
+            // instead of one per pivot and iteration on the sequential path)
+            const double dlast = D[n - 1];
+            __syncwarp();
+            for (int i = lane; i < n; i += 32) D[i] = 1.0 / D[i];
             for (int i = lane; i < n; i += 32) {
                 const unsigned h = hash32((unsigned)(i * 2654435761u) ^ (unsigned)(j * 40503u + 17u));
                 x[i] = ((double)(h & 0xffffff) / 8388608.0) - 1.0;
@@ -761,7 +767,7 @@ __global__ void __launch_bounds__(32) invit_smem_kernel(const double *d, const d
                 double s1 = 0.0;
                 for (int i = lane; i < n; i += 32) s1 += fabs(x[i]);
                 s1 = warp_sum(s1);
-                const double sc = (double)n * onenrm * fmax(eps, fabs(D[n - 1])) / fmax(s1, DBL_MIN);
+                const double sc = (double)n * onenrm * fmax(eps, fabs(dlast)) / fmax(s1, DBL_MIN);
                 for (int i = lane; i < n; i += 32) x[i] *= sc;
                 __syncwarp();
                 if (lane == 0) {
@@ -777,7 +783,7 @@ __global__ void __launch_bounds__(32) invit_smem_kernel(const double *d, const d
                     }
                     double x1 = 0.0, x2 = 0.0;
                     for (int i = n - 1; i >= 0; --i) {
-                        const double xi = (x[i] - E1[i] * x1 - E2[i] * x2) / D[i];
+                        const double xi = (x[i] - E1[i] * x1 - E2[i] * x2) * D[i];
                         x[i] = xi;
                         x2 = x1;
                         x1 = xi;
