@@ -15,10 +15,10 @@
 //                    entry, is applied from the left to the rest of O_s, from both sides to
 //                    D_s and from the right to O_{s+1}; the remainder of the bulge is
 //                    eliminated by later sweeps.
-// One warp runs a task on 32 x 32 blocks in its shared memory (lane = row); a warp owns a
-// whole sweep, keeping O_{s+1} between its tasks. Sweep j+1 may start task s once sweep j
-// has finished task s + 2 (their blocks are then disjoint), published through per-sweep
-// progress counters with release / acquire ordering and bounded waits.
+// One CTA owns a whole sweep (five warps with fixed roles, 32 x 32 blocks in shared memory,
+// lane = row), keeping O_{s+1} between its tasks. Sweep j+1 may start task s once sweep j has
+// written the beta of its task s + 2 (the only entry the two share), published through
+// per-sweep progress counters with release / acquire ordering and bounded waits.
 // Back-transformation: Q = prod over sweeps (in order) of prod over tasks of H; the
 // reflectors of one sweep act on disjoint rows, so a CTA holding a slab of eigenvector
 // columns in shared memory applies sweep after sweep (last first), its warps taking the

@@ -19,8 +19,9 @@ struct BandTri {
     double *taus;           // out: [n - 2][ntmax]
     unsigned int *progress; // [n] tasks finished per sweep (zeroed by the launcher)
     int *err;
-    long long *prof;        // optional [5]: summed clock cycles of the chase's warps (wait,
-                            // loads, reflector + bulge, diagonal block, hand-off), or null
+    long long *prof;        // optional [5]: clock cycles of the chase's thread 0 summed over
+                            // CTAs (sweep start, reflector, O_s part with the hand-off,
+                            // end-of-task wait, unused), or null
 };
 
 // Zeroes the bulge space (lower triangle, b < i - j <= 2b) and records the largest dropped
@@ -29,7 +30,7 @@ cudaError_t launch_band_prepare(double *A, long long lda, int n, int b, unsigned
                                 cudaStream_t st);
 size_t band_reflector_doubles(int n, int b);  // vs
 size_t band_tau_doubles(int n, int b);        // taus
-// Bulge chasing (one warp per sweep at a time, sweeps pipelined through progress flags),
+// Bulge chasing (one CTA per sweep in flight, sweeps pipelined through progress flags),
 // then d and e from the reduced matrix.
 cudaError_t launch_band_chase(BandTri &t, cudaStream_t st);
 // Z (n x nev, ldz) <- Q Z with Q the product of the chase's reflectors (A = Q T Q^T).
