@@ -3,7 +3,9 @@
 * ``dvr3d_b200/libdvr3d_b200.so`` -- the product: CUDA kernels for sm_100a plus the host
   code behind the C ABI of ``include/dvr3d_b200.h``; compiled with nvcc only for
   ``-gencode arch=compute_100a,code=sm_100a``.
-* ``oracle/libdvr3d_oracle.so`` -- the CPU checker (test infrastructure), compiled with g++.
+
+The CPU checker (``oracle/libdvr3d_oracle.so``, test infrastructure) has its own recipe in
+``oracle/build.py``.
 
 Usage: ``python -m dvr3d_b200.build [--force]``. Object files go to ``_build/``.
 """
@@ -20,8 +22,6 @@ PKG = ROOT / "dvr3d_b200"
 CSRC = PKG / "csrc"
 BUILD = ROOT / "_build"
 LIB = PKG / "libdvr3d_b200.so"
-ORACLE_SRC = ROOT / "oracle" / "dvr3d_oracle.cpp"
-ORACLE_LIB = ROOT / "oracle" / "libdvr3d_oracle.so"
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
@@ -75,18 +75,8 @@ def build_product(force: bool = False, verbose: bool = False) -> Path:
     return LIB
 
 
-def build_oracle(force: bool = False) -> Path:
-    deps = [ORACLE_SRC, ORACLE_SRC.with_suffix(".h"), ROOT / "include" / "dvr3d_b200.h"]
-    if not force and not _stale(ORACLE_LIB, deps):
-        return ORACLE_LIB
-    cxx = shutil.which("g++") or "g++"
-    _run([cxx, "-O2", "-std=c++17", "-fPIC", "-shared", "-o", str(ORACLE_LIB), str(ORACLE_SRC), "-ldl"])
-    return ORACLE_LIB
-
-
 def main(argv: list[str]) -> int:
     force = "--force" in argv
-    build_oracle(force)
     build_product(force, verbose="-v" in argv)
     print(LIB)
     return 0

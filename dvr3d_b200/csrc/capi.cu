@@ -288,6 +288,8 @@ int dvr3d_b200_diag_batched(dvr3d_ctx *ctx, int nblk, const int *n_host, const l
         dvr3d::launch_eigvals_batched(bdc, d, e, w, cnt, 0, 0.0, st);
         for (int b = 0; b < nblk; ++b)
             cudaMemcpyAsync(w_dev + woff_host[b], w + voff[b], sizeof(double) * n[b], cudaMemcpyDeviceToDevice, st);
+        int *err = ctx->arena.get_t<int>("err", 1);
+        int err_host = 0;
         if (vecs) {
             std::vector<int> zld(n);
             std::vector<long long> woff(nblk);
@@ -297,13 +299,14 @@ int dvr3d_b200_diag_batched(dvr3d_ctx *ctx, int nblk, const int *n_host, const l
                 wt += 5LL * n[b] * std::min(128, n[b]) + (long long)n[b] * n[b];
             }
             double *work = ctx->arena.get_t<double>("dg_work", wt);
-            int *err = ctx->arena.get_t<int>("err", 1);
             cudaMemsetAsync(err, 0, sizeof(int), st);
             dvr3d::launch_eigvecs_batched(bdc, ac, d, e, tau, w, bd.n, up("dg_zoff", aoff), up("dg_zld", n), a_dev,
                                           work, up("dg_woff", woff), nmax, err, st);
+            cudaMemcpyAsync(&err_host, err, sizeof(int), cudaMemcpyDeviceToHost, st);
         }
         cudaError_t ce = cudaStreamSynchronize(st);
         if (ce != cudaSuccess) throw CudaFail{ce, "diag_batched"};
+        if (err_host != 0) return fail_ctx(ctx, DVR3D_ERR_NOCONV, "inverse iteration did not converge for some eigenvector");
         return DVR3D_OK;
     });
 }
@@ -354,7 +357,7 @@ int dvr3d_b200_run_deck(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_optio
             }
             // zpfun levels file (:2708-2719): header 6i4, then 4d20.12
             const int ip = d.jrot - p.kmin;
-            if (d.zpfun && std::abs(d.jrot) <= 1 && (d.jrot == 0 || ip == 1)) {
+            if (d.zpfun && (d.jrot == 0 || ip == 1)) {
                 const int jdia = std::max(0, d.idia), jpar = std::min(jdia, p.ipar);
                 int isym = std::abs(std::min(0, d.idia));
                 if (p.ipar == 1) isym = -isym;

@@ -11,6 +11,11 @@ namespace dvr3d {
 extern long long g_kernel_launches;
 #define DVR3D_COUNT_LAUNCH(k) (::dvr3d::g_kernel_launches += (k))
 
+// Kernel attributes such as cudaFuncAttributeMaxDynamicSharedMemorySize are per device:
+// launchers that raise them keep one "done" flag per device ordinal below this bound (and set
+// the attribute on every launch for ordinals beyond it).
+constexpr int kMaxAttrDevices = 64;
+
 // Device-side error flags written by kernels (never __trap): the host reads them after a
 // stage and turns them into DVR3D_ERR_* codes.
 enum DeviceErr : int {

@@ -263,7 +263,7 @@ __global__ void __launch_bounds__(kVecThreads) eigvecs_kernel(BatchDesc bd, cons
     double *X = wk + (size_t)5 * n * T;      // n * m, interleaved by eigenvalue
     if (tid < T)
         for (int c = tid; c < ncl; c += T)
-            invit_cluster(d, e, n, w, cstart[c], cstart[c + 1], s_onenrm, fac, T, tid, X, m);
+            invit_cluster(d, e, n, w, cstart[c], cstart[c + 1], s_onenrm, fac, T, tid, X, m, err);
     __syncthreads();
     const int TT = blockDim.x;
     // copy to Z (column per eigenvalue) -- coalesced over rows
@@ -304,7 +304,7 @@ constexpr int kFastPanel = 16;
 
 __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double *dg, const double *eo,
                                     const double *tauo, const double *wo, const int *sel, const long long *zoff,
-                                    const int *zld, double *Z) {
+                                    const int *zld, double *Z, int *err) {
     // gridDim.y CTAs share a block: CTA y takes the eigenvalue clusters c = y (mod gridDim.y)
     // and back-transforms their columns
     const int b = blockIdx.x, part = blockIdx.y, nparts = gridDim.y;
@@ -400,7 +400,9 @@ __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double 
                     x[i] = ((double)(h & 0xffffff) / 8388608.0) - 1.0;
                 }
                 __syncwarp();
-                for (int it = 0; it < 4; ++it) {
+                const double grow_lim = invit_growth_limit(n);
+                int grown = 0;
+                for (int it = 0; it < kInvitPasses; ++it) {
                     double s1 = 0.0;
                     for (int i = lane; i < n; i += 32) s1 += fabs(x[i]);
                     s1 = warp_sum(s1);
@@ -434,13 +436,20 @@ __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double 
                         dot = warp_sum(dot);
                         for (int i = lane; i < n; i += 32) x[i] -= dot * zc[i];
                     }
-                    double nrm = 0.0;
-                    for (int i = lane; i < n; i += 32) nrm += x[i] * x[i];
+                    double nrm = 0.0, xinf = 0.0;
+                    for (int i = lane; i < n; i += 32) {
+                        nrm += x[i] * x[i];
+                        xinf = fmax(xinf, fabs(x[i]));
+                    }
                     nrm = sqrt(warp_sum(nrm));
+#pragma unroll
+                    for (int o = 16; o > 0; o >>= 1) xinf = fmax(xinf, __shfl_xor_sync(0xffffffffu, xinf, o));
+                    grown += (xinf >= grow_lim);
                     const double inv = (nrm > 0.0) ? 1.0 / nrm : 0.0;
                     for (int i = lane; i < n; i += 32) x[i] *= inv;
                     __syncwarp();
                 }
+                if (grown < kInvitGrowPasses && lane == 0 && err) *err = 1;
                 // sign convention: the first largest component positive
                 double big = 0.0;
                 int bi = n;
@@ -624,24 +633,25 @@ size_t eigvecs_fast_smem(int nmax, int nwarp) {
 
 void launch_eigvecs_batched_fast(const BatchDesc &bd, const double *A, const double *d, const double *e,
                                  const double *tau, const double *w, const int *sel, const long long *zoff,
-                                 const int *zld, double *Z, int nmax, cudaStream_t st) {
+                                 const int *zld, double *Z, int nmax, int *err, cudaStream_t st) {
     if (bd.nblk <= 0) return;
     const size_t cap = 200 * 1024;
     int nwarp = 8;
     while (nwarp > 1 && eigvecs_fast_smem(nmax, nwarp) > cap) --nwarp;
     const size_t smem = eigvecs_fast_smem(nmax, nwarp);
-    static bool attr = false;
-    if (!attr) {
-        cudaFuncSetAttribute(eigvecs_fast_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
-        attr = true;
-    }
     // fewer blocks than SMs: two CTAs per block (their clusters split between them)
     int dev = 0, nsm = 0;
     cudaGetDevice(&dev);
+    // the shared-memory limit is a per-device attribute of the kernel
+    static bool attr[kMaxAttrDevices] = {};
+    if (dev < 0 || dev >= kMaxAttrDevices || !attr[dev]) {
+        cudaFuncSetAttribute(eigvecs_fast_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)cap);
+        if (dev >= 0 && dev < kMaxAttrDevices) attr[dev] = true;
+    }
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     const int parts = (bd.nblk < nsm) ? 2 : 1;
     DVR3D_COUNT_LAUNCH(1);
-    eigvecs_fast_kernel<<<dim3(bd.nblk, parts), 32 * nwarp, smem, st>>>(bd, A, d, e, tau, w, sel, zoff, zld, Z);
+    eigvecs_fast_kernel<<<dim3(bd.nblk, parts), 32 * nwarp, smem, st>>>(bd, A, d, e, tau, w, sel, zoff, zld, Z, err);
 }
 
 }  // namespace dvr3d

@@ -48,8 +48,10 @@ void launch_eigvecs_batched(const BatchDesc &bd, const double *A, const double *
 
 // Same output as launch_eigvecs_batched (n <= 1024), without work buffer: inverse iteration
 // with the factors in shared memory (one warp per cluster) and a blocked back-transformation.
+// Both set *err = 1 (err may be null) when inverse iteration fails its growth test for some
+// vector (dstein's convergence criterion); the flag is never cleared by the kernels.
 void launch_eigvecs_batched_fast(const BatchDesc &bd, const double *A, const double *d, const double *e,
                                  const double *tau, const double *w, const int *sel, const long long *zoff,
-                                 const int *zld, double *Z, int nmax, cudaStream_t st);
+                                 const int *zld, double *Z, int nmax, int *err, cudaStream_t st);
 
 }  // namespace dvr3d

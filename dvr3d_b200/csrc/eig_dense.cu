@@ -657,7 +657,7 @@ __global__ void invit_dense_kernel(const double *d, const double *e, int n, cons
     const int nc = *ncl;
     if (t >= T) return;
     for (int c = t; c < nc; c += T)
-        invit_cluster(d, e, n, w, cstart[c], cstart[c + 1], info[3], fac, T, t, X, nev);
+        invit_cluster(d, e, n, w, cstart[c], cstart[c + 1], info[3], fac, T, t, X, nev, nullptr);
 }
 
 // Z[:, j] = X[:, j] (interleaved -> column-major), then back-transform by the reflectors.
@@ -1030,10 +1030,12 @@ void launch_tridiag_eigvecs(const double *d, const double *e, int n, const doubl
     clusters_kernel<<<1, 32, 0, st>>>(w, nev, info, ortol_rel, cstart, ncl);
     const size_t smem = invit_smem_bytes(n);
     if (smem <= (size_t)kInvitSmemMax) {
-        static bool attr = false;
-        if (!attr) {
+        int dev = 0;
+        cudaGetDevice(&dev);
+        static bool attr[kMaxAttrDevices] = {};
+        if (dev < 0 || dev >= kMaxAttrDevices || !attr[dev]) {
             cudaFuncSetAttribute(invit_smem_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, kInvitSmemMax);
-            attr = true;
+            if (dev >= 0 && dev < kMaxAttrDevices) attr[dev] = true;
         }
         DVR3D_COUNT_LAUNCH(1);
         invit_smem_kernel<<<nev, 32, smem, st>>>(d, e, n, w, cstart, ncl, info, Z, ldz);

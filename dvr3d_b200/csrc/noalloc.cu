@@ -54,6 +54,9 @@ cudaError_t scratch_address(void **out) {
 
 inline size_t align256(size_t x) { return (x + 255) & ~(size_t)255; }
 
+// Blocks per call: the copy-in and symmetrisation launches put the block index in blockIdx.y.
+constexpr int kMaxNoallocBlocks = 65535;
+
 // Offsets of every block inside the scratch regions (one thread; nblk is small).
 __global__ void noalloc_plan_kernel(int nblk, const int *n, long long *voff, long long *asz,
                                     long long *wkoff) {
@@ -92,6 +95,7 @@ extern "C" int dvr3d_b200_diag_batched_noalloc(void *stream, int nblk, const int
                                                 const long long *off_host, const long long *woff_host,
                                                 double *a_dev, double *w_dev, int vecs) {
     if (nblk <= 0 || !n_host || !off_host || !woff_host || !a_dev || !w_dev) return DVR3D_ERR_ARG;
+    if (nblk > kMaxNoallocBlocks) return DVR3D_ERR_ARG;
     cudaStream_t st = (cudaStream_t)stream;
     // size the request with host arithmetic only
     int nmax = 0;
@@ -104,7 +108,8 @@ extern "C" int dvr3d_b200_diag_batched_noalloc(void *stream, int nblk, const int
         sum_n2 += (size_t)nb * nb;
         sum_work += 5 * (size_t)nb * std::min(nb, 128) + (size_t)nb * nb;
     }
-    const size_t meta = align256(sizeof(int) * nblk) * 3 + align256(sizeof(long long) * nblk) * 5 + 256;
+    const size_t meta =
+        align256(sizeof(int) * nblk) * 2 + align256(sizeof(int)) + align256(sizeof(long long) * nblk) * 5 + 256;
     const size_t need = meta + align256(sizeof(double) * sum_n) * 4 + align256(sizeof(double) * sum_n2) +
                         (vecs ? align256(sizeof(double) * sum_work) : 0);
     if (need > (size_t)DVR3D_NOALLOC_SCRATCH_BYTES) return DVR3D_ERR_SCRATCH;
@@ -122,7 +127,7 @@ extern "C" int dvr3d_b200_diag_batched_noalloc(void *stream, int nblk, const int
     };
     int *d_n = reinterpret_cast<int *>(take(sizeof(int) * nblk));
     int *d_cnt = reinterpret_cast<int *>(take(sizeof(int) * nblk));
-    int *d_err = reinterpret_cast<int *>(take(sizeof(int) * nblk));
+    int *d_err = reinterpret_cast<int *>(take(sizeof(int)));
     long long *d_off = reinterpret_cast<long long *>(take(sizeof(long long) * nblk));
     long long *d_woff = reinterpret_cast<long long *>(take(sizeof(long long) * nblk));
     long long *d_voff = reinterpret_cast<long long *>(take(sizeof(long long) * nblk));
@@ -142,27 +147,44 @@ extern "C" int dvr3d_b200_diag_batched_noalloc(void *stream, int nblk, const int
     ck(cudaMemcpyAsync(d_off, off_host, sizeof(long long) * nblk, cudaMemcpyHostToDevice, st));
     ck(cudaMemcpyAsync(d_woff, woff_host, sizeof(long long) * nblk, cudaMemcpyHostToDevice, st));
     ck(cudaMemsetAsync(d_err, 0, sizeof(int), st));  // the error flag starts at zero
+    // Stop before anything is written to the caller's a_dev / w_dev when a launch fails: the
+    // caller's blocks must survive a failed call, as they do with dvr3d_b200_diag_batched.
+    auto bail = [&]() {
+        cudaStreamSynchronize(st);
+        cudaGetLastError();
+        return DVR3D_ERR_CUDA;
+    };
+    if (e != cudaSuccess) return bail();
     noalloc_plan_kernel<<<1, 32, 0, st>>>(nblk, d_n, d_voff, d_asz, d_wk);
-    noalloc_copy_in_kernel<<<dim3(64, nblk), 256, 0, st>>>(d_n, d_off, d_asz, a_dev, d_acopy);
-    DVR3D_COUNT_LAUNCH(2);
     ck(cudaGetLastError());
+    noalloc_copy_in_kernel<<<dim3(64, nblk), 256, 0, st>>>(d_n, d_off, d_asz, a_dev, d_acopy);
+    ck(cudaGetLastError());
+    DVR3D_COUNT_LAUNCH(2);
+    if (e != cudaSuccess) return bail();
     const dvr3d::BatchDesc bd{nblk, d_n, d_asz, d_voff};
     dvr3d::launch_symmetrize_lower(bd, d_acopy, nmax, st);
+    ck(cudaGetLastError());
     dvr3d::launch_tridiag_batched(bd, d_acopy, d_d, d_e, d_tau, nmax, st);
+    ck(cudaGetLastError());
     dvr3d::launch_eigvals_batched(bd, d_d, d_e, d_w, d_cnt, 0, 0.0, st);  // all eigenvalues
+    ck(cudaGetLastError());
+    if (e != cudaSuccess) return bail();
     noalloc_copy_w_kernel<<<nblk, 128, 0, st>>>(d_n, d_voff, d_woff, d_w, w_dev);
     DVR3D_COUNT_LAUNCH(1);
     ck(cudaGetLastError());
-    if (vecs) {
+    if (vecs && e == cudaSuccess) {
         // eigenvectors of all eigenvalues written over the caller's blocks (ld = n)
         dvr3d::launch_eigvecs_batched(bd, d_acopy, d_d, d_e, d_tau, d_w, d_n, d_off, d_n, a_dev, d_work, d_wk,
                                       nmax, d_err, st);
         ck(cudaGetLastError());
     }
+    int err_host = 0;
+    if (vecs) ck(cudaMemcpyAsync(&err_host, d_err, sizeof(int), cudaMemcpyDeviceToHost, st));
     ck(cudaStreamSynchronize(st));
     if (e != cudaSuccess) {
         cudaGetLastError();
         return DVR3D_ERR_CUDA;
     }
+    if (err_host != 0) return DVR3D_ERR_NOCONV;  // inverse iteration failed its growth test
     return DVR3D_OK;
 }

@@ -101,6 +101,10 @@ void check_dev_err(dvr3d_ctx *ctx, const int *err_dev, const char *stage) {
     if (e != 0) throw HostError{DVR3D_ERR_NOCONV, std::string(stage) + ": device error flag " + std::to_string(e)};
 }
 
+// Flag raised by the batched eigenvector kernels when inverse iteration fails its growth
+// test; cleared at the start of each solve, read after the 1D/2D stage and at the end.
+int *ev_err(dvr3d_ctx *ctx) { return ctx->arena.get_t<int>("ev_err", 1); }
+
 // ---------------------------------------------------------------- Radau (nfmain)
 void radau_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
     cudaStream_t st = ctx->stream;
@@ -216,7 +220,7 @@ void radau_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
         col += sel[b];
     }
     launch_eigvecs_batched_fast(bd, H, d, e, tau, w, upload(ctx, "sel", sel), upload(ctx, "zoff", zoff),
-                                upload(ctx, "zld", zld), out.Vt, n, st);
+                                upload(ctx, "zld", zld), out.Vt, n, ev_err(ctx), st);
     CK(cudaGetLastError());
     // sqrt of the pair weight w_p = 1/(2 mu r_a^2) + 1/(2 mu r_b^2) (blc2d2 :3537-3539)
     std::vector<double> sw(out.ldv, 0.0);
@@ -315,7 +319,7 @@ void jacobi_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
     {
         std::vector<int> zld1(nb1, na);
         launch_eigvecs_batched_fast(bd1, H1, d1, e1, t1, w1, upload(ctx, "sel1", iv1), upload(ctx, "zoff1", zoff1),
-                                    upload(ctx, "zld1", zld1), U, na, st);
+                                    upload(ctx, "zld1", zld1), U, na, ev_err(ctx), st);
         CK(cudaGetLastError());
     }
     // 1D eigenvalues and coordinate-b index of each 2D basis function
@@ -438,7 +442,7 @@ void jacobi_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
     double *V2 = ctx->arena.get_t<double>("v2", (size_t)std::max<long long>(v2t, 1));
     {
         launch_eigvecs_batched_fast(bd2, H2, d2, e2d, t2, w2, upload(ctx, "sel2", sel2), upload(ctx, "zoff2", zoff2),
-                                    upload(ctx, "zld2", zld2), V2, n2max, st);
+                                    upload(ctx, "zld2", zld2), V2, n2max, ev_err(ctx), st);
         CK(cudaGetLastError());
     }
     // contracted basis (mkham3 first part :2362-2411)
@@ -568,7 +572,7 @@ void channel_setup(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contra
     int *cnt = ctx->arena.get_t<int>("ch_cnt", kmax);
     launch_tridiag_batched(bd, A, d, e, tau, nmax, st);
     launch_eigvals_batched(bd, d, e, lam, cnt, 0, 0.0, st);
-    launch_eigvecs_batched_fast(bd, A, d, e, tau, lam, dn, dq, dn, Q, nmax, st);
+    launch_eigvecs_batched_fast(bd, A, d, e, tau, lam, dn, dq, dn, Q, nmax, ev_err(ctx), st);
     CK(cudaGetLastError());
     // per-mode features
     std::vector<double> lh = download(ctx, lam, N), e2h = download(ctx, C.e2, N);
@@ -759,11 +763,13 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
     res.dom_launches = 0;
     std::memset(res.dom_kernel, 0, sizeof(res.dom_kernel));
     cudaStream_t st = ctx->stream;
+    CK(cudaMemsetAsync(ev_err(ctx), 0, sizeof(int), st));
     CK(cudaEventRecord(ctx->ev[0], st));
     Contracted C;
     if (p.radau) radau_stage(ctx, p, C);
     else jacobi_stage(ctx, p, C);
     CK(cudaEventRecord(ctx->ev[1], st));
+    check_dev_err(ctx, ev_err(ctx), "batched inverse iteration (1D/2D eigenvectors)");
     const int N = C.N;
     res.kz = p.kz;
     res.ipar = p.ipar;
@@ -846,6 +852,7 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
         std::vector<double> rn;
         DavidsonStats ds;
         const bool ok = davidson_solve(ctx, H3, ldh, C, opt, meval, mode, lpw, wv, rn, Z, ds);
+        check_dev_err(ctx, ev_err(ctx), "batched inverse iteration (channel blocks)");
         res.iterations = ds.iterations;
         res.matvecs = ds.matvecs;
         if (ds.trained) {

@@ -171,7 +171,7 @@ __global__ void __launch_bounds__(kSmallThreads) small_syev_kernel(SmallSyev p) 
     }
     __syncthreads();
     const int T = kSmallThreads;
-    for (int c = tid; c < s_ncl; c += T) invit_cluster(dd, ee, n, wv, cst[c], cst[c + 1], s_norm, fac, T, tid, X, n);
+    for (int c = tid; c < s_ncl; c += T) invit_cluster(dd, ee, n, wv, cst[c], cst[c + 1], s_norm, fac, T, tid, X, n, nullptr);
     __syncthreads();
     for (int q = tid; q < n * n; q += blockDim.x) {
         const int j = q / n, i = q % n;
@@ -205,13 +205,15 @@ cudaError_t launch_small_syev(const SmallSyev &p, int nmax, cudaStream_t st) {
     if (p.nmat <= 0) return cudaSuccess;
     if (nmax > kSmallSyevMax) return cudaErrorInvalidValue;
     const size_t smem = small_syev_smem(nmax);
-    static bool attr = false;
-    if (!attr) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    static bool attr[kMaxAttrDevices] = {};
+    if (dev < 0 || dev >= kMaxAttrDevices || !attr[dev]) {
         // dynamic shared memory of the largest supported problem (static memory comes on top)
         const cudaError_t e = cudaFuncSetAttribute(small_syev_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                                    (int)small_syev_smem(kSmallSyevMax));
         if (e != cudaSuccess) return e;
-        attr = true;
+        if (dev >= 0 && dev < kMaxAttrDevices) attr[dev] = true;
     }
     DVR3D_COUNT_LAUNCH(1);
     small_syev_kernel<<<p.nmat, kSmallThreads, smem, st>>>(p);

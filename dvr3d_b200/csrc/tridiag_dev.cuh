@@ -46,11 +46,21 @@ static __device__ __forceinline__ unsigned hash32(unsigned x) {
     return x;
 }
 
+// Convergence test of one inverse-iteration pass, as dstein applies it: with the right-hand
+// side scaled to 1-norm n ||T||_1 max(eps, |u_nn|), the solve has converged when the largest
+// component of the (orthogonalised) solution reaches sqrt(0.1 / n). A vector is accepted when
+// at least kInvitGrowPasses of the kInvitPasses passes grew that much; otherwise the kernel
+// raises its error flag (non-convergence, reported to the host as DVR3D_ERR_NOCONV).
+constexpr int kInvitPasses = 4;
+constexpr int kInvitGrowPasses = 2;
+static __device__ __forceinline__ double invit_growth_limit(int n) { return sqrt(0.1 / (double)n); }
+
 // One thread: eigenvectors of the cluster [j0, j1) of T. Factor arrays interleaved with
-// stride T (thread slots), vectors interleaved with stride nsel (eigenvalue slots).
+// stride T (thread slots), vectors interleaved with stride nsel (eigenvalue slots). A vector
+// that fails the growth test sets *err = 1 (when err is not null).
 static __device__ __noinline__ void invit_cluster(const double *d, const double *e, int n, const double *w, int j0,
                               int j1, double onenrm, double *fac, int T, int t, double *X,
-                              int nsel) {
+                              int nsel, int *err) {
     double *D = fac, *E1 = fac + (size_t)n * T, *E2 = fac + 2 * (size_t)n * T;
     double *Lm = fac + 3 * (size_t)n * T, *P = fac + 4 * (size_t)n * T;
 #define F(arr, i) arr[(size_t)(i) * T + t]
@@ -98,7 +108,9 @@ static __device__ __noinline__ void invit_cluster(const double *d, const double 
             const unsigned h = hash32((unsigned)(i * 2654435761u) ^ (unsigned)(j * 40503u + 17u));
             XV(i, j) = ((double)(h & 0xffffff) / 8388608.0) - 1.0;
         }
-        for (int it = 0; it < 4; ++it) {
+        const double grow_lim = invit_growth_limit(n);
+        int grown = 0;
+        for (int it = 0; it < kInvitPasses; ++it) {
             // scale the right-hand side so the solve cannot overflow (as dstein does)
             double s1 = 0.0;
             for (int i = 0; i < n; ++i) s1 += fabs(XV(i, j));
@@ -129,12 +141,17 @@ static __device__ __noinline__ void invit_cluster(const double *d, const double 
                 for (int i = 0; i < n; ++i) dot += XV(i, jj) * XV(i, j);
                 for (int i = 0; i < n; ++i) XV(i, j) -= dot * XV(i, jj);
             }
-            double nrm = 0.0;
-            for (int i = 0; i < n; ++i) nrm += XV(i, j) * XV(i, j);
+            double nrm = 0.0, xinf = 0.0;
+            for (int i = 0; i < n; ++i) {
+                nrm += XV(i, j) * XV(i, j);
+                xinf = fmax(xinf, fabs(XV(i, j)));
+            }
+            grown += (xinf >= grow_lim);
             nrm = sqrt(nrm);
             const double inv = (nrm > 0.0) ? 1.0 / nrm : 0.0;
             for (int i = 0; i < n; ++i) XV(i, j) *= inv;
         }
+        if (grown < kInvitGrowPasses && err) *err = 1;
         // sign convention: largest component positive
         double big = 0.0;
         for (int i = 0; i < n; ++i)

@@ -219,9 +219,8 @@ int dvr3d_b200_diag_batched(dvr3d_ctx *ctx, int nblk, const int *n_host,
                             const long long *off_host, const long long *woff_host,
                             double *a_dev, double *w_dev, int vecs);
 
-/* ---- allocation-free variant ---------------------------------------------------------- */
-/* ---- learned Davidson preconditioner (no counterpart in the reference) ----
- * A solve with options.learned_precond = 2 records (residual, ideal correction) pairs and
+/* ---- learned Davidson preconditioner (no counterpart in the reference) ---------------- */
+/* A solve with options.learned_precond = 2 records (residual, ideal correction) pairs and
  * trains the context's network; later solves with learned_precond = 1 use it (for example
  * trained on k = 0 and reused for the other k blocks, or on one surface of a fit and reused
  * for the next). Its parameters can be read out and loaded into another context. */
@@ -242,6 +241,7 @@ int dvr3d_b200_lp_eval(dvr3d_ctx *ctx, const double *w, int nmode, int ncol, con
  * (learned_precond = 2). */
 int dvr3d_b200_lp_train_loss(dvr3d_ctx *ctx, const double *w, double *loss, double *grad);
 
+/* ---- allocation-free variant ---------------------------------------------------------- */
 /* No counterpart in the reference. Same computation and arguments as
  * dvr3d_b200_diag_batched, for callers that must not allocate device memory (a host whose
  * framework's memory pool owns the GPU memory and forbids outside cudaMalloc, or a latency-
@@ -251,7 +251,9 @@ int dvr3d_b200_lp_train_loss(dvr3d_ctx *ctx, const double *w, double *loss, doub
  * DVR3D_NOALLOC_SCRATCH_BYTES compiled into the library, held by every GPU that loads it.
  * Limit: requests needing more scratch than that -- about 8*(4n + 2n^2 + 5n*min(n,128)) bytes
  * summed over the blocks with vecs != 0 -- return DVR3D_ERR_SCRATCH; split them into several
- * calls. The first call on a device looks the array up (do it before any stream capture on
+ * calls. At most 65535 blocks per call (DVR3D_ERR_ARG beyond). A failed launch returns
+ * DVR3D_ERR_CUDA before the caller's a_dev / w_dev are written; inverse iteration that does
+ * not converge returns DVR3D_ERR_NOCONV, as dvr3d_b200_diag_batched does. The first call on a device looks the array up (do it before any stream capture on
  * that device). All calls share the array: calls that may overlap on the GPU race and must
  * be serialised by the caller. Synchronises `stream` before returning. */
 #define DVR3D_NOALLOC_SCRATCH_BYTES (64u * 1024u * 1024u)

@@ -19,6 +19,10 @@ extern "C" {
  * as scipy_dsyev_ ...). `prefix` is the symbol prefix ("scipy_" or ""). */
 int oracle_load_lapack(const char *path, const char *prefix);
 
+/* The oracle's own reader of a job deck (deck_reader.cpp), independent of the product's
+ * dvr3d_b200_parse_deck: namelist PRT, cards 2-10 and the optional EZERO card. */
+int oracle_parse_deck(const char *text, dvr3d_deck *out);
+
 /* Quadrature known-answer data of one k block (what lagpt / jacobi print). */
 typedef struct oracle_quad {
     int npnt1, npnt2, nang2, nidvr;

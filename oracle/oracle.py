@@ -1,7 +1,10 @@
 """ctypes wrapper of the CPU oracle (``oracle/libdvr3d_oracle.so``).
 
-TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the CPU-baseline
-leg of bench.py to check / time the reference algorithm; never by the product package.
+TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and the CPU legs of
+bench.py to check / time the reference algorithm; never by the product package, and it never
+imports the product package itself: it has its own deck reader (deck_reader.cpp), its own
+build recipe (oracle/build.py) and its own mirrors of the two interface structures of
+include/dvr3d_b200.h that it fills (struct dvr3d_deck, struct dvr3d_result).
 The oracle restates source/dvr3drjz_segmented.f90 of the reference (see dvr3d_oracle.cpp)
 and calls LAPACK dsyev from the OpenBLAS library bundled with scipy.
 """
@@ -18,11 +21,41 @@ import numpy as np
 ROOT = Path(__file__).resolve().parent.parent
 LIB = Path(__file__).resolve().parent / "libdvr3d_oracle.so"
 
-import sys  # noqa: E402
+_DECK_INTS = ["zpham", "zprad", "zp1d", "zp2d", "zpmin", "zpvec", "zlmat", "zcut", "zrot", "zperp", "zembed",
+              "zlin", "zmors1", "zmors2", "zladd", "ztwod", "zvec", "zall", "ztheta", "zr2r1", "ztran", "zquad2",
+              "zdiag", "zpfun", "zx", "zs0", "zs1", "ncoord", "npnt2", "jrot", "neval", "nalf", "max2d", "max3d",
+              "idia", "kmin", "npnt1", "ipar", "max3d2"]
 
-if str(ROOT) not in sys.path:
-    sys.path.insert(0, str(ROOT))
-from dvr3d_b200._abi import Deck, Result  # noqa: E402  (interface structs only)
+
+class Deck(C.Structure):
+    """struct dvr3d_deck (include/dvr3d_b200.h), as the oracle's deck reader fills it."""
+
+    _fields_ = ([(n, C.c_int) for n in _DECK_INTS] +
+                [("title", C.c_char * 80), ("fixcos", C.c_double),
+                 ("xmass", C.c_double * 3), ("xmassr", C.c_double * 3),
+                 ("emax1", C.c_double), ("emax2", C.c_double),
+                 ("re1", C.c_double), ("diss1", C.c_double), ("we1", C.c_double),
+                 ("re2", C.c_double), ("diss2", C.c_double), ("we2", C.c_double),
+                 ("ezero", C.c_double), ("have_ezero", C.c_int)])
+
+
+class Result(C.Structure):
+    """struct dvr3d_result (include/dvr3d_b200.h): the oracle writes eval, meval and status."""
+
+    _fields_ = [("kz", C.c_int), ("ipar", C.c_int), ("nham3", C.c_int), ("meval", C.c_int),
+                ("nblocks", C.c_int), ("iterations", C.c_int), ("fallback", C.c_int),
+                ("stage_ms", C.c_double * 6), ("max_resid", C.c_double),
+                ("dom_ms", C.c_double), ("dom_bytes", C.c_double), ("dom_flops", C.c_double),
+                ("dom_launches", C.c_int), ("launches", C.c_int),
+                ("h2d_bytes", C.c_longlong), ("d2h_bytes", C.c_longlong),
+                ("dom_kernel", C.c_char * 48),
+                ("eval", C.POINTER(C.c_double)), ("eval_cap", C.c_int),
+                ("iv2", C.POINTER(C.c_int)), ("iv2_cap", C.c_int),
+                ("resid", C.POINTER(C.c_double)), ("resid_cap", C.c_int),
+                ("evec", C.POINTER(C.c_double)), ("evec_cap", C.c_size_t),
+                ("h3", C.POINTER(C.c_double)), ("h3_cap", C.c_size_t),
+                ("path", C.c_int), ("matvecs", C.c_int), ("lp_pairs", C.c_int),
+                ("lp_loss_first", C.c_double), ("lp_loss_last", C.c_double)]
 
 
 class Quad(C.Structure):
@@ -71,12 +104,13 @@ def load(build: bool = True) -> C.CDLL:
     if _lib is not None:
         return _lib
     if build or not LIB.exists():
-        from dvr3d_b200.build import build_oracle
+        from oracle.build import build as build_oracle
 
         build_oracle()
     lib = C.CDLL(str(LIB))
     P = C.POINTER
     lib.oracle_load_lapack.argtypes = [C.c_char_p, C.c_char_p]
+    lib.oracle_parse_deck.argtypes = [C.c_char_p, P(Deck)]
     lib.oracle_quadrature.argtypes = [P(Deck), C.c_int, P(Quad)]
     lib.oracle_solve_block.argtypes = [P(Deck), C.c_int, C.c_int, P(C.c_double), C.c_int, P(C.c_double),
                                        C.c_size_t, C.c_int, P(Trace), P(Result)]
@@ -92,13 +126,43 @@ def load(build: bool = True) -> C.CDLL:
     return lib
 
 
-def quadrature(deck: Deck, kk: int = 0) -> Quad:
+def parse_deck(text: str) -> Deck:
+    """Read a job deck with the oracle's own reader (deck_reader.cpp)."""
+    d = Deck()
+    rc = load().oracle_parse_deck(text.encode(), C.byref(d))
+    if rc != 0:
+        raise ValueError(f"oracle deck reader rejected the deck ({rc})")
+    return d
+
+
+def as_deck(deck) -> Deck:
+    """A deck for the oracle: deck text is read by the oracle's reader; a structure of the
+    same C layout (struct dvr3d_deck) is copied byte for byte."""
+    if isinstance(deck, str):
+        return parse_deck(deck)
+    if isinstance(deck, Deck):
+        return deck
+    if C.sizeof(deck) != C.sizeof(Deck):
+        raise TypeError("not a struct dvr3d_deck")
+    d = Deck()
+    C.memmove(C.byref(d), C.byref(deck), C.sizeof(Deck))
+    return d
+
+
+def k_blocks(deck) -> list[int]:
+    """k-loop indices [kd .. ku] of ccmain (:811-819) for a deck (from oracle_sizes)."""
+    s = sizes(deck, 0)
+    return list(range(s["kd"], s["ku"] + 1))
+
+
+def quadrature(deck, kk: int = 0) -> Quad:
     q = Quad()
-    load().oracle_quadrature(C.byref(deck), kk, C.byref(q))
+    load().oracle_quadrature(C.byref(as_deck(deck)), kk, C.byref(q))
     return q
 
 
-def sizes(deck: Deck, kk: int = 0) -> dict:
+def sizes(deck, kk: int = 0) -> dict:
+    deck = as_deck(deck)
     o = (C.c_int * 16)()
     rc = load().oracle_sizes(C.byref(deck), kk, o)
     if rc != 0:
@@ -125,8 +189,10 @@ class OracleResult:
 
 def solve(deck: Deck, kk: int = 0, pes=None, vgrid=None, final_mode: int = 0, want_h3: bool = False,
           want_eigs2d: bool = True, h3_cap: int = 0) -> OracleResult:
-    """Run the oracle on one k block. pes: 13 MORSE_SUM parameters, or vgrid: table."""
+    """Run the oracle on one k block. pes: 13 MORSE_SUM parameters, or vgrid: table.
+    deck: deck text (read by the oracle's reader) or a struct dvr3d_deck."""
     lib = load()
+    deck = as_deck(deck)
     s = sizes(deck, kk)
     nblk = max(s["nalf"], s["npntc"], 1)
     neval = max(s["neval"], 1)

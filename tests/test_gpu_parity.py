@@ -17,10 +17,12 @@ TOL_CM = 1e-6
 
 
 def _compare(ctx, oracle_mod, w, kk=None, tol_cm=TOL_CM, check_resid=True):
+    # each side reads the deck text with its own reader
     d = parse_deck(w.deck)
     ks = dvr3d_b200.k_blocks(d) if kk is None else [kk]
+    assert ks == oracle_mod.k_blocks(w.deck)
     for k in ks:
-        ref = oracle_mod.solve(d, k, pes=w.pes, final_mode=1)
+        ref = oracle_mod.solve(w.deck, k, pes=w.pes, final_mode=1)
         assert ref.status == 0, ref.status
         ctx.set_pes(w.pes)
         got = ctx.solve(d, k, want_resid=check_resid)
@@ -100,7 +102,7 @@ def test_config1_full_size(ctx, oracle_mod):
 def test_h3_assembly_matches_oracle(ctx, oracle_mod):
     w = configs.radau_water_like(10, 12, 30000.0, 20, title="radau h3")
     d = parse_deck(w.deck)
-    ref = oracle_mod.solve(d, 0, pes=w.pes, final_mode=2, want_h3=True)
+    ref = oracle_mod.solve(w.deck, 0, pes=w.pes, final_mode=2, want_h3=True)
     ctx.set_pes(w.pes)
     got = ctx.solve(d, 0, want_h3=True)
     n = ref.nham3
@@ -129,7 +131,7 @@ def test_pes_grid_table_equals_closed_form(ctx, oracle_mod):
     ctx.set_pes_grid(tab)
     b = ctx.solve(d, 0)
     np.testing.assert_allclose(b.eval, a.eval, rtol=0, atol=1e-13)
-    ref = oracle_mod.solve(d, 0, vgrid=tab, final_mode=1)
+    ref = oracle_mod.solve(w.deck, 0, vgrid=tab, final_mode=1)
     np.testing.assert_allclose(b.eval, ref.eval, rtol=0, atol=TOL_CM / AUTOCM)
     ctx.set_pes(w.pes)
 

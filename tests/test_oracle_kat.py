@@ -15,13 +15,19 @@ CASES = ["water_J0", "h3p_jacobi_J0", "hcn_J2"]
 
 
 def _deck(kat, name):
+    """The deck as the product reads it (dvr3d_b200_parse_deck)."""
     return parse_deck(kat["cases"][name]["deck"])
+
+
+def _odeck(oracle_mod, kat, name):
+    """The deck as the oracle reads it (its own reader)."""
+    return oracle_mod.parse_deck(kat["cases"][name]["deck"])
 
 
 @pytest.mark.parametrize("name", CASES)
 def test_laguerre_points_match_reference(kat, oracle_mod, name):
-    d = _deck(kat, name)
-    q = oracle_mod.quadrature(d, dvr3d_b200.k_blocks(d)[0])
+    d = _odeck(oracle_mod, kat, name)
+    q = oracle_mod.quadrature(d, oracle_mod.k_blocks(d)[0])
     assert q.status == 0
     for lag in kat["cases"][name]["laguerre"]:
         n = lag["n"]
@@ -39,8 +45,8 @@ def test_laguerre_points_match_reference(kat, oracle_mod, name):
 
 @pytest.mark.parametrize("name", CASES)
 def test_legendre_points_weights_and_sums_match_reference(kat, oracle_mod, name):
-    d = _deck(kat, name)
-    ks = dvr3d_b200.k_blocks(d)
+    d = _odeck(oracle_mod, kat, name)
+    ks = oracle_mod.k_blocks(d)
     legs = kat["cases"][name]["legendre"]
     assert len(legs) == len(ks)
     for kk, leg in zip(ks, legs):
@@ -78,7 +84,7 @@ def test_product_host_grid_matches_reference(kat, name):
 def test_product_host_grid_equals_oracle(kat, oracle_mod, name):
     d = _deck(kat, name)
     for kk in dvr3d_b200.k_blocks(d):
-        q = oracle_mod.quadrature(d, kk)
+        q = oracle_mod.quadrature(_odeck(oracle_mod, kat, name), kk)
         r1, r2, xa = dvr3d_b200.host_grid(d, kk)
         np.testing.assert_array_equal(r1, np.array(q.r1[:len(r1)]))
         if d.idia != -2:
@@ -86,10 +92,11 @@ def test_product_host_grid_equals_oracle(kat, oracle_mod, name):
         np.testing.assert_array_equal(xa, np.array(q.xalf[:len(xa)]))
 
 
-def test_water_deck_card_order_quirk(kat):
+@pytest.mark.parametrize("reader", ["product", "oracle"])
+def test_water_deck_card_order_quirk(kat, oracle_mod, reader):
     """setcon reads EMAX1/EMAX2 before the Morse cards (:1058-1095); the water deck has no
     separate EMAX card, so its first Morse line is consumed as EMAX1, EMAX2."""
-    d = _deck(kat, "water_J0")
+    d = _deck(kat, "water_J0") if reader == "product" else _odeck(oracle_mod, kat, "water_J0")
     assert (d.npnt2, d.jrot, d.neval, d.nalf, d.max2d, d.max3d, d.idia, d.kmin) == (21, 0, 25, 40, 500, 500, -2, 2)
     assert (d.emax1, d.emax2) == (2.55, 0.25)
     assert (d.re1, d.diss1, d.we1) == (2.55, 0.25, 0.007)
@@ -97,19 +104,48 @@ def test_water_deck_card_order_quirk(kat):
     assert list(d.xmass) == [1.007825, 1.007825, 15.990726]
 
 
-def test_hcn_deck_namelist_spanning_lines(kat):
-    d = _deck(kat, "hcn_J2")
+@pytest.mark.parametrize("reader", ["product", "oracle"])
+def test_hcn_deck_namelist_spanning_lines(kat, oracle_mod, reader):
+    d = _deck(kat, "hcn_J2") if reader == "product" else _odeck(oracle_mod, kat, "hcn_J2")
     assert d.ztheta == 0 and d.zr2r1 == 0 and d.zembed == 0 and d.zp1d == 0 and d.zp2d == 0
     assert (d.npnt2, d.jrot, d.neval, d.nalf, d.idia, d.kmin, d.npnt1) == (30, 2, 40, 45, 1, 2, 16)
     assert d.emax1 == 45000.0
-    assert dvr3d_b200.k_blocks(d) == [0, 1, 2]
+    ks = dvr3d_b200.k_blocks(d) if reader == "product" else oracle_mod.k_blocks(d)
+    assert ks == [0, 1, 2]
 
 
 def test_reduced_masses_match_printed(kat, oracle_mod):
     # water output: reduced mass 0.1732801D+04, beta 0.4121, a 0.1428571D+03, u 143
-    q = oracle_mod.quadrature(_deck(kat, "water_J0"), 0)
+    q = oracle_mod.quadrature(_odeck(oracle_mod, kat, "water_J0"), 0)
     assert abs(q.ur1 - 1732.801) < 5e-4 and abs(q.beta1 - 0.4121) < 5e-5 and q.iu1 == 143
     # H3+ Jacobi: 0.9183139D+03 / 0.7996 / u=34 ; 0.1224419D+04 / 0.4367 / u=116
-    q = oracle_mod.quadrature(_deck(kat, "h3p_jacobi_J0"), 0)
+    q = oracle_mod.quadrature(_odeck(oracle_mod, kat, "h3p_jacobi_J0"), 0)
     assert abs(q.ur1 - 918.3139) < 5e-5 and abs(q.beta1 - 0.7996) < 5e-5 and q.iu1 == 34
     assert abs(q.ur2 - 1224.419) < 5e-4 and abs(q.beta2 - 0.4367) < 5e-5 and q.iu2 == 116
+
+
+def _deck_fields(d):
+    out = {}
+    for f, _ in d._fields_:
+        v = getattr(d, f)
+        out[f] = v if isinstance(v, (int, float, bytes)) else list(v)
+    return out
+
+
+def _variant_decks(kat):
+    from dvr3d_b200 import configs
+
+    texts = [c["deck"] for c in kat["cases"].values()]
+    texts += [w.deck for w in (configs.config1(), configs.config2(), configs.config4(), configs.config5())]
+    texts += [w.deck for w in configs.config3(nprob=4)]
+    j = configs.jacobi_h3p_like(9, 10, 14, 45000.0, 40000.0, 20, title="variants")
+    texts.append(j.deck.replace("ZCUT=.TRUE.", "ZCUT=.FALSE.").replace("ZR2R1=.TRUE.", "ZR2R1=F"))
+    texts.append(j.deck.replace(", /", ",\n ZTHETA=.true, ZPFUN=T /") + "           4362.208278\n")
+    return texts
+
+
+def test_oracle_and_product_deck_readers_agree(kat, oracle_mod):
+    """The two independent readers give the same struct dvr3d_deck for every deck used by the
+    tests and the benchmark (the reference's example decks, the seeded workloads, variants)."""
+    for text in _variant_decks(kat):
+        assert _deck_fields(oracle_mod.parse_deck(text)) == _deck_fields(parse_deck(text))
