@@ -88,3 +88,15 @@ def test_noalloc_rejects_requests_beyond_its_scratch(ctx):
     offs, woffs, flat, nw, sym = _blocks(3)
     a, w = _call(lib, None, offs, woffs, flat, nw, noalloc=True)
     np.testing.assert_allclose(w[woffs[-1]:], np.linalg.eigvalsh(sym[-1]), rtol=0, atol=1e-12)
+
+
+def test_noalloc_rejects_more_blocks_than_one_launch_indexes(ctx):
+    """Block counts beyond 65535 are refused on the host, before any device work (the
+    copy-in launch indexes blocks by blockIdx.y); the caller's pointers are not touched."""
+    lib = _abi.load_library()
+    nb = 65536
+    n_arr = (C.c_int * nb)(*([1] * nb))
+    o_arr = (C.c_longlong * nb)(*range(nb))
+    w_arr = (C.c_longlong * nb)(*range(nb))
+    rc = lib.dvr3d_b200_diag_batched_noalloc(None, nb, n_arr, o_arr, w_arr, C.c_void_p(16), C.c_void_p(16), 1)
+    assert rc == _abi.DVR3D_ERR_ARG
