@@ -146,6 +146,10 @@ class Context:
     def set_stream(self, stream_ptr: int) -> None:
         self._check(self._lib.dvr3d_b200_set_stream(self._h, C.c_void_p(stream_ptr)))
 
+    def set_wait_limit(self, polls: int) -> None:
+        """Poll limit of every bounded device wait of later solves (0: the defaults)."""
+        self._check(self._lib.dvr3d_b200_set_wait_limit(self._h, int(polls)))
+
     def set_pes(self, params) -> None:
         p = np.ascontiguousarray(np.asarray(params, dtype=np.float64))
         if p.size != DVR3D_PES_MORSE_SUM_NPARAM:

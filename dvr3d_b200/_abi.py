@@ -122,6 +122,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "dvr3d_b200_strerror": (C.c_char_p, [C.c_int]),
         "dvr3d_b200_last_error": (C.c_char_p, [vp]),
         "dvr3d_b200_set_stream": (C.c_int, [vp, vp]),
+        "dvr3d_b200_set_wait_limit": (C.c_int, [vp, C.c_longlong]),
         "dvr3d_b200_parse_deck": (C.c_int, [C.c_char_p, P(Deck)]),
         "dvr3d_b200_set_pes": (C.c_int, [vp, C.c_int, P(C.c_double), C.c_int]),
         "dvr3d_b200_set_pes_grid": (C.c_int, [vp, P(C.c_double), C.c_size_t]),

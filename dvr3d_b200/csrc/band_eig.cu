@@ -117,6 +117,7 @@ __global__ void __launch_bounds__(kChaseThreads) band_chase_kernel(BandTri t) {
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int n = t.n, b = t.b;
     const long long ld = t.lda;
+    const unsigned long long spin_limit = t.wait_limit ? t.wait_limit : kSpinLimit;
     double *A = t.A;
     for (int q = tid; q < 6 * kBlk + 3 * kBW; q += kChaseThreads) sm[q] = 0.0;
     if (tid == 0) s_abort = 0;
@@ -138,7 +139,7 @@ __global__ void __launch_bounds__(kChaseThreads) band_chase_kernel(BandTri t) {
             if (lane == 0) {
                 unsigned long long spins = 0;
                 while (ld_acquire_u32(t.progress + j - 1) < (unsigned)need) {
-                    if (++spins > kSpinLimit) {
+                    if (++spins > spin_limit) {
                         atomicExch(t.err, (int)kDevBarrierTimeout);
                         ok = 0;
                         break;

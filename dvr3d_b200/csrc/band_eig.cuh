@@ -22,6 +22,7 @@ struct BandTri {
     long long *prof;        // optional [5]: clock cycles of the chase's thread 0 summed over
                             // CTAs (sweep start, reflector, O_s part with the hand-off,
                             // end-of-task wait, unused), or null
+    unsigned long long wait_limit;  // polls of one hand-off wait before it gives up (0: 2^24)
 };
 
 // Zeroes the bulge space (lower triangle, b < i - j <= 2b) and records the largest dropped

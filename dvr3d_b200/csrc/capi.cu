@@ -311,6 +311,12 @@ int dvr3d_b200_diag_batched(dvr3d_ctx *ctx, int nblk, const int *n_host, const l
     });
 }
 
+int dvr3d_b200_set_wait_limit(dvr3d_ctx *ctx, long long polls) {
+    if (!ctx || polls < 0) return DVR3D_ERR_ARG;
+    ctx->wait_limit = (unsigned long long)polls;
+    return DVR3D_OK;
+}
+
 int dvr3d_b200_run_deck(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_options *opt, char *out, size_t outcap,
                         size_t *outlen, char *lev, size_t levcap, size_t *levlen) {
     if (!ctx || !deck_text) return DVR3D_ERR_ARG;

@@ -98,10 +98,12 @@ __device__ __forceinline__ bool grid_sync(GridBarrier *b, int *err, unsigned lon
 // Grid barrier on a counter that only grows: barrier number e of a sequence completes when
 // the counter reaches (e + 1) * gridDim; `target` carries the running count (start it at the
 // arrivals made by earlier launches on the same counter, which is zeroed once before them).
-// No reset step, so the last arrival releases everybody at once. Bounded like grid_sync; a
-// CTA that sees another's error flag while waiting returns false as well.
+// No reset step, so the last arrival releases everybody at once. Bounded like grid_sync (a
+// limit of 0 means the default 2^26 polls); a CTA that sees another's error flag while
+// waiting returns false as well.
 __device__ __forceinline__ bool grid_sync_counted(unsigned int *count, unsigned int &target, int *err,
                                                   unsigned long long limit = (1ull << 26)) {
+    if (limit == 0) limit = 1ull << 26;
     __syncthreads();
     __shared__ int s_okc;
     target += gridDim.x * gridDim.y * gridDim.z;

@@ -167,7 +167,7 @@ __global__ void __launch_bounds__(kPnThreads, 3) dense_panel_kernel(DenseTri t) 
             ss = block_sum(ss, red);
             if (tid == 0) part_n[cta] = ss;
         }
-        if (!grid_sync_counted(&t.bar->count, bar_target, t.err)) return;
+        if (!grid_sync_counted(&t.bar->count, bar_target, t.err, t.wait_limit)) return;
         // ---- phase B: reflector (redundantly in every CTA)
         PROF_MARK(1);
         if (tid < 32) {
@@ -413,7 +413,7 @@ __global__ void __launch_bounds__(kPnThreads, 3) dense_panel_kernel(DenseTri t) 
                 if (lane == 0) part_q[(size_t)c * 2 * nbmax + ((q < i) ? q : nbmax + (q - i))] = s;
             }
         }
-        if (!grid_sync_counted(&t.bar->count, bar_target, t.err)) return;
+        if (!grid_sync_counted(&t.bar->count, bar_target, t.err, t.wait_limit)) return;
         // ---- phase D (all CTAs, eight lanes per row): y_r = sum of the partial products of
         // row r - V (W^T v) - W (V^T v); p = tau y; partial p.v per CTA
         PROF_MARK(3);
@@ -472,7 +472,7 @@ __global__ void __launch_bounds__(kPnThreads, 3) dense_panel_kernel(DenseTri t) 
             pvl = block_sum(pvl, red);
             if (tid == 0) part_d[cta] = pvl;
         }
-        if (!grid_sync_counted(&t.bar->count, bar_target, t.err)) return;
+        if (!grid_sync_counted(&t.bar->count, bar_target, t.err, t.wait_limit)) return;
     }
     // w of the panel's last column (the kernel boundary orders it before the trailing update)
     PROF_MARK(4);

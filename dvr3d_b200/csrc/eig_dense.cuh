@@ -26,6 +26,7 @@ struct DenseTri {
     int nev;
     int npanel;                   // out: panel launches made
     int cache_tiles;              // > 0: resident mode, tiles kept in shared memory per CTA
+    unsigned long long wait_limit;  // polls of one grid-barrier wait before it gives up (0: 2^26)
 };
 
 // Resident mode for small matrices: returns the tiles per CTA (0: not applicable) and the

@@ -640,6 +640,7 @@ void dense_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int nev, bool
     dt.err = ctx->arena.get_t<int>(t + "err", 1);
     CK(cudaMemsetAsync(dt.bar, 0, sizeof(GridBarrier), st));
     CK(cudaMemsetAsync(dt.err, 0, sizeof(int), st));
+    dt.wait_limit = ctx->wait_limit;
     const char *prof_env = std::getenv("DVR3D_PROF");
     const bool prof = prof_env && prof_env[0] == '1';
     if (prof) {
@@ -728,6 +729,7 @@ bool band_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int b, int nev
     t.taus = ctx->arena.get_t<double>("bd_tau", band_tau_doubles(n, b));
     t.progress = ctx->arena.get_t<unsigned int>("bd_prog", n);
     t.err = ctx->arena.get_t<int>("bd_err", 1);
+    t.wait_limit = ctx->wait_limit;
     CK(cudaMemsetAsync(t.err, 0, sizeof(int), st));
     CK(launch_band_chase(t, st));
     check_dev_err(ctx, t.err, "band reduction");

@@ -54,6 +54,7 @@ struct dvr3d_ctx {
     int sm_count = 0;
     int dense_grid = 0;
     std::vector<cudaEvent_t> panel_ev;  // timing pool for the reduction panels
+    unsigned long long wait_limit = 0;  // polls of each bounded device wait (0: kernel defaults)
     bool lp_trained = false;            // arena "lp_w" holds a trained preconditioner network
     struct LpSet {                      // training pairs of the last training solve
         bool valid = false;

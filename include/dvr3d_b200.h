@@ -172,6 +172,15 @@ const char *dvr3d_b200_last_error(const dvr3d_ctx *ctx);
 /* Use `stream` (a cudaStream_t) for all work of this context; NULL = the ctx's own. */
 int dvr3d_b200_set_stream(dvr3d_ctx *ctx, void *stream);
 
+/* Every device-side wait of the library is bounded: the grid barriers of the cooperative
+ * dense reduction (default 2^26 polls) and the hand-off waits of the band reduction's bulge
+ * chase (default 2^24 polls). A wait that runs out raises the kernel's error flag, every CTA
+ * leaves its kernel, and the solve returns DVR3D_ERR_NOCONV with the context still usable.
+ * This sets the poll limit of every such wait of later solves on the context (0 restores the
+ * defaults); a small limit lets a caller check that the waits end. No counterpart in the
+ * reference (which has no device waits). */
+int dvr3d_b200_set_wait_limit(dvr3d_ctx *ctx, long long polls);
+
 /* Reads a job deck in the reference's stdin format: namelist PRT (dvr3d :65, defaults of
  * block data :158-167), card 2 (insize :232), card 3 (:238), title (:372) and the setcon
  * cards (:1042-1095, in the source's order FIXCOS, XMASS, XMASSR, EMAX1/EMAX2, r1 Morse,
