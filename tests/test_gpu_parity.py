@@ -184,3 +184,34 @@ def test_mixed_radau_config2(ctx):
 def test_mixed_config4_500_levels(ctx):
     a, b, err = _mixed_vs_dense(ctx, configs.config4())
     assert b.nham3 > 12000 and len(b.eval) == 500
+
+
+# ---------------------------------------------------------------- full-size workloads vs the oracle
+# tests/golden/config{2,4}_oracle.npz: the oracle's N, per-block selection counts and levels of
+# the benchmark's workloads (made by tests/golden/make_config_fixtures.py: the oracle needs
+# minutes at these sizes). Plain FP64 path: identical counts, levels within 1e-6 cm-1;
+# the chosen (iterative) form: within 1e-3 cm-1.
+def _fixture(k):
+    from pathlib import Path
+
+    f = np.load(Path(__file__).resolve().parent / "golden" / f"config{k}_oracle.npz")
+    return {q: f[q] for q in f.files}
+
+
+@pytest.mark.parametrize("k", [2, 4])
+def test_full_size_workload_matches_oracle_fixture(ctx, k):
+    fx = _fixture(k)
+    w = {2: configs.config2, 4: configs.config4}[k]()
+    assert str(fx["deck"]) == w.deck and np.array_equal(fx["pes"], w.pes)
+    d = parse_deck(w.deck)
+    ctx.set_pes(w.pes)
+    nlev = len(fx["levels"])
+    plain = ctx.solve(d, 0, nlevels=nlev)
+    assert plain.nham3 == int(fx["nham3"])
+    np.testing.assert_array_equal(plain.iv2, fx["iv2"])
+    err = np.abs(plain.eval - fx["levels"]) * AUTOCM
+    assert err.max() <= TOL_CM, f"plain path: max level error {err.max():.3e} cm-1"
+    mixed = ctx.solve(d, 0, nlevels=nlev, precision=dvr3d_b200.DVR3D_PREC_MIXED_DAVIDSON)
+    np.testing.assert_array_equal(mixed.iv2, fx["iv2"])
+    err_m = np.abs(mixed.eval - fx["levels"]) * AUTOCM
+    assert err_m.max() <= TOL_MIXED_CM, f"chosen form: max level error {err_m.max():.3e} cm-1"
