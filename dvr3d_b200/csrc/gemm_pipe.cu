@@ -27,11 +27,30 @@ namespace {
 constexpr int kBM = 64, kBK = 16, kThr = 128;
 constexpr int kSK = kBK + 4;  // stride of [m][k] tiles
 constexpr int kMaxClusterSplit = 8;  // portable cluster size
+// Instruction shape of the inner product: m16n8k16 (one instruction per 16-deep k tile and
+// 16 x 8 output block) or the m8n8k4 of sm_80.
+#ifndef DVR3D_GEMM_K16
+#define DVR3D_GEMM_K16 1
+#endif
+constexpr bool kUseK16 = DVR3D_GEMM_K16 != 0;
 
 __device__ __forceinline__ void dmma(double &c0, double &c1, double a, double b) {
     asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0,%1}, {%2}, {%3}, {%0,%1};\n"
                  : "+d"(c0), "+d"(c1)
                  : "d"(a), "d"(b));
+}
+
+// The larger FP64 shape of sm_90+: one instruction does a 16 x 8 x 16 product. With
+// g = lane / 4 and t = lane % 4 the fragments are A(g + 8 (i % 2), t + 4 (i / 2)) for
+// a[0..7], B(k = t + 4 i, n = g) for b[0..3], and C(g, 2t), C(g, 2t+1), C(g+8, 2t),
+// C(g+8, 2t+1) for c[0..3].
+__device__ __forceinline__ void dmma16(double (&c)[4], const double (&a)[8], const double (&b)[4]) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f64.f64.f64.f64 {%0,%1,%2,%3}, {%4,%5,%6,%7,%8,%9,%10,%11}, "
+        "{%12,%13,%14,%15}, {%0,%1,%2,%3};\n"
+        : "+d"(c[0]), "+d"(c[1]), "+d"(c[2]), "+d"(c[3])
+        : "d"(a[0]), "d"(a[1]), "d"(a[2]), "d"(a[3]), "d"(a[4]), "d"(a[5]), "d"(a[6]), "d"(a[7]), "d"(b[0]),
+          "d"(b[1]), "d"(b[2]), "d"(b[3]));
 }
 
 __device__ __forceinline__ void cp16(void *smem, const void *gmem, int bytes) {
@@ -74,7 +93,7 @@ struct TileLoader {
 
 // op(A)(i, k): TA ? A[i * lda + k] : A[k * lda + i]   (k-contiguous when TA)
 // op(B)(k, j): TB ? B[k * ldb + j] : B[j * ldb + k]   (k-contiguous when !TB)
-template <bool TA, bool TB, int BN, bool CL>
+template <bool TA, bool TB, int BN, bool CL, bool K16 = kUseK16>
 __global__ void __launch_bounds__(kThr) gemm_pipe_kernel(GemmOp p, int tiles_m) {
     using LA = TileLoader<kBM, TA>;
     using LB = TileLoader<BN, !TB>;
@@ -115,11 +134,18 @@ __global__ void __launch_bounds__(kThr) gemm_pipe_kernel(GemmOp p, int tiles_m) 
     const int t0 = (int)((long long)ntk * z / S), t1 = (int)((long long)ntk * (z + 1) / S);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int wm = (warp >> 1) * 32, wn = (warp & 1) * WN;
-    double acc[4][FN][2];
+    // accumulators: K16 -> [two 16-row tiles][FN 8-column tiles][4]; else [four 8-row
+    // tiles][FN][2]; either way 8 FN doubles per thread
+    double acc[K16 ? 2 : 4][FN][K16 ? 4 : 2];
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < (K16 ? 2 : 4); ++a)
 #pragma unroll
-        for (int b = 0; b < FN; ++b) acc[a][b][0] = acc[a][b][1] = 0.0;
+        for (int b = 0; b < FN; ++b)
+#pragma unroll
+            for (int h = 0; h < (K16 ? 4 : 2); ++h) acc[a][b][h] = 0.0;
+    // row / column of accumulator element (a, b, h) within the CTA tile
+    auto acc_row = [&](int a, int h) { return K16 ? wm + a * 16 + (lane >> 2) + 8 * (h >> 1) : wm + a * 8 + (lane >> 2); };
+    auto acc_col = [&](int b, int h) { return wn + b * 8 + (lane & 3) * 2 + (K16 ? (h & 1) : h); };
     auto load = [&](int st, int kt) {
         const int k0 = kb + kt * kBK;
         const int kmax = ke - k0;
@@ -146,21 +172,37 @@ __global__ void __launch_bounds__(kThr) gemm_pipe_kernel(GemmOp p, int tiles_m) 
             asm volatile("cp.async.wait_group 0;\n" ::);
         }
         __syncthreads();
+        if constexpr (K16) {
+            double af[2][8], bf[FN][4];
 #pragma unroll
-        for (int kk = 0; kk < kBK; kk += 4) {
-            double af[4], bf[FN];
+            for (int a = 0; a < 2; ++a)
 #pragma unroll
-            for (int t = 0; t < 4; ++t) af[t] = LA::at(As[st], wm + t * 8 + r, kk + c);
+                for (int i = 0; i < 8; ++i) af[a][i] = LA::at(As[st], wm + a * 16 + r + 8 * (i & 1), c + 4 * (i >> 1));
 #pragma unroll
-            for (int t = 0; t < FN; ++t) bf[t] = LB::at(Bs[st], wn + t * 8 + r, kk + c);
+            for (int b = 0; b < FN; ++b)
 #pragma unroll
-            for (int a = 0; a < 4; ++a)
+                for (int i = 0; i < 4; ++i) bf[b][i] = LB::at(Bs[st], wn + b * 8 + r, c + 4 * i);
 #pragma unroll
-                for (int b = 0; b < FN; ++b) dmma(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+            for (int a = 0; a < 2; ++a)
+#pragma unroll
+                for (int b = 0; b < FN; ++b) dmma16(*reinterpret_cast<double(*)[4]>(acc[a][b]), af[a], bf[b]);
+        } else {
+#pragma unroll
+            for (int kk = 0; kk < kBK; kk += 4) {
+                double af[4], bf[FN];
+#pragma unroll
+                for (int t = 0; t < 4; ++t) af[t] = LA::at(As[st], wm + t * 8 + r, kk + c);
+#pragma unroll
+                for (int t = 0; t < FN; ++t) bf[t] = LB::at(Bs[st], wn + t * 8 + r, kk + c);
+#pragma unroll
+                for (int a = 0; a < 4; ++a)
+#pragma unroll
+                    for (int b = 0; b < FN; ++b) dmma(acc[a][b][0], acc[a][b][1], af[a], bf[b]);
+            }
         }
         __syncthreads();
     }
-    const int c2 = c * 2;
+    constexpr int NA = K16 ? 2 : 4, NH = K16 ? 4 : 2;
     if constexpr (CL) {
         // cluster split-K: stage this slice's tile, sum the S slices through distributed
         // shared memory, each CTA of the cluster finishing 64/S rows of the tile
@@ -169,11 +211,11 @@ __global__ void __launch_bounds__(kThr) gemm_pipe_kernel(GemmOp p, int tiles_m) 
         __syncthreads();
         double *stage = smem_all;
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int a = 0; a < NA; ++a)
 #pragma unroll
             for (int b = 0; b < FN; ++b)
 #pragma unroll
-                for (int h = 0; h < 2; ++h) stage[(wm + a * 8 + r) * BN + wn + b * 8 + c2 + h] = acc[a][b][h];
+                for (int h = 0; h < NH; ++h) stage[acc_row(a, h) * BN + acc_col(b, h)] = acc[a][b][h];
         cluster.sync();
         const int rank = (int)cluster.block_rank();
         const int r0 = rank * kBM / S, r1 = (rank + 1) * kBM / S;
@@ -193,12 +235,12 @@ __global__ void __launch_bounds__(kThr) gemm_pipe_kernel(GemmOp p, int tiles_m) 
     }
     const bool split = (S > 1);
 #pragma unroll
-    for (int a = 0; a < 4; ++a)
+    for (int a = 0; a < NA; ++a)
 #pragma unroll
         for (int b = 0; b < FN; ++b)
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const int i = i0 + wm + a * 8 + r, j = j0 + wn + b * 8 + c2 + h;
+            for (int h = 0; h < NH; ++h) {
+                const int i = i0 + acc_row(a, h), j = j0 + acc_col(b, h);
                 if (i >= p.M || j >= p.N) continue;
                 if (p.lower_out && j > i) continue;
                 if (split) {

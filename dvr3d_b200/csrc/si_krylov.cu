@@ -149,9 +149,15 @@ struct Timer {
 
 int si_krylov_first_size(int nwant, int block) {
     // about 5 Krylov vectors per wanted level, and at least 20 block steps (the polynomial
-    // degree, not only the dimension, sets the convergence of the last wanted levels)
+    // degree, not only the dimension, sets the convergence of the last wanted levels);
+    // DVR3D_SI_FIRST overrides the vectors per level (tuning)
+    double per = 5.2;
+    if (const char *e = std::getenv("DVR3D_SI_FIRST")) {
+        const double v = std::atof(e);
+        if (v >= 1.5 && v <= 10.0) per = v;
+    }
     const int b = block;
-    return (int)std::max(rup((long long)std::ceil(5.2 * nwant) + b, b), 20LL * b);
+    return (int)std::max(rup((long long)std::ceil(per * nwant) + b, b), 20LL * b);
 }
 
 bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, double emin_bound,

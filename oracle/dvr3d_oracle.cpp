@@ -16,6 +16,10 @@
 
 #include <algorithm>
 #include <chrono>
+#include <condition_variable>
+#include <functional>
+#include <mutex>
+#include <thread>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -92,7 +96,19 @@ struct Run {
     std::vector<double> pes;
     const double *vgrid = nullptr;
     size_t nvgrid = 0;
+    // unit boundary of a stepwise run (oracle_session_*): called before each unit of work of
+    // nfmain / jhmain; empty for a plain run
+    std::function<void()> gate;
+    // selection outcome, published when the selection unit ends (per block: kept 2D states
+    // and 2D dimension), for callers of a stepwise run
+    std::vector<int> sel_iv2, sel_n2d;
+    void tick() const {
+        if (gate) gate();
+    }
 };
+
+// Units of work of one k block for a stepwise run: the gates nfmain / jhmain pass.
+int work_units(const Run &R) { return R.idia <= -2 ? 2 * R.nalf + 2 : 4 * R.npntc + 2; }
 
 double pes_morse_sum(const double *p, double r1, double r2, double x) {
     double d1 = r1 - p[2], d2 = r2 - p[5];
@@ -832,6 +848,7 @@ void nfmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     double emaxau = R.emax2 / autocm;
     int npos = 1;
     for (int ig = 0; ig < nalf; ++ig) {
+        R.tick();
         blc2d1(R, ig, R.xalf[ig], ham2, nham2, term, term2, term3, xtscw);
         diag(ham2.data(), nham2, nham2, eig2.data());
         if (tr && tr->eig2all && (size_t)(ig + 1) * nham2 <= (size_t)tr->eig2all_cap)
@@ -859,6 +876,7 @@ void nfmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
             npos += nvec;
         }
     }
+    R.tick();
     if (!R.zcut) {  // choosr final selection (:3284-3311)
         int itotal = (int)eigtmp.size();
         double emax = (itotal <= R.max3d) ? eigtmp[itotal - 1] : eigtmp[R.max3d - 1];
@@ -900,6 +918,8 @@ void nfmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
         }
     }
     int nham3 = iv2a[nalf - 1] + iv2b[nalf - 1] - 1;  // :3092
+    R.sel_iv2 = iv2b;
+    R.sel_n2d = nv2;
     auto t1 = std::chrono::steady_clock::now();
     if (final_mode == 3) {
         if (tr) {
@@ -918,6 +938,7 @@ void nfmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     std::vector<double> hama(nham2);
     int ndim1g = 1;
     for (int ig = 0; ig < nalf; ++ig) {
+        R.tick();
         if (iv2b[ig] <= 0) continue;
         int ndim2g = 1;
         for (int igp = 0; igp <= ig; ++igp) {
@@ -974,6 +995,7 @@ void nfmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     // diag3d :2661-2764
     int meval = std::min(R.neval, nham3);
     std::vector<double> eval(nham3);
+    R.tick();
     if (final_mode != 2) diag(ham3.data(), nham3, nham3, eval.data(), final_mode);
     auto t3 = std::chrono::steady_clock::now();
     if (tr) {
@@ -1060,6 +1082,7 @@ void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     std::vector<double> ham1, eig1(npnta);
     double emax1au = R.emax1 / autocm;
     for (int ione = 0; ione < npntc; ++ione) {
+        R.tick();
         std::vector<double> e1;
         std::vector<std::vector<double>> cols;  // each selected vector over npnta
         for (int itwo = 0; itwo < npntb; ++itwo) {
@@ -1096,6 +1119,7 @@ void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     double emax2au = R.emax2 / autocm;
     size_t eoff = 0;
     for (int ione = 0; ione < npntc; ++ione) {
+        R.tick();
         int nham2 = 0;
         for (int itwo = 0; itwo < npntb; ++itwo) nham2 += iv1[(size_t)ione * npntb + itwo];
         ndim2d[ione] = nham2;
@@ -1156,6 +1180,7 @@ void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
             low3d = R.max3d;
         }
     }
+    R.tick();
     if (!zcut) {  // choose :2767-2867
         int nhamsm = 0;
         std::vector<int> ptr(npntc, 1);
@@ -1181,6 +1206,8 @@ void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
         }
     }
     int nham3 = low3d;
+    R.sel_iv2 = iv2;
+    R.sel_n2d = ndim2d;
     auto t1 = std::chrono::steady_clock::now();
     if (final_mode == 3) {
         if (tr) {
@@ -1201,6 +1228,7 @@ void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     int ncint = npnta * npntb;
     std::vector<std::vector<double>> cint(npntc);
     for (int ione = 0; ione < npntc; ++ione) {
+        R.tick();
         int nham2 = ndim2d[ione];
         if (nham2 == 0 || iv2[ione] == 0) continue;
         std::vector<double> &C = cint[ione];
@@ -1238,6 +1266,7 @@ void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     std::vector<double> ham3((size_t)nham3 * nham3, 0.0);
     int ivsm = 0;
     for (int ione = 0; ione < npntc; ++ione) {
+        R.tick();
         int iv = iv2[ione];
         if (ndim2d[ione] == 0) continue;
         int ivpsm = 0;
@@ -1284,6 +1313,7 @@ void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     }
     int meval = std::min(R.neval, nham3);
     std::vector<double> eval(nham3);
+    R.tick();
     if (final_mode != 2) diag(ham3.data(), nham3, nham3, eval.data(), final_mode);
     auto t3 = std::chrono::steady_clock::now();
     if (tr) {
@@ -1412,6 +1442,150 @@ int oracle_solve_block(const dvr3d_deck *deck, int kk, int pes_kind, const doubl
     } catch (std::exception &) {
         return DVR3D_ERR_NOMEM;
     }
+}
+
+// ------------------------------------------------------------------ stepwise runs
+// One k-block solve executed on a worker thread in units of work, so a caller can time one
+// complete solve as a sequence of bounded steps: each oracle_session_step call lets the
+// worker run the next `units` units (gates of nfmain / jhmain) and returns when they are
+// done. The worker is blocked between steps.
+struct OracleSession {
+    Run R;
+    int final_mode = 0;
+    int units = 0;
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv;
+    long long granted = 0, passed = 0;
+    bool blocked = false, finished = false, cancel = false;
+    int status = 0;
+    std::vector<double> eval;
+    std::vector<int> iv2;
+    oracle_trace tr{};
+    dvr3d_result res{};
+};
+
+struct Cancelled {};
+
+int oracle_session_begin(const dvr3d_deck *deck, int kk, int pes_kind, const double *pes, int npes,
+                         const double *vgrid, size_t nvgrid, int final_mode, void **out) {
+    if (!deck || !out) return DVR3D_ERR_ARG;
+    auto *S = new OracleSession();
+    try {
+        Run &R = S->R;
+        insize_setcon(R, *deck);
+        R.pes_kind = pes_kind;
+        if (pes_kind == DVR3D_PES_MORSE_SUM) {
+            if (!pes || npes < DVR3D_PES_MORSE_SUM_NPARAM) {
+                delete S;
+                return DVR3D_ERR_ARG;
+            }
+            R.pes.assign(pes, pes + DVR3D_PES_MORSE_SUM_NPARAM);
+        }
+        R.vgrid = vgrid;
+        R.nvgrid = nvgrid;
+        ccmain_setup(R, kk);
+    } catch (Fail &f) {
+        delete S;
+        return f.code;
+    }
+    S->final_mode = final_mode;
+    S->units = work_units(S->R);
+    S->eval.assign(std::max(S->R.neval, 1), 0.0);
+    S->iv2.assign(std::max(std::max(S->R.nalf, S->R.npntc), 1), 0);
+    S->res.eval = S->eval.data();
+    S->res.eval_cap = (int)S->eval.size();
+    S->tr.iv2 = S->iv2.data();
+    S->tr.iv2_cap = (int)S->iv2.size();
+    S->R.gate = [S]() {
+        std::unique_lock<std::mutex> lk(S->mu);
+        S->blocked = true;
+        S->cv.notify_all();
+        S->cv.wait(lk, [S] { return S->cancel || S->passed < S->granted; });
+        S->blocked = false;
+        if (S->cancel) throw Cancelled{};
+        ++S->passed;
+    };
+    S->worker = std::thread([S]() {
+        int st = DVR3D_OK;
+        try {
+            if (S->R.idia <= -2) nfmain(S->R, S->final_mode, &S->tr, &S->res);
+            else jhmain(S->R, S->final_mode, &S->tr, &S->res);
+        } catch (Fail &f) {
+            st = f.code;
+        } catch (Cancelled &) {
+            st = DVR3D_ERR_ARG;
+        } catch (std::exception &) {
+            st = DVR3D_ERR_NOMEM;
+        }
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->status = st;
+        S->finished = true;
+        S->cv.notify_all();
+    });
+    *out = S;
+    return DVR3D_OK;
+}
+
+int oracle_session_units(void *h) { return h ? static_cast<OracleSession *>(h)->units : DVR3D_ERR_ARG; }
+
+int oracle_session_counts(void *h, int *iv2, int *n2d, int cap) {
+    if (!h) return DVR3D_ERR_ARG;
+    auto *S = static_cast<OracleSession *>(h);
+    std::lock_guard<std::mutex> lk(S->mu);
+    if (!(S->blocked || S->finished)) return DVR3D_ERR_ARG;  // only between steps
+    const int nb = (int)S->R.sel_iv2.size();
+    if (nb == 0) return 0;  // the selection has not run yet
+    if (cap < nb) return DVR3D_ERR_BUFFER;
+    for (int b = 0; b < nb; ++b) {
+        if (iv2) iv2[b] = S->R.sel_iv2[b];
+        if (n2d) n2d[b] = S->R.sel_n2d[b];
+    }
+    return nb;
+}
+
+int oracle_session_step(void *h, int units) {
+    if (!h || units < 0) return DVR3D_ERR_ARG;
+    auto *S = static_cast<OracleSession *>(h);
+    std::unique_lock<std::mutex> lk(S->mu);
+    S->granted += units;
+    S->cv.notify_all();
+    // done when the worker waits at the gate after the granted units, or has finished
+    S->cv.wait(lk, [S] { return S->finished || (S->blocked && S->passed == S->granted); });
+    if (S->finished && S->status != DVR3D_OK) return S->status;
+    return S->finished ? 0 : (int)(S->units - S->passed);
+}
+
+int oracle_session_end(void *h, oracle_trace *trace, dvr3d_result *res) {
+    if (!h) return DVR3D_ERR_ARG;
+    auto *S = static_cast<OracleSession *>(h);
+    {
+        std::lock_guard<std::mutex> lk(S->mu);
+        if (!S->finished) S->cancel = true;
+        S->cv.notify_all();
+    }
+    S->worker.join();
+    const int st = S->status;
+    if (st == DVR3D_OK) {
+        if (res) {
+            res->nham3 = S->res.nham3;
+            res->meval = S->res.meval;
+            res->nblocks = S->res.nblocks;
+            res->kz = S->res.kz;
+            res->ipar = S->res.ipar;
+            if (res->eval && res->eval_cap >= S->res.meval)
+                std::memcpy(res->eval, S->eval.data(), sizeof(double) * S->res.meval);
+        }
+        if (trace) {
+            trace->nblocks = S->tr.nblocks;
+            trace->nham3 = S->tr.nham3;
+            std::memcpy(trace->stage_s, S->tr.stage_s, sizeof(trace->stage_s));
+            if (trace->iv2 && trace->iv2_cap >= S->tr.nblocks)
+                std::memcpy(trace->iv2, S->iv2.data(), sizeof(int) * S->tr.nblocks);
+        }
+    }
+    delete S;
+    return st;
 }
 
 double oracle_time_dsyev(int n, int reps, int mode) {

@@ -62,6 +62,21 @@ int oracle_solve_block(const dvr3d_deck *deck, int kk, int pes_kind, const doubl
                        int npes, const double *vgrid, size_t nvgrid, int final_mode,
                        oracle_trace *trace, dvr3d_result *res);
 
+/* Stepwise run of oracle_solve_block (same arguments and results), for timing one complete
+ * solve as a sequence of bounded steps: _begin sets the block up and starts a worker thread
+ * that waits before each unit of work (per block of the 1D and 2D stages, the selection,
+ * per block row of the assembly, the final diagonalisation); _step lets it run `units`
+ * more units and returns the units left (0 when the solve is complete, < 0 on error);
+ * _end cancels an unfinished run or collects the results, and frees the session. */
+int oracle_session_begin(const dvr3d_deck *deck, int kk, int pes_kind, const double *pes, int npes,
+                         const double *vgrid, size_t nvgrid, int final_mode, void **out);
+int oracle_session_units(void *session);
+int oracle_session_step(void *session, int units);
+/* Between steps, after the selection unit: per block kept 2D states (iv2) and 2D dimension
+ * (n2d); returns the number of blocks (0 before the selection has run). */
+int oracle_session_counts(void *session, int *iv2, int *n2d, int cap);
+int oracle_session_end(void *session, oracle_trace *trace, dvr3d_result *res);
+
 /* Derived sizes of insize (:171-638) for one k block (kk = loop index of ccmain :857). */
 int oracle_sizes(const dvr3d_deck *deck, int kk, int *out16);
 

@@ -117,6 +117,12 @@ def load(build: bool = True) -> C.CDLL:
     lib.oracle_sizes.argtypes = [P(Deck), C.c_int, P(C.c_int)]
     lib.oracle_pes_morse_sum.argtypes = [P(C.c_double), C.c_double, C.c_double, C.c_double]
     lib.oracle_pes_morse_sum.restype = C.c_double
+    lib.oracle_session_begin.argtypes = [P(Deck), C.c_int, C.c_int, P(C.c_double), C.c_int, P(C.c_double),
+                                         C.c_size_t, C.c_int, P(C.c_void_p)]
+    lib.oracle_session_units.argtypes = [C.c_void_p]
+    lib.oracle_session_step.argtypes = [C.c_void_p, C.c_int]
+    lib.oracle_session_counts.argtypes = [C.c_void_p, P(C.c_int), P(C.c_int), C.c_int]
+    lib.oracle_session_end.argtypes = [C.c_void_p, P(Trace), P(Result)]
     lib.oracle_time_dsyev.argtypes = [C.c_int, C.c_int, C.c_int]
     lib.oracle_time_dsyev.restype = C.c_double
     rc = lib.oracle_load_lapack(_lapack_path().encode(), b"scipy_")
@@ -250,3 +256,69 @@ def pes_morse_sum(p, r1: float, r2: float, x: float) -> float:
 
 def time_dsyev(n: int, reps: int = 1, mode: int = 0) -> float:
     return load().oracle_time_dsyev(n, reps, mode)
+
+
+class Session:
+    """One k-block solve of the oracle run in steps (oracle_session_*): ``units`` units of
+    work in total (per block of the 1D and 2D stages, the selection, per block row of the
+    assembly, the final diagonalisation); ``step(n)`` runs the next n of them and returns
+    the units left; ``finish()`` returns the result of a complete run (or cancels an
+    unfinished one and returns None)."""
+
+    def __init__(self, deck, kk: int = 0, pes=None, vgrid=None, final_mode: int = 0):
+        lib = load()
+        self._deck = as_deck(deck)
+        self._keep = []
+        kind, pp, npes, vg, nvg = 0, None, 0, None, 0
+        if pes is not None:
+            p = np.ascontiguousarray(np.asarray(pes, dtype=np.float64))
+            kind, pp, npes = 1, p.ctypes.data_as(C.POINTER(C.c_double)), p.size
+            self._keep.append(p)
+        if vgrid is not None:
+            g = np.ascontiguousarray(np.asarray(vgrid, dtype=np.float64).ravel())
+            kind, vg, nvg = 2, g.ctypes.data_as(C.POINTER(C.c_double)), g.size
+            self._keep.append(g)
+        self._h = C.c_void_p()
+        rc = lib.oracle_session_begin(C.byref(self._deck), kk, kind, pp, npes, vg, nvg, final_mode,
+                                      C.byref(self._h))
+        if rc != 0:
+            raise RuntimeError(f"oracle_session_begin failed: {rc}")
+        self.units = lib.oracle_session_units(self._h)
+        self._s = sizes(self._deck, kk)
+
+    def step(self, n: int) -> int:
+        rc = load().oracle_session_step(self._h, int(n))
+        if rc < 0:
+            raise RuntimeError(f"oracle session step failed: {rc}")
+        return rc
+
+    def counts(self):
+        """(iv2, n2d) per block once the selection unit has run, else None."""
+        cap = max(self._s["nalf"], self._s["npntc"], 1) + 8
+        iv2 = np.zeros(cap, dtype=np.int32)
+        n2d = np.zeros(cap, dtype=np.int32)
+        ip = C.POINTER(C.c_int)
+        nb = load().oracle_session_counts(self._h, iv2.ctypes.data_as(ip), n2d.ctypes.data_as(ip), cap)
+        if nb <= 0:
+            return None
+        return iv2[:nb].copy(), n2d[:nb].copy()
+
+    def finish(self):
+        lib = load()
+        neval = max(self._s["neval"], 1)
+        nblk = max(self._s["nalf"], self._s["npntc"], 1)
+        ev = np.zeros(neval + 8)
+        iv2 = np.zeros(nblk + 8, dtype=np.int32)
+        r = Result()
+        r.eval = ev.ctypes.data_as(C.POINTER(C.c_double))
+        r.eval_cap = ev.size
+        t = Trace()
+        t.iv2 = iv2.ctypes.data_as(C.POINTER(C.c_int))
+        t.iv2_cap = iv2.size
+        rc = lib.oracle_session_end(self._h, C.byref(t), C.byref(r))
+        self._h = None
+        if rc != 0:
+            return None
+        return OracleResult(status=rc, eval=ev[:r.meval].copy(), nham3=r.nham3, iv2=iv2[:t.nblocks].copy(), iv1=None,
+                            n2d=np.zeros(0, dtype=np.int32), eigs2d=None, h3=None, stage_s=np.array(t.stage_s[:]),
+                            kz=r.kz, ipar=r.ipar)
