@@ -377,9 +377,10 @@ def main() -> int:
         roof = {"bound": "tensor", "kernel": kern, "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
                 "frac": (achieved / fp64_peak) if achieved else None, "traffic": None,
                 "peak_source": "measured in this run: cuBLAS DGEMM (torch.matmul float64) 8192^3, best of 5",
-                "alg_flops_per_step": dom_flops / args.steps,
-                "note": "achieved = algorithmic flops of the Cholesky-inverse (2/3 N^3) and of the Krylov steps "
-                        "(2 N^2 b + 8 N m b + 8 N b^2 per block) / their CUDA-event time",
+                "alg_flops_per_step": dom_flops / args.steps, "launches": dom_launch / args.steps,
+                "note": "achieved = algorithmic flops of the DMMA GEMM launches of a solve (Cholesky-inverse, "
+                        "Krylov steps, Ritz vectors, H3 X; per launch from M, N, K and its triangular structure) "
+                        "/ the sum of their durations, each launch timed by a CUDA event pair on the solve's stream",
                 "share_of_step": dom_ms / ms if ms > 0 else None}
     else:
         achieved = dom_bytes / (dom_ms / 1000.0) / 1e9 if dom_ms > 0 else None

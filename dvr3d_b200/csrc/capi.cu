@@ -147,6 +147,7 @@ void dvr3d_b200_destroy(dvr3d_ctx *ctx) {
     for (auto &e : ctx->ev)
         if (e) cudaEventDestroy(e);
     for (auto &e : ctx->panel_ev) cudaEventDestroy(e);
+    for (auto &e : ctx->gemm_ev) cudaEventDestroy(e);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
 }

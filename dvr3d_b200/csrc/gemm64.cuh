@@ -77,4 +77,23 @@ struct GemmOp {
 size_t gemm_splitk_work(int M, int N, int splitk);
 cudaError_t launch_gemm(const GemmOp &p, cudaStream_t st);
 
+// Algorithmic flops of one launch_gemm: 2 per multiply-add of a nonzero term (triangular
+// operands and a lower-triangle output count only their nonzero / computed part).
+double gemm_alg_flops(const GemmOp &p);
+
+// Per-launch timing of launch_gemm, the dominant kernel family of the iterative solves: while
+// a log is installed on the calling host thread, each launch_gemm records a CUDA event before
+// and after its kernels (events from `ev`, two per launch) and adds its algorithmic flops.
+struct GemmLaunchLog {
+    cudaEvent_t *ev = nullptr;
+    int nev = 0;
+    int used = 0;        // events recorded
+    int launches = 0;    // launches timed
+    int untimed = 0;     // launches after the event pool ran out
+    double flops = 0.0;  // algorithmic flops of the timed launches
+};
+void set_gemm_launch_log(GemmLaunchLog *log);  // nullptr: stop logging
+// Sum of the timed launches' durations (ms); synchronises on the last event.
+double gemm_launch_log_ms(const GemmLaunchLog &log);
+
 }  // namespace dvr3d

@@ -322,7 +322,60 @@ cudaError_t launch_bn(const GemmOp &p, int S, cudaStream_t st) {
 
 size_t gemm_splitk_work(int M, int N, int S) { return S > kMaxClusterSplit ? (size_t)S * M * N : 0; }
 
-cudaError_t launch_gemm(const GemmOp &p0, cudaStream_t st) {
+double gemm_alg_flops(const GemmOp &p) {
+    const double M = p.M, N = p.N, K = p.K;
+    if (p.M <= 0 || p.N <= 0 || p.K <= 0) return 0.0;
+    // sum over i < n of min(i + 1, k), and of max(k - i, 0)
+    auto head = [](double n, double k) { return n <= k ? n * (n + 1.0) * 0.5 : k * (k + 1.0) * 0.5 + (n - k) * k; };
+    auto tail = [](double n, double k) {
+        const double t = n < k ? n : k;
+        return t * k - t * (t - 1.0) * 0.5;
+    };
+    if (p.lower_out) return 2.0 * K * M * (M + 1.0) * 0.5;
+    if (p.tri == 1) return 2.0 * N * head(M, K);
+    if (p.tri == 2) return 2.0 * N * tail(M, K);
+    if (p.tri_b == 1) return 2.0 * M * tail(N, K);
+    if (p.tri_b == 2) return 2.0 * M * head(N, K);
+    return 2.0 * M * N * K;
+}
+
+namespace {
+thread_local GemmLaunchLog *t_gemm_log = nullptr;
+cudaError_t launch_gemm_kernels(const GemmOp &p0, cudaStream_t st);
+}  // namespace
+
+void set_gemm_launch_log(GemmLaunchLog *log) { t_gemm_log = log; }
+
+double gemm_launch_log_ms(const GemmLaunchLog &log) {
+    if (log.used < 2) return 0.0;
+    cudaEventSynchronize(log.ev[log.used - 1]);
+    double ms = 0.0;
+    for (int q = 0; q + 1 < log.used; q += 2) {
+        float m = 0.f;
+        if (cudaEventElapsedTime(&m, log.ev[q], log.ev[q + 1]) == cudaSuccess) ms += m;
+    }
+    return ms;
+}
+
+cudaError_t launch_gemm(const GemmOp &p, cudaStream_t st) {
+    GemmLaunchLog *lg = t_gemm_log;
+    if (!lg || p.M <= 0 || p.N <= 0) return launch_gemm_kernels(p, st);
+    if (lg->used + 2 > lg->nev) {
+        ++lg->untimed;
+        return launch_gemm_kernels(p, st);
+    }
+    cudaEventRecord(lg->ev[lg->used], st);
+    const cudaError_t e = launch_gemm_kernels(p, st);
+    cudaEventRecord(lg->ev[lg->used + 1], st);
+    lg->used += 2;
+    ++lg->launches;
+    lg->flops += gemm_alg_flops(p);
+    return e;
+}
+
+namespace {
+
+cudaError_t launch_gemm_kernels(const GemmOp &p0, cudaStream_t st) {
     GemmOp p = p0;
     if (p.M <= 0 || p.N <= 0) return cudaSuccess;
     if (p.lower_out && p.M != p.N) return cudaErrorInvalidValue;
@@ -343,5 +396,7 @@ cudaError_t launch_gemm(const GemmOp &p0, cudaStream_t st) {
     splitk_reduce_kernel<<<dim3((unsigned)((p.M + 31) / 32), (unsigned)p.N), 256, 0, st>>>(p, S);
     return cudaGetLastError();
 }
+
+}  // namespace
 
 }  // namespace dvr3d

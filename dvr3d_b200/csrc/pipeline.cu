@@ -904,11 +904,12 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
             res.iterations = ks.blocks;
             double ms1, ms2, ms3;
             finish_times(ms1, ms2, ms3);
-            // dominant kernel: the DMMA GEMM of the factorisation and Krylov steps
-            res.dom_ms = ks.factor_ms + ks.krylov_ms;
+            // dominant kernel family: the DMMA GEMM (Cholesky-inverse, Krylov steps, Ritz
+            // vectors, H3 X): its launches' own event-timed durations and algorithmic flops
+            res.dom_ms = ks.gemm_ms;
             res.dom_bytes = 0.0;
-            res.dom_flops = ks.flops;
-            res.dom_launches = 0;
+            res.dom_flops = ks.gemm_flops;
+            res.dom_launches = ks.gemm_launches;
             std::snprintf(res.dom_kernel, sizeof(res.dom_kernel), "gemm_pipe_kernel");
             res.launches = (int)(g_kernel_launches - launches0);
             res.h2d_bytes = t_h2d;

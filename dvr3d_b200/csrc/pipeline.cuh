@@ -55,6 +55,7 @@ struct dvr3d_ctx {
     int dense_grid = 0;
     std::vector<cudaEvent_t> panel_ev;  // timing pool for the reduction panels
     unsigned long long wait_limit = 0;  // polls of each bounded device wait (0: kernel defaults)
+    std::vector<cudaEvent_t> gemm_ev;   // timing pool of the GEMM launches of an iterative solve
     bool lp_trained = false;            // arena "lp_w" holds a trained preconditioner network
     struct LpSet {                      // training pairs of the last training solve
         bool valid = false;
@@ -148,6 +149,9 @@ struct KrylovStats {
     double factor_ms = 0.0, krylov_ms = 0.0, rr_ms = 0.0;
     double flops = 0.0;    // algorithmic flops of the factorisation, Krylov steps and checks
     double max_resid = 0.0;
+    // the GEMM launches of the solve, each timed with CUDA events (gemm64.cuh GemmLaunchLog)
+    double gemm_ms = 0.0, gemm_flops = 0.0;
+    int gemm_launches = 0, gemm_untimed = 0;
 };
 int si_krylov_first_size(int nwant, int block);
 bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, double emin_bound,

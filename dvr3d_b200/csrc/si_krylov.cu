@@ -191,6 +191,18 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
     const bool trace = trace_env && trace_env[0] == '1';
     ks = KrylovStats{};
     ks.block = b;
+    // every GEMM launch of this solve timed by an event pair (4096 launches at most)
+    if (ctx->gemm_ev.empty()) {
+        ctx->gemm_ev.resize(8192);
+        for (auto &e : ctx->gemm_ev) CK(cudaEventCreate(&e));
+    }
+    GemmLaunchLog glog;
+    glog.ev = ctx->gemm_ev.data();
+    glog.nev = (int)ctx->gemm_ev.size();
+    struct LogScope {
+        explicit LogScope(GemmLaunchLog *l) { set_gemm_launch_log(l); }
+        ~LogScope() { set_gemm_launch_log(nullptr); }
+    } log_scope(&glog);
     // ---- (1)+(2) shift, factor, invert
     tf.start(st);
     double sigma = emin_bound - std::max(1.0e-6, 1.0e-3 * std::fabs(emin_bound));
@@ -429,6 +441,10 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
     ks.factor_ms = tf.ms();
     ks.krylov_ms = tk_ms;
     ks.rr_ms = tr_ms;
+    ks.gemm_ms = gemm_launch_log_ms(glog);
+    ks.gemm_flops = glog.flops;
+    ks.gemm_launches = glog.launches;
+    ks.gemm_untimed = glog.untimed;
     ks.blocks = s;
     ks.flops = flops + 2.0 / 3.0 * (double)N * N * N;
     if (!done) return false;
