@@ -282,15 +282,22 @@ class Context:
                                    max_resid=r.max_resid))
         return out
 
-    def run_deck(self, text: str, precision: int = DVR3D_PREC_FP64) -> tuple[str, str]:
-        """Run a job like program DVR3DRJZ; returns (printed output, fort.14 levels text)."""
+    def run_deck(self, text: str, precision: int = DVR3D_PREC_FP64, wave_path: str | None = None) -> tuple[str, str]:
+        """Run a job like program DVR3DRJZ; returns (printed output, fort.14 levels text).
+        With wave_path (and ZTRAN in the deck) the wavefunction file is written there."""
         o = Options(precision=precision)
         need = C.c_size_t(0)
         needl = C.c_size_t(0)
+        # the first call sizes the text buffers (and writes no wavefunction file)
         self._check(self._lib.dvr3d_b200_run_deck(self._h, text.encode(), C.byref(o), None, 0, C.byref(need),
                                                   None, 0, C.byref(needl)))
         out = C.create_string_buffer(need.value + 1)
         lev = C.create_string_buffer(needl.value + 1)
-        self._check(self._lib.dvr3d_b200_run_deck(self._h, text.encode(), C.byref(o), out, len(out), C.byref(need),
-                                                  lev, len(lev), C.byref(needl)))
+        if wave_path is None:
+            self._check(self._lib.dvr3d_b200_run_deck(self._h, text.encode(), C.byref(o), out, len(out),
+                                                      C.byref(need), lev, len(lev), C.byref(needl)))
+        else:
+            self._check(self._lib.dvr3d_b200_run_deck_wave(self._h, text.encode(), C.byref(o), out, len(out),
+                                                           C.byref(need), lev, len(lev), C.byref(needl),
+                                                           str(wave_path).encode()))
         return out.value.decode(), lev.value.decode()

@@ -134,6 +134,9 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "dvr3d_b200_run_deck": (C.c_int, [vp, C.c_char_p, P(Options), C.c_char_p, C.c_size_t,
                                           P(C.c_size_t), C.c_char_p, C.c_size_t,
                                           P(C.c_size_t)]),
+        "dvr3d_b200_run_deck_wave": (C.c_int, [vp, C.c_char_p, P(Options), C.c_char_p, C.c_size_t,
+                                               P(C.c_size_t), C.c_char_p, C.c_size_t, P(C.c_size_t),
+                                               C.c_char_p]),
         "dvr3d_b200_diag_batched": (C.c_int, [vp, C.c_int, P(C.c_int), P(C.c_longlong),
                                               P(C.c_longlong), vp, vp, C.c_int]),
         "dvr3d_b200_diag_batched_noalloc": (C.c_int, [vp, C.c_int, P(C.c_int), P(C.c_longlong),

@@ -318,8 +318,134 @@ int dvr3d_b200_set_wait_limit(dvr3d_ctx *ctx, long long polls) {
     return DVR3D_OK;
 }
 
-int dvr3d_b200_run_deck(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_options *opt, char *out, size_t outcap,
-                        size_t *outlen, char *lev, size_t levcap, size_t *levlen) {
+namespace {
+
+// Sequential unformatted Fortran records: each record's bytes framed by its length as a
+// 4-byte little-endian count before and after (the sequential unformatted layout of gfortran
+// and of ifort's default record type). Logicals are 4-byte integers, .TRUE. = -1 (ifort's
+// default representation, read as true by ifort and gfortran alike).
+struct FortranRecords {
+    FILE *f = nullptr;
+    std::vector<unsigned char> rec;
+    void i4(int v) { put(&v, 4); }
+    void l4(bool v) { i4(v ? -1 : 0); }
+    void r8(double v) { put(&v, 8); }
+    void r8s(const double *v, size_t n) { put(v, 8 * n); }
+    void put(const void *p, size_t n) {
+        const unsigned char *c = static_cast<const unsigned char *>(p);
+        rec.insert(rec.end(), c, c + n);
+    }
+    void end() {
+        if (rec.size() > 0x7fffffffu) throw HostError{DVR3D_ERR_UNSUPPORTED, "wavefunction record above 2 GiB"};
+        const unsigned int n = (unsigned int)rec.size();
+        if (std::fwrite(&n, 4, 1, f) != 1 || (n && std::fwrite(rec.data(), 1, n, f) != n) ||
+            std::fwrite(&n, 4, 1, f) != 1)
+            throw HostError{DVR3D_ERR_ARG, "writing the wavefunction file failed"};
+        rec.clear();
+    }
+};
+
+struct FileCloser {
+    FILE *f;
+    ~FileCloser() {
+        if (f) std::fclose(f);
+    }
+};
+
+// Records of the wavefunction file that precede the k loop: setcon's header (:1176-1184)
+// and ccmain's r**(-2) term or basis sizes plus the radial grids (:820-845).
+void write_wave_header(FortranRecords &wr, const dvr3d_deck &d, int kd, int ku) {
+    dvr3d::BlockPlan p0;
+    dvr3d::plan_block(d, kd, p0);
+    const bool radau = p0.radau;
+    int nlim = 0;
+    if (p0.zrot) nlim = p0.zembed ? p0.npnt2 : p0.npnt1;  // zquad2 = T on this path
+    wr.i4(d.idia);
+    wr.i4(p0.ipar);
+    wr.i4(p0.idvr);
+    wr.i4(p0.npnt1);
+    wr.i4(radau ? p0.npnt1 : p0.npnt2);
+    wr.i4(p0.jrot);
+    wr.i4(p0.kmin);
+    wr.i4(d.neval);
+    wr.i4(nlim);
+    wr.end();
+    wr.l4(p0.zembed);
+    wr.l4(true);  // zmors1
+    wr.l4(true);  // zmors2 (Radau: zmors1 again)
+    wr.r8s(d.xmass, 3);
+    wr.r8(p0.g1);
+    wr.r8(p0.g2);
+    wr.l4(!p0.zrot);  // zncor
+    wr.l4(true);      // zquad2
+    wr.end();
+    const double rad[6] = {d.re1, d.diss1, d.we1, radau ? d.re1 : d.re2, radau ? d.diss1 : d.diss2,
+                           radau ? d.we1 : d.we2};
+    wr.r8s(rad, 6);
+    wr.end();
+    if (ku > kd) {
+        // (symmetric Radau: one radial grid, r2 = r1)
+        if (p0.zembed && !radau)
+            for (int i = 0; i < p0.npnt2; ++i) wr.r8(0.5 / (p0.r2[i] * p0.r2[i] * p0.urr2));
+        else
+            for (int i = 0; i < p0.npnt1; ++i) wr.r8(0.5 / (p0.r1[i] * p0.r1[i] * p0.urr1));
+    } else {
+        const int jdia = std::max(1, d.idia);
+        int jstart = p0.kmin;
+        if (jstart % jdia != p0.ipar) ++jstart;
+        const int nang = (p0.maxleg - jstart) / jdia + 1;
+        const int mbass = radau ? p0.idvr * p0.max2d : p0.idvr * p0.npnt1 * p0.npnt2;
+        wr.i4(mbass);
+        wr.i4(jstart);
+        wr.i4(nang);
+        wr.i4(mbass);
+    }
+    wr.end();
+    wr.r8s(p0.r1.data(), p0.npnt1);
+    wr.end();
+    if (!radau) {
+        wr.r8s(p0.r2.data(), p0.npnt2);
+        wr.end();
+    }
+}
+
+// Records of one k block: angular grid and polynomials (:972-976), for Radau testiv's
+// selection (:3446-3448), then the levels and one amplitude record per level (trans
+// :3733-3841, transr :3622-3641).
+void write_wave_block(FortranRecords &wr, const dvr3d::BlockPlan &p, const dvr3d_result &r, const int *iv2,
+                      const double *ev, const dvr3d::WaveOut &wave) {
+    wr.r8s(p.xalf.data(), p.idvr);
+    wr.end();
+    wr.i4(p.kz);
+    wr.i4(p.maxleg);
+    wr.i4(p.nidvr);
+    wr.i4(p.lincr);
+    wr.end();
+    wr.r8s(p.pleg_walf.data(), p.pleg_walf.size());
+    wr.end();
+    if (p.radau) {
+        int iang = 0;
+        for (int b = 0; b < r.nblocks; ++b) iang += (iv2[b] > 0);
+        wr.i4(iang);
+        wr.i4(iang * p.max2d);
+        wr.end();
+        for (int b = 0; b < r.nblocks; ++b) wr.i4(iv2[b]);
+        wr.end();
+    }
+    wr.i4(r.meval);
+    wr.end();
+    wr.r8s(ev, r.meval);
+    wr.end();
+    for (int l = 0; l < wave.nlev; ++l) {
+        wr.r8s(wave.psi.data() + (size_t)l * wave.len, (size_t)wave.len);
+        wr.end();
+    }
+}
+
+}  // namespace
+
+static int run_deck_impl(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_options *opt, char *out, size_t outcap,
+                         size_t *outlen, char *lev, size_t levcap, size_t *levlen, const char *wave_path) {
     if (!ctx || !deck_text) return DVR3D_ERR_ARG;
     dvr3d_options o{};
     if (opt) o = *opt;
@@ -331,6 +457,16 @@ int dvr3d_b200_run_deck(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_optio
         dvr3d::k_range(d, kd, ku);
         const double autocm = 2.19474624e+05;
         std::string s, lv;
+        // the wavefunction file (unit IWAVE): written when the deck sets ZTRAN and a path is given
+        const bool ztran = d.ztran && wave_path && wave_path[0];
+        FortranRecords wr;
+        FileCloser closer{nullptr};
+        if (ztran) {
+            closer.f = std::fopen(wave_path, "wb");
+            if (!closer.f) throw HostError{DVR3D_ERR_ARG, std::string("cannot open ") + wave_path};
+            wr.f = closer.f;
+            write_wave_header(wr, d, kd, ku);
+        }
         appendf(s, "     Program DVR3DRJZ (B200 hot path)\n\n     Title: %s\n", d.title);
         for (int kk = kd; kk <= ku; ++kk) {
             dvr3d::BlockPlan p;
@@ -342,7 +478,9 @@ int dvr3d_b200_run_deck(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_optio
             r.eval_cap = (int)ev.size();
             r.iv2 = iv2.data();
             r.iv2_cap = (int)iv2.size();
-            dvr3d::solve_block(ctx, d, kk, o, r);
+            dvr3d::WaveOut wave;
+            dvr3d::solve_block(ctx, d, kk, o, r, ztran ? &wave : nullptr);
+            if (ztran) write_wave_block(wr, p, r, iv2.data(), ev.data(), wave);
             if (d.jrot != 0 && p.zrot) appendf(s, "\n     Solutions with J =%3d k =%3d\n", p.jrot, p.kz);
             if (p.radau && d.jrot != 0 && p.zrot)
                 appendf(s, p.ipar == 0 ? "\n     even parity solutions\n" : "\n     odd parity solutions\n");
@@ -396,6 +534,18 @@ int dvr3d_b200_run_deck(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_optio
         copy_out(lv, lev, levcap, levlen);
         return DVR3D_OK;
     });
+}
+
+int dvr3d_b200_run_deck(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_options *opt, char *out, size_t outcap,
+                        size_t *outlen, char *lev, size_t levcap, size_t *levlen) {
+    return run_deck_impl(ctx, deck_text, opt, out, outcap, outlen, lev, levcap, levlen, nullptr);
+}
+
+int dvr3d_b200_run_deck_wave(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_options *opt, char *out,
+                             size_t outcap, size_t *outlen, char *lev, size_t levcap, size_t *levlen,
+                             const char *wave_path) {
+    if (!wave_path) return DVR3D_ERR_ARG;
+    return run_deck_impl(ctx, deck_text, opt, out, outcap, outlen, lev, levcap, levlen, wave_path);
 }
 
 int dvr3d_b200_lp_get_weights(dvr3d_ctx *ctx, double *w, int n) {

@@ -710,6 +710,10 @@ void plan_block(const dvr3d_deck &d, int kk, BlockPlan &p) {
     }
     for (int i = 0; i < nidvr; ++i)
         for (int jj = 0; jj < nl; ++jj) pl[(size_t)i * std::max(nl, 2) + jj] *= pnorm[jj];
+    p.pleg_walf.assign((size_t)(maxleg + 1) * nidvr, 0.0);
+    for (int i = 0; i < nidvr; ++i)
+        for (int jj = 0; jj <= maxleg && jj < nl; ++jj)
+            p.pleg_walf[(size_t)i * (maxleg + 1) + jj] = pl[(size_t)i * std::max(nl, 2) + jj] * p.walf[i];
     // angular kinetic matrix L(k,k') (lmatrx :1846-1911, in-plane)
     const int jdia = std::max(1, idia);
     const int ipar0 = (idia == 2 && ipar == 1) ? 1 : 0;

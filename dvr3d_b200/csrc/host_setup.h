@@ -44,6 +44,9 @@ struct BlockPlan {
     // kinetic matrices, column-major
     std::vector<double> xk1, xk2;      // npnt1^2, npnt2^2
     std::vector<double> xlmatr;        // idvr^2
+    // pleg(j, i) * walf(i), j = 0..maxleg, i < nidvr, column-major ((maxleg+1) x nidvr): the
+    // angular record of the wavefunction file (:976); orders asleg does not form are zero
+    std::vector<double> pleg_walf;
     // J > 0 terms
     double term = 0;                   // jhmain :1970
     double nf_term = 0, nf_term2 = 0, nf_term3 = 0;  // nfmain :3055-3064

@@ -229,6 +229,7 @@ void radau_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
         sw[q] = std::sqrt(0.5 / (ra * ra * p.ur1) + 0.5 / (rbv * rbv * p.ur1));
     }
     launch_scale_rows(out.Vt, (int)out.ldv, N, upload(ctx, "sw", sw), st);
+    out.sw.assign(sw.begin(), sw.begin() + n);
     out.g = upload(ctx, "gcol", gcol);
     out.e2 = ctx->arena.get_t<double>("e2", N);
     launch_gather(w, upload(ctx, "emap", emap), out.e2, N, st);
@@ -488,6 +489,7 @@ void jacobi_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
     ct.gstart = upload(ctx, "gstart", gstart);
     ct.col0 = upload(ctx, "col0", col0);
     ct.sw = upload(ctx, "sw", sw);
+    out.sw = sw;
     ct.ldv = out.ldv;
     launch_jacobi_ctrans(j2, ct, ncp, s2max, V2, out.Vt, st);
     out.g = upload(ctx, "gcol", gcol);
@@ -751,7 +753,7 @@ bool band_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int b, int nev
 
 // ---------------------------------------------------------------- one k block
 void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_options &opt,
-                 dvr3d_result &res) {
+                 dvr3d_result &res, WaveOut *wave) {
     auto th0 = std::chrono::steady_clock::now();
     if (ctx->pes.kind != DVR3D_PES_MORSE_SUM && ctx->pes.kind != DVR3D_PES_GRID)
         throw HostError{DVR3D_ERR_ARG, "no potential selected (dvr3d_b200_set_pes)"};
@@ -848,7 +850,7 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
     if (mixed && meval <= kDavidsonMaxLevels) {
         // ---- few levels: block-Davidson with the channel-block preconditioner
         double *wv = ctx->arena.get_t<double>("dt_w", meval);
-        double *Z = res.evec ? ctx->arena.get_t<double>("dv_z", (size_t)N * meval) : nullptr;
+        double *Z = (res.evec || wave) ? ctx->arena.get_t<double>("dv_z", (size_t)N * meval) : nullptr;
         double *lpw = ctx->arena.get_t<double>("lp_w", kLpParams);
         const int mode = opt.learned_precond == 2 ? 2 : (opt.learned_precond == 1 ? 1 : 0);
         std::vector<double> rn;
@@ -866,6 +868,7 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
         if (ok) {
             CK(cudaEventRecord(ctx->ev[3], st));
             put_levels(wv, Z);
+            if (wave) compute_wavefunctions(ctx, p, C, Z, N, meval, *wave);
             if (res.resid)
                 for (int j = 0; j < std::min(meval, res.resid_cap); ++j) res.resid[j] = rn[j];
             res.max_resid = ds.max_resid;
@@ -889,7 +892,7 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
         std::vector<double> e2h = download(ctx, C.e2, N);
         const double emin = *std::min_element(e2h.begin(), e2h.end());
         double *wv = ctx->arena.get_t<double>("dt_w", meval);
-        double *Z = res.evec ? ctx->arena.get_t<double>("dv_z", (size_t)N * meval) : nullptr;
+        double *Z = (res.evec || wave) ? ctx->arena.get_t<double>("dv_z", (size_t)N * meval) : nullptr;
         std::vector<double> rn;
         KrylovStats ks;
         const bool ok = si_krylov_solve(ctx, H3, ldh, N, emin, opt, meval, wv, rn, Z, ks);
@@ -898,6 +901,7 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
             res.matvecs = ks.m;
             CK(cudaEventRecord(ctx->ev[3], st));
             put_levels(wv, Z);
+            if (wave) compute_wavefunctions(ctx, p, C, Z, N, meval, *wave);
             if (res.resid)
                 for (int j = 0; j < std::min(meval, res.resid_cap); ++j) res.resid[j] = rn[j];
             res.max_resid = ks.max_resid;
@@ -924,7 +928,7 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
     CK(cudaMemcpy2DAsync(Hw, ldw * sizeof(double), H3, (size_t)ldh * sizeof(double), (size_t)N * sizeof(double), N,
                          cudaMemcpyDeviceToDevice, st));
     double *wv = ctx->arena.get_t<double>("dt_w", meval);
-    const bool vecs = opt.want_vectors || res.evec || res.resid;
+    const bool vecs = opt.want_vectors || res.evec || res.resid || wave;
     double *Z = vecs ? ctx->arena.get_t<double>("dv_z", (size_t)N * meval) : nullptr;
     DenseOut dout;
     dense_lowest(ctx, Hw, ldw, N, meval, vecs, wv, Z, N, "dt_", true, &dout);
@@ -944,6 +948,7 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
             for (int j = 0; j < std::min(meval, res.resid_cap); ++j) res.resid[j] = rv[j];
     }
     put_levels(wv, Z);
+    if (wave) compute_wavefunctions(ctx, p, C, Z, N, meval, *wave);
     double ms1, ms2, ms3;
     finish_times(ms1, ms2, ms3);
     // dominant kernel: the panel kernel of the Householder reduction; its algorithmic

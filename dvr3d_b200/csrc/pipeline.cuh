@@ -80,6 +80,17 @@ struct Contracted {
     int ldt = 0;
     std::vector<int> iv2;   // per block selected counts (host)
     int nblocks = 0;
+    std::vector<double> sw; // [P] the row scaling sqrt(w_p) applied to Vt (1 where none; host)
+};
+
+// Wavefunction amplitudes of the returned levels on the DVR grid, in the record layout of the
+// reference's wavefunction file (filled by solve_block when requested): psi holds `nlev`
+// records of `len` doubles (Jacobi: psi(idvr, npnt1, npnt2) as trans writes it, :3733-3841;
+// Radau: wvfunc(nbass) as transr writes it, :3596-3643).
+struct WaveOut {
+    long long len = 0;
+    int nlev = 0;
+    std::vector<double> psi;
 };
 
 // Channel blocks of the assembled H3 (full storage, ldh) and their eigen-decompositions,
@@ -158,8 +169,15 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
                      const dvr3d_options &opt, int nwant, double *wv_dev, std::vector<double> &rn_host,
                      double *evec_dev, KrylovStats &ks);
 
-// Solve one k block. Throws HostError / CudaFail.
+// Solve one k block. Throws HostError / CudaFail. With `wave`, the eigenvectors of the
+// returned levels are also back-transformed to the DVR grid (wavefn.cu).
 void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_options &opt,
-                 dvr3d_result &res);
+                 dvr3d_result &res, WaveOut *wave = nullptr);
+
+// psi = the contracted basis (Vt with its sqrt(w) row scaling removed) times the eigenvector
+// coefficients Z (N x nlev, ldz), per block one DMMA GEMM, scattered into the record layout
+// of the wavefunction file. Downloads the records into wave.
+void compute_wavefunctions(dvr3d_ctx *ctx, const BlockPlan &p, const Contracted &C, const double *Z,
+                           long long ldz, int nlev, WaveOut &wave);
 
 }  // namespace dvr3d

@@ -220,6 +220,19 @@ int dvr3d_b200_run_deck(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_optio
                         char *out, size_t outcap, size_t *outlen,
                         char *lev, size_t levcap, size_t *levlen);
 
+/* dvr3d_b200_run_deck plus the wavefunction file the reference writes to unit IWAVE
+ * (fort.26) when the deck sets ZTRAN, written to `wave_path` record by record as DVR3DRJZ
+ * writes it: the setcon header (:1176-1184), the ccmain records (:820-845), per k block the
+ * angular grid and polynomials (:972-976), for Radau testiv's selection (:3446-3448), and the
+ * levels and each level's amplitudes on the DVR grid from trans (Jacobi, psi(idvr, npnt1,
+ * npnt2), :3733-3841) or transr (Radau, wvfunc(nbass), :3622-3641). Records are sequential
+ * unformatted with a 4-byte length count before and after each; logicals are 4-byte with
+ * .TRUE. = -1. Amplitudes are defined up to the sign of each eigenvector. The readers are
+ * ROTLEV3 / ROTLEV3B / DIPOLE3 (source/wfnread.f90:101-215 reads the same records). */
+int dvr3d_b200_run_deck_wave(dvr3d_ctx *ctx, const char *deck_text, const dvr3d_options *opt,
+                             char *out, size_t outcap, size_t *outlen,
+                             char *lev, size_t levcap, size_t *levlen, const char *wave_path);
+
 /* Batched replacement of diag(ham,maxham,nham,eig) -> dsyev('V','L',...) (:2638-2659) for
  * many independent symmetric blocks already on the device: block b is n[b] x n[b] at
  * a + off[b] with leading dimension n[b] (lower triangle read). Eigenvalues ascending go

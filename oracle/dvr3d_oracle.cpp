@@ -1004,6 +1004,32 @@ void nfmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
         tr->stage_s[2] = std::chrono::duration<double>(t3 - t2).count();
         tr->stage_s[3] = std::chrono::duration<double>(t3 - t0).count();
     }
+    if (tr && tr->psi && final_mode != 2) {
+        // transr (:3622-3641): wvfunc(nbass), index over the pairs irs (outer) and the angles
+        // with kept states (inner); nbass = iang * max2d
+        int iang = 0;
+        for (int ig = 0; ig < nalf; ++ig) iang += (iv2b[ig] > 0);
+        const long long len = (long long)iang * R.max2d;
+        tr->psi_len = len;
+        tr->psi_nlev = 0;
+        if (tr->psi_cap >= (size_t)len * meval) {
+            std::fill(tr->psi, tr->psi + (size_t)len * meval, 0.0);
+            for (int l = 0; l < meval; ++l) {
+                double *w = tr->psi + (size_t)l * len;
+                long long index = 0;
+                for (int irs = 0; irs < nham2; ++irs)
+                    for (int ig = 0; ig < nalf; ++ig) {
+                        if (iv2b[ig] == 0) continue;
+                        for (int lev2 = 0; lev2 < iv2b[ig]; ++lev2) {
+                            const int ivec2 = iv2a[ig] - 1 + lev2;
+                            w[index] += V(ivec2)[irs] * ham3[(size_t)l * nham3 + ivec2];
+                        }
+                        ++index;
+                    }
+            }
+            tr->psi_nlev = meval;
+        }
+    }
     if (res) {
         res->nham3 = nham3;
         res->meval = (final_mode == 2) ? 0 : meval;
@@ -1227,6 +1253,8 @@ void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     // mkham3 :2301-2552, first part: cint per block (P x iv2), P = npnta*npntb
     int ncint = npnta * npntb;
     std::vector<std::vector<double>> cint(npntc);
+    const bool want_psi = tr && tr->psi;
+    std::vector<std::vector<double>> phi(want_psi ? npntc : 0);  // trans: phi before the sqrt(w) scaling
     for (int ione = 0; ione < npntc; ++ione) {
         R.tick();
         int nham2 = ndim2d[ione];
@@ -1246,6 +1274,10 @@ void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
                     }
                     ++ind2;
                 }
+            }
+            if (want_psi) {
+                if (phi[ione].empty()) phi[ione].assign((size_t)ncint * iv2[ione], 0.0);
+                std::memcpy(&phi[ione][(size_t)j * ncint], &C[(size_t)j * ncint], sizeof(double) * ncint);
             }
             if (!R.ztheta) {
                 int in2 = 0;
@@ -1321,6 +1353,33 @@ void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
         tr->stage_s[1] = std::chrono::duration<double>(t2 - t1).count();
         tr->stage_s[2] = std::chrono::duration<double>(t3 - t2).count();
         tr->stage_s[3] = std::chrono::duration<double>(t3 - t0).count();
+    }
+    if (want_psi && final_mode != 2) {
+        // trans (:3733-3841): psi(idvr, npnt1, npnt2) for each level, summed block by block
+        const long long I = R.idvr, n1 = R.npnt1, len = I * R.npnt1 * R.npnt2;
+        tr->psi_len = len;
+        tr->psi_nlev = 0;
+        if (tr->psi_cap >= (size_t)len * meval) {
+            std::fill(tr->psi, tr->psi + (size_t)len * meval, 0.0);
+            for (int l = 0; l < meval; ++l) {
+                double *psi = tr->psi + (size_t)l * len;
+                const double *z = &ham3[(size_t)l * nham3];
+                int ind2 = 0;
+                for (int ic = 0; ic < npntc; ++ic) {
+                    for (int j = 0; j < iv2[ic]; ++j, ++ind2) {
+                        const double *ph = &phi[ic][(size_t)j * ncint];
+                        for (int ia = 0; ia < npnta; ++ia)
+                            for (int ib = 0; ib < npntb; ++ib) {
+                                long long f;
+                                if (!R.ztheta) f = R.zr2r1 ? ic + I * (ib + n1 * ia) : ic + I * (ia + n1 * ib);
+                                else f = R.zr2r1 ? ia + I * (ic + n1 * ib) : ia + I * (ib + n1 * ic);
+                                psi[f] += z[ind2] * ph[(size_t)ia * npntb + ib];
+                            }
+                    }
+                }
+            }
+            tr->psi_nlev = meval;
+        }
     }
     if (res) {
         res->nham3 = nham3;

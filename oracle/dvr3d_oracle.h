@@ -52,6 +52,10 @@ typedef struct oracle_trace {
     double *h3; size_t h3_cap;          /* assembled final Hamiltonian (lower valid)        */
     double stage_s[4];           /* wall seconds: 1D/2D stage, assembly, final diag, total */
     int nham3;
+    /* wavefunction amplitudes of the returned levels on the DVR grid (trans :3649-3843 /
+     * transr :3596-3643): psi_nlev records of psi_len doubles, as the reference writes them */
+    double *psi; size_t psi_cap;
+    long long psi_len; int psi_nlev;
 } oracle_trace;
 
 /* final_mode: 0 = dsyev('V','L') with lwork = 3*N as diag() does (:2650-2654);

@@ -82,7 +82,9 @@ class Trace(C.Structure):
                 ("eig2all", C.POINTER(C.c_double)), ("eig2all_cap", C.c_int),
                 ("eigs2d", C.POINTER(C.c_double)), ("eigs2d_cap", C.c_int),
                 ("h3", C.POINTER(C.c_double)), ("h3_cap", C.c_size_t),
-                ("stage_s", C.c_double * 4), ("nham3", C.c_int)]
+                ("stage_s", C.c_double * 4), ("nham3", C.c_int),
+                ("psi", C.POINTER(C.c_double)), ("psi_cap", C.c_size_t),
+                ("psi_len", C.c_longlong), ("psi_nlev", C.c_int)]
 
 
 def _lapack_path() -> str:
@@ -191,10 +193,11 @@ class OracleResult:
     stage_s: np.ndarray
     kz: int
     ipar: int
+    psi: np.ndarray | None = None  # (levels, record length): amplitudes as trans / transr write them
 
 
 def solve(deck: Deck, kk: int = 0, pes=None, vgrid=None, final_mode: int = 0, want_h3: bool = False,
-          want_eigs2d: bool = True, h3_cap: int = 0) -> OracleResult:
+          want_eigs2d: bool = True, h3_cap: int = 0, want_psi: bool = False) -> OracleResult:
     """Run the oracle on one k block. pes: 13 MORSE_SUM parameters, or vgrid: table.
     deck: deck text (read by the oracle's reader) or a struct dvr3d_deck."""
     lib = load()
@@ -230,6 +233,12 @@ def solve(deck: Deck, kk: int = 0, pes=None, vgrid=None, final_mode: int = 0, wa
         h3 = np.zeros(cap)
         t.h3 = h3.ctypes.data_as(C.POINTER(C.c_double))
         t.h3_cap = h3.size
+    psi = None
+    if want_psi:
+        cap = max(s["idvr"] * s["npnt1"] * s["npnt2"], s["nalf"] * max(s["max2d"], 1)) * neval
+        psi = np.zeros(cap)
+        t.psi = psi.ctypes.data_as(C.POINTER(C.c_double))
+        t.psi_cap = psi.size
     kind, pp, npes, vg, nvg = 0, None, 0, None, 0
     if pes is not None:
         p = np.ascontiguousarray(np.asarray(pes, dtype=np.float64))
@@ -246,7 +255,9 @@ def solve(deck: Deck, kk: int = 0, pes=None, vgrid=None, final_mode: int = 0, wa
                         n2d=n2d[:t.nblocks].copy(),
                         eigs2d=None if e2 is None else e2[:n].copy(),
                         h3=None if h3 is None or n == 0 else h3[:n * n].reshape(n, n, order="F").copy(),
-                        stage_s=np.array(t.stage_s[:]), kz=t.kz, ipar=t.ipar)
+                        stage_s=np.array(t.stage_s[:]), kz=t.kz, ipar=t.ipar,
+                        psi=None if psi is None or t.psi_nlev == 0 else
+                        psi[:t.psi_len * t.psi_nlev].reshape(t.psi_nlev, t.psi_len).copy())
 
 
 def pes_morse_sum(p, r1: float, r2: float, x: float) -> float:
