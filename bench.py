@@ -253,6 +253,63 @@ def run_reference(args, rank: int, world: int) -> int:
     return 0 if ok else 1
 
 
+def run_batch64(args) -> int:
+    """64 independent J=0 Radau problems (configs.config3: seeded sizes and surfaces, the
+    lowest 100 levels of each) per step through dvr3d_b200_solve_batch, reported in
+    problems/s; the same problems solved one solve_block call at a time are timed beside it."""
+    import torch
+
+    import dvr3d_b200
+    from dvr3d_b200 import configs, parse_deck
+
+    dev = 0
+    torch.cuda.set_device(dev)
+    ctx = dvr3d_b200.Context(dev)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+    ws = configs.config3()
+    decks = [parse_deck(w.deck) for w in ws]
+    pes = np.array([w.pes for w in ws])
+
+    def timed(fn, k):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize(dev)
+        e0.record(stream)
+        for _ in range(k):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize(dev)
+        return e0.elapsed_time(e1) / k
+
+    def one_by_one():
+        for w, d in zip(ws, decks):
+            ctx.set_pes(w.pes)
+            ctx.solve(d, 0)
+
+    def batched():
+        return ctx.solve_batch(decks, pes)
+
+    for _ in range(args.warmup):
+        batched()
+    with ClockSampler(dev) as clk:
+        ms = timed(batched, args.steps)
+    one_by_one()
+    ms1 = timed(one_by_one, min(args.steps, 2))
+    res = batched()
+    line = {"metric": "problems/s, 64 independent J=0 Radau problems, lowest 100 levels each", "value": 64000.0 / ms,
+            "unit": "problems/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded sizes and Morse + bend surfaces)",
+            "config": {"workload": "64 Radau problems, NPNT U{16..32}, NALF U{24..64}, final H 800-3000, 100 levels",
+                       "sizes": [int(r.nham3) for r in res],
+                       "one_by_one": {"ms_per_step": ms1, "problems_per_s": 64000.0 / ms1}},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    return 0
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -261,10 +318,14 @@ def main() -> int:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="cfg4", choices=["cfg4", "batch64"],
+                    help="cfg4: the headline solve; batch64: 64 independent Radau problems per step")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.workload == "batch64" and args.impl == "ours":
+        return run_batch64(args)
     if args.impl == "reference":
         return run_reference(args, rank, world)
 

@@ -145,7 +145,12 @@ def config4(emax1: float = CFG4_EMAX1, emax2: float = CFG4_EMAX2) -> Workload:
 HCN_MASSES = (1.007825, 12.0, 14.003074)
 
 
-def config5(emax1: float = 50000.0, emax2: float = 40000.0) -> Workload:
+# cut-offs of the J=2 workload, fixed once against the oracle's 1D/2D stages (N ~ 20500 per k)
+CFG5_EMAX1 = 65000.0
+CFG5_EMAX2 = 64000.0
+
+
+def config5(emax1: float = CFG5_EMAX1, emax2: float = CFG5_EMAX2) -> Workload:
     """Jacobi, H/C/N masses, J=2 with k = 0, 1, 2 blocks, NPNT1=50, NPNT2=30, NALF=100."""
     ur1, ur2 = reduced_masses(HCN_MASSES, 1)
     re1, de1, we1 = 2.18, 0.30, 0.0095

@@ -1,4 +1,5 @@
 // capi.cu -- extern "C" entry points declared in include/dvr3d_b200.h.
+#include <chrono>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -231,15 +232,52 @@ int dvr3d_b200_solve_batch(dvr3d_ctx *ctx, const dvr3d_deck *decks, const double
     return guarded(ctx, [&]() -> int {
         cudaSetDevice(ctx->device);
         const dvr3d::PesParams saved = ctx->pes;
+        struct Restore {
+            dvr3d_ctx *c;
+            dvr3d::PesParams p;
+            ~Restore() { c->pes = p; }
+        } restore{ctx, saved};
+        const auto th0 = std::chrono::steady_clock::now();
+        std::vector<dvr3d::BlockPlan> plans(nprob);
+        std::vector<dvr3d::PesParams> pes(nprob);
+        bool radau = true;
         for (int i = 0; i < nprob; ++i) {
-            ctx->pes.kind = DVR3D_PES_MORSE_SUM;
-            for (int k = 0; k < DVR3D_PES_MORSE_SUM_NPARAM; ++k)
-                ctx->pes.p[k] = pes_params[(size_t)i * DVR3D_PES_MORSE_SUM_NPARAM + k];
             int kd, ku;
             dvr3d::k_range(decks[i], kd, ku);
-            dvr3d::solve_block(ctx, decks[i], kd, o, res[i]);
+            dvr3d::plan_block(decks[i], kd, plans[i]);
+            radau = radau && plans[i].radau;
+            pes[i] = dvr3d::PesParams{};
+            pes[i].kind = DVR3D_PES_MORSE_SUM;
+            for (int k = 0; k < DVR3D_PES_MORSE_SUM_NPARAM; ++k)
+                pes[i].p[k] = pes_params[(size_t)i * DVR3D_PES_MORSE_SUM_NPARAM + k];
         }
-        ctx->pes = saved;
+        if (!radau) {  // Jacobi problems: one pipeline each
+            for (int i = 0; i < nprob; ++i) {
+                ctx->pes = pes[i];
+                int kd, ku;
+                dvr3d::k_range(decks[i], kd, ku);
+                dvr3d::solve_block(ctx, decks[i], kd, o, res[i]);
+            }
+            return DVR3D_OK;
+        }
+        // Radau problems: the 2D stages of all of them as one batched workload, then each
+        // problem's assembly and final eigensolve on its own resident contracted basis
+        const auto th1 = std::chrono::steady_clock::now();
+        const long long launches0 = dvr3d::g_kernel_launches;
+        cudaStream_t st = ctx->stream;
+        if (cudaMemsetAsync(dvr3d::eigvec_err_flag(ctx), 0, sizeof(int), st) != cudaSuccess ||
+            cudaEventRecord(ctx->ev[0], st) != cudaSuccess)
+            throw CudaFail{cudaGetLastError(), "solve_batch"};
+        std::vector<dvr3d::Contracted> cs;
+        dvr3d::radau_stage_batch(ctx, plans, pes, cs);
+        if (cudaEventRecord(ctx->ev[1], st) != cudaSuccess) throw CudaFail{cudaGetLastError(), "solve_batch"};
+        dvr3d::check_eigvec_err(ctx, "batched inverse iteration (2D eigenvectors)");
+        for (int i = 0; i < nprob; ++i) {
+            res[i].dom_ms = res[i].dom_bytes = res[i].dom_flops = 0.0;
+            res[i].dom_launches = 0;
+            std::memset(res[i].dom_kernel, 0, sizeof(res[i].dom_kernel));
+            dvr3d::solve_contracted(ctx, plans[i], cs[i], o, res[i], nullptr, th0, th1, launches0);
+        }
         return DVR3D_OK;
     });
 }

@@ -752,28 +752,188 @@ bool band_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int b, int nev
 }
 
 // ---------------------------------------------------------------- one k block
-void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_options &opt,
-                 dvr3d_result &res, WaveOut *wave) {
-    auto th0 = std::chrono::steady_clock::now();
-    if (ctx->pes.kind != DVR3D_PES_MORSE_SUM && ctx->pes.kind != DVR3D_PES_GRID)
-        throw HostError{DVR3D_ERR_ARG, "no potential selected (dvr3d_b200_set_pes)"};
-    BlockPlan p;
-    plan_block(deck, kk, p);
-    auto th1 = std::chrono::steady_clock::now();
-    const long long launches0 = g_kernel_launches;
-    t_h2d = 0;
-    t_d2h = 0;
-    res.dom_ms = res.dom_bytes = res.dom_flops = 0.0;
-    res.dom_launches = 0;
-    std::memset(res.dom_kernel, 0, sizeof(res.dom_kernel));
+// ---------------------------------------------------------------- many Radau problems at once
+// The 2D stage of independent Radau problems (the repeated DVR3DRJZ runs of a fitting
+// driver) as one workload: the blocks of every problem are built into one buffer and go
+// through ONE launch of each batched eigensolver phase (tridiagonalisation, eigenvalues,
+// eigenvectors of the kept states), so the GPU works on the blocks of all problems together
+// instead of on one problem's few dozen angles. All eigenvalues come back in one copy and
+// each problem's selection (cut2dr / choosr, testiv) is made on the host. Per-problem
+// buffers are named with the problem index so every contracted basis stays resident until
+// its problem's assembly and final solve (solve_contracted).
+void radau_stage_batch(dvr3d_ctx *ctx, const std::vector<BlockPlan> &plans, const std::vector<PesParams> &pes,
+                       std::vector<Contracted> &outs) {
     cudaStream_t st = ctx->stream;
-    CK(cudaMemsetAsync(ev_err(ctx), 0, sizeof(int), st));
-    CK(cudaEventRecord(ctx->ev[0], st));
-    Contracted C;
-    if (p.radau) radau_stage(ctx, p, C);
-    else jacobi_stage(ctx, p, C);
-    CK(cudaEventRecord(ctx->ev[1], st));
-    check_dev_err(ctx, ev_err(ctx), "batched inverse iteration (1D/2D eigenvectors)");
+    const int np = (int)plans.size();
+    outs.assign(np, Contracted{});
+    std::vector<int> nb_n, first(np + 1, 0);  // per block: dimension; first block of each problem
+    std::vector<long long> aoff, voff;
+    long long at = 0, vt = 0;
+    int nmax = 0;
+    for (int i = 0; i < np; ++i) {
+        const BlockPlan &p = plans[i];
+        const int n = p.npnt1 * (p.npnt1 + 1 - 2 * p.ipar) / 2;
+        if (n > 1024) throw HostError{DVR3D_ERR_UNSUPPORTED, "Radau 2D block larger than 1024"};
+        nmax = std::max(nmax, n);
+        first[i] = (int)nb_n.size();
+        for (int b = 0; b < p.nalf; ++b) {
+            nb_n.push_back(n);
+            aoff.push_back(at);
+            voff.push_back(vt);
+            at += (long long)n * n;
+            vt += n;
+        }
+    }
+    first[np] = (int)nb_n.size();
+    const int nblk = (int)nb_n.size();
+    double *H = ctx->arena.get_t<double>("bt_blk2", (size_t)at);
+    std::vector<std::vector<int>> pa(np), pb(np);
+    for (int i = 0; i < np; ++i) {
+        const BlockPlan &p = plans[i];
+        const int npnt = p.npnt1;
+        for (int beta = 1; beta <= npnt; ++beta)
+            for (int alpha = 1; alpha <= beta - p.ipar; ++alpha) {
+                pa[i].push_back(alpha - 1);
+                pb[i].push_back(beta - 1);
+            }
+        const std::string sfx = "_" + std::to_string(i);
+        RadauBuild rb{};
+        rb.n = (int)pa[i].size();
+        rb.npnt = npnt;
+        rb.ipar = p.ipar;
+        rb.jrot = p.jrot;
+        rb.kz = p.kz;
+        rb.pa = upload(ctx, "bt_pa" + sfx, pa[i]);
+        rb.pb = upload(ctx, "bt_pb" + sfx, pb[i]);
+        rb.r = upload(ctx, "bt_r1" + sfx, p.r1);
+        rb.hr = upload(ctx, "bt_xk1" + sfx, p.xk1);
+        rb.xalf = upload(ctx, "bt_xalf" + sfx, p.xalf);
+        rb.term = p.nf_term;
+        rb.term2 = p.nf_term2;
+        rb.term3 = p.nf_term3;
+        rb.urr1 = p.urr1;
+        rb.pes = pes[i];
+        if (rb.pes.kind != DVR3D_PES_MORSE_SUM)
+            throw HostError{DVR3D_ERR_ARG, "batched problems take DVR3D_PES_MORSE_SUM surfaces"};
+        launch_radau_build(rb, p.nalf, H + aoff[first[i]], st);
+        outs[i].T = upload(ctx, "bt_xl" + sfx, p.xlmatr);
+        outs[i].ldt = p.idvr;
+    }
+    CK(cudaGetLastError());
+    BatchDesc bd{nblk, upload(ctx, "bt_n", nb_n), upload(ctx, "bt_aoff", aoff), upload(ctx, "bt_voff", voff)};
+    double *d = ctx->arena.get_t<double>("bt_d", (size_t)vt);
+    double *e = ctx->arena.get_t<double>("bt_e", (size_t)vt);
+    double *tau = ctx->arena.get_t<double>("bt_tau", (size_t)vt);
+    double *w = ctx->arena.get_t<double>("bt_w", (size_t)vt);
+    int *cnt = ctx->arena.get_t<int>("bt_cnt", nblk);
+    launch_tridiag_batched(bd, H, d, e, tau, nmax, st);
+    launch_eigvals_batched(bd, d, e, w, cnt, 0, 0.0, st);  // every eigenvalue: selection on the host
+    CK(cudaGetLastError());
+    const std::vector<double> all = download(ctx, w, (size_t)vt);
+    std::vector<int> sel(nblk, 0);
+    std::vector<long long> zoff(nblk, 0);
+    std::vector<int> zld(nblk, 0);
+    std::vector<long long> vtoff(np, 0);
+    long long vtot = 0;
+    for (int i = 0; i < np; ++i) {
+        const BlockPlan &p = plans[i];
+        const int n = nb_n[first[i]], nalf = p.nalf;
+        const double *wi = all.data() + voff[first[i]];
+        int *si = sel.data() + first[i];
+        if (p.zcut) {  // cut2dr (:3323-3377)
+            long long tot = 0;
+            for (int b = 0; b < nalf; ++b) {
+                int c = 0;
+                while (c < n && wi[(size_t)b * n + c] < p.emax2_au) ++c;
+                si[b] = c;
+                tot += c;
+                if (tot > p.max3d) throw HostError{DVR3D_ERR_CORE_MAX3D, "number of 2d eigenvalues greater than max3d"};
+            }
+        } else {  // choosr (:3223-3319)
+            std::vector<double> srt(wi, wi + (size_t)nalf * n);
+            std::sort(srt.begin(), srt.end());
+            const double emax = ((long long)srt.size() <= p.max3d) ? srt.back() : srt[p.max3d - 1];
+            for (int b = 0; b < nalf; ++b) {
+                int c = 0;
+                while (c < n && wi[(size_t)b * n + c] <= emax) ++c;
+                si[b] = c;
+            }
+        }
+        if (p.jrot > 0) {  // testiv (:3380-3451)
+            int iend = nalf;
+            for (int q = nalf / 2; q <= nalf; ++q)
+                if (q >= 1 && si[q - 1] == 0) {
+                    iend = q;
+                    break;
+                }
+            for (int q = iend + 1; q <= nalf; ++q) si[q - 1] = 0;
+            if (si[nalf - 1] > 0) {
+                if (p.zlin) si[nalf - 1] = 0;
+                else throw HostError{DVR3D_ERR_THETA0, "bisector embedding: wavefunction has amplitude for theta = 0"};
+            }
+        }
+        Contracted &o = outs[i];
+        o.iv2.assign(si, si + nalf);
+        o.nblocks = nalf;
+        o.N = std::accumulate(o.iv2.begin(), o.iv2.end(), 0);
+        o.P = n;
+        o.ldv = round_up(n, 16);
+        vtoff[i] = vtot;
+        long long col = 0;
+        for (int b = 0; b < nalf; ++b) {
+            zoff[first[i] + b] = vtot + col * o.ldv;
+            zld[first[i] + b] = (int)o.ldv;
+            col += si[b];
+        }
+        vtot += o.ldv * round_up(std::max(o.N, 1), 64);
+    }
+    double *Vpool = ctx->arena.get_t<double>("bt_vt", (size_t)vtot);
+    CK(cudaMemsetAsync(Vpool, 0, sizeof(double) * vtot, st));
+    launch_eigvecs_batched_fast(bd, H, d, e, tau, w, upload(ctx, "bt_sel", sel), upload(ctx, "bt_zoff", zoff),
+                                upload(ctx, "bt_zld", zld), Vpool, nmax, ev_err(ctx), st);
+    CK(cudaGetLastError());
+    for (int i = 0; i < np; ++i) {
+        const BlockPlan &p = plans[i];
+        Contracted &o = outs[i];
+        o.Vt = Vpool + vtoff[i];
+        const std::string sfx = "_" + std::to_string(i);
+        std::vector<double> sw(o.ldv, 0.0);
+        for (int q = 0; q < o.P; ++q) {
+            const double ra = p.r1[pa[i][q]], rbv = p.r1[pb[i][q]];
+            sw[q] = std::sqrt(0.5 / (ra * ra * p.ur1) + 0.5 / (rbv * rbv * p.ur1));
+        }
+        if (o.N == 0) continue;
+        launch_scale_rows(o.Vt, (int)o.ldv, o.N, upload(ctx, "bt_sw" + sfx, sw), st);
+        o.sw.assign(sw.begin(), sw.begin() + o.P);
+        std::vector<int> gcol(o.N);
+        std::vector<long long> emap(o.N);
+        long long col = 0;
+        for (int b = 0; b < o.nblocks; ++b) {
+            for (int j = 0; j < o.iv2[b]; ++j) {
+                gcol[col + j] = b;
+                emap[col + j] = voff[first[i] + b] + j;
+            }
+            col += o.iv2[b];
+        }
+        o.g = upload(ctx, "bt_gcol" + sfx, gcol);
+        o.e2 = ctx->arena.get_t<double>("bt_e2" + sfx, o.N);
+        launch_gather(w, upload(ctx, "bt_emap" + sfx, emap), o.e2, o.N, st);
+    }
+    CK(cudaGetLastError());
+}
+
+// The eigenvector error flag of a solve, for callers outside this file that run the stages
+// themselves (batched problems): cleared before the stage, checked after it.
+int *eigvec_err_flag(dvr3d_ctx *ctx) { return ev_err(ctx); }
+void check_eigvec_err(dvr3d_ctx *ctx, const char *stage) { check_dev_err(ctx, ev_err(ctx), stage); }
+
+// Everything after the 1D/2D stages of one block: selection outputs, assembly, the final
+// eigensolve (plain, Davidson or shift-invert), levels, vectors, timings and counters.
+// ev[0] / ev[1] of the context bracket the stage that produced C.
+void solve_contracted(dvr3d_ctx *ctx, const BlockPlan &p, const Contracted &C, const dvr3d_options &opt,
+                      dvr3d_result &res, WaveOut *wave, std::chrono::steady_clock::time_point th0,
+                      std::chrono::steady_clock::time_point th1, long long launches0) {
+    cudaStream_t st = ctx->stream;
     const int N = C.N;
     res.kz = p.kz;
     res.ipar = p.ipar;
@@ -966,6 +1126,31 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
     res.launches = (int)(g_kernel_launches - launches0);
     res.h2d_bytes = t_h2d;
     res.d2h_bytes = t_d2h;
+}
+
+void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_options &opt,
+                 dvr3d_result &res, WaveOut *wave) {
+    auto th0 = std::chrono::steady_clock::now();
+    if (ctx->pes.kind != DVR3D_PES_MORSE_SUM && ctx->pes.kind != DVR3D_PES_GRID)
+        throw HostError{DVR3D_ERR_ARG, "no potential selected (dvr3d_b200_set_pes)"};
+    BlockPlan p;
+    plan_block(deck, kk, p);
+    auto th1 = std::chrono::steady_clock::now();
+    const long long launches0 = g_kernel_launches;
+    t_h2d = 0;
+    t_d2h = 0;
+    res.dom_ms = res.dom_bytes = res.dom_flops = 0.0;
+    res.dom_launches = 0;
+    std::memset(res.dom_kernel, 0, sizeof(res.dom_kernel));
+    cudaStream_t st = ctx->stream;
+    CK(cudaMemsetAsync(ev_err(ctx), 0, sizeof(int), st));
+    CK(cudaEventRecord(ctx->ev[0], st));
+    Contracted C;
+    if (p.radau) radau_stage(ctx, p, C);
+    else jacobi_stage(ctx, p, C);
+    CK(cudaEventRecord(ctx->ev[1], st));
+    check_dev_err(ctx, ev_err(ctx), "batched inverse iteration (1D/2D eigenvectors)");
+    solve_contracted(ctx, p, C, opt, res, wave, th0, th1, launches0);
 }
 
 }  // namespace dvr3d

@@ -1,6 +1,8 @@
 // pipeline.cuh -- device context and the per-k-block solve pipeline.
 #pragma once
 
+#include <chrono>
+
 #include <cuda_runtime.h>
 
 #include <map>
@@ -173,6 +175,22 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
 // returned levels are also back-transformed to the DVR grid (wavefn.cu).
 void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_options &opt,
                  dvr3d_result &res, WaveOut *wave = nullptr);
+
+// The 2D stages of several independent Radau k blocks (each with its own surface) as one
+// batched device workload; outs[i] is problem i's contracted basis.
+void radau_stage_batch(dvr3d_ctx *ctx, const std::vector<BlockPlan> &plans, const std::vector<PesParams> &pes,
+                       std::vector<Contracted> &outs);
+
+// The error flag of the batched eigenvector kernels (cleared by the caller before a stage) and
+// its check (throws DVR3D_ERR_NOCONV when raised).
+int *eigvec_err_flag(dvr3d_ctx *ctx);
+void check_eigvec_err(dvr3d_ctx *ctx, const char *stage);
+
+// The part of solve_block after the 1D/2D stages (assembly, final eigensolve, outputs), for a
+// block whose contracted basis C is already on the device (ev[0] / ev[1] bracket its stage).
+void solve_contracted(dvr3d_ctx *ctx, const BlockPlan &p, const Contracted &C, const dvr3d_options &opt,
+                      dvr3d_result &res, WaveOut *wave, std::chrono::steady_clock::time_point th0,
+                      std::chrono::steady_clock::time_point th1, long long launches0);
 
 // psi = the contracted basis (Vt with its sqrt(w) row scaling removed) times the eigenvector
 // coefficients Z (N x nlev, ldz), per block one DMMA GEMM, scattered into the record layout
