@@ -318,6 +318,8 @@ def main() -> int:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--profile-solve", action="store_true",
+                    help="one solve of the workload and nothing else (for ncu captures of its kernels)")
     ap.add_argument("--workload", default="cfg4", choices=["cfg4", "batch64"],
                     help="cfg4: the headline solve; batch64: 64 independent Radau problems per step")
     args = ap.parse_args()
@@ -326,6 +328,19 @@ def main() -> int:
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "batch64" and args.impl == "ours":
         return run_batch64(args)
+    if args.profile_solve:
+        # the chosen form once: the 1D/2D stage, assembly, the Cholesky-inverse (764 GEMM
+        # launches at this size, counting the start block's Cholesky-QR), then the Krylov steps
+        import dvr3d_b200
+        from dvr3d_b200 import configs, parse_deck
+
+        ctx = dvr3d_b200.Context(0)
+        w = configs.config4()
+        ctx.set_pes(w.pes)
+        r = ctx.solve(parse_deck(w.deck), 0, precision=dvr3d_b200.DVR3D_PREC_MIXED_DAVIDSON, nlevels=500)
+        print(json.dumps({"profile_solve": WORKLOAD, "nham3": r.nham3, "stage_ms": list(r.stage_ms)}), flush=True)
+        ctx.close()
+        return 0
     if args.impl == "reference":
         return run_reference(args, rank, world)
 
@@ -425,24 +440,45 @@ def main() -> int:
     value = total / (ms / 1000.0)
     e2e = total / wall_s
     hbm, bf16, src = _peaks()
-    dom_ms = sum(r.extra["dom_ms"] for r in results)
-    dom_bytes = sum(r.extra["dom_bytes"] for r in results)
-    dom_flops = sum(r.extra["dom_flops"] for r in results)
-    dom_launch = sum(r.extra["dom_launches"] for r in results)
+    prof = results
+    if mixed:
+        # the dominant kernel family's launches, each timed by its own CUDA event pair, on one
+        # more solve of the same workload right after the timed region (per-launch events are
+        # off in the timed solves: recording and reading them costs host time between solves)
+        os.environ["DVR3D_GEMM_EVENTS"] = "1"
+        prof = [step()]
+        os.environ.pop("DVR3D_GEMM_EVENTS")
+        torch.cuda.synchronize(dev)
+    nprof = len(prof)
+    dom_ms = sum(r.extra["dom_ms"] for r in prof)
+    dom_bytes = sum(r.extra["dom_bytes"] for r in prof)
+    dom_flops = sum(r.extra["dom_flops"] for r in prof)
+    dom_launch = sum(r.extra["dom_launches"] for r in prof)
     kern = results[0].extra["dom_kernel"]
     if dom_flops > 0:
         # tensor-bound FP64 GEMM: against cuBLAS DGEMM measured here (no FP64 figure is in
         # MEASURED_PEAKS.json)
         fp64_peak = _fp64_peak(dev)
         achieved = dom_flops / (dom_ms / 1000.0) / 1e12 if dom_ms > 0 else None
+        # DRAM bytes per launch from the ncu capture of the family's most frequent large launch,
+        # the Krylov triangular product (profiles/traffic.json, profiles/gemm_pipe_kernel_*.md)
+        traffic, traffic_note = None, None
+        tp = ROOT / "profiles" / "traffic.json"
+        if tp.exists():
+            ent = json.loads(tp.read_text()).get("gemm_pipe_kernel")
+            if ent:
+                traffic = ent["dram_bytes_per_launch"]
+                traffic_note = ent["launch"]
         roof = {"bound": "tensor", "kernel": kern, "achieved": achieved, "peak": fp64_peak, "unit": "TFLOP/s",
-                "frac": (achieved / fp64_peak) if achieved else None, "traffic": None,
+                "frac": (achieved / fp64_peak) if achieved else None, "traffic": traffic,
+                "traffic_launch": traffic_note,
                 "peak_source": "measured in this run: cuBLAS DGEMM (torch.matmul float64) 8192^3, best of 5",
-                "alg_flops_per_step": dom_flops / args.steps, "launches": dom_launch / args.steps,
+                "alg_flops_per_step": dom_flops / nprof, "launches": dom_launch / nprof,
                 "note": "achieved = algorithmic flops of the DMMA GEMM launches of a solve (Cholesky-inverse, "
                         "Krylov steps, Ritz vectors, H3 X; per launch from M, N, K and its triangular structure) "
-                        "/ the sum of their durations, each launch timed by a CUDA event pair on the solve's stream",
-                "share_of_step": dom_ms / ms if ms > 0 else None}
+                        "/ the sum of their durations, each launch timed by a CUDA event pair on the solve's stream "
+                        "(one solve after the timed region)",
+                "share_of_step": (dom_ms / nprof) / (ms / args.steps) if ms > 0 else None}
     else:
         achieved = dom_bytes / (dom_ms / 1000.0) / 1e9 if dom_ms > 0 else None
         traffic = None

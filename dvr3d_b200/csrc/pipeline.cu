@@ -1070,9 +1070,10 @@ void solve_contracted(dvr3d_ctx *ctx, const BlockPlan &p, const Contracted &C, c
             finish_times(ms1, ms2, ms3);
             // dominant kernel family: the DMMA GEMM (Cholesky-inverse, Krylov steps, Ritz
             // vectors, H3 X): its launches' own event-timed durations and algorithmic flops
+            // when they were logged (DVR3D_GEMM_EVENTS=1), else zero
             res.dom_ms = ks.gemm_ms;
             res.dom_bytes = 0.0;
-            res.dom_flops = ks.gemm_flops;
+            res.dom_flops = ks.gemm_ms > 0.0 ? ks.gemm_flops : 0.0;
             res.dom_launches = ks.gemm_launches;
             std::snprintf(res.dom_kernel, sizeof(res.dom_kernel), "gemm_pipe_kernel");
             res.launches = (int)(g_kernel_launches - launches0);

@@ -191,8 +191,12 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
     const bool trace = trace_env && trace_env[0] == '1';
     ks = KrylovStats{};
     ks.block = b;
-    // every GEMM launch of this solve timed by an event pair (4096 launches at most)
-    if (ctx->gemm_ev.empty()) {
+    // with DVR3D_GEMM_EVENTS=1, every GEMM launch of this solve is timed by an event pair
+    // (4096 launches at most); off by default: the event records and the read-out after the
+    // solve cost host time that delays the next solve
+    const char *gev = std::getenv("DVR3D_GEMM_EVENTS");
+    const bool log_gemms = gev && gev[0] == '1';
+    if (log_gemms && ctx->gemm_ev.empty()) {
         ctx->gemm_ev.resize(8192);
         for (auto &e : ctx->gemm_ev) CK(cudaEventCreate(&e));
     }
@@ -202,7 +206,7 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
     struct LogScope {
         explicit LogScope(GemmLaunchLog *l) { set_gemm_launch_log(l); }
         ~LogScope() { set_gemm_launch_log(nullptr); }
-    } log_scope(&glog);
+    } log_scope(log_gemms ? &glog : nullptr);
     // ---- (1)+(2) shift, factor, invert
     tf.start(st);
     double sigma = emin_bound - std::max(1.0e-6, 1.0e-3 * std::fabs(emin_bound));
@@ -441,7 +445,7 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
     ks.factor_ms = tf.ms();
     ks.krylov_ms = tk_ms;
     ks.rr_ms = tr_ms;
-    ks.gemm_ms = gemm_launch_log_ms(glog);
+    ks.gemm_ms = log_gemms ? gemm_launch_log_ms(glog) : 0.0;
     ks.gemm_flops = glog.flops;
     ks.gemm_launches = glog.launches;
     ks.gemm_untimed = glog.untimed;
