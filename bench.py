@@ -282,13 +282,23 @@ def run_batch64(args) -> int:
         torch.cuda.synchronize(dev)
         return e0.elapsed_time(e1) / k
 
+    prec = dvr3d_b200.DVR3D_PREC_FP64 if args.precision == "fp64" else dvr3d_b200.DVR3D_PREC_MIXED_DAVIDSON
+
     def one_by_one():
         for w, d in zip(ws, decks):
             ctx.set_pes(w.pes)
-            ctx.solve(d, 0)
+            ctx.solve(d, 0, precision=prec)
 
     def batched():
-        return ctx.solve_batch(decks, pes)
+        return ctx.solve_batch(decks, pes, precision=prec)
+
+    # every level of every problem against the plain FP64 path solved problem by problem
+    ref = ctx.solve_batch(decks, pes)
+    got = batched()
+    err = max(float(np.abs(g.eval - r.eval).max()) for g, r in zip(got, ref)) * dvr3d_b200.AUTOCM
+    if err > 1e-3:
+        print(json.dumps({"error": "batched levels outside 1e-3 cm-1 of the plain FP64 path", "max_err_cm": err}))
+        return 1
 
     for _ in range(args.warmup):
         batched()
@@ -302,6 +312,8 @@ def run_batch64(args) -> int:
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
             "data": "synthetic (seeded sizes and Morse + bend surfaces)",
             "config": {"workload": "64 Radau problems, NPNT U{16..32}, NALF U{24..64}, final H 800-3000, 100 levels",
+                       "path": "fp64-dense" if prec == dvr3d_b200.DVR3D_PREC_FP64 else "mixed (Davidson / shift-invert)",
+                       "max_level_err_vs_plain_cm": err,
                        "sizes": [int(r.nham3) for r in res],
                        "one_by_one": {"ms_per_step": ms1, "problems_per_s": 64000.0 / ms1}},
             "clocks": clk.summary()}
@@ -329,15 +341,18 @@ def main() -> int:
     if args.workload == "batch64" and args.impl == "ours":
         return run_batch64(args)
     if args.profile_solve:
-        # the chosen form once: the 1D/2D stage, assembly, the Cholesky-inverse (764 GEMM
-        # launches at this size, counting the start block's Cholesky-QR), then the Krylov steps
+        # one solve of the workload and nothing else. The chosen form: the 1D/2D stage,
+        # assembly, the Cholesky-inverse (764 GEMM launches at this size, counting the start
+        # block's Cholesky-QR), then the Krylov steps. --precision fp64: the plain path (one
+        # dense_panel_kernel launch per 32-column panel of the reduction).
         import dvr3d_b200
         from dvr3d_b200 import configs, parse_deck
 
         ctx = dvr3d_b200.Context(0)
         w = configs.config4()
         ctx.set_pes(w.pes)
-        r = ctx.solve(parse_deck(w.deck), 0, precision=dvr3d_b200.DVR3D_PREC_MIXED_DAVIDSON, nlevels=500)
+        prec = dvr3d_b200.DVR3D_PREC_FP64 if args.precision == "fp64" else dvr3d_b200.DVR3D_PREC_MIXED_DAVIDSON
+        r = ctx.solve(parse_deck(w.deck), 0, precision=prec, nlevels=500)
         print(json.dumps({"profile_solve": WORKLOAD, "nham3": r.nham3, "stage_ms": list(r.stage_ms)}), flush=True)
         ctx.close()
         return 0

@@ -256,7 +256,8 @@ class Context:
                                                        grad.ctypes.data_as(P) if want_grad else None))
         return float(loss[0]), grad
 
-    def solve_batch(self, decks: list[Deck], pes_rows) -> list[SolveResult]:
+    def solve_batch(self, decks: list[Deck], pes_rows, precision: int = DVR3D_PREC_FP64,
+                    nlevels: int = 0) -> list[SolveResult]:
         n = len(decks)
         arr = (Deck * n)(*decks)
         P = np.ascontiguousarray(np.asarray(pes_rows, dtype=np.float64).reshape(n, DVR3D_PES_MORSE_SUM_NPARAM))
@@ -270,7 +271,7 @@ class Context:
             res[i].eval_cap = ev.size
             res[i].iv2 = iv2.ctypes.data_as(C.POINTER(C.c_int))
             res[i].iv2_cap = iv2.size
-        o = Options()
+        o = Options(precision=precision, nlevels=nlevels)
         self._check(self._lib.dvr3d_b200_solve_batch(self._h, arr, P.ctypes.data_as(C.POINTER(C.c_double)), n,
                                                      C.byref(o), res))
         out = []

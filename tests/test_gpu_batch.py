@@ -58,3 +58,18 @@ def test_batch_of_64_equals_problem_by_problem(ctx):
         assert g.nham3 == one.nham3
         np.testing.assert_array_equal(g.iv2, one.iv2)
         assert np.abs(g.eval - one.eval).max() * AUTOCM <= 1e-7
+
+
+def test_batch_chosen_form_within_bar_of_plain(ctx):
+    """The iterative final solve per problem (Davidson / shift-invert) inside the batch: every
+    level within 1e-3 cm-1 of the plain FP64 batch."""
+    import dvr3d_b200
+
+    ws = configs.config3(nprob=12)
+    decks = [parse_deck(w.deck) for w in ws]
+    pes = np.array([w.pes for w in ws])
+    plain = ctx.solve_batch(decks, pes)
+    mixed = ctx.solve_batch(decks, pes, precision=dvr3d_b200.DVR3D_PREC_MIXED_DAVIDSON)
+    for a, b in zip(plain, mixed):
+        np.testing.assert_array_equal(a.iv2, b.iv2)
+        assert np.abs(a.eval - b.eval).max() * AUTOCM <= 1e-3
