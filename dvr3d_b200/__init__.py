@@ -16,13 +16,13 @@ import numpy as np
 from . import _abi
 from ._abi import (DVR3D_LP_NPARAM, DVR3D_PATH_DAVIDSON, DVR3D_PATH_DENSE, DVR3D_PATH_SHIFT_INVERT,
                    DVR3D_PES_GRID, DVR3D_PES_MORSE_SUM, DVR3D_PES_MORSE_SUM_NPARAM, DVR3D_PREC_FP64,
-                   DVR3D_PREC_MIXED_DAVIDSON, Deck, Options, Result)
+                   DVR3D_PREC_MIXED_DAVIDSON, DVR3D_PREC_SPLIT_BF16, Deck, Options, Result)
 
 AUTOCM = 2.19474624e5  # hartree -> cm-1, as diag3d (:2681)
 
 __all__ = ["Context", "Deck", "DVR3DError", "SolveResult", "parse_deck", "AUTOCM",
            "DVR3D_PES_MORSE_SUM", "DVR3D_PES_GRID", "DVR3D_PREC_FP64",
-           "DVR3D_PREC_MIXED_DAVIDSON", "DVR3D_LP_NPARAM", "DVR3D_PATH_DENSE", "DVR3D_PATH_SHIFT_INVERT",
+           "DVR3D_PREC_MIXED_DAVIDSON", "DVR3D_PREC_SPLIT_BF16", "DVR3D_LP_NPARAM", "DVR3D_PATH_DENSE", "DVR3D_PATH_SHIFT_INVERT",
            "DVR3D_PATH_DAVIDSON", "k_blocks", "host_grid"]
 
 
@@ -107,7 +107,8 @@ def _counters(r: Result) -> dict:
             "dom_launches": r.dom_launches, "launches": r.launches, "h2d_bytes": r.h2d_bytes,
             "d2h_bytes": r.d2h_bytes, "dom_kernel": r.dom_kernel.decode(), "path": r.path,
             "matvecs": r.matvecs, "lp_pairs": r.lp_pairs, "lp_loss_first": r.lp_loss_first,
-            "lp_loss_last": r.lp_loss_last}
+            "lp_loss_last": r.lp_loss_last, "low_iterations": r.low_iterations,
+            "low_matvecs": r.low_matvecs}
 
 
 class Context:
@@ -149,6 +150,22 @@ class Context:
     def set_wait_limit(self, polls: int) -> None:
         """Poll limit of every bounded device wait of later solves (0: the defaults)."""
         self._check(self._lib.dvr3d_b200_set_wait_limit(self._h, int(polls)))
+
+    def split_gemm(self, a, b, nslice: int = 2) -> np.ndarray:
+        """a^T b on the tensor cores from split-BF16 operands (dvr3d_b200_split_gemm):
+        a is k x m, b is k x n (FP64); nslice 1 = one BF16 product, 2 = BF16x3."""
+        a = np.asfortranarray(np.asarray(a, dtype=np.float64))
+        b = np.asfortranarray(np.asarray(b, dtype=np.float64))
+        if a.ndim != 2 or b.ndim != 2 or a.shape[0] != b.shape[0]:
+            raise ValueError("a (k x m) and b (k x n) must share k")
+        k, m = a.shape
+        n = b.shape[1]
+        c = np.zeros((m, n), dtype=np.float64, order="F")
+        dp = C.POINTER(C.c_double)
+        self._check(self._lib.dvr3d_b200_split_gemm(
+            self._h, m, n, k, a.ctypes.data_as(dp), k, b.ctypes.data_as(dp), k, int(nslice),
+            c.ctypes.data_as(dp), max(m, 1)))
+        return c
 
     def set_pes(self, params) -> None:
         p = np.ascontiguousarray(np.asarray(params, dtype=np.float64))

@@ -41,6 +41,7 @@ DVR3D_PES_MORSE_SUM_NPARAM = 13
 
 DVR3D_PREC_FP64 = 0
 DVR3D_PREC_MIXED_DAVIDSON = 1
+DVR3D_PREC_SPLIT_BF16 = 2
 
 _DECK_INTS_1 = ["zpham", "zprad", "zp1d", "zp2d", "zpmin", "zpvec", "zlmat", "zcut", "zrot",
                 "zperp", "zembed", "zlin", "zmors1", "zmors2", "zladd", "ztwod", "zvec", "zall",
@@ -91,7 +92,8 @@ class Result(C.Structure):
                 ("evec", C.POINTER(C.c_double)), ("evec_cap", C.c_size_t),
                 ("h3", C.POINTER(C.c_double)), ("h3_cap", C.c_size_t),
                 ("path", C.c_int), ("matvecs", C.c_int), ("lp_pairs", C.c_int),
-                ("lp_loss_first", C.c_double), ("lp_loss_last", C.c_double)]
+                ("lp_loss_first", C.c_double), ("lp_loss_last", C.c_double),
+                ("low_iterations", C.c_int), ("low_matvecs", C.c_int)]
 
 
 def header_entry_points() -> list[str]:
@@ -123,6 +125,9 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "dvr3d_b200_last_error": (C.c_char_p, [vp]),
         "dvr3d_b200_set_stream": (C.c_int, [vp, vp]),
         "dvr3d_b200_set_wait_limit": (C.c_int, [vp, C.c_longlong]),
+        "dvr3d_b200_split_gemm": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, P(C.c_double), C.c_longlong,
+                                            P(C.c_double), C.c_longlong, C.c_int, P(C.c_double),
+                                            C.c_longlong]),
         "dvr3d_b200_parse_deck": (C.c_int, [C.c_char_p, P(Deck)]),
         "dvr3d_b200_set_pes": (C.c_int, [vp, C.c_int, P(C.c_double), C.c_int]),
         "dvr3d_b200_set_pes_grid": (C.c_int, [vp, P(C.c_double), C.c_size_t]),

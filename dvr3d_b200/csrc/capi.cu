@@ -12,6 +12,13 @@
 #include "eig_dense.cuh"
 #include "learned_precond.cuh"
 #include "pipeline.cuh"
+#include "tc_gemm.cuh"
+
+#define CK(x)                                          \
+    do {                                               \
+        cudaError_t e_ = (x);                          \
+        if (e_ != cudaSuccess) throw CudaFail{e_, #x}; \
+    } while (0)
 
 using dvr3d::CudaFail;
 using dvr3d::HostError;
@@ -354,6 +361,56 @@ int dvr3d_b200_set_wait_limit(dvr3d_ctx *ctx, long long polls) {
     if (!ctx || polls < 0) return DVR3D_ERR_ARG;
     ctx->wait_limit = (unsigned long long)polls;
     return DVR3D_OK;
+}
+
+int dvr3d_b200_split_gemm(dvr3d_ctx *ctx, int m, int n, int k, const double *a, long long lda, const double *b,
+                          long long ldb, int nslice, double *c, long long ldc) {
+    if (!ctx || m < 0 || n < 0 || k < 1 || !a || !b || !c || lda < k || ldb < k || ldc < m ||
+        (nslice != 1 && nslice != 2))
+        return DVR3D_ERR_ARG;
+    if (m == 0 || n == 0) return DVR3D_OK;
+    return guarded(ctx, [&]() -> int {
+        cudaSetDevice(ctx->device);
+        cudaStream_t st = ctx->stream;
+        const long long lds = (k + 7) / 8 * 8;
+        double *da = ctx->arena.get_t<double>("sg_a", (size_t)m * k), *db = ctx->arena.get_t<double>("sg_b", (size_t)n * k);
+        double *dc = ctx->arena.get_t<double>("sg_c", (size_t)m * n);
+        auto *ah = ctx->arena.get_t<__nv_bfloat16>("sg_ah", (size_t)m * lds);
+        auto *al = ctx->arena.get_t<__nv_bfloat16>("sg_al", (size_t)m * lds);
+        auto *bh = ctx->arena.get_t<__nv_bfloat16>("sg_bh", (size_t)n * lds);
+        auto *bl = ctx->arena.get_t<__nv_bfloat16>("sg_bl", (size_t)n * lds);
+        int *err = ctx->arena.get_t<int>("sg_err", 1);
+        CK(cudaMemcpy2DAsync(da, sizeof(double) * k, a, sizeof(double) * lda, sizeof(double) * k, m,
+                             cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpy2DAsync(db, sizeof(double) * k, b, sizeof(double) * ldb, sizeof(double) * k, n,
+                             cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+        CK(dvr3d::launch_split_bf16(da, k, m, k, ah, al, lds, st));
+        CK(dvr3d::launch_split_bf16(db, k, n, k, bh, bl, lds, st));
+        dvr3d::TcGemm g;
+        g.M = m;
+        g.N = n;
+        g.K = k;
+        g.nslice = nslice;
+        g.A_hi = ah;
+        g.A_lo = al;
+        g.lda = lds;
+        g.B_hi = bh;
+        g.B_lo = bl;
+        g.ldb = lds;
+        g.C = dc;
+        g.cm = 1;
+        g.cn = m;
+        g.err = err;
+        CK(dvr3d::launch_tc_gemm(g, st));
+        int err_host = 0;
+        CK(cudaMemcpyAsync(&err_host, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpy2DAsync(c, sizeof(double) * ldc, dc, sizeof(double) * m, sizeof(double) * m, n,
+                             cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (err_host != 0) return fail_ctx(ctx, DVR3D_ERR_NOCONV, "tensor-core pipeline wait timed out");
+        return DVR3D_OK;
+    });
 }
 
 namespace {

@@ -27,6 +27,7 @@
 #include "learned_precond.cuh"
 #include "pipeline.cuh"
 #include "small_syev.cuh"
+#include "tc_gemm.cuh"
 
 #define CK(x)                                          \
     do {                                               \
@@ -202,16 +203,19 @@ double lp_train_loss(dvr3d_ctx *ctx, const double *w, double *grad) {
 }
 
 // ---------------------------------------------------------------- Davidson
-bool davidson_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contracted &C, const dvr3d_options &opt,
-                    int nwant, int mode, double *lp_w, double *wv_dev, std::vector<double> &rn_host,
-                    double *evec_dev, DavidsonStats &stats) {
+bool davidson_solve(dvr3d_ctx *ctx, const H3Op &op, const Contracted &C, const dvr3d_options &opt, int nwant,
+                    int mode, double *lp_w, double *wv_dev, std::vector<double> &rn_host, double *evec_dev,
+                    DavidsonStats &stats) {
     cudaStream_t st = ctx->stream;
     const int N = C.N;
-    if (ldh & 1) return false;
-    int bs = std::min(kDavidsonMaxBlock, nwant + std::max(8, nwant / 2));
+    const bool split = (op.H3 == nullptr);
+    if (split ? (!op.hi || !op.lo) : (op.ldh & 1)) return false;
+    int bs = nwant <= kDavidsonMaxLevels ? std::min(kDavidsonMaxBlock, nwant + std::max(8, nwant / 2))
+                                         : nwant + std::max(16, nwant / 4);
     bs += (bs & 1);
     const int keep = 2 * bs, mmax = 3 * bs;
-    if (mmax > kSmallSyevMax || mmax >= N) return false;
+    if (mmax >= N) return false;
+    const bool big_rr = mmax > kSmallSyevMax;  // Rayleigh-Ritz on the dense eigensolver
     const double tolE = (opt.tol_cm > 0.0 ? opt.tol_cm : 1.0e-4) / 2.19474624e5;
     const int max_iter = opt.max_iter > 0 ? opt.max_iter : 300;
     const long long ld = rup(N, 8);
@@ -219,7 +223,8 @@ bool davidson_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contr
     double *V = A("dv_V", ld * mmax), *HV = A("dv_HV", ld * mmax);
     double *V2 = A("dv_V2", ld * keep), *HV2 = A("dv_HV2", ld * keep);
     double *X = A("dv_X", ld * bs), *HX = A("dv_HX", ld * bs), *R = A("dv_R", ld * bs), *Tc = A("dv_T", ld * bs);
-    double *G = A("dv_G", (size_t)mmax * mmax), *Y = A("dv_Y", (size_t)mmax * mmax), *th = A("dv_th", mmax);
+    const long long ldg_max = big_rr ? rup(mmax, 8) : mmax;
+    double *G = A("dv_G", (size_t)ldg_max * mmax), *Y = A("dv_Y", (size_t)mmax * mmax), *th = A("dv_th", mmax);
     double *rn = A("dv_rn", bs), *proj = A("dv_proj", (size_t)mmax * bs);
     double *Gb = A("dv_Gb", 64 * 64), *Gi = A("dv_Gi", 64 * 64);
     double *cn0 = A("dv_cn0", bs), *cn1 = A("dv_cn1", bs), *ones = A("dv_ones", bs);
@@ -228,19 +233,27 @@ bool davidson_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contr
         CK(cudaMemcpyAsync(ones, o.data(), sizeof(double) * bs, cudaMemcpyHostToDevice, st));
         CK(cudaStreamSynchronize(st));
     }
-    double *work = A("dv_work", (size_t)std::max<long long>(64LL * mmax * mmax, 16LL * N * bs));
-    double *ssw = A("dv_ssw", (size_t)small_syev_work_doubles(kSmallSyevMax));
-    int *err = ctx->arena.get_t<int>("dv_err", 2);
+    double *work = A("dv_work", (size_t)std::max<long long>(std::min<long long>(64LL * mmax * mmax, 1LL << 22),
+                                                          16LL * N * bs));
+    double *ssw = big_rr ? nullptr : A("dv_ssw", (size_t)small_syev_work_doubles(kSmallSyevMax));
+    int *err = ctx->arena.get_t<int>("dv_err", 3);
     int *ssn = ctx->arena.get_t<int>("dv_ssn", 1);
     long long *ssoff = ctx->arena.get_t<long long>("dv_ssoff", 1);
-    CK(cudaMemsetAsync(err, 0, 2 * sizeof(int), st));
+    CK(cudaMemsetAsync(err, 0, 3 * sizeof(int), st));
     CK(cudaMemsetAsync(ssoff, 0, sizeof(long long), st));
+    // BF16 slices of the vectors multiplied on the tensor cores (split form)
+    const long long ldvb = rup(N, 8);
+    __nv_bfloat16 *vb_hi = nullptr, *vb_lo = nullptr;
+    if (split) {
+        vb_hi = ctx->arena.get_t<__nv_bfloat16>("dv_vbh", (size_t)ldvb * mmax);
+        vb_lo = ctx->arena.get_t<__nv_bfloat16>("dv_vbl", (size_t)ldvb * mmax);
+    }
     // channel blocks; the start block is the bs lowest channel modes (approximate
     // eigenvectors of H3 in which the coupling between channels is left out)
     ChanPrec cp;
     std::vector<double> lam;
     std::vector<int> mch;
-    channel_setup(ctx, H3, ldh, C, cp, &lam, &mch);
+    channel_setup(ctx, op, C, cp, &lam, &mch);
     {
         std::vector<int> order(N);
         std::iota(order.begin(), order.end(), 0);
@@ -264,7 +277,13 @@ bool davidson_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contr
         CK(cudaGetLastError());
         CK(cudaStreamSynchronize(st));
     }
-    auto syev = [&](const double *Gm, int m, double *w, double *Z) {
+    // Rayleigh-Ritz eigensolve of G (m x m, ldg): eigenvalues w (ascending), eigenvectors Z
+    // (ld m; at least the `keep` lowest)
+    auto rr_eig = [&](double *Gm, long long ldg, int m, double *w, double *Z) {
+        if (big_rr) {
+            dense_lowest(ctx, Gm, ldg, m, std::min(m, keep), true, w, Z, m, "dvrr_", false, nullptr);
+            return;
+        }
         CK(cudaMemcpyAsync(ssn, &m, sizeof(int), cudaMemcpyHostToDevice, st));
         SmallSyev p{};
         p.nmat = 1;
@@ -279,6 +298,107 @@ bool davidson_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contr
         p.workoff = ssoff;
         CK(launch_small_syev(p, m, st));
     };
+    // HV[:, c0:c0+nc] = H3 V[:, c0:c0+nc]: BF16x3 tensor-core GEMM (split form, phase 1), the
+    // matrix-free FP64 operator (split form, residual correction), or the FP64 DMMA GEMM
+    int phase = split ? 1 : 2;
+    auto hv_product = [&](int c0, int nc) {
+        if (nc <= 0) return;
+        if (split && phase == 1) {
+            CK(launch_split_bf16(V + (size_t)c0 * ld, ld, nc, N, vb_hi, vb_lo, ldvb, st));
+            TcGemm g;
+            g.M = N;
+            g.N = nc;
+            g.K = N;
+            g.nslice = 2;
+            g.A_hi = op.hi;
+            g.A_lo = op.lo;
+            g.lda = op.ld;
+            g.B_hi = vb_hi;
+            g.B_lo = vb_lo;
+            g.ldb = ldvb;
+            g.C = HV + (size_t)c0 * ld;
+            g.cm = 1;
+            g.cn = ld;
+            g.err = err + 2;
+            CK(launch_tc_gemm(g, st));
+            stats.low_matvecs += nc;
+        } else if (split) {
+            apply_h3_fp64(ctx, C, V + (size_t)c0 * ld, ld, nc, HV + (size_t)c0 * ld, ld);
+        } else {
+            GemmOp hv;
+            hv.M = N;
+            hv.N = nc;
+            hv.K = N;
+            hv.A = op.H3;
+            hv.lda = op.ldh;
+            hv.B = V + (size_t)c0 * ld;
+            hv.ldb = ld;
+            hv.C = HV + (size_t)c0 * ld;
+            hv.ldc = ld;
+            gemm_split(hv, 600, work, st);
+        }
+        stats.matvecs += nc;
+    };
+    // orthonormalise Tb (N x nb, nb <= 64) in place: Cholesky-QR twice
+    auto cholqr = [&](double *Tb, int nb) {
+        for (int pass = 0; pass < 2; ++pass) {
+            GemmOp q;
+            q.M = nb;
+            q.N = nb;
+            q.K = N;
+            q.A = Tb;
+            q.lda = ld;
+            q.ta = true;
+            q.B = Tb;
+            q.ldb = ld;
+            q.C = Gb;
+            q.ldc = nb;
+            gemm_split(q, 256, work, st);
+            CK(launch_chol_small(Gb, nb, Gi, 1.0e-24, err + 1, st));
+            GemmOp s2;
+            s2.M = N;
+            s2.N = nb;
+            s2.K = nb;
+            s2.A = Tb;
+            s2.lda = ld;
+            s2.B = Gi;
+            s2.ldb = 64;
+            s2.tb = true;
+            s2.C = Tb;
+            s2.ldc = ld;
+            gemm_split(s2, 0, work, st);
+        }
+    };
+    // Tb -= W (W^T Tb), twice (W: N x nw orthonormal columns)
+    auto project_out = [&](const double *W, int nw, double *Tb, int nb) {
+        for (int pass = 0; pass < 2; ++pass) {
+            GemmOp c;
+            c.M = nw;
+            c.N = nb;
+            c.K = N;
+            c.A = W;
+            c.lda = ld;
+            c.ta = true;
+            c.B = Tb;
+            c.ldb = ld;
+            c.C = proj;
+            c.ldc = nw;
+            gemm_split(c, 600, work, st);
+            GemmOp u;
+            u.M = N;
+            u.N = nb;
+            u.K = nw;
+            u.alpha = -1.0;
+            u.beta = 1.0;
+            u.A = W;
+            u.lda = ld;
+            u.B = proj;
+            u.ldb = nw;
+            u.C = Tb;
+            u.ldc = ld;
+            gemm_split(u, 0, work, st);
+        }
+    };
     const int max_snaps = 16;
     const char *trace_env = std::getenv("DVR3D_DAV_TRACE");
     const bool trace = trace_env && trace_env[0] == '1';
@@ -288,20 +408,11 @@ bool davidson_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contr
     int m = bs, nnew = bs;
     std::vector<double> thh(mmax), rnh(bs);
     bool done = false;
+    double rprev = HUGE_VAL;
     int it = 0;
     for (; it < max_iter; ++it) {
-        GemmOp hv;  // HV[:, m-nnew:m] = H3 V[:, m-nnew:m]
-        hv.M = N;
-        hv.N = nnew;
-        hv.K = N;
-        hv.A = H3;
-        hv.lda = ldh;
-        hv.B = V + (size_t)(m - nnew) * ld;
-        hv.ldb = ld;
-        hv.C = HV + (size_t)(m - nnew) * ld;
-        hv.ldc = ld;
-        gemm_split(hv, 600, work, st);
-        stats.matvecs += nnew;
+        hv_product(m - nnew, nnew);
+        const long long ldg = big_rr ? rup(m, 8) : m;
         GemmOp g;  // G = V^T HV
         g.M = m;
         g.N = m;
@@ -312,9 +423,9 @@ bool davidson_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contr
         g.B = HV;
         g.ldb = ld;
         g.C = G;
-        g.ldc = m;
+        g.ldc = ldg;
         gemm_split(g, 600, work, st);
-        syev(G, m, th, Y);
+        rr_eig(G, ldg, m, th, Y);
         GemmOp x;  // X = V Y[:, :bs], HX = HV Y[:, :bs]
         x.M = N;
         x.N = bs;
@@ -332,21 +443,38 @@ bool davidson_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contr
         DVR3D_COUNT_LAUNCH(1);
         residual_kernel<<<bs, 256, 0, st>>>(X, HX, ld, th, N, R, rn);
         CK(cudaGetLastError());
-        CK(cudaMemcpyAsync(thh.data(), th, sizeof(double) * m, cudaMemcpyDeviceToHost, st));
+        const int nth = big_rr ? std::min(m, keep) : m;
+        int herr[3] = {0, 0, 0};
+        CK(cudaMemcpyAsync(thh.data(), th, sizeof(double) * nth, cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpyAsync(rnh.data(), rn, sizeof(double) * bs, cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(herr, err, sizeof(herr), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
-        note_d2h(sizeof(double) * (m + bs));
+        note_d2h(sizeof(double) * (nth + bs) + sizeof(herr));
+        if (herr[2] != 0) break;  // a tensor-core pipeline wait timed out: give up (the caller falls back)
         int nconv = 0;
+        double rmax = 0.0;
         for (int j = 0; j < nwant; ++j) {
             double gap = thh[j + 1] - thh[j];
             if (j > 0) gap = std::min(gap, thh[j] - thh[j - 1]);
             const double bound = rnh[j] * rnh[j] / std::max(gap, rnh[j]);
             if (bound <= tolE && std::isfinite(bound)) ++nconv;
+            rmax = std::max(rmax, rnh[j]);
         }
         if (trace)
-            std::fprintf(stderr, "davidson it %d m %d converged %d/%d max residual %.3e theta0 %.8f\n", it, m, nconv,
-                         nwant, *std::max_element(rnh.begin(), rnh.begin() + nwant), thh[0]);
-        if (nconv == nwant) {
+            std::fprintf(stderr, "davidson it %d phase %d m %d converged %d/%d max residual %.3e theta0 %.10f\n", it,
+                         phase, m, nconv, nwant, rmax, thh[0]);
+        if (phase == 1) {
+            ++stats.low_iterations;
+            if (nconv == nwant || !(rmax < 0.7 * rprev) || it + 1 >= max_iter / 2) {
+                // residual correction: the whole basis multiplied by the FP64 operator; the
+                // next pass redoes the Rayleigh-Ritz step with these products
+                phase = 2;
+                hv_product(0, m);
+                nnew = 0;
+                continue;
+            }
+            rprev = rmax;
+        } else if (nconv == nwant) {
             done = true;
             break;
         }
@@ -383,65 +511,18 @@ bool davidson_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contr
         colnorm_kernel<<<bs, 256, 0, st>>>(Tc, ld, N, cn0);
         normalize_or_refill_kernel<<<bs, 256, 0, st>>>(Tc, ld, N, cn0, ones, 1.0e-300, 17u * it + 1u);
         for (int sweep = 0; sweep < 2; ++sweep) {
-        for (int pass = 0; pass < 2; ++pass) {
-            GemmOp c;  // proj = V^T Tc ; Tc -= V proj
-            c.M = m;
-            c.N = bs;
-            c.K = N;
-            c.A = V;
-            c.lda = ld;
-            c.ta = true;
-            c.B = Tc;
-            c.ldb = ld;
-            c.C = proj;
-            c.ldc = m;
-            gemm_split(c, 600, work, st);
-            GemmOp u;
-            u.M = N;
-            u.N = bs;
-            u.K = m;
-            u.alpha = -1.0;
-            u.beta = 1.0;
-            u.A = V;
-            u.lda = ld;
-            u.B = proj;
-            u.ldb = m;
-            u.C = Tc;
-            u.ldc = ld;
-            gemm_split(u, 0, work, st);
+            project_out(V, m, Tc, bs);
+            // a correction (nearly) inside span(V) would make the block singular: replace it
+            // by a random direction and orthogonalise once more
+            DVR3D_COUNT_LAUNCH(2);
+            colnorm_kernel<<<bs, 256, 0, st>>>(Tc, ld, N, cn1);
+            normalize_or_refill_kernel<<<bs, 256, 0, st>>>(Tc, ld, N, cn1, ones, 1.0e-8, 31u * it + 5u + sweep);
         }
-        // a correction (nearly) inside span(V) would make the block singular: replace it
-        // by a random direction and orthogonalise once more
-        DVR3D_COUNT_LAUNCH(2);
-        colnorm_kernel<<<bs, 256, 0, st>>>(Tc, ld, N, cn1);
-        normalize_or_refill_kernel<<<bs, 256, 0, st>>>(Tc, ld, N, cn1, ones, 1.0e-8, 31u * it + 5u + sweep);
-        }
-        for (int pass = 0; pass < 2; ++pass) {
-            GemmOp q;
-            q.M = bs;
-            q.N = bs;
-            q.K = N;
-            q.A = Tc;
-            q.lda = ld;
-            q.ta = true;
-            q.B = Tc;
-            q.ldb = ld;
-            q.C = Gb;
-            q.ldc = bs;
-            gemm_split(q, 256, work, st);
-            CK(launch_chol_small(Gb, bs, Gi, 1.0e-24, err + 1, st));
-            GemmOp s2;
-            s2.M = N;
-            s2.N = bs;
-            s2.K = bs;
-            s2.A = Tc;
-            s2.lda = ld;
-            s2.B = Gi;
-            s2.ldb = 64;
-            s2.tb = true;
-            s2.C = Tc;
-            s2.ldc = ld;
-            gemm_split(s2, 0, work, st);
+        // orthonormal block, 64 columns at a time
+        for (int c0 = 0; c0 < bs; c0 += 64) {
+            const int nb = std::min(64, bs - c0);
+            if (c0 > 0) project_out(Tc, c0, Tc + (size_t)c0 * ld, nb);
+            cholqr(Tc + (size_t)c0 * ld, nb);
         }
         int qe = 0;
         CK(cudaMemcpyAsync(&qe, err + 1, sizeof(int), cudaMemcpyDeviceToHost, st));

@@ -19,6 +19,7 @@
 #include "gemm64.cuh"
 #include "learned_precond.cuh"
 #include "pipeline.cuh"
+#include "tc_gemm.cuh"
 
 #define CK(x)                                          \
     do {                                               \
@@ -523,19 +524,21 @@ __global__ void resid_kernel(const double *R, const double *Z, const double *w, 
 
 // ---------------------------------------------------------------- channel blocks of H3
 namespace {
-__global__ void chan_gather_kernel(const double *H, long long ldh, const int *idx, const int *off,
-                                   const long long *qoff, const int *n, double *A) {
+// H null: the entries come from the split-BF16 slices (hi + lo).
+__global__ void chan_gather_kernel(const double *H, const __nv_bfloat16 *hi, const __nv_bfloat16 *lo, long long ldh,
+                                   const int *idx, const int *off, const long long *qoff, const int *n, double *A) {
     const int c = blockIdx.y, nc = n[c];
     const int *ix = idx + off[c];
     double *a = A + qoff[c];
     for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < nc * nc; t += gridDim.x * blockDim.x) {
         const int p = t % nc, q = t / nc;
-        a[t] = H[(size_t)ix[q] * ldh + ix[p]];
+        const size_t e = (size_t)ix[q] * ldh + ix[p];
+        a[t] = H ? H[e] : (double)__bfloat162float(hi[e]) + (double)__bfloat162float(lo[e]);
     }
 }
 }  // namespace
 
-void channel_setup(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contracted &C, ChanPrec &cp,
+void channel_setup(dvr3d_ctx *ctx, const H3Op &op, const Contracted &C, ChanPrec &cp,
                    std::vector<double> *lam_host, std::vector<int> *chan_of_mode) {
     cudaStream_t st = ctx->stream;
     const int N = C.N, nb = C.nblocks;
@@ -566,7 +569,8 @@ void channel_setup(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contra
     double *A = ctx->arena.get_t<double>("ch_A", (size_t)qt);
     double *Q = ctx->arena.get_t<double>("ch_Q", (size_t)qt);
     DVR3D_COUNT_LAUNCH(1);
-    chan_gather_kernel<<<dim3((unsigned)((nmax * nmax + 255) / 256), kmax), 256, 0, st>>>(H3, ldh, didx, doff, dq, dn, A);
+    chan_gather_kernel<<<dim3((unsigned)((nmax * nmax + 255) / 256), kmax), 256, 0, st>>>(
+        op.H3, op.hi, op.lo, op.H3 ? op.ldh : op.ld, didx, doff, dq, dn, A);
     CK(cudaGetLastError());
     BatchDesc bd{kmax, dn, dq, dv};
     double *d = ctx->arena.get_t<double>("ch_d", N), *e = ctx->arena.get_t<double>("ch_e", N);
@@ -956,6 +960,9 @@ void solve_contracted(dvr3d_ctx *ctx, const BlockPlan &p, const Contracted &C, c
     }
     if (res.eval && res.eval_cap < meval) throw HostError{DVR3D_ERR_BUFFER, "eval buffer smaller than min(neval, N)"};
     const bool mixed = (opt.precision == DVR3D_PREC_MIXED_DAVIDSON);
+    const bool split_form = (opt.precision == DVR3D_PREC_SPLIT_BF16);
+    res.low_iterations = 0;
+    res.low_matvecs = 0;
     auto finish_times = [&](double &ms1, double &ms2, double &ms3) {
         CK(cudaStreamSynchronize(st));
         float a = 0, b = 0, c = 0;
@@ -983,42 +990,96 @@ void solve_contracted(dvr3d_ctx *ctx, const BlockPlan &p, const Contracted &C, c
             t_d2h += (long long)sizeof(double) * N * meval;
         }
     };
-    // ---- assembly (bloc3d / mkham3+loadh)
-    const long long ldh = mixed ? round_up(N, 8) : N;
-    double *H3 = ctx->arena.get_t<double>("h3", (size_t)ldh * N);
-    AsmParams ap{};
-    ap.Vt = C.Vt;
-    ap.ldv = C.ldv;
-    ap.n = N;
-    ap.g = C.g;
-    ap.T = C.T;
-    ap.ldt = C.ldt;
-    ap.e2 = C.e2;
-    ap.H = H3;
-    ap.ldh = ldh;
-    launch_assemble_h3(ap, st);
-    CK(cudaGetLastError());
+    // ---- assembly (bloc3d / mkham3+loadh): FP64 DMMA, or BF16x3 on the tensor cores into the
+    // split matrix of the split-BF16 form
+    const long long ldh = (mixed || split_form) ? round_up(N, 8) : N;
+    double *H3 = nullptr;
+    auto assemble_fp64 = [&]() {
+        H3 = ctx->arena.get_t<double>("h3", (size_t)ldh * N);
+        AsmParams ap{};
+        ap.Vt = C.Vt;
+        ap.ldv = C.ldv;
+        ap.n = N;
+        ap.g = C.g;
+        ap.T = C.T;
+        ap.ldt = C.ldt;
+        ap.e2 = C.e2;
+        ap.H = H3;
+        ap.ldh = ldh;
+        launch_assemble_h3(ap, st);
+        CK(cudaGetLastError());
+    };
+    H3Op op;
+    int *tc_err = nullptr;
+    if (split_form) {
+        const long long ldk = round_up(C.P, 8);
+        auto *vh = ctx->arena.get_t<__nv_bfloat16>("vt_hi", (size_t)ldk * N);
+        auto *vl = ctx->arena.get_t<__nv_bfloat16>("vt_lo", (size_t)ldk * N);
+        auto *hh = ctx->arena.get_t<__nv_bfloat16>("h3_hi", (size_t)ldh * N);
+        auto *hl = ctx->arena.get_t<__nv_bfloat16>("h3_lo", (size_t)ldh * N);
+        tc_err = ctx->arena.get_t<int>("tc_err", 1);
+        CK(cudaMemsetAsync(tc_err, 0, sizeof(int), st));
+        CK(launch_split_bf16(C.Vt, C.ldv, N, C.P, vh, vl, ldk, st));
+        TcGemm g;
+        g.M = N;
+        g.N = N;
+        g.K = C.P;
+        g.nslice = 2;
+        g.A_hi = g.B_hi = vh;
+        g.A_lo = g.B_lo = vl;
+        g.lda = g.ldb = ldk;
+        g.epilogue = kTcAssemble;
+        g.g = C.g;
+        g.T = C.T;
+        g.ldt = C.ldt;
+        g.e2 = C.e2;
+        g.H_hi = hh;
+        g.H_lo = hl;
+        g.ldh = ldh;
+        g.err = tc_err;
+        CK(launch_tc_gemm(g, st));
+        op.hi = hh;
+        op.lo = hl;
+        op.ld = ldh;
+        int herr = 0;
+        CK(cudaMemcpyAsync(&herr, tc_err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (herr != 0) throw HostError{DVR3D_ERR_NOCONV, "tensor-core assembly: a pipeline wait timed out"};
+    } else {
+        assemble_fp64();
+        op.H3 = H3;
+        op.ldh = ldh;
+    }
     CK(cudaEventRecord(ctx->ev[2], st));
     if (opt.want_h3 && res.h3) {
         if (res.h3_cap < (size_t)N * N) throw HostError{DVR3D_ERR_BUFFER, "h3 buffer too small"};
-        CK(cudaMemcpy2DAsync(res.h3, (size_t)N * sizeof(double), H3, (size_t)ldh * sizeof(double),
+        const double *src = H3;
+        if (split_form) {  // the split matrix as the solver uses it: hi + lo
+            double *hs = ctx->arena.get_t<double>("h3_sum", (size_t)ldh * N);
+            CK(launch_split_sum(op.hi, op.lo, ldh, N, hs, st));
+            src = hs;
+        }
+        CK(cudaMemcpy2DAsync(res.h3, (size_t)N * sizeof(double), src, (size_t)ldh * sizeof(double),
                              (size_t)N * sizeof(double), N, cudaMemcpyDeviceToHost, st));
         t_d2h += (long long)sizeof(double) * N * N;
     }
     if (opt.learned_precond == 1 && !ctx->lp_trained)
         throw HostError{DVR3D_ERR_ARG, "no trained preconditioner (train one with learned_precond = 2 or load weights)"};
-    if (mixed && meval <= kDavidsonMaxLevels) {
-        // ---- few levels: block-Davidson with the channel-block preconditioner
+    if ((mixed && meval <= kDavidsonMaxLevels) || split_form) {
+        // ---- block-Davidson with the channel-block preconditioner (few levels in the mixed
+        // form; any number in the split-BF16 form)
         double *wv = ctx->arena.get_t<double>("dt_w", meval);
         double *Z = (res.evec || wave) ? ctx->arena.get_t<double>("dv_z", (size_t)N * meval) : nullptr;
         double *lpw = ctx->arena.get_t<double>("lp_w", kLpParams);
         const int mode = opt.learned_precond == 2 ? 2 : (opt.learned_precond == 1 ? 1 : 0);
         std::vector<double> rn;
         DavidsonStats ds;
-        const bool ok = davidson_solve(ctx, H3, ldh, C, opt, meval, mode, lpw, wv, rn, Z, ds);
+        const bool ok = davidson_solve(ctx, op, C, opt, meval, mode, lpw, wv, rn, Z, ds);
         check_dev_err(ctx, ev_err(ctx), "batched inverse iteration (channel blocks)");
         res.iterations = ds.iterations;
         res.matvecs = ds.matvecs;
+        res.low_iterations = ds.low_iterations;
+        res.low_matvecs = ds.low_matvecs;
         if (ds.trained) {
             ctx->lp_trained = true;
             res.lp_pairs = ds.pairs;
@@ -1040,11 +1101,15 @@ void solve_contracted(dvr3d_ctx *ctx, const BlockPlan &p, const Contracted &C, c
             res.dom_bytes = 0.0;
             res.dom_flops = 2.0 * (double)N * N * ds.matvecs;
             res.dom_launches = 0;
-            std::snprintf(res.dom_kernel, sizeof(res.dom_kernel), "gemm_pipe_kernel");
+            std::snprintf(res.dom_kernel, sizeof(res.dom_kernel), split_form ? "tc_gemm_kernel" : "gemm_pipe_kernel");
             res.launches = (int)(g_kernel_launches - launches0);
             res.h2d_bytes = t_h2d;
             res.d2h_bytes = t_d2h;
             return;
+        }
+        if (split_form) {
+            res.fallback = 1;
+            assemble_fp64();  // the dense FP64 fallback below works on the assembled FP64 matrix
         }
     }
     if (mixed) {

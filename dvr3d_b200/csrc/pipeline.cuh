@@ -3,6 +3,7 @@
 
 #include <chrono>
 
+#include <cuda_bf16.h>
 #include <cuda_runtime.h>
 
 #include <map>
@@ -95,31 +96,57 @@ struct WaveOut {
     std::vector<double> psi;
 };
 
-// Channel blocks of the assembled H3 (full storage, ldh) and their eigen-decompositions,
-// with the per-mode features of the learned correction (learned_precond.cuh).
-// lam_host / chan_of_mode (optional): the channel eigenvalues and the channel of every mode.
-void channel_setup(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contracted &C, ChanPrec &cp,
+// The assembled H3 as the iterative solvers see it: FP64 full symmetric storage (H3, ldh
+// even), or, in the split-BF16 form (H3 null), its BF16 slices hi + lo (full symmetric
+// storage, ld a multiple of 8) for the tensor-core products, the FP64 products then coming
+// from the matrix-free operator of the contracted basis (apply_h3_fp64).
+struct H3Op {
+    const double *H3 = nullptr;
+    long long ldh = 0;
+    const __nv_bfloat16 *hi = nullptr, *lo = nullptr;
+    long long ld = 0;
+};
+
+// Y (N x nvec, ldy) = H3 X (ldx) in FP64 without H3: per block g of the contracted basis
+//   Y_g = C_g^T sum_g' T[g, g'] (C_g' X_g')  +  e2_g o X_g
+// (three DMMA GEMM launches: block products, the block mix by T, the transposed block
+// products; then the diagonal). 4 P N + 2 P G^2 flops per vector instead of 2 N^2.
+void apply_h3_fp64(dvr3d_ctx *ctx, const Contracted &C, const double *X, long long ldx, int nvec, double *Y,
+                   long long ldy);
+
+// Channel blocks of the assembled H3 and their eigen-decompositions, with the per-mode
+// features of the learned correction (learned_precond.cuh). lam_host / chan_of_mode
+// (optional): the channel eigenvalues and the channel of every mode.
+void channel_setup(dvr3d_ctx *ctx, const H3Op &op, const Contracted &C, ChanPrec &cp,
                    std::vector<double> *lam_host = nullptr, std::vector<int> *chan_of_mode = nullptr);
 
-// Block-Davidson for the lowest `nwant` (<= kDavidsonMaxLevels) levels of the assembled H3
-// (full symmetric storage, ldh even) with the channel-block preconditioner. mode 0: exact
-// channel inverse; 1: with the learned correction (parameters lp_w, device); 2: exact channel
-// inverse, record (residual, correction) pairs and fit the network into lp_w. Writes the
-// levels (device wv_dev), FP64 residual norms and optionally the vectors (N x nwant, ld N).
-// Returns false when it does not converge within its limits (the caller falls back).
+// Block-Davidson for the lowest `nwant` levels of H3 with the channel-block preconditioner.
+// mode 0: exact channel inverse; 1: with the learned correction (parameters lp_w, device);
+// 2: exact channel inverse, record (residual, correction) pairs and fit the network into
+// lp_w. Block b = nwant + max(8, nwant/2) up to kDavidsonMaxLevels levels (b <= 48), else
+// nwant + max(16, nwant/4); Rayleigh-Ritz on the shared-memory eigensolver up to 160 basis
+// vectors, on the dense FP64 eigensolver beyond.
+// Split-BF16 form: the products H3 V are BF16x3 tensor-core GEMMs until the largest residual
+// stops falling (by less than 30 % in an iteration); then the residual correction: the
+// products of the whole basis are recomputed in FP64 (apply_h3_fp64) and the iteration goes
+// on with FP64 products until the FP64 residual test holds. Writes the levels (device wv_dev),
+// FP64 residual norms and optionally the vectors (N x nwant, ld N). Returns false when it
+// does not converge within its limits (the caller falls back).
 constexpr int kDavidsonMaxLevels = 32;
 constexpr int kDavidsonMaxBlock = 48;
 struct DavidsonStats {
     int iterations = 0;
     int matvecs = 0;
+    int low_iterations = 0;    // split-BF16 form: iterations with tensor-core products
+    int low_matvecs = 0;       //                  vectors multiplied on the tensor cores
     double max_resid = 0.0;
     int pairs = 0;             // training pairs recorded (mode 2)
     bool trained = false;
     double loss_first = 0.0, loss_last = 0.0;
 };
-bool davidson_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, const Contracted &C, const dvr3d_options &opt,
-                    int nwant, int mode, double *lp_w, double *wv_dev, std::vector<double> &rn_host,
-                    double *evec_dev, DavidsonStats &stats);
+bool davidson_solve(dvr3d_ctx *ctx, const H3Op &op, const Contracted &C, const dvr3d_options &opt, int nwant,
+                    int mode, double *lp_w, double *wv_dev, std::vector<double> &rn_host, double *evec_dev,
+                    DavidsonStats &stats);
 
 // Training loss of the learned correction (and, when grad is not null, its gradient, device)
 // at parameters w (device) on the pairs recorded by the context's last training solve.

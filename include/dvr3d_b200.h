@@ -95,12 +95,20 @@ typedef enum dvr3d_pes_kind {
 /* ---- solve options and results ------------------------------------------------------- */
 typedef enum dvr3d_precision {
     DVR3D_PREC_FP64 = 0,             /* plain FP64 GPU path: dense FP64 final eigensolve  */
-    DVR3D_PREC_MIXED_DAVIDSON = 1    /* iterative lowest-level solve on the FP64 tensor
+    DVR3D_PREC_MIXED_DAVIDSON = 1,   /* iterative lowest-level solve on the FP64 tensor
                                         cores: block-Davidson (<= 32 levels; channel-block
                                         preconditioner, optionally with the learned
                                         correction) or shift-invert block Krylov; FP64
                                         Rayleigh-Ritz and residual judge; dense FP64
                                         fallback                                          */
+    DVR3D_PREC_SPLIT_BF16 = 2        /* split-BF16 form: assembly and H3 V as BF16x3
+                                        products on the BF16 tensor cores (tcgen05, FP32
+                                        accumulation), block-Davidson for any number of
+                                        levels with FP64 Rayleigh-Ritz and residual norms;
+                                        once the BF16x3 residuals stop falling, the FP64
+                                        residual correction (products of the basis with
+                                        the matrix-free FP64 operator) until the FP64
+                                        residual test holds; dense FP64 fallback           */
 } dvr3d_precision;
 
 typedef enum dvr3d_path {
@@ -158,6 +166,8 @@ typedef struct dvr3d_result {
     int lp_pairs;           /* training pairs recorded when learned_precond = 2              */
     double lp_loss_first;   /* learned preconditioner loss before / after training          */
     double lp_loss_last;
+    int low_iterations;     /* split-BF16 form: Davidson iterations on tensor-core products */
+    int low_matvecs;        /* split-BF16 form: vectors multiplied on the BF16 tensor cores */
 } dvr3d_result;
 
 /* ---- entry points ----------------------------------------------------------------- */
@@ -180,6 +190,17 @@ int dvr3d_b200_set_stream(dvr3d_ctx *ctx, void *stream);
  * defaults); a small limit lets a caller check that the waits end. No counterpart in the
  * reference (which has no device waits). */
 int dvr3d_b200_set_wait_limit(dvr3d_ctx *ctx, long long polls);
+
+/* The split-BF16 tensor-core product of the mixed-precision form, on host buffers:
+ *     c (m x n, ldc) = a^T b,   a: k x m (lda), b: k x n (ldb), all column-major FP64.
+ * Each operand is split on the device into BF16 slices (x ~= hi + lo); nslice = 1 keeps hi
+ * only (one BF16 product), nslice = 2 forms the BF16x3 product hi.hi + hi.lo + lo.hi with FP32
+ * accumulation in tensor memory (relative error of order 2^-16 of |a|^T |b|). The same
+ * kernel assembles the contracted Hamiltonian (mkham3 :2508-2523, bloc3d :3455-3505) and
+ * forms H3 V in the mixed-precision solve. No counterpart in the reference; exposed for tests
+ * and for callers that want the product itself. */
+int dvr3d_b200_split_gemm(dvr3d_ctx *ctx, int m, int n, int k, const double *a, long long lda, const double *b,
+                          long long ldb, int nslice, double *c, long long ldc);
 
 /* Reads a job deck in the reference's stdin format: namelist PRT (dvr3d :65, defaults of
  * block data :158-167), card 2 (insize :232), card 3 (:238), title (:372) and the setcon

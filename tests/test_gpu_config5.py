@@ -66,3 +66,14 @@ def test_config5_preconditioner_trained_on_k0_reused_for_k1_k2(ctx, cfg5):
         lv = fx[f"levels_k{k}"][:nl]
         assert np.abs(reuse.eval - lv).max() * AUTOCM <= 1e-3
         assert np.abs(base.eval - lv).max() * AUTOCM <= 1e-3
+
+
+def test_config5_split_form_k1_against_oracle(ctx, cfg5):
+    """The split-BF16 form (BF16x3 assembly and products, FP64 residual correction) on the
+    N ~ 20500 block k = 1: the lowest 24 levels within 1e-3 cm-1 of the oracle."""
+    w, fx = cfg5
+    d = parse_deck(w.deck)
+    ctx.set_pes(w.pes)
+    r = ctx.solve(d, 1, precision=dvr3d_b200.DVR3D_PREC_SPLIT_BF16, nlevels=24)
+    assert r.fallback == 0 and r.extra["low_matvecs"] > 0
+    assert np.abs(r.eval - fx["levels_k1"][:24]).max() * AUTOCM <= 1e-3
