@@ -6,7 +6,7 @@ Legendre points, cut-offs EMAX1 = 50000 / EMAX2 = 40000 cm-1 (final basis N = 12
 seeded synthetic Morse + P1/P2 surface (dvr3d_b200/configs.py:config4), lowest 500 levels.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--precision mixed|fp64]
+                    [--precision mixed|fp64|split]
 
 Multi-GPU: one process per GPU (torchrun), each rank solves its own replica of the
 workload (the path has no exchange step); value = solves of all ranks / max elapsed.
@@ -328,7 +328,10 @@ def main() -> int:
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed"])
+    ap.add_argument("--precision", default="auto", choices=["auto", "fp64", "mixed", "split"],
+                    help="mixed (default): the chosen form; fp64: the plain path; split (--profile-solve "
+                         "only): the split-BF16 tensor-core form")
+    ap.add_argument("--levels", type=int, default=500, help="--profile-solve: levels of the solve")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-solve", action="store_true",
                     help="one solve of the workload and nothing else (for ncu captures of its kernels)")
@@ -351,13 +354,17 @@ def main() -> int:
         ctx = dvr3d_b200.Context(0)
         w = configs.config4()
         ctx.set_pes(w.pes)
-        prec = dvr3d_b200.DVR3D_PREC_FP64 if args.precision == "fp64" else dvr3d_b200.DVR3D_PREC_MIXED_DAVIDSON
-        r = ctx.solve(parse_deck(w.deck), 0, precision=prec, nlevels=500)
+        prec = {"fp64": dvr3d_b200.DVR3D_PREC_FP64, "split": dvr3d_b200.DVR3D_PREC_SPLIT_BF16}.get(
+            args.precision, dvr3d_b200.DVR3D_PREC_MIXED_DAVIDSON)
+        r = ctx.solve(parse_deck(w.deck), 0, precision=prec, nlevels=args.levels)
         print(json.dumps({"profile_solve": WORKLOAD, "nham3": r.nham3, "stage_ms": list(r.stage_ms)}), flush=True)
         ctx.close()
         return 0
     if args.impl == "reference":
         return run_reference(args, rank, world)
+    if args.precision == "split":
+        print(json.dumps({"error": "--precision split is a --profile-solve mode (the headline arms are mixed and fp64)"}))
+        return 2
 
     import torch
 

@@ -52,6 +52,8 @@ def k_blocks(deck: Deck) -> list[int]:
     zrot = bool(deck.zrot) and jrot != 0
     if jrot == 0:
         kmin = 0
+    if deck.zperp and deck.idia == -2:  # KMIN carries the Q symmetry; k starts at 0 (:257-261)
+        kmin = 1 if jrot else 0
     if zrot:
         zbisc = deck.idia == -2
         if kmin != 0 and not zbisc:

@@ -10,8 +10,9 @@ namespace dvr3d {
 
 namespace {
 
-// Radau 2D Hamiltonian of one angle (blc2d1 :3125-3219) in the symmetrised pair basis
-// (alpha <= beta - ipar, beta outer), full symmetric storage. One thread per element.
+// Radau 2D Hamiltonian of one angle (blc2d1 :3125-3219; z_blc2d1 :4038-4127 for the z-perp
+// embedding) in the symmetrised pair basis (alpha <= beta - ipar, beta outer), full
+// symmetric storage. One thread per element.
 __global__ void radau_build_kernel(RadauBuild rb, double *H) {
     const int g = blockIdx.y;
     const int n = rb.n;
@@ -25,7 +26,16 @@ __global__ void radau_build_kernel(RadauBuild rb, double *H) {
     const int np = rb.npnt;
     auto hr = [&](int i, int j) { return rb.hr[(size_t)j * np + i]; };
     double h = 0.0;
-    if (row == col && rb.jrot != 0) {
+    if (row == col && rb.jrot != 0 && rb.zperp) {
+        // z-perp J > 0 diagonal (:4059-4085): k^2/4 (+ the Q term x / (1 - x^2) for k = 1) and
+        // the s (J(J+1) - k^2)/4 / (1 - x^2) term; doubled for alpha = beta as in the reference
+        double fact = rb.term;
+        if (rb.kz == 1) fact = fact + rb.term3 * x / (1.0 - x * x);
+        const double fact2 = rb.term2 / (1.0 - x * x);
+        const double wa = 0.5 / (rb.r[a] * rb.r[a] * rb.urr1), wb = 0.5 / (rb.r[b] * rb.r[b] * rb.urr1);
+        const double ws = (wa + wb) * fact + (wa + wb) * fact2;
+        h += (a == b && rb.ipar == 0) ? 2.0 * ws : ws;
+    } else if (row == col && rb.jrot != 0) {
         // J > 0 diagonal term (:3155-3177); doubled for alpha = beta as in the reference
         double fact = rb.term + rb.term2 / (1.0 - x);
         if (rb.kz == 1) fact += rb.term3 * (1.0 + x) / (1.0 - x);

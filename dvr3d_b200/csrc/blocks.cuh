@@ -10,6 +10,7 @@ namespace dvr3d {
 // Radau (idia = -2) 2D blocks: one per angle, n = npnt (npnt + 1 - 2 ipar) / 2.
 struct RadauBuild {
     int n, npnt, ipar, jrot, kz;
+    int zperp;                // z axis perpendicular to the plane: z_blc2d1's J > 0 terms
     const int *pa, *pb;       // pair -> (alpha, beta) radial indices, 0-based
     const double *r;          // radial grid (npnt)
     const double *hr;         // DVR kinetic matrix xk1 (npnt x npnt)

@@ -321,6 +321,107 @@ void gauss_laguerre(int n, double alf, double cc, std::vector<double> &x, std::v
     }
 }
 
+// ln Gamma(x) by the six-term Lanczos series the reference uses (gammln :4265-4286); its
+// coefficients are kept so that the z-perp weights and polynomial norms match the
+// reference's to the last digits it prints.
+double lanczos_lngamma(double xx) {
+    constexpr double c[6] = {76.18009173, -86.50532033, 24.01409822, -1.231739516, 0.120858003e-2, -0.536382e-5};
+    double x = xx - 1.0;
+    const double t = x + 5.5;
+    const double lead = (x + 0.5) * std::log(t) - t;
+    double ser = 1.0;
+    for (double cj : c) {
+        x += 1.0;
+        ser += cj / x;
+    }
+    return lead + std::log(2.50662827465 * ser);
+}
+
+// n-point Gauss-Jacobi rule for the weight (1-x)^a (1+x)^b, points descending from +1
+// (gaujac :4190-4263): Newton iteration on the three-term recurrence, stopping at 3e-14 or
+// 10 steps, from the reference's asymptotic first guesses (one of its constants is a REAL*4
+// literal, 0.012, and is used as such).
+void gauss_jacobi_full(int n, double a, double b, std::vector<double> &x, std::vector<double> &w) {
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    const double dn = n, nn = (double)(n * n), ab = a + b;
+    double z = 0.0;
+    for (int i = 0; i < n; ++i) {
+        const int ii = i + 1;
+        if (ii == 1) {
+            const double an = a / dn, bn = b / dn;
+            z = 1.0 - (1.0 + a) * (2.78 / (4.0 + nn) + 0.768 * an / dn) /
+                          (1.0 + 1.48 * an + 0.96 * bn + 0.452 * an * an + 0.83 * an * bn);
+        } else if (ii == 2) {
+            z -= (1.0 - z) * ((4.1 + a) / ((1.0 + a) * (1.0 + 0.156 * a))) *
+                 (1.0 + 0.06 * (dn - 8.0) * (1.0 + 0.12 * a) / dn) *
+                 (1.0 + (double)0.012f * b * (1.0 + 0.25 * std::fabs(a)) / dn);
+        } else if (ii == 3) {
+            z -= (x[0] - z) * ((1.67 + 0.28 * a) / (1.0 + 0.37 * a)) * (1.0 + 0.22 * (dn - 8.0) / dn) *
+                 (1.0 + 8.0 * b / ((6.28 + b) * nn));
+        } else if (ii == n - 1) {
+            z += (z - x[n - 4]) * ((1.0 + 0.235 * b) / (0.766 + 0.119 * b)) *
+                 (1.0 / (1.0 + 0.639 * (dn - 4.0) / (1.0 + 0.71 * (dn - 4.0)))) *
+                 (1.0 / (1.0 + 20.0 * a / ((7.5 + a) * nn)));
+        } else if (ii == n) {
+            z += (z - x[n - 3]) * ((1.0 + 0.37 * b) / (1.67 + 0.28 * b)) *
+                 (1.0 / (1.0 + 0.22 * (double)(n - 8) / dn)) * (1.0 / (1.0 + 8.0 * a / ((6.28 + a) * nn)));
+        } else {
+            z = 3.0 * x[i - 1] - 3.0 * x[i - 2] + x[i - 3];
+        }
+        double p1 = 0.0, p2 = 0.0, dp = 0.0, t = 0.0;
+        for (int it = 0; it < 10; ++it) {
+            t = 2.0 + ab;
+            p1 = (a - b + t * z) / 2.0;
+            p2 = 1.0;
+            for (int j = 2; j <= n; ++j) {
+                const double p3 = p2;
+                p2 = p1;
+                t = 2.0 * j + ab;
+                const double c1 = 2.0 * j * (j + ab) * (t - 2.0);
+                const double c2 = (t - 1.0) * (a * a - b * b + t * (t - 2.0) * z);
+                const double c3 = 2.0 * (j - 1 + a) * (j - 1 + b) * t;
+                p1 = (c2 * p2 - c3 * p3) / c1;
+            }
+            dp = (dn * (a - b - t * z) * p1 + 2.0 * (dn + a) * (dn + b) * p2) / (t * (1.0 - z * z));
+            const double zold = z;
+            z = zold - p1 / dp;
+            if (std::fabs(z - zold) <= 3.0e-14) break;
+        }
+        x[i] = z;
+        w[i] = std::exp(lanczos_lngamma(a + dn) + lanczos_lngamma(b + dn) - lanczos_lngamma(dn + 1.0) -
+                        lanczos_lngamma(dn + ab + 1.0)) *
+               t * std::pow(2.0, ab) / (dp * p2);
+    }
+}
+
+// Normalised Jacobi polynomials P_l^(a,b)(x_i), l = 0..lmax, at the points x (jac_basis
+// :4136-4154, jacgt :4158-4186, norms2 :4288-4308); column i of the result holds point i.
+std::vector<double> jacobi_poly_basis(const std::vector<double> &x, int npt, int lmax, double a, double b) {
+    const double lam = a + b + 1.0;
+    std::vector<double> out((size_t)(lmax + 1) * npt);
+    std::vector<double> nrm(lmax + 1);
+    for (int l = 0; l <= lmax; ++l)
+        nrm[l] = std::sqrt(std::pow(2.0, -lam) * (2.0 * l + lam) *
+                           std::exp(lanczos_lngamma(l + 1.0) + lanczos_lngamma(l + lam) - lanczos_lngamma(l + a + 1.0) -
+                                    lanczos_lngamma(l + b + 1.0)));
+    for (int i = 0; i < npt; ++i) {
+        double *col = &out[(size_t)i * (lmax + 1)];
+        col[0] = 1.0;
+        if (lmax >= 1) col[1] = (a - b + (lam + 1.0) * x[i]) / 2.0;
+        for (int l = 2; l <= lmax; ++l) {
+            const int m = l - 1;  // recurrence coefficients of degree m
+            const double d1 = 2.0 * (m + 1.0) * (m + lam) * (2.0 * m + lam - 1.0);
+            const double d2 = (2.0 * m + lam) * (a * a - b * b);
+            const double d3 = (2.0 * m + lam - 1.0) * (2.0 * m + lam) * (2.0 * m + lam + 1.0);
+            const double d4 = 2.0 * (m + a) * (m + b) * (2.0 * m + lam + 1.0);
+            col[l] = ((d2 + d3 * x[i]) * col[l - 1] - d4 * col[l - 2]) / d1;
+        }
+        for (int l = 0; l <= lmax; ++l) col[l] *= nrm[l];
+    }
+    return out;
+}
+
 // Gauss-Jacobi (alpha = beta = nu) roots on the half range and weights, found by the
 // reference's downward sign scan from x=1 in REAL*4 steps of 1e-4 followed by Newton with
 // absolute stopping 1e-12 (jacobi :1635-1699, root :1702-1721, recur :1722-1744).
@@ -470,6 +571,7 @@ void k_range(const dvr3d_deck &d, int &kd, int &ku) {
     int jrot = std::abs(d.jrot), kmin = d.kmin;
     bool zrot = d.zrot && jrot != 0;
     if (jrot == 0) kmin = 0;
+    if (d.zperp && d.idia == -2) kmin = (jrot == 0) ? 0 : 1;  // KMIN is the Q symmetry (:257-261)
     if (zrot) {
         bool zbisc = (d.idia == -2);
         if (kmin != 0 && !zbisc) kmin = 1;
@@ -484,7 +586,7 @@ void k_range(const dvr3d_deck &d, int &kd, int &ku) {
 void plan_block(const dvr3d_deck &d, int kk, BlockPlan &p) {
     p = BlockPlan();
     if (d.ztwod) raise(DVR3D_ERR_UNSUPPORTED, "ztwod (fixed-angle 2D) is not on this path");
-    if (d.zperp) raise(DVR3D_ERR_UNSUPPORTED, "zperp (mkmain z-perpendicular) is not on this path");
+    if (d.zperp && d.idia == 2) raise(DVR3D_ERR_ARG, "ZPERP is for Radau coordinates (IDIA = -2), not IDIA = 2");
     if (d.ncoord == 2) raise(DVR3D_ERR_UNSUPPORTED, "ncoord=2 (rigid diatom) is not on this path");
     if (!d.zquad2) raise(DVR3D_ERR_UNSUPPORTED, "zquad2=F is not on this path");
     if (!d.zmors1 || !d.zmors2) raise(DVR3D_ERR_UNSUPPORTED, "spherical oscillators (zmors=F) are not on this path");
@@ -501,11 +603,22 @@ void plan_block(const dvr3d_deck &d, int kk, BlockPlan &p) {
         zrot = false;
     }
     int idvr = nalf;
+    const bool zperp = d.zperp != 0;
+    int iq = 0;
     if (idia == -2) {
         npnt1 = npnt2;
         ztheta = false;
         if (jrot != 0) zbisc = true;
+        if (zperp) {  // Q symmetry from the KMIN card field, k from 0 (:255-261)
+            iq = kmin;
+            kmin = (jrot == 0) ? 0 : 1;
+        }
     }
+    // the z-perp angular grid holds 2 nang2 Gauss-Jacobi points in an array of nalf (:945):
+    // an odd nalf, or a later k block with fewer angles (zladd = F), would read points the
+    // reference leaves undefined
+    if (zperp && (idia != -2 || (nalf & 1) || !d.zladd))
+        raise(DVR3D_ERR_UNSUPPORTED, "zperp needs IDIA = -2, an even NALF and ZLADD = T");
     if (npnt1 < 2 || npnt2 < 2 || nalf < 2 || npnt1 > 120 || npnt2 > 120 || nalf > 250)
         raise(DVR3D_ERR_ARG, "grid sizes out of range (2..120 radial, 2..250 angular)");
     const int nalf2 = (nalf + 1) / 2;
@@ -625,7 +738,7 @@ void plan_block(const dvr3d_deck &d, int kk, BlockPlan &p) {
         } else {
             kz = 1;
             kmin = 0;
-            ipar = (ipar + jrot) % 2;
+            if (!zperp) ipar = (ipar + jrot) % 2;
         }
         if (d.zladd || kz == kd) {
             nidvr = idvr;
@@ -653,93 +766,133 @@ void plan_block(const dvr3d_deck &d, int kk, BlockPlan &p) {
             else npntc = nidvr;
         }
         if (idia <= -2 && zrot) {
-            if (kz > kd) ipar = (ipar + 1) % 2;
+            if (kz > kd && !zperp) ipar = (ipar + 1) % 2;
             max2d = ipar > 0 ? max2d2 : max2d1;
             max3d = ipar > 0 ? max3d2 : max3d1;
         }
     }
-    // Gauss-(associated) Legendre points (:887-944) and allpts (:1747-1772)
-    double tswalf = std::pow(2.0, kz + kz + 1) / (double)(kz + 1);
-    for (int ia = 1; ia <= kz; ++ia) tswalf = tswalf * (double)ia / (double)(kz + ia + 1);
-    gauss_jacobi_half(nang, nang2, (double)kz, tswalf, p.xhalf, p.whalf, p.cswalf);
-    p.tswalf = tswalf;
-    if (std::fabs((p.cswalf - tswalf) / tswalf) > 1.0e-8)
-        raise(DVR3D_ERR_QUADRATURE, "Gauss-Legendre points & weights in error");
-    p.xalf.assign(idvr, 0.0);
-    p.walf.assign(idvr, 0.0);
-    const double scale = (double)std::max(1, idia);
-    for (int i = 0; i < nang2; ++i) {
-        const double wv = std::sqrt(scale * p.whalf[i]);
-        if (idia == 2) {
-            p.xalf[i] = p.xhalf[i];
-            p.walf[i] = wv;
-        } else {
-            p.xalf[nang - 1 - i] = p.xhalf[i];
-            p.walf[nang - 1 - i] = wv;
-            p.xalf[i] = -p.xhalf[i];
-            p.walf[i] = wv;
+    const int maxleg = nalf - 1;
+    if (zperp) {
+        // Gauss-Jacobi points with alpha = beta = sqrt((J(J+1) - k^2)/2), normalised Jacobi
+        // polynomials, square-rooted weights (ccmain :945-966); L matrix with the weights
+        // (j+1+alpha)(j+alpha) from j = 0 (lmatrx :1870-1903)
+        const double rj = jrot, rk = kz;
+        p.alf = std::sqrt(0.5 * ((rj * rj + rj) - rk * rk));
+        std::vector<double> xg, wg;
+        gauss_jacobi_full(2 * nang2, p.alf, p.alf, xg, wg);
+        p.xalf.assign(idvr, 0.0);
+        p.walf.assign(idvr, 0.0);
+        for (int i = 0; i < idvr && i < (int)xg.size(); ++i) {
+            p.xalf[i] = xg[i];
+            p.walf[i] = std::sqrt(wg[i]);
         }
-    }
-    // normalised associated Legendre polynomial parts (asleg :1775-1843)
-    const int maxleg = nalf - 1, m = kz;
-    const int nl = maxleg + lincr - m + 1;  // orders j = m .. maxleg+lincr
-    std::vector<double> pl((size_t)std::max(nl, 2) * nidvr, 0.0);
-    for (int i = 0; i < nidvr; ++i) {
-        double pmm = 1.0, f = 1.0;
-        for (int j = 1; j <= m; ++j) {
-            pmm = -pmm * f;
-            f += 2.0;
-        }
-        double *col = &pl[(size_t)i * std::max(nl, 2)];
-        col[0] = pmm;
-        double pmmp1 = p.xalf[i] * (m + m + 1) * pmm;
-        col[1] = pmmp1;
-        int ll = 1;
-        for (int l = 2 + m; l <= maxleg + lincr; ++l) {
-            const double pll = (p.xalf[i] * (double)(l + l - 1) * pmmp1 - (double)(l + m - 1) * pmm) / (double)(l - m);
-            pmm = pmmp1;
-            pmmp1 = pll;
-            col[++ll] = pll;
-        }
-    }
-    std::vector<double> pnorm(std::max(nl, 1));
-    for (int j = m, jj = 0; j <= maxleg + lincr; ++j, ++jj) {
-        double f = 1.0;
-        for (int i = j - m + 1; i <= j + m; ++i) f *= (double)i;
-        pnorm[jj] = std::sqrt(((double)j + (double)j + 1.0) / (f + f));
-    }
-    for (int i = 0; i < nidvr; ++i)
-        for (int jj = 0; jj < nl; ++jj) pl[(size_t)i * std::max(nl, 2) + jj] *= pnorm[jj];
-    p.pleg_walf.assign((size_t)(maxleg + 1) * nidvr, 0.0);
-    for (int i = 0; i < nidvr; ++i)
-        for (int jj = 0; jj <= maxleg && jj < nl; ++jj)
-            p.pleg_walf[(size_t)i * (maxleg + 1) + jj] = pl[(size_t)i * std::max(nl, 2) + jj] * p.walf[i];
-    // angular kinetic matrix L(k,k') (lmatrx :1846-1911, in-plane)
-    const int jdia = std::max(1, idia);
-    const int ipar0 = (idia == 2 && ipar == 1) ? 1 : 0;
-    int jstart = kz, jj0 = -jdia;
-    if (jstart % jdia != ipar0) {
-        ++jj0;
-        ++jstart;
-    }
-    p.xlmatr.assign((size_t)idvr * idvr, 0.0);
-    const int ld = std::max(nl, 2);
-    for (int k = 0; k < nidvr; ++k) {
-        for (int kp = k; kp < nidvr; ++kp) {
-            double s = 0.0;
-            int jj = jj0;
-            for (int j = jstart; j <= maxleg + lincr; j += jdia) {
-                jj += jdia;
-                s += pl[(size_t)k * ld + jj] * pl[(size_t)kp * ld + jj] * (double)((j + 1) * j);
+        p.whalf.assign(wg.begin(), wg.begin() + nang2);
+        p.xhalf.assign(xg.begin(), xg.begin() + nang2);
+        const std::vector<double> pj = jacobi_poly_basis(p.xalf, nidvr, maxleg, p.alf, p.alf);
+        p.pleg_walf.assign((size_t)(maxleg + 1) * nidvr, 0.0);
+        for (int i = 0; i < nidvr; ++i)
+            for (int l = 0; l <= maxleg; ++l)
+                p.pleg_walf[(size_t)i * (maxleg + 1) + l] = pj[(size_t)i * (maxleg + 1) + l] * p.walf[i];
+        p.xlmatr.assign((size_t)idvr * idvr, 0.0);
+        for (int k = 0; k < nidvr; ++k)
+            for (int kp = k; kp < nidvr; ++kp) {
+                double sum = 0.0;
+                for (int j = 0; j <= maxleg; ++j)
+                    sum += pj[(size_t)k * (maxleg + 1) + j] * pj[(size_t)kp * (maxleg + 1) + j] *
+                           ((j + 1 + p.alf) * (j + p.alf));
+                const double v = sum * p.walf[k] * p.walf[kp];
+                p.xlmatr[(size_t)k * idvr + kp] = v;
+                p.xlmatr[(size_t)kp * idvr + k] = v;
             }
-            const double v = s * p.walf[k] * p.walf[kp];
-            p.xlmatr[(size_t)k * idvr + kp] = v;
-            p.xlmatr[(size_t)kp * idvr + k] = v;
+    } else {
+        // Gauss-(associated) Legendre points (:887-944) and allpts (:1747-1772)
+        double tswalf = std::pow(2.0, kz + kz + 1) / (double)(kz + 1);
+        for (int ia = 1; ia <= kz; ++ia) tswalf = tswalf * (double)ia / (double)(kz + ia + 1);
+        gauss_jacobi_half(nang, nang2, (double)kz, tswalf, p.xhalf, p.whalf, p.cswalf);
+        p.tswalf = tswalf;
+        if (std::fabs((p.cswalf - tswalf) / tswalf) > 1.0e-8)
+            raise(DVR3D_ERR_QUADRATURE, "Gauss-Legendre points & weights in error");
+        p.xalf.assign(idvr, 0.0);
+        p.walf.assign(idvr, 0.0);
+        const double scale = (double)std::max(1, idia);
+        for (int i = 0; i < nang2; ++i) {
+            const double wv = std::sqrt(scale * p.whalf[i]);
+            if (idia == 2) {
+                p.xalf[i] = p.xhalf[i];
+                p.walf[i] = wv;
+            } else {
+                p.xalf[nang - 1 - i] = p.xhalf[i];
+                p.walf[nang - 1 - i] = wv;
+                p.xalf[i] = -p.xhalf[i];
+                p.walf[i] = wv;
+            }
+        }
+        // normalised associated Legendre polynomial parts (asleg :1775-1843)
+        const int m = kz;
+        const int nl = maxleg + lincr - m + 1;  // orders j = m .. maxleg+lincr
+        std::vector<double> pl((size_t)std::max(nl, 2) * nidvr, 0.0);
+        for (int i = 0; i < nidvr; ++i) {
+            double pmm = 1.0, f = 1.0;
+            for (int j = 1; j <= m; ++j) {
+                pmm = -pmm * f;
+                f += 2.0;
+            }
+            double *col = &pl[(size_t)i * std::max(nl, 2)];
+            col[0] = pmm;
+            double pmmp1 = p.xalf[i] * (m + m + 1) * pmm;
+            col[1] = pmmp1;
+            int ll = 1;
+            for (int l = 2 + m; l <= maxleg + lincr; ++l) {
+                const double pll = (p.xalf[i] * (double)(l + l - 1) * pmmp1 - (double)(l + m - 1) * pmm) / (double)(l - m);
+                pmm = pmmp1;
+                pmmp1 = pll;
+                col[++ll] = pll;
+            }
+        }
+        std::vector<double> pnorm(std::max(nl, 1));
+        for (int j = m, jj = 0; j <= maxleg + lincr; ++j, ++jj) {
+            double f = 1.0;
+            for (int i = j - m + 1; i <= j + m; ++i) f *= (double)i;
+            pnorm[jj] = std::sqrt(((double)j + (double)j + 1.0) / (f + f));
+        }
+        for (int i = 0; i < nidvr; ++i)
+            for (int jj = 0; jj < nl; ++jj) pl[(size_t)i * std::max(nl, 2) + jj] *= pnorm[jj];
+        p.pleg_walf.assign((size_t)(maxleg + 1) * nidvr, 0.0);
+        for (int i = 0; i < nidvr; ++i)
+            for (int jj = 0; jj <= maxleg && jj < nl; ++jj)
+                p.pleg_walf[(size_t)i * (maxleg + 1) + jj] = pl[(size_t)i * std::max(nl, 2) + jj] * p.walf[i];
+        // angular kinetic matrix L(k,k') (lmatrx :1846-1911, in-plane)
+        const int jdia = std::max(1, idia);
+        const int ipar0 = (idia == 2 && ipar == 1) ? 1 : 0;
+        int jstart = kz, jj0 = -jdia;
+        if (jstart % jdia != ipar0) {
+            ++jj0;
+            ++jstart;
+        }
+        p.xlmatr.assign((size_t)idvr * idvr, 0.0);
+        const int ld = std::max(nl, 2);
+        for (int k = 0; k < nidvr; ++k) {
+            for (int kp = k; kp < nidvr; ++kp) {
+                double s = 0.0;
+                int jj = jj0;
+                for (int j = jstart; j <= maxleg + lincr; j += jdia) {
+                    jj += jdia;
+                    s += pl[(size_t)k * ld + jj] * pl[(size_t)kp * ld + jj] * (double)((j + 1) * j);
+                }
+                const double v = s * p.walf[k] * p.walf[kp];
+                p.xlmatr[(size_t)k * idvr + kp] = v;
+                p.xlmatr[(size_t)kp * idvr + k] = v;
+            }
         }
     }
     // J > 0 angular-momentum terms
     p.term = (double)(jrot * jrot + jrot - 2 * kz * kz);  // jhmain :1970
-    if (jrot != 0) {                                        // nfmain :3057-3064
+    if (jrot != 0 && zperp) {  // z_blc2d1 :4059-4073
+        const double rj = jrot, rk = kz;
+        p.nf_term = rk * rk / 4.0;                                           // k^2 / 4
+        p.nf_term2 = (1.0 - p.urr1 / p.ur1) * (rj * rj + rj - rk * rk) / 4.0;  // s (J(J+1) - k^2) / 4
+        p.nf_term3 = (iq == 0) ? -rj * (rj + 1.0) / 4.0 : rj * (rj + 1.0) / 4.0;
+    } else if (jrot != 0) {  // nfmain :3057-3064
         p.nf_term = (double)(jrot * jrot + jrot - kz * kz) / 8.0;
         p.nf_term2 = (double)(jrot * jrot + jrot - 3 * kz * kz) / 4.0;
         if (std::abs(kz) == 1) {
@@ -768,6 +921,8 @@ void plan_block(const dvr3d_deck &d, int kk, BlockPlan &p) {
     p.npntb = npntb;
     p.npntc = npntc;
     p.radau = (idia == -2);
+    p.zperp = zperp;
+    p.iq = iq;
     p.ztheta = ztheta;
     p.zr2r1 = d.zr2r1;
     p.zcut = d.zcut || zall;

@@ -29,6 +29,9 @@ struct BlockPlan {
     bool radau = false;   // idia == -2: nfmain path
     bool ztheta = false, zr2r1 = true, zcut = false, zall = false, zembed = true, zlin = false;
     bool zrot = false;
+    bool zperp = false;   // z axis perpendicular to the plane (mkmain :3934 instead of nfmain)
+    int iq = 0;           // z-perp Q symmetry (insize :255-261)
+    double alf = 0;       // z-perp Gauss-Jacobi exponent alpha = beta of this k (:945)
     // masses and radial constants (setcon)
     double g1 = 0, g2 = 0, ur1 = 0, ur2 = 0, urr1 = 0, urr2 = 0;
     double beta1 = 0, a1 = 0, beta2 = 0, a2 = 0;
@@ -49,7 +52,8 @@ struct BlockPlan {
     std::vector<double> pleg_walf;
     // J > 0 terms
     double term = 0;                   // jhmain :1970
-    double nf_term = 0, nf_term2 = 0, nf_term3 = 0;  // nfmain :3055-3064
+    double nf_term = 0, nf_term2 = 0, nf_term3 = 0;  // nfmain :3055-3064; z-perp: z_blc2d1 :4059-4073
+                                                     // (k^2/4, s (J(J+1)-k^2)/4, -+J(J+1)/4)
 };
 
 // Reads the job deck text (namelist PRT + cards). Throws HostError.

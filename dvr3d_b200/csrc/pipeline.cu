@@ -139,6 +139,7 @@ void radau_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
     rb.term = p.nf_term;
     rb.term2 = p.nf_term2;
     rb.term3 = p.nf_term3;
+    rb.zperp = p.zperp ? 1 : 0;
     rb.urr1 = p.urr1;
     rb.pes = ctx->pes;
     if (rb.pes.kind == DVR3D_PES_GRID) {
@@ -815,6 +816,7 @@ void radau_stage_batch(dvr3d_ctx *ctx, const std::vector<BlockPlan> &plans, cons
         rb.term = p.nf_term;
         rb.term2 = p.nf_term2;
         rb.term3 = p.nf_term3;
+        rb.zperp = p.zperp ? 1 : 0;
         rb.urr1 = p.urr1;
         rb.pes = pes[i];
         if (rb.pes.kind != DVR3D_PES_MORSE_SUM)

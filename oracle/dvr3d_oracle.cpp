@@ -76,6 +76,8 @@ struct Run {
     // COMMON /outp/ (hot-path subset)
     bool zrot, zembed, zmors1, zmors2, zcut, zall, zlin, zladd, zquad2, ztheta, zr2r1;
     bool zbisc, zperp, ztwod, zladd_;
+    int iq = 0;        // z-perp Q symmetry (insize :255-261)
+    double alf = 0.0;  // z-perp Gauss-Jacobi exponent alpha = beta of this k (ccmain :945-947)
     // COMMON /oupb/
     double xp0, xp1, xp2;
     // COMMON /split1/, /split2/, /mass/
@@ -172,7 +174,8 @@ void insize_setcon(Run &R, const dvr3d_deck &d) {
         R.xmass[i] = d.xmass[i];
         R.xmassr[i] = d.xmassr[i];
     }
-    if (R.ztwod || R.zperp || d.ncoord == 2) fail(DVR3D_ERR_UNSUPPORTED);
+    if (R.ztwod || d.ncoord == 2) fail(DVR3D_ERR_UNSUPPORTED);
+    if (R.zperp && R.idia == 2) fail(DVR3D_ERR_ARG);  // :367-371
     if (!R.zmors1 || !R.zmors2) fail(DVR3D_ERR_UNSUPPORTED);  // keint2 path not restated
     // :241-264
     R.zbisc = false;
@@ -188,7 +191,16 @@ void insize_setcon(Run &R, const dvr3d_deck &d) {
         R.zmors1 = R.zmors2;
         R.ztheta = false;
         if (R.jrot != 0) R.zbisc = true;
+        if (R.zperp) {  // :257-261
+            R.iq = R.kmin;
+            R.kmin = 1;
+            if (R.jrot == 0) R.kmin = 0;
+        }
     }
+    // the z-perp angular grid has 2 nang2 points in an array of nalf (gaujac at :945); an odd
+    // nalf, or a later k block with fewer angles (zladd = F), would read points the reference
+    // leaves undefined
+    if (R.zperp && (R.idia != -2 || (R.nalf & 1) || !R.zladd)) fail(DVR3D_ERR_UNSUPPORTED);
     R.nalf2 = (R.nalf + 1) / 2;  // :281
     R.ncoord = 3;
     R.maxleg = R.nalf - 1;  // :306-308
@@ -631,14 +643,15 @@ void asleg(Run &R) {
     }
 }
 
-// lmatrx :1846-1911 (in-plane branch) -> xlmatr(idvr,idvr) column-major
+// lmatrx :1846-1911 -> xlmatr(idvr,idvr) column-major (z-perp: j from 0 with the weights
+// (j+1+alf)(j+alf) of the Jacobi polynomials)
 void lmatrx(Run &R, int ipar0) {
     int idvr = R.idvr, nidvr = R.nidvr, lmax = R.maxleg;
     R.xlmatr.assign((size_t)idvr * idvr, 0.0);
-    int jstart = R.kz, iparam = R.lincr;
+    int jstart = R.zperp ? 0 : R.kz, iparam = R.zperp ? 0 : R.lincr;
     int jdia = std::max(1, R.idia);
     int jj0 = -jdia;
-    if (jstart % jdia != ipar0) {
+    if (!R.zperp && jstart % jdia != ipar0) {
         ++jj0;
         ++jstart;
     }
@@ -650,12 +663,124 @@ void lmatrx(Run &R, int ipar0) {
             int jj = jj0;
             for (int j = jstart; j <= lmax + iparam; j += jdia) {
                 jj = jj + jdia;
-                sumj1 = sumj1 + P(jj, k) * P(jj, kp) * (double)((j + 1) * j);
+                if (R.zperp)
+                    sumj1 = sumj1 + P(jj, k) * P(jj, kp) * ((j + 1 + R.alf) * (j + R.alf));
+                else
+                    sumj1 = sumj1 + P(jj, k) * P(jj, kp) * (double)((j + 1) * j);
             }
             double v = sumj1 * term * R.walf[kp];
             R.xlmatr[(size_t)k * idvr + kp] = v;
             R.xlmatr[(size_t)kp * idvr + k] = v;
         }
+    }
+}
+
+// gammln :4265-4286: log Gamma by the six-term Lanczos series of the reference (the
+// coefficients are the reference's; its weights and normalisations carry their ~1e-10 error).
+double gammln(double xx) {
+    static const double cof[6] = {76.18009173, -86.50532033, 24.01409822, -1.231739516, 0.120858003e-2,
+                                  -0.536382e-5};
+    const double stp = 2.50662827465;
+    double x = xx - 1.0;
+    double tmp = x + 5.5;
+    tmp = (x + 0.5) * std::log(tmp) - tmp;
+    double ser = 1.0;
+    for (int j = 0; j < 6; ++j) {
+        x = x + 1.0;
+        ser = ser + cof[j] / x;
+    }
+    return tmp + std::log(stp * ser);
+}
+
+// gaujac :4190-4263: n Gauss-Jacobi points (descending) and weights for weight
+// (1-x)^alf (1+x)^bet; Newton on the three-term recurrence from the reference's initial
+// guesses (its 0.012 is a REAL*4 literal).
+void gaujac(std::vector<double> &x, std::vector<double> &w, int n, double alf, double bet) {
+    const double eps = 3.0e-14;
+    const int maxit = 10;
+    const double c012 = (double)0.012f;
+    double z = 0.0, pp = 0.0, p2 = 0.0, temp = 0.0;
+    for (int i = 1; i <= n; ++i) {
+        const double dn = (double)n;
+        if (i == 1) {
+            const double an = alf / dn, bn = bet / dn;
+            const double r1 = (1.0 + alf) * (2.78 / (4.0 + (double)(n * n)) + 0.768 * an / dn);
+            const double r2 = 1.0 + 1.48 * an + 0.96 * bn + 0.452 * an * an + 0.83 * an * bn;
+            z = 1.0 - r1 / r2;
+        } else if (i == 2) {
+            const double r1 = (4.1 + alf) / ((1.0 + alf) * (1.0 + 0.156 * alf));
+            const double r2 = 1.0 + 0.06 * (dn - 8.0) * (1.0 + 0.12 * alf) / dn;
+            const double r3 = 1.0 + c012 * bet * (1.0 + 0.25 * std::fabs(alf)) / dn;
+            z = z - (1.0 - z) * r1 * r2 * r3;
+        } else if (i == 3) {
+            const double r1 = (1.67 + 0.28 * alf) / (1.0 + 0.37 * alf);
+            const double r2 = 1.0 + 0.22 * (dn - 8.0) / dn;
+            const double r3 = 1.0 + 8.0 * bet / ((6.28 + bet) * (double)(n * n));
+            z = z - (x[0] - z) * r1 * r2 * r3;
+        } else if (i == n - 1) {
+            const double r1 = (1.0 + 0.235 * bet) / (0.766 + 0.119 * bet);
+            const double r2 = 1.0 / (1.0 + 0.639 * (dn - 4.0) / (1.0 + 0.71 * (dn - 4.0)));
+            const double r3 = 1.0 / (1.0 + 20.0 * alf / ((7.5 + alf) * (double)(n * n)));
+            z = z + (z - x[n - 4]) * r1 * r2 * r3;
+        } else if (i == n) {
+            const double r1 = (1.0 + 0.37 * bet) / (1.67 + 0.28 * bet);
+            const double r2 = 1.0 / (1.0 + 0.22 * (double)(n - 8) / dn);
+            const double r3 = 1.0 / (1.0 + 8.0 * alf / ((6.28 + alf) * (double)(n * n)));
+            z = z + (z - x[n - 3]) * r1 * r2 * r3;
+        } else {
+            z = 3.0 * x[i - 2] - 3.0 * x[i - 3] + x[i - 4];
+        }
+        const double alfbet = alf + bet;
+        for (int its = 1; its <= maxit; ++its) {
+            temp = 2.0 + alfbet;
+            double p1 = (alf - bet + temp * z) / 2.0;
+            p2 = 1.0;
+            for (int j = 2; j <= n; ++j) {
+                const double p3 = p2;
+                p2 = p1;
+                temp = 2.0 * (double)j + alfbet;
+                const double c1 = 2.0 * (double)j * ((double)j + alfbet) * (temp - 2.0);
+                const double c2 = (temp - 1.0) * (alf * alf - bet * bet + temp * (temp - 2.0) * z);
+                const double c3 = 2.0 * ((double)(j - 1) + alf) * ((double)(j - 1) + bet) * temp;
+                p1 = (c2 * p2 - c3 * p3) / c1;
+            }
+            pp = (dn * (alf - bet - temp * z) * p1 + 2.0 * (dn + alf) * (dn + bet) * p2) / (temp * (1.0 - z * z));
+            const double z1 = z;
+            z = z1 - p1 / pp;
+            if (std::fabs(z - z1) <= eps) break;
+        }
+        x[i - 1] = z;
+        w[i - 1] = std::exp(gammln(alf + dn) + gammln(bet + dn) - gammln(dn + 1.0) - gammln(dn + alfbet + 1.0)) *
+                   temp * std::pow(2.0, alfbet) / (pp * p2);
+    }
+}
+
+// jac_basis :4136-4154 with jacgt :4158-4186 and norms2 :4288-4308: normalised Jacobi
+// polynomials P_i^(alf,bet)(x_n), i = 0..nb, n < nn -> basis (0:nb, nn) column-major
+void jac_basis(int nn, int nb, double alf, double bet, const std::vector<double> &x, std::vector<double> &basis) {
+    const double lmd = alf + bet + 1.0;
+    std::vector<double> norm(nb + 1);
+    for (int n = 0; n <= nb; ++n) {
+        const double a1 = gammln((double)(n + 1)), a2 = gammln((double)n + lmd);
+        const double a3 = gammln((double)n + alf + 1.0), a4 = gammln((double)n + bet + 1.0);
+        const double norm1 = std::pow(2.0, -lmd) * (2.0 * (double)n + lmd) * std::exp(a1 + a2 - a3 - a4);
+        norm[n] = std::sqrt(norm1);
+    }
+    std::vector<double> A1(nb + 1), A2(nb + 1), A3(nb + 1), A4(nb + 1);
+    for (int n = 1; n <= nb; ++n) {
+        A1[n] = 2.0 * (n + 1.0) * (n + lmd) * (2.0 * n + lmd - 1.0);
+        A2[n] = (2.0 * n + lmd) * (alf * alf - bet * bet);
+        A3[n] = (2.0 * n + lmd - 1.0) * (2.0 * n + lmd) * (2.0 * n + lmd + 1.0);
+        A4[n] = 2.0 * (n + alf) * (n + bet) * (2.0 * n + lmd + 1.0);
+    }
+    basis.assign((size_t)(nb + 1) * nn, 0.0);
+    std::vector<double> b(nb + 1);
+    for (int i = 0; i < nn; ++i) {
+        b[0] = 1.0;
+        if (nb >= 1) b[1] = (alf - bet + (lmd + 1.0) * x[i]) / 2.0;
+        for (int n = 2; n <= nb; ++n)
+            b[n] = ((A2[n - 1] + A3[n - 1] * x[i]) * b[n - 1] - A4[n - 1] * b[n - 2]) / A1[n - 1];
+        for (int n = 0; n <= nb; ++n) basis[(size_t)i * (nb + 1) + n] = b[n] * norm[n];
     }
 }
 
@@ -706,7 +831,7 @@ void ccmain_setup(Run &R, int kk) {
         } else {
             R.kz = 1;
             R.kmin = 0;
-            R.ipar = (R.ipar + R.jrot) % 2;
+            if (!R.zperp) R.ipar = (R.ipar + R.jrot) % 2;
         }
         if (R.zladd || R.kz == R.kd) {
             R.nidvr = R.idvr;
@@ -736,7 +861,7 @@ void ccmain_setup(Run &R, int kk) {
             else R.npntc = R.nidvr;
         }
         if (R.idia <= -2 && R.zrot) {  // :989-998
-            if (R.kz > R.kd) R.ipar = (R.ipar + 1) % 2;
+            if (R.kz > R.kd && !R.zperp) R.ipar = (R.ipar + 1) % 2;
             if (R.ipar > 0) {
                 R.max2d = R.max2d2;
                 R.max3d = R.max3d2;
@@ -745,6 +870,17 @@ void ccmain_setup(Run &R, int kk) {
                 R.max3d = max3d1;
             }
         }
+    }
+    if (R.zperp) {  // :945-966: Gauss-Jacobi points, Jacobi polynomials, square-rooted weights
+        const double rj = (double)R.jrot, rk = (double)R.kz;
+        R.alf = std::sqrt(0.5 * ((rj * rj + rj) - rk * rk));
+        R.xalf.assign(R.idvr, 0.0);
+        R.walf.assign(R.idvr, 0.0);
+        gaujac(R.xalf, R.walf, 2 * R.nang2, R.alf, R.alf);
+        jac_basis(R.nidvr, R.maxleg, R.alf, R.alf, R.xalf, R.pleg);
+        for (int i = 0; i < R.nidvr; ++i) R.walf[i] = std::sqrt(R.walf[i]);
+        lmatrx(R, 0);
+        return;
     }
     // Gauss-(associated) Legendre points for this k (:887-944)
     double realkz = (double)R.kz;
@@ -819,7 +955,63 @@ void blc2d1(const Run &R, int ig, double xcos, std::vector<double> &ham2, int nh
     }
 }
 
-// nfmain :3006-3121 with cut2dr :3323-3377, choosr :3223-3319, testiv :3380-3451,
+// z_blc2d1 :4038-4127 (z-perp embedding, mkmain :3934-4034) -> ham2 (nham2 x nham2)
+void z_blc2d1(const Run &R, int ig, double xcos, std::vector<double> &ham2, int nham2) {
+    int npnt = R.npnt, ipar = R.ipar;
+    const double factr2 = std::sqrt(0.5);
+    ham2.assign((size_t)nham2 * nham2, 0.0);
+    auto H = [&](int i, int j) -> double & { return ham2[(size_t)(j - 1) * nham2 + (i - 1)]; };
+    auto hr = [&](int i, int j) { return R.xk1[(size_t)(j - 1) * R.npnt1 + (i - 1)]; };
+    const std::vector<double> &r = R.r1;
+    if (R.jrot != 0) {
+        const double realj = (double)R.jrot, realkz = (double)R.kz;
+        const double term = (R.iq == 0) ? -realj * (realj + 1.0) / 4.0 : realj * (realj + 1.0) / 4.0;
+        double fact = (realkz * realkz) / 4.0;
+        if (R.kz == 1) fact = fact + term * xcos / (1.0 - xcos * xcos);
+        const double s = 1.0 - R.urr1 / R.ur1;
+        const double term2 = (realj * realj + realj - realkz * realkz) / 4.0;
+        const double fact2 = s * term2 * 1.0 / (1.0 - xcos * xcos);
+        int ia = 0;
+        double wsum = 0.0, wsum2 = 0.0;
+        for (int ibeta = 1; ibeta <= npnt; ++ibeta) {
+            for (int ialpha = 1; ialpha <= ibeta - ipar; ++ialpha) {
+                const double walpha = 0.5 / (r[ialpha - 1] * r[ialpha - 1] * R.urr1);
+                const double wbeta = 0.5 / (r[ibeta - 1] * r[ibeta - 1] * R.urr1);
+                wsum = (walpha + wbeta) * fact;
+                wsum2 = (walpha + wbeta) * fact2;
+                H(ialpha + ia, ialpha + ia) += wsum + wsum2;
+            }
+            ia = ia + ibeta - ipar;
+            if (ipar == 0) H(ia, ia) += wsum + wsum2;
+        }
+    }
+    const double q = (ipar == 1) ? -1.0 : 1.0;
+    int iap = 0;
+    for (int ibetap = 1; ibetap <= npnt; ++ibetap) {
+        int ia = 0;
+        for (int ibeta = 1; ibeta <= npnt; ++ibeta) {
+            for (int ialphp = 1; ialphp <= ibetap - ipar; ++ialphp) {
+                for (int ialpha = 1; ialpha <= ibeta - ipar; ++ialpha) {
+                    double &h = H(ialphp + iap, ialpha + ia);
+                    if (ibeta == ibetap) h = h + hr(ialphp, ialpha);
+                    if (ibeta == ialphp) h = h + q * hr(ibetap, ialpha);
+                    if (ialpha == ibetap) h = h + q * hr(ialphp, ibeta);
+                    if (ialpha == ialphp) h = h + hr(ibetap, ibeta);
+                    if (ialpha == ialphp && ibeta == ibetap)
+                        h = h + potv(R, r[ialpha - 1], r[ibeta - 1], xcos, ialpha - 1, ibeta - 1, ig);
+                    if (ialpha == ibetap && ibeta == ialphp)
+                        h = h + q * potv(R, r[ibeta - 1], r[ialpha - 1], xcos, ibeta - 1, ialpha - 1, ig);
+                    if (ialphp == ibetap) h = h * factr2;
+                    if (ialpha == ibeta) h = h * factr2;
+                }
+            }
+            ia = ia + ibeta - ipar;
+        }
+        iap = iap + ibetap - ipar;
+    }
+}
+
+// nfmain :3006-3121 (mkmain :3934-4034 for the z-perp embedding) with cut2dr :3323-3377, choosr :3223-3319, testiv :3380-3451,
 // bloc3d :3455-3505, blc2d2 :3509-3566, vecmul :3570-3595, diag3d :2661-2764.
 void nfmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     auto t0 = std::chrono::steady_clock::now();
@@ -849,7 +1041,10 @@ void nfmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     int npos = 1;
     for (int ig = 0; ig < nalf; ++ig) {
         R.tick();
-        blc2d1(R, ig, R.xalf[ig], ham2, nham2, term, term2, term3, xtscw);
+        if (R.zperp)
+            z_blc2d1(R, ig, R.xalf[ig], ham2, nham2);
+        else
+            blc2d1(R, ig, R.xalf[ig], ham2, nham2, term, term2, term3, xtscw);
         diag(ham2.data(), nham2, nham2, eig2.data());
         if (tr && tr->eig2all && (size_t)(ig + 1) * nham2 <= (size_t)tr->eig2all_cap)
             std::memcpy(tr->eig2all + (size_t)ig * nham2, eig2.data(), sizeof(double) * nham2);

@@ -2,8 +2,9 @@
 
 Reads the job decks and printed outputs shipped with the reference (ExoMol/dvr3d) and
 writes ``quadrature_kat.json`` next to this script: for each example the deck text and,
-per k block, the printed Gauss-Laguerre points / r values / check sums (lagpt :1315-1361)
-and Gauss-(associated) Legendre points / weights / check sums (ccmain :932-938).
+per k block, the printed Gauss-Laguerre points / r values / check sums (lagpt :1315-1361),
+Gauss-(associated) Legendre points / weights / check sums (ccmain :932-938) and, for the
+z-perpendicular embedding, Gauss-Jacobi points / weights (ccmain :956-960).
 
 The printed Laguerre "weights" column of these outputs comes from a later build of the
 program (outputs say "version of June 2010", the source "March 2002") that prints a
@@ -25,6 +26,9 @@ CASES = {
     "water_J0": ("water/jobs/dvr0.job", "water/results/result-0.water.dvr"),
     "h3p_jacobi_J0": ("H3+Jacobi/jobs/dvrJ0.job", "H3+Jacobi/results/result.H3p.J0.dvr"),
     "hcn_J2": ("HCN/jobs/dvr.job", "HCN/results/result.HCN.dvr"),
+    "h3p_radau_zperp_J0": ("H3+Radau/jobs/dvr_J0.job", "H3+Radau/results/result.H3p_J0.dvr"),
+    "h3p_radau_zperp_J1_ipar0": ("H3+Radau/jobs/dvr_J1_0.job", "H3+Radau/results/result.H3p_J1_0.dvr"),
+    "h3p_radau_zperp_J1_ipar1": ("H3+Radau/jobs/dvr_J1_1.job", "H3+Radau/results/result.H3p_J1_1.dvr"),
 }
 
 FNUM = r"[-+]?\d*\.\d+(?:[DdEe][-+]?\d+)?"
@@ -38,6 +42,7 @@ def parse_output(text: str) -> dict:
     lines = text.splitlines()
     lag = []
     leg = []
+    jac = []
     i = 0
     while i < len(lines):
         ln = lines[i]
@@ -83,8 +88,26 @@ def parse_output(text: str) -> dict:
             leg.append({"nang": nang, "k": k, "x": xs, "w": ws, "computed_sum": comp, "exact_sum": exact})
             i = j + 2
             continue
+        # z-perp embedding: gaujac points and weights (ccmain :956-960), no check sums
+        m = re.search(r"(\d+) point Gauss-Jacobi integration with alpha = beta =\s*(" + FNUM + ")", ln)
+        if m:
+            nang, alf = int(m.group(1)), float(m.group(2))
+            xs, ws = [], []
+            j = i + 1
+            while len(xs) < (nang + 1) // 2 and j < len(lines):
+                t = lines[j].split()
+                if len(t) == 2:
+                    try:
+                        xs.append(fnum(t[0]))
+                        ws.append(fnum(t[1]))
+                    except ValueError:
+                        pass
+                j += 1
+            jac.append({"nang": nang, "alpha_printed": alf, "x": xs, "w": ws})
+            i = j
+            continue
         i += 1
-    return {"laguerre": lag, "legendre": leg}
+    return {"laguerre": lag, "legendre": leg, "gauss_jacobi": jac}
 
 
 def main(ref: str) -> None:

@@ -149,3 +149,57 @@ def test_oracle_and_product_deck_readers_agree(kat, oracle_mod):
     tests and the benchmark (the reference's example decks, the seeded workloads, variants)."""
     for text in _variant_decks(kat):
         assert _deck_fields(oracle_mod.parse_deck(text)) == _deck_fields(parse_deck(text))
+
+
+ZPERP = ["h3p_radau_zperp_J0", "h3p_radau_zperp_J1_ipar0", "h3p_radau_zperp_J1_ipar1"]
+
+
+@pytest.mark.parametrize("name", ZPERP)
+def test_zperp_gauss_jacobi_points_weights_match_reference(kat, oracle_mod, name):
+    """z-perpendicular embedding (mkmain): Gauss-Jacobi rule with alpha = beta =
+    sqrt((J(J+1) - k^2)/2) from gaujac / gammln (:4190-4286), against the printed points (15
+    decimals) and weights (12 digits) of the reference's H3+ Radau runs. Their output comes
+    from a later build whose k loop also repeats k = 1 with the other Q symmetry (same rule),
+    so each printed block is matched to the k whose alpha it prints.
+
+    For alpha = 0 the printed rule is matched to the printed digits. For alpha = 1 and
+    sqrt(1/2) the printed points sit up to 1.4e-13 from the exact Gauss-Jacobi roots while the
+    source's gaujac (Newton to 3e-14, quadratic) lands on them: the restatement is held to the
+    exact rule (scipy.special.roots_jacobi, 1e-15) and to the printed output within the printing
+    build's own deviation (2e-13 points, 1e-10 weights, which also carry gammln's ~1e-11)."""
+    from scipy.special import roots_jacobi
+
+    d = _odeck(oracle_mod, kat, name)
+    ks = oracle_mod.k_blocks(d)
+    blocks = kat["cases"][name]["gauss_jacobi"]
+    assert blocks
+    jrot = abs(d.jrot)
+    for blk in blocks:
+        kk = [k for k in ks if abs(np.sqrt(0.5 * (jrot * (jrot + 1) - k * k)) - blk["alpha_printed"]) < 5e-4]
+        assert len(kk) == 1, (blk["alpha_printed"], ks)
+        q = oracle_mod.quadrature(d, kk[0])
+        assert q.status == 0
+        n2 = len(blk["x"])
+        assert n2 == blk["nang"] // 2
+        exact = blk["alpha_printed"] == 0.0
+        np.testing.assert_allclose(np.array(q.xalf[:n2]), blk["x"], rtol=0, atol=1.01e-15 if exact else 2e-13)
+        np.testing.assert_allclose(np.array(q.walf[:n2]) ** 2, blk["w"], rtol=1e-11 if exact else 1e-10, atol=0)
+        alf = np.sqrt(0.5 * (jrot * (jrot + 1) - kk[0] ** 2))
+        xr, wr = roots_jacobi(blk["nang"], alf, alf)
+        np.testing.assert_allclose(np.array(q.xalf[:blk["nang"]]), xr[::-1], rtol=0, atol=1e-15)
+        np.testing.assert_allclose(np.array(q.walf[:blk["nang"]]) ** 2, wr[::-1], rtol=5e-11, atol=0)
+        # the full rule is symmetric: x(n+1-i) = -x(i)
+        xa = np.array(q.xalf[:blk["nang"]])
+        np.testing.assert_allclose(xa[::-1], -xa, rtol=0, atol=1e-14)
+
+
+@pytest.mark.parametrize("name", ZPERP)
+def test_zperp_product_host_grid_equals_oracle(kat, oracle_mod, name):
+    d = _deck(kat, name)
+    ks = dvr3d_b200.k_blocks(d)
+    assert ks == oracle_mod.k_blocks(_odeck(oracle_mod, kat, name))
+    for kk in ks:
+        q = oracle_mod.quadrature(_odeck(oracle_mod, kat, name), kk)
+        r1, r2, xa = dvr3d_b200.host_grid(d, kk)
+        np.testing.assert_array_equal(r1, np.array(q.r1[:len(r1)]))
+        np.testing.assert_array_equal(xa, np.array(q.xalf[:len(xa)]))
