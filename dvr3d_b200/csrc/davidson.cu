@@ -23,6 +23,7 @@
 
 #include "chol.cuh"
 #include "common.cuh"
+#include "eig_batched.cuh"
 #include "gemm64.cuh"
 #include "learned_precond.cuh"
 #include "pipeline.cuh"
@@ -235,12 +236,15 @@ bool davidson_solve(dvr3d_ctx *ctx, const H3Op &op, const Contracted &C, const d
     }
     double *work = A("dv_work", (size_t)std::max<long long>(std::min<long long>(64LL * mmax * mmax, 1LL << 22),
                                                           16LL * N * bs));
-    double *ssw = big_rr ? nullptr : A("dv_ssw", (size_t)small_syev_work_doubles(kSmallSyevMax));
     int *err = ctx->arena.get_t<int>("dv_err", 3);
-    int *ssn = ctx->arena.get_t<int>("dv_ssn", 1);
-    long long *ssoff = ctx->arena.get_t<long long>("dv_ssoff", 1);
     CK(cudaMemsetAsync(err, 0, 3 * sizeof(int), st));
-    CK(cudaMemsetAsync(ssoff, 0, sizeof(long long), st));
+    // Rayleigh-Ritz eigensolver of the small path: the batched solver's kernels on one block
+    // (descriptor: n, selected count, zld as ints; aoff, voff, zoff as zeros)
+    int *rr_int = ctx->arena.get_t<int>("dv_rri", 4);
+    long long *rr_zero = ctx->arena.get_t<long long>("dv_rrz", 1);
+    double *rr_a = big_rr ? nullptr : A("dv_rra", (size_t)mmax * mmax);
+    double *rr_d = A("dv_rrd", mmax), *rr_e = A("dv_rre", mmax), *rr_tau = A("dv_rrt", mmax);
+    CK(cudaMemsetAsync(rr_zero, 0, sizeof(long long), st));
     // BF16 slices of the vectors multiplied on the tensor cores (split form)
     const long long ldvb = rup(N, 8);
     __nv_bfloat16 *vb_hi = nullptr, *vb_lo = nullptr;
@@ -284,19 +288,19 @@ bool davidson_solve(dvr3d_ctx *ctx, const H3Op &op, const Contracted &C, const d
             dense_lowest(ctx, Gm, ldg, m, std::min(m, keep), true, w, Z, m, "dvrr_", false, nullptr);
             return;
         }
-        CK(cudaMemcpyAsync(ssn, &m, sizeof(int), cudaMemcpyHostToDevice, st));
-        SmallSyev p{};
-        p.nmat = 1;
-        p.n = ssn;
-        p.A = Gm;
-        p.aoff = ssoff;
-        p.W = w;
-        p.woff = ssoff;
-        p.Z = Z;
-        p.zoff = ssoff;
-        p.work = ssw;
-        p.workoff = ssoff;
-        CK(launch_small_syev(p, m, st));
+        // tridiagonalisation, all m eigenvalues by bisection, the keep lowest eigenvectors by
+        // inverse iteration and a blocked back-transformation (eig_batched.cuh)
+        const int nsel = std::min(m, keep);
+        const int hi[3] = {m, nsel, m};
+        CK(cudaMemcpyAsync(rr_int, hi, sizeof(hi), cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpy2DAsync(rr_a, sizeof(double) * m, Gm, sizeof(double) * ldg, sizeof(double) * m, m,
+                             cudaMemcpyDeviceToDevice, st));
+        BatchDesc bd{1, rr_int, rr_zero, rr_zero};
+        launch_symmetrize_lower(bd, rr_a, m, st);
+        launch_tridiag_batched(bd, rr_a, rr_d, rr_e, rr_tau, m, st);
+        launch_eigvals_batched(bd, rr_d, rr_e, w, rr_int + 3, 0, 0.0, st);
+        launch_eigvecs_batched_fast(bd, rr_a, rr_d, rr_e, rr_tau, w, rr_int + 1, rr_zero, rr_int + 2, Z, m, err, st);
+        CK(cudaGetLastError());
     };
     // HV[:, c0:c0+nc] = H3 V[:, c0:c0+nc]: BF16x3 tensor-core GEMM (split form, phase 1), the
     // matrix-free FP64 operator (split form, residual correction), or the FP64 DMMA GEMM
@@ -450,7 +454,9 @@ bool davidson_solve(dvr3d_ctx *ctx, const H3Op &op, const Contracted &C, const d
         CK(cudaMemcpyAsync(herr, err, sizeof(herr), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         note_d2h(sizeof(double) * (nth + bs) + sizeof(herr));
-        if (herr[2] != 0) break;  // a tensor-core pipeline wait timed out: give up (the caller falls back)
+        if (herr[0] != 0 || herr[2] != 0) break;  // Rayleigh-Ritz inverse iteration failed its growth
+                                                    // test, or a tensor-core pipeline wait timed
+                                                    // out: give up (the caller falls back)
         int nconv = 0;
         double rmax = 0.0;
         for (int j = 0; j < nwant; ++j) {

@@ -60,6 +60,7 @@ struct dvr3d_ctx {
     unsigned long long wait_limit = 0;  // polls of each bounded device wait (0: kernel defaults)
     std::vector<cudaEvent_t> gemm_ev;   // timing pool of the GEMM launches of an iterative solve
     bool lp_trained = false;            // arena "lp_w" holds a trained preconditioner network
+    std::map<long long, int> tuned_split;  // autotuned split-K of the Krylov products per (N, b)
     struct LpSet {                      // training pairs of the last training solve
         bool valid = false;
         int N = 0, nwant = 0, npair = 0;
@@ -192,6 +193,7 @@ struct KrylovStats {
     // the GEMM launches of the solve, each timed with CUDA events (gemm64.cuh GemmLaunchLog)
     double gemm_ms = 0.0, gemm_flops = 0.0;
     int gemm_launches = 0, gemm_untimed = 0;
+    int trmm_split = 0;    // split-K of the Krylov triangular products (autotuned)
 };
 int si_krylov_first_size(int nwant, int block);
 bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, double emin_bound,

@@ -145,6 +145,42 @@ struct Timer {
     }
 };
 
+// Autotuned split-K of the Krylov triangular products (L^-1 Q and its transpose have the same
+// shape): on the first solve of an (N, b) shape in a context, each candidate split is timed by
+// CUDA events (one untimed launch, then two timed) on the start block and the fastest is kept
+// for every later block step and solve; candidates are the fixed rule's choice and 4..8 slices
+// (reduced by the thread-block cluster through distributed shared memory). DVR3D_NO_AUTOTUNE=1
+// keeps the rule.
+int tuned_trmm_split(dvr3d_ctx *ctx, GemmOp y, int rule, cudaStream_t st) {
+    const long long key = ((long long)y.M << 16) | (long long)y.N;
+    auto it = ctx->tuned_split.find(key);
+    if (it != ctx->tuned_split.end()) return it->second;
+    const char *env = std::getenv("DVR3D_NO_AUTOTUNE");
+    if (env && env[0] == '1') return rule;
+    const int ktiles = (y.K + 15) / 16;
+    Timer t;
+    int best = rule;
+    double best_ms = 1.0e30;
+    std::vector<int> cand{rule};
+    for (int c = 4; c <= 8; ++c)
+        if (c != rule && c <= ktiles) cand.push_back(c);
+    for (int c : cand) {
+        y.splitk = c;
+        CK(launch_gemm(y, st));
+        t.start(st);
+        CK(launch_gemm(y, st));
+        CK(launch_gemm(y, st));
+        t.stop(st);
+        const double ms = t.ms();
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = c;
+        }
+    }
+    ctx->tuned_split[key] = best;
+    return best;
+}
+
 }  // namespace
 
 int si_krylov_first_size(int nwant, int block) {
@@ -265,7 +301,23 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
     CK(cudaGetLastError());
     cholqr(Q);
     const int tiles_n = (N + 63) / 64;
-    const int trmm_s = splits(tiles_n, (N + 15) / 16, 1200, 16);
+    int trmm_s = splits(tiles_n, (N + 15) / 16, 1200, 16);
+    {
+        GemmOp y;
+        y.M = N;
+        y.N = b;
+        y.K = N;
+        y.A = Lb;
+        y.lda = ldw;
+        y.tri = 1;
+        y.B = Q;
+        y.ldb = ldq;
+        y.C = Y1;
+        y.ldc = ldq;
+        y.work = work;
+        trmm_s = tuned_trmm_split(ctx, y, trmm_s, st);
+    }
+    ks.trmm_split = trmm_s;
     double flops = 0.0;
     int s = 0;  // blocks with their T column computed
     int next = mfirst / b;
