@@ -153,6 +153,20 @@ class Context:
         """Poll limit of every bounded device wait of later solves (0: the defaults)."""
         self._check(self._lib.dvr3d_b200_set_wait_limit(self._h, int(polls)))
 
+    def rotlev3b(self, deck_text: str, wave_path: str) -> tuple[np.ndarray, str]:
+        """The second variational step (ROTLEV3B) on a first-step wavefunction file
+        (dvr3d_b200_rotlev3b): the lowest levels (Eh) and the printed level table."""
+        lv = np.zeros(20000)
+        n = C.c_int(0)
+        ln = C.c_size_t(0)
+        self._check(self._lib.dvr3d_b200_rotlev3b(self._h, deck_text.encode(), str(wave_path).encode(),
+                                                  lv.ctypes.data_as(C.POINTER(C.c_double)), lv.size,
+                                                  C.byref(n), None, 0, C.byref(ln)))
+        buf = C.create_string_buffer(ln.value)
+        self._check(self._lib.dvr3d_b200_rotlev3b(self._h, deck_text.encode(), str(wave_path).encode(),
+                                                  None, 0, C.byref(n), buf, ln.value, None))
+        return lv[:n.value].copy(), buf.value.decode()
+
     def split_gemm(self, a, b, nslice: int = 2) -> np.ndarray:
         """a^T b on the tensor cores from split-BF16 operands (dvr3d_b200_split_gemm):
         a is k x m, b is k x n (FP64); nslice 1 = one BF16 product, 2 = BF16x3."""

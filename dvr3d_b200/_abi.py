@@ -125,6 +125,8 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "dvr3d_b200_last_error": (C.c_char_p, [vp]),
         "dvr3d_b200_set_stream": (C.c_int, [vp, vp]),
         "dvr3d_b200_set_wait_limit": (C.c_int, [vp, C.c_longlong]),
+        "dvr3d_b200_rotlev3b": (C.c_int, [vp, C.c_char_p, C.c_char_p, P(C.c_double), C.c_int, P(C.c_int),
+                                          C.c_char_p, C.c_size_t, P(C.c_size_t)]),
         "dvr3d_b200_split_gemm": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, P(C.c_double), C.c_longlong,
                                             P(C.c_double), C.c_longlong, C.c_int, P(C.c_double),
                                             C.c_longlong]),

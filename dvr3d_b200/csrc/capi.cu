@@ -12,6 +12,7 @@
 #include "eig_dense.cuh"
 #include "learned_precond.cuh"
 #include "pipeline.cuh"
+#include "rotlev.cuh"
 #include "tc_gemm.cuh"
 
 #define CK(x)                                          \
@@ -361,6 +362,25 @@ int dvr3d_b200_set_wait_limit(dvr3d_ctx *ctx, long long polls) {
     if (!ctx || polls < 0) return DVR3D_ERR_ARG;
     ctx->wait_limit = (unsigned long long)polls;
     return DVR3D_OK;
+}
+
+int dvr3d_b200_rotlev3b(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, double *levels, int cap,
+                        int *nlev, char *out, size_t outcap, size_t *outlen) {
+    if (!ctx || !deck_text || !wave_path || !nlev) return DVR3D_ERR_ARG;
+    return guarded(ctx, [&]() -> int {
+        cudaSetDevice(ctx->device);
+        std::vector<double> lv;
+        std::string table;
+        dvr3d::RotInfo info;
+        dvr3d::rotlev3b_solve(ctx, deck_text, wave_path, lv, table, info);
+        *nlev = (int)lv.size();
+        if (levels) {
+            if (cap < (int)lv.size()) return fail_ctx(ctx, DVR3D_ERR_BUFFER, "levels buffer smaller than neval");
+            std::memcpy(levels, lv.data(), sizeof(double) * lv.size());
+        }
+        copy_out(table, out, outcap, outlen);
+        return DVR3D_OK;
+    });
 }
 
 int dvr3d_b200_split_gemm(dvr3d_ctx *ctx, int m, int n, int k, const double *a, long long lda, const double *b,

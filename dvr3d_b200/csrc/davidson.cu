@@ -157,9 +157,10 @@ double lp_train_loss(dvr3d_ctx *ctx, const double *w, double *grad) {
     const double *R = A("lp_R", ld * P), *E = A("lp_E", ld * P), *th = A("lp_theta", P);
     double *T = A("lp_T", ld * P), *PT = A("lp_PT", ld * P), *G = A("lp_G", ld * P);
     double *zraw = A("lp_zraw", (size_t)N * P), *delta = A("lp_delta", (size_t)N * P);
-    double *proj = A("lp_proj", (size_t)kDavidsonMaxBlock * 3 * nw);
+    const size_t msnap = (size_t)*std::max_element(S.snap_m.begin(), S.snap_m.end());
+    double *proj = A("lp_proj", msnap * nw);
     double *sums = A("lp_sums", 3 * (size_t)P), *coef = A("lp_coef", 2 * (size_t)P), *loss = A("lp_loss", 8);
-    double *work = A("lp_gwork", std::max(lp_grad_work_doubles(), (size_t)64 * 3 * kDavidsonMaxBlock * nw));
+    double *work = A("lp_gwork", std::max({lp_grad_work_doubles(), (size_t)64 * msnap * nw, (size_t)1 << 22}));
     CK(launch_chan_apply(S.cp, w, R, ld, th, P, T, ld, zraw, st));
     copy_cols(PT, ld, T, ld, N, P, st);
     for (size_t s = 0; s < S.snap_m.size(); ++s) {
@@ -548,7 +549,7 @@ bool davidson_solve(dvr3d_ctx *ctx, const H3Op &op, const Contracted &C, const d
         // training pairs: e = (x_final - x) outside the basis of the snapshot
         const int P = (int)snap_m.size() * nwant;
         double *RP = A("lp_R", ld * P), *EP = A("lp_E", ld * P), *TP = A("lp_theta", P);
-        double *pj = A("lp_proj", (size_t)kDavidsonMaxBlock * 3 * nwant);
+        double *pj = A("lp_proj", (size_t)*std::max_element(snap_m.begin(), snap_m.end()) * nwant);
         for (size_t s = 0; s < snap_m.size(); ++s) {
             const std::string k = std::to_string(s);
             const double *Xs = A("lp_X" + k, ld * nwant), *Vs = A("lp_V" + k, ld * snap_m[s]);

@@ -1,0 +1,594 @@
+// rotlev.cu -- the second variational step for J > 0 in symmetrised Radau coordinates with the
+// bisector embedding: the reference's ROTLEV3B (source/rotlev3b_segmented.f90).
+//
+// Input: the wavefunction file (unit IVEC, fort.26) that the first step wrote for the k blocks
+// of one J (dvr3d_b200_run_deck_wave with ZROT, ZTRAN), and ROTLEV3B's job deck. The rotational
+// Hamiltonian in the basis of the lowest vibrational functions of every k block has
+//   * on its diagonal the vibrational levels of each block (select :306-510);
+//   * Coriolis blocks between k and k+1 and between k and k+2 (solrt :1339-1620): an angular
+//     matrix in the DVR of the two blocks (angin1 :719-814, angin2 :816-873, from a Gauss-
+//     associated Legendre quadrature in the FBR), combined with the symmetrised radial r^-2
+//     matrix elements (radint / mkrad :665-717) and the two blocks' first-step vectors
+//     (solofd :1682-1729).
+// solofd's sum over radial pairs of radmat(ir) (A C2_ir2)^T C1_ir1 runs here as two DMMA GEMMs
+// per block pair: W = A C2 over all radial blocks and vectors at once, then offdg = W''^T C1''
+// with W'' and C1'' the radial blocks each pair uses, gathered (and W'' scaled) by one kernel.
+// The Hamiltonian is assembled on the device and its lowest levels come from the dense FP64
+// eigensolver (dgrot's dsyev path :1752-1757; its iterative path gives the same levels).
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <fstream>
+#include <iterator>
+#include <string>
+#include <vector>
+
+#include "../../include/dvr3d_b200.h"
+#include "common.cuh"
+#include "gemm64.cuh"
+#include "pipeline.cuh"
+#include "rotlev.cuh"
+
+#define CK(x)                                          \
+    do {                                               \
+        cudaError_t e_ = (x);                          \
+        if (e_ != cudaSuccess) throw CudaFail{e_, #x}; \
+    } while (0)
+
+namespace dvr3d {
+
+namespace {
+
+[[noreturn]] void bad(int code, const std::string &m) { throw HostError{code, m}; }
+
+// ---- the wavefunction file: sequential unformatted records (4-byte length before and after)
+struct Records {
+    std::vector<unsigned char> buf;
+    std::vector<std::pair<size_t, size_t>> rec;  // (offset, bytes)
+    size_t next = 0;
+
+    explicit Records(const std::string &path) {
+        std::ifstream f(path, std::ios::binary);
+        if (!f) bad(DVR3D_ERR_ARG, "cannot open the wavefunction file " + path);
+        buf.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
+        size_t pos = 0;
+        while (pos + 8 <= buf.size()) {
+            int32_t n = 0, m = 0;
+            std::memcpy(&n, &buf[pos], 4);
+            if (n < 0 || pos + 8 + (size_t)n > buf.size()) bad(DVR3D_ERR_ARG, "wavefunction file: broken record framing");
+            std::memcpy(&m, &buf[pos + 4 + n], 4);
+            if (m != n) bad(DVR3D_ERR_ARG, "wavefunction file: record lengths before and after differ");
+            rec.emplace_back(pos + 4, (size_t)n);
+            pos += 8 + (size_t)n;
+        }
+        if (pos != buf.size()) bad(DVR3D_ERR_ARG, "wavefunction file: trailing bytes");
+    }
+    bool more() const { return next < rec.size(); }
+    std::pair<const unsigned char *, size_t> take() {
+        if (next >= rec.size()) bad(DVR3D_ERR_ARG, "wavefunction file: ends before the expected record");
+        const auto r = rec[next++];
+        return {&buf[r.first], r.second};
+    }
+    std::vector<int> ints(size_t want_min = 0) {
+        auto r = take();
+        std::vector<int> v(r.second / 4);
+        std::memcpy(v.data(), r.first, v.size() * 4);
+        if (v.size() < want_min) bad(DVR3D_ERR_ARG, "wavefunction file: integer record too short");
+        return v;
+    }
+    std::vector<double> dbls(size_t want_min = 0) {
+        auto r = take();
+        std::vector<double> v(r.second / 8);
+        std::memcpy(v.data(), r.first, v.size() * 8);
+        if (v.size() < want_min) bad(DVR3D_ERR_ARG, "wavefunction file: real record too short");
+        return v;
+    }
+    const double *vec(size_t idx, size_t n) const {
+        if (idx >= rec.size() || rec[idx].second < n * 8) bad(DVR3D_ERR_ARG, "wavefunction file: vector record too short");
+        return reinterpret_cast<const double *>(&buf[rec[idx].first]);
+    }
+};
+
+// One k block of the file (ccmain :972-976, testiv :3446-3448, transr :3622-3641).
+struct KBlock {
+    int k = 0, maxleg = 0, nang = 0, lincr = 0, iang = 0, ibass = 0, meval = 0;
+    std::vector<double> pleg;  // pleg(j, i) * walf(i), (maxleg + 1) x nang
+    std::vector<int> iv;       // kept 2D states per angle
+    std::vector<double> ev;    // levels (Eh)
+    size_t vec0 = 0;           // record index of the first vector
+};
+
+// ROTLEV3B's cards after the namelist (insize :157-161): nvib, neval, kmin, ibass, neval2,
+// npnt (12i5), the title, and the optional EZERO card (vrmain :593-596).
+struct RotDeck {
+    int nvib = 0, neval = 0, kmin = 0, ibass = 0, neval2 = 0, npnt = 0;
+    std::string title;
+    double ezero = 0.0;
+};
+
+int field_i5(const std::string &ln, int i) {
+    if ((size_t)(5 * i) >= ln.size()) return 0;
+    const std::string s = ln.substr(5 * i, 5);
+    try {
+        size_t used = 0;
+        const std::string t = s.substr(s.find_first_not_of(' ') == std::string::npos ? s.size() : s.find_first_not_of(' '));
+        if (t.empty()) return 0;
+        return std::stoi(t, &used);
+    } catch (...) {
+        bad(DVR3D_ERR_DECK, "ROTLEV3B card: not an integer in columns " + std::to_string(5 * i + 1));
+    }
+}
+
+RotDeck parse_rot_deck(const char *text) {
+    std::vector<std::string> lines;
+    std::string cur;
+    for (const char *c = text; *c; ++c) {
+        if (*c == '\n') {
+            lines.push_back(cur);
+            cur.clear();
+        } else if (*c != '\r') {
+            cur += *c;
+        }
+    }
+    if (!cur.empty()) lines.push_back(cur);
+    // the namelist: from the line with '&' up to the line holding its closing '/'
+    size_t i = 0;
+    while (i < lines.size() && lines[i].find('&') == std::string::npos) ++i;
+    if (i == lines.size()) bad(DVR3D_ERR_DECK, "ROTLEV3B deck: no namelist PRT");
+    while (i < lines.size() && lines[i].find('/') == std::string::npos) ++i;
+    ++i;
+    if (i >= lines.size()) bad(DVR3D_ERR_DECK, "ROTLEV3B deck: no card after the namelist");
+    RotDeck d;
+    d.nvib = field_i5(lines[i], 0);
+    d.neval = field_i5(lines[i], 1);
+    d.kmin = field_i5(lines[i], 2);
+    d.ibass = field_i5(lines[i], 3);
+    d.neval2 = field_i5(lines[i], 4);
+    d.npnt = field_i5(lines[i], 5);
+    if (i + 1 < lines.size()) d.title = lines[i + 1].substr(0, 72);
+    if (i + 2 < lines.size()) {
+        const std::string e = lines[i + 2].substr(0, std::min<size_t>(20, lines[i + 2].size()));
+        if (e.find_first_not_of(' ') != std::string::npos) {
+            std::string t = e;
+            for (auto &ch : t)
+                if (ch == 'd' || ch == 'D') ch = 'e';
+            try {
+                d.ezero = std::stod(t);
+            } catch (...) {
+                bad(DVR3D_ERR_DECK, "ROTLEV3B deck: EZERO card is not a number");
+            }
+        }
+    }
+    return d;
+}
+
+// Gauss-associated Legendre rule of ROTLEV3B's jacobi (:941-1007): zeros of the Jacobi
+// polynomial P_n^(k,k) found by a downward sign scan from x = 1 in steps of 1e-6, refined by
+// Newton (10 steps at most, |dx| <= 1e-12) with the derivative of the last evaluation; weights
+// from the recurrence constant. Returned over the full range, ascending (angin1 :760-764).
+void rot_quadrature(int n, int k, std::vector<double> &x, std::vector<double> &w, double &cs, double &ts) {
+    const double a = k, b = k;
+    std::vector<double> c(n + 1, 0.0);
+    for (int i = 2; i <= n; ++i) {
+        const double xi = (float)i;
+        c[i] = 4.0 * (xi - 1.0) * (a + xi - 1.0) * (b + xi - 1.0) * (a + b + xi - 1.0) /
+               ((a + b + 2.0 * xi - 1.0) * (a + b + 2.0 * xi - 2.0) * (a + b + 2.0 * xi - 2.0) * (a + b + 2.0 * xi - 3.0));
+    }
+    ts = std::pow(2.0, k + k + 1) / (double)(k + 1);
+    for (int i = 1; i <= k; ++i) ts = ts * (double)i / (double)(k + i + 1);
+    double cc = ts;
+    for (int i = 2; i <= n; ++i) cc *= c[i];
+    auto recur = [&](double xx, double &p, double &dp, double &p1) {
+        double pa = 1.0, pb = xx + (a - b) / (a + b + 2.0), da = 0.0, db = 1.0;
+        for (int j = 2; j <= n; ++j) {
+            const double q = xx * pb - c[j] * pa;
+            const double dq = xx * db + pb - c[j] * da;
+            pa = pb;
+            pb = q;
+            da = db;
+            db = dq;
+        }
+        p = pb;
+        dp = db;
+        p1 = pa;
+    };
+    const int n2 = (n + 1) / 2;
+    std::vector<double> xt;
+    const double xstep = 1.0e-6;
+    double pm1 = 1.0, xx = 1.0;
+    for (;;) {
+        double p, dp, p1;
+        recur(xx, p, dp, p1);
+        if (pm1 * p < 0.0) {
+            pm1 = -pm1;
+            xt.push_back(xx - 0.5 * xstep);
+        }
+        if ((int)xt.size() == n2) break;
+        xx -= xstep;
+        if (!(xx > -1.5 * xstep)) bad(DVR3D_ERR_QUADRATURE, "ROTLEV3B quadrature: wrong number of zeros found");
+    }
+    std::vector<double> xh(n2), wh(n2);
+    cs = 0.0;
+    for (int i = 0; i < n2; ++i) {
+        double z = xt[i], p = 0, dp = 1, p1 = 0;
+        for (int it = 0; it < 10; ++it) {
+            recur(z, p, dp, p1);
+            const double dlt = p / dp;
+            z -= dlt;
+            if (std::fabs(dlt) <= 1.0e-12) break;
+        }
+        xh[i] = z;
+        wh[i] = cc / (dp * p1);
+        cs += wh[i] + wh[i];
+    }
+    if (2 * n2 != n) cs -= wh[n2 - 1];
+    x.assign(n, 0.0);
+    w.assign(n, 0.0);
+    for (int i = 0; i < n2; ++i) {
+        x[n - 1 - i] = xh[i];
+        w[n - 1 - i] = wh[i];
+        x[i] = -xh[i];
+        w[i] = wh[i];
+    }
+}
+
+// ROTLEV3B's asleg (:1051-1157) for m < 90: polynomial parts of the normalised associated
+// Legendre functions P_l^m, l = m .. m + lmax, at the points x -> p((lmax+1) x npt).
+std::vector<double> rot_asleg(const std::vector<double> &x, int lmax, int m) {
+    const int npt = (int)x.size();
+    if (m < 0 || m >= 90) bad(DVR3D_ERR_UNSUPPORTED, "ROTLEV3B angular functions for k >= 90");
+    std::vector<double> p((size_t)(lmax + 1) * npt, 0.0);
+    for (int i = 0; i < npt; ++i) {
+        double pmm = 1.0, f = 1.0;
+        for (int j = 1; j <= m; ++j) {
+            pmm = -pmm * f;
+            f += 2.0;
+        }
+        double *col = &p[(size_t)i * (lmax + 1)];
+        col[0] = pmm;
+        double pmmp1 = x[i] * (m + m + 1) * pmm;
+        if (lmax >= 1) col[1] = pmmp1;
+        int ll = 1;
+        for (int l = 2 + m; l <= lmax + m; ++l) {
+            const double pll = (x[i] * (double)(l + l - 1) * pmmp1 - (double)(l + m - 1) * pmm) / (double)(l - m);
+            pmm = pmmp1;
+            pmmp1 = pll;
+            col[++ll] = pll;
+        }
+    }
+    for (int j = m, jj = 0; j <= lmax + m; ++j, ++jj) {
+        double f = 1.0;
+        for (int i = j - m + 1; i <= j + m; ++i) f *= std::sqrt((double)i);
+        const double nrm = std::sqrt(((double)j + (double)j + 1.0) / 2) / f;
+        for (int i = 0; i < npt; ++i) p[(size_t)i * (lmax + 1) + jj] *= nrm;
+    }
+    return p;
+}
+
+// Angular Coriolis matrix between the kept angles of two k blocks (angin1 / angin2): the FBR
+// integral over the quadrature, transformed to the two DVRs by the blocks' own pleg * walf.
+// step 1: blocks k1 and k1+1, weight (1 + x); step 2: k1 and k1+2, weight (1 + x)^2.
+std::vector<double> angular_block(int step, int k1, const KBlock &b1, const KBlock &b2, int npnt,
+                                  double angfac) {
+    std::vector<double> x, w;
+    double cs = 0, ts = 0;
+    rot_quadrature(npnt, k1, x, w, cs, ts);
+    if (std::fabs((cs - ts) / ts) > 1.0e-8) bad(DVR3D_ERR_QUADRATURE, "ROTLEV3B points & weights in error");
+    const int n1 = b1.nang, n2 = b2.nang;
+    const std::vector<double> pa = rot_asleg(x, n1 - 1, k1);
+    const std::vector<double> pb = rot_asleg(x, n2 - 1, k1 + step);
+    std::vector<double> fbr((size_t)n1 * n2, 0.0);  // fbr(j, k), column-major n1 x n2
+    for (int i = 0; i < npnt; ++i) {
+        const double t = step == 1 ? w[i] * (1.0 + x[i]) : w[i] * ((1.0 + x[i]) * (1.0 + x[i]));
+        for (int j = 0; j < n1; ++j) {
+            const double f = t * pa[(size_t)i * n1 + j];
+            for (int k = 0; k < n2; ++k) fbr[(size_t)k * n1 + j] += f * pb[(size_t)i * n2 + k];
+        }
+    }
+    // the file's transforms: pleg(j, i) with leading dimension maxleg + 1
+    const int ld1 = b1.maxleg + 1, ld2 = b2.maxleg + 1;
+    auto P1 = [&](int j, int i) { return b1.pleg[(size_t)i * ld1 + j]; };
+    auto P2 = [&](int j, int i) { return b2.pleg[(size_t)i * ld2 + j]; };
+    std::vector<double> ang((size_t)b1.iang * b2.iang, 0.0);  // column-major iang1 x iang2
+    const double kkp1 = (double)k1 * (k1 + 1), xkph = k1 + 0.5;
+    int i1 = 0;
+    for (int i = 0; i < n1; ++i) {
+        if (b1.iv[i] == 0) continue;
+        int i2 = 0;
+        for (int ip = 0; ip < n2; ++ip) {
+            if (b2.iv[ip] == 0) continue;
+            double sum1 = 0.0, sum2 = 0.0;
+            for (int j = 0; j < n1; ++j) {
+                if (step == 1 && j > 0) {
+                    const double jj = k1 + j;
+                    sum1 += P1(j, i) * P2(j - 1, ip) * std::sqrt(jj * (jj + 1.0) - kkp1);
+                }
+                for (int jp = 0; jp < n2; ++jp) sum2 += P1(j, i) * P2(jp, ip) * fbr[(size_t)jp * n1 + j];
+            }
+            ang[(size_t)i2 * b1.iang + i1] = (step == 1 ? sum1 + xkph * sum2 : sum2) * angfac;
+            ++i2;
+        }
+        ++i1;
+    }
+    return ang;
+}
+
+// W''[(ir, a), v] = rad[ir] * W[a + (m2[ir] + v * nrad2) * iang1];  C1''[(ir, a), v] = C1[a + m1[ir] * iang1 + v * ldc1]
+__global__ void rot_gather_kernel(const double *W, int iang1, int nrad2, int nvec2, const double *C1, long long ldc1,
+                                  int nvec1, const int *m1, const int *m2, const double *rad, int npair, double *Wg,
+                                  double *Cg) {
+    const long long K = (long long)npair * iang1;
+    const long long tot = K * (long long)(nvec1 > nvec2 ? nvec1 : nvec2);
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const long long row = t % K;
+        const int v = (int)(t / K);
+        const int ir = (int)(row / iang1), a = (int)(row % iang1);
+        if (v < nvec2) Wg[(size_t)v * K + row] = rad[ir] * W[a + ((long long)m2[ir] + (long long)v * nrad2) * iang1];
+        if (v < nvec1) Cg[(size_t)v * K + row] = C1[a + (long long)m1[ir] * iang1 + (long long)v * ldc1];
+    }
+}
+
+// H(r0 + v1, c0 + v2) = H(c0 + v2, r0 + v1) = off(v2, v1) (off: n2 x n1)
+__global__ void rot_place_kernel(const double *off, int n2, int n1, double *H, long long ldh, int r0, int c0) {
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < (long long)n1 * n2;
+         t += (long long)gridDim.x * blockDim.x) {
+        const int v2 = (int)(t % n2), v1 = (int)(t / n2);
+        const double x = off[t];
+        H[(size_t)(c0 + v2) * ldh + (r0 + v1)] = x;
+        H[(size_t)(r0 + v1) * ldh + (c0 + v2)] = x;
+    }
+}
+
+__global__ void rot_diag_kernel(const double *e, int n, double *H, long long ldh) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) H[(size_t)i * ldh + i] = e[i];
+}
+
+unsigned nblocks256(long long n) { return (unsigned)std::min<long long>((n + 255) / 256, 4096); }
+
+std::string fmt_d(double v, int w, int d) {
+    // Fortran Dw.d: 0.ddddD+ee
+    char buf[64];
+    if (v == 0.0) {
+        std::snprintf(buf, sizeof(buf), "0.%0*dD+00", d, 0);
+    } else {
+        int ex = (int)std::floor(std::log10(std::fabs(v))) + 1;
+        double mant = std::fabs(v) / std::pow(10.0, ex);
+        const double scale = std::pow(10.0, d);
+        double rm = std::round(mant * scale);
+        if (rm >= scale) {
+            rm /= 10.0;
+            ex += 1;
+        }
+        if (rm < scale / 10.0) {
+            rm *= 10.0;
+            ex -= 1;
+        }
+        std::snprintf(buf, sizeof(buf), "%s0.%0*.0fD%c%02d", v < 0 ? "-" : "", d, rm, ex < 0 ? '-' : '+', std::abs(ex));
+    }
+    std::string s(buf);
+    if ((int)s.size() < w) s = std::string(w - s.size(), ' ') + s;
+    return s;
+}
+
+}  // namespace
+
+void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, std::vector<double> &levels,
+                    std::string &table, RotInfo &info) {
+    const RotDeck rd = parse_rot_deck(deck_text);
+    Records f(wave_path);
+    // ---- header (setcon :1176-1184 as insize :155 reads it)
+    const std::vector<int> h = f.ints(9);
+    const int idia = h[0], ipar0 = h[1], ndvr = h[2], nmax = h[3], jrot = h[5], kmin0 = h[6], meval = h[7];
+    if (idia != -2) bad(DVR3D_ERR_UNSUPPORTED, "ROTLEV3B reads Radau (IDIA = -2) wavefunction files");
+    if (jrot <= 0) bad(DVR3D_ERR_ARG, "ROTLEV3B needs a J > 0 wavefunction file");
+    const int kmin = rd.kmin;
+    if (kmin != kmin0 && kmin0 != 2) bad(DVR3D_ERR_ARG, "ROTLEV3B: kmin differs from the first step's kmin");
+    if (kmin > 1 || (kmin == 0 && kmin0 != 0))
+        bad(DVR3D_ERR_UNSUPPORTED, "ROTLEV3B: one parity per run, from a file of that parity (kmin 0 or 1)");
+    f.take();                                // logical flags, masses, g1, g2
+    f.take();                                // Morse constants
+    const std::vector<double> rm2 = f.dbls((size_t)nmax);  // r^-2 term (ccmain :824-833)
+    f.take();                                // r
+    // ---- k blocks
+    const int nblk = kmin > 0 ? jrot + 1 : jrot;
+    std::vector<KBlock> kb;
+    while ((int)kb.size() < nblk && f.more()) {
+        KBlock b;
+        f.take();  // xalf
+        const std::vector<int> hk = f.ints(4);
+        b.k = hk[0];
+        b.maxleg = hk[1];
+        b.nang = hk[2];
+        b.lincr = hk[3];
+        b.pleg = f.dbls((size_t)(b.maxleg + 1) * b.nang);
+        const std::vector<int> ib = f.ints(2);
+        b.iang = ib[0];
+        b.ibass = ib[1];
+        b.iv = f.ints((size_t)b.nang);
+        b.meval = f.ints(1)[0];
+        b.ev = f.dbls((size_t)b.meval);
+        b.vec0 = f.next;
+        f.next += (size_t)b.meval;
+        if (f.next > f.rec.size()) bad(DVR3D_ERR_ARG, "wavefunction file: ends inside the vectors of a k block");
+        if (b.iang <= 0 || b.ibass % b.iang != 0) bad(DVR3D_ERR_ARG, "wavefunction file: inconsistent basis sizes");
+        kb.push_back(std::move(b));
+    }
+    if ((int)kb.size() < nblk) bad(DVR3D_ERR_ARG, "wavefunction file holds fewer k blocks than J + 1 - kmin");
+    for (int i = 0; i < nblk; ++i)
+        if (kb[i].k != (kmin > 0 ? i : i + 1)) bad(DVR3D_ERR_ARG, "wavefunction file: unexpected k block order");
+    // ---- basis selection (select :306-510)
+    const int nvib = std::min(rd.nvib, meval);
+    std::vector<int> mvib(nblk);
+    int ipt = 0;
+    for (int i = 0; i < nblk; ++i) {
+        mvib[i] = std::min({nvib, kb[i].ibass, kb[i].meval});
+        ipt += mvib[i];
+    }
+    int nbass = ipt;
+    if (rd.ibass > 0 && rd.ibass < ipt) {  // the ibass lowest functions over all blocks
+        std::vector<int> iv(nblk, 0);
+        for (int n = 0; n < rd.ibass; ++n) {
+            int jpt = -1;
+            double e = 0.0;
+            for (int j = 0; j < nblk; ++j) {
+                if (iv[j] >= mvib[j]) continue;
+                if (jpt < 0 || kb[j].ev[iv[j]] < e) {
+                    e = kb[j].ev[iv[j]];
+                    jpt = j;
+                }
+            }
+            ++iv[jpt];
+        }
+        mvib = iv;
+        nbass = rd.ibass;
+    }
+    int neval = rd.neval <= 0 ? 10 : rd.neval;
+    neval = std::min(neval, nbass);
+    const int npnt = std::max(ndvr, rd.npnt);
+    // ---- symmetrised radial r^-2 matrix elements (mkrad :698-717)
+    auto mkrad = [&](int iq, int ip, int is) {
+        std::vector<double> r;
+        const double symm = 1 - 2 * ip, sign = 1 - 2 * is;
+        for (int i1 = 0; i1 < nmax; ++i1)
+            for (int i2 = 0; i2 < i1 + 1 - iq; ++i2) r.push_back(sign * (rm2[i2] + symm * rm2[i1]));
+        return r;
+    };
+    const std::vector<double> radmee = mkrad(0, 0, 0), radmoo = mkrad(1, 0, 0), radmeo = mkrad(1, 1, 0),
+                              radmoe = mkrad(1, 1, 1);
+    // ---- device Hamiltonian
+    cudaStream_t st = ctx->stream;
+    std::vector<int> off(nblk + 1, 0);
+    for (int i = 0; i < nblk; ++i) off[i + 1] = off[i] + mvib[i];
+    const long long ldh = (nbass + 7) / 8 * 8;
+    double *H = ctx->arena.get_t<double>("rt_h", (size_t)ldh * nbass);
+    CK(cudaMemsetAsync(H, 0, sizeof(double) * ldh * nbass, st));
+    {
+        std::vector<double> dg(nbass);
+        for (int i = 0; i < nblk; ++i)
+            for (int v = 0; v < mvib[i]; ++v) dg[off[i] + v] = kb[i].ev[v];
+        double *dd = ctx->arena.get_t<double>("rt_dg", nbass);
+        CK(cudaMemcpyAsync(dd, dg.data(), sizeof(double) * nbass, cudaMemcpyHostToDevice, st));
+        DVR3D_COUNT_LAUNCH(1);
+        rot_diag_kernel<<<nblocks256(nbass), 256, 0, st>>>(dd, nbass, H, ldh);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+    }
+    // first-step vectors of a block, on the device (ibass x mvib)
+    auto upload_vectors = [&](const KBlock &b, int nv, const char *name) {
+        double *d = ctx->arena.get_t<double>(name, (size_t)b.ibass * std::max(nv, 1));
+        for (int v = 0; v < nv; ++v)
+            CK(cudaMemcpyAsync(d + (size_t)v * b.ibass, f.vec(b.vec0 + v, (size_t)b.ibass), sizeof(double) * b.ibass,
+                               cudaMemcpyHostToDevice, st));
+        CK(cudaStreamSynchronize(st));
+        return d;
+    };
+    const double jjp1 = (double)jrot * (jrot + 1);
+    info.offdiag_flops = 0.0;
+    // one Coriolis block (solofd): off (mvib2 x mvib1), placed at rows of block i, columns of block j
+    auto coriolis = [&](int i, int j, const std::vector<double> &ang, const std::vector<double> &rad, int iq, int iq1,
+                        int iq2) {
+        const KBlock &b1 = kb[i], &b2 = kb[j];
+        const int n1 = mvib[i], n2 = mvib[j];
+        if (n1 == 0 || n2 == 0) return;
+        const int nrad2 = b2.ibass / b2.iang;
+        std::vector<int> m1, m2;
+        int ir1 = 0, ir2 = 0;
+        for (int a1 = 0; a1 < nmax; ++a1) {
+            for (int a2 = 0; a2 < a1 + 1 - iq; ++a2) {
+                m1.push_back(ir1++);
+                m2.push_back(ir2++);
+            }
+            ir1 += iq1;
+            ir2 += iq2;
+        }
+        const int npair = (int)m1.size();
+        if (ir1 > b1.ibass / b1.iang || ir2 > nrad2 || (int)rad.size() != npair)
+            bad(DVR3D_ERR_ARG, "wavefunction file: radial basis does not match the block parities");
+        double *C1 = upload_vectors(b1, n1, "rt_c1");
+        double *C2 = upload_vectors(b2, n2, "rt_c2");
+        double *A = ctx->arena.get_t<double>("rt_ang", ang.size());
+        CK(cudaMemcpyAsync(A, ang.data(), sizeof(double) * ang.size(), cudaMemcpyHostToDevice, st));
+        const long long K = (long long)npair * b1.iang;
+        double *W = ctx->arena.get_t<double>("rt_w", (size_t)b1.iang * nrad2 * n2);
+        double *Wg = ctx->arena.get_t<double>("rt_wg", (size_t)K * n2);
+        double *Cg = ctx->arena.get_t<double>("rt_cg", (size_t)K * n1);
+        double *O = ctx->arena.get_t<double>("rt_off", (size_t)n1 * n2);
+        int *dm1 = ctx->arena.get_t<int>("rt_m1", npair), *dm2 = ctx->arena.get_t<int>("rt_m2", npair);
+        double *dr = ctx->arena.get_t<double>("rt_rad", npair);
+        CK(cudaMemcpyAsync(dm1, m1.data(), sizeof(int) * npair, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(dm2, m2.data(), sizeof(int) * npair, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(dr, rad.data(), sizeof(double) * npair, cudaMemcpyHostToDevice, st));
+        // W (iang1 x nrad2 n2) = A (iang1 x iang2) C2 (iang2 x nrad2 n2)
+        launch_dgemm(false, false, b1.iang, nrad2 * n2, b2.iang, 1.0, A, b1.iang, C2, b2.iang, 0.0, W, b1.iang, st);
+        CK(cudaGetLastError());
+        DVR3D_COUNT_LAUNCH(1);
+        rot_gather_kernel<<<nblocks256(K * std::max(n1, n2)), 256, 0, st>>>(W, b1.iang, nrad2, n2, C1, b1.ibass, n1,
+                                                                             dm1, dm2, dr, npair, Wg, Cg);
+        CK(cudaGetLastError());
+        // off (n2 x n1) = W''^T C1''
+        launch_dgemm(true, false, n2, n1, (int)K, 1.0, Wg, K, Cg, K, 0.0, O, n2, st);
+        CK(cudaGetLastError());
+        DVR3D_COUNT_LAUNCH(1);
+        rot_place_kernel<<<nblocks256((long long)n1 * n2), 256, 0, st>>>(O, n2, n1, H, ldh, off[i], off[j]);
+        CK(cudaGetLastError());
+        CK(cudaStreamSynchronize(st));
+        info.offdiag_flops += 2.0 * b1.iang * b2.iang * (double)nrad2 * n2 + 2.0 * (double)K * n1 * n2;
+    };
+    int ip = ipar0;
+    for (int i = 1; i < nblk; ++i) {
+        const int k1 = kb[i - 1].k;
+        // k and k + 1 (solrt :1468-1486)
+        double angfac = std::sqrt(jjp1 - (double)k1 * (k1 + 1)) / 2.0;
+        if (k1 == 0) angfac = 1.4142135623731 * angfac;
+        if (mvib[i - 1] * mvib[i] > 0) {
+            const std::vector<double> ang = angular_block(1, k1, kb[i - 1], kb[i], npnt, angfac);
+            if (ip == 0) coriolis(i - 1, i, ang, radmeo, 1, 1, 0);
+            else coriolis(i - 1, i, ang, radmoe, 1, 0, 1);
+        }
+        // k and k + 2 (:1488-1520)
+        if (i + 1 < nblk && mvib[i - 1] * mvib[i + 1] > 0) {
+            double af = -std::sqrt((jjp1 - (double)(k1 + 1) * (k1 + 2)) * (jjp1 - (double)k1 * (k1 + 1))) / 16.0;
+            if (k1 == 0) af = 1.4142135623731 * af;
+            const std::vector<double> ang = angular_block(2, k1, kb[i - 1], kb[i + 1], npnt, af);
+            if (ip == 0) coriolis(i - 1, i + 1, ang, radmee, 0, 0, 0);
+            else coriolis(i - 1, i + 1, ang, radmoo, 1, 0, 0);
+        }
+        ip = 1 - ip;
+    }
+    // ---- lowest levels (dgrot)
+    double *wv = ctx->arena.get_t<double>("rt_w_ev", neval);
+    dense_lowest(ctx, H, ldh, nbass, neval, false, wv, nullptr, 1, "rtd_", false, nullptr);
+    levels.resize(neval);
+    CK(cudaMemcpyAsync(levels.data(), wv, sizeof(double) * neval, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    info.nbass = nbass;
+    info.nblk = nblk;
+    info.neval = neval;
+    info.mvib = mvib;
+    // ---- printed table (dgrot :1767-1769, :1795-1799)
+    table.clear();
+    char ln[160];
+    std::snprintf(ln, sizeof(ln), "\n     J =%3d rotational state,%7d basis functions\n", jrot, nbass);
+    table += ln;
+    table += kmin >= 1 ? "            e parity, symmetric |jk> + |j-k> functions in basis\n"
+                       : "            f parity, anti-symmetric |jk> - |j-k> functions in basis\n";
+    std::snprintf(ln, sizeof(ln), "\n\n     lowest%4d eigenvalues in Hartrees\n\n", neval);
+    table += ln;
+    auto rows = [&](const std::vector<double> &v) {
+        for (size_t i = 0; i < v.size(); ++i) {
+            table += fmt_d(v[i], 24, 12);
+            if (i % 5 == 4 || i + 1 == v.size()) table += "\n\n";
+        }
+    };
+    rows(levels);
+    std::vector<double> cm(neval);
+    for (int i = 0; i < neval; ++i) cm[i] = levels[i] * 2.19474624e5 - rd.ezero;
+    std::snprintf(ln, sizeof(ln), "\n\n     lowest%4d eigenvalues in wavenumbers relative to ezero =", neval);
+    table += ln;
+    table += fmt_d(rd.ezero, 24, 12) + "\n\n";
+    rows(cm);
+}
+
+}  // namespace dvr3d

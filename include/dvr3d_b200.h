@@ -191,6 +191,20 @@ int dvr3d_b200_set_stream(dvr3d_ctx *ctx, void *stream);
  * reference (which has no device waits). */
 int dvr3d_b200_set_wait_limit(dvr3d_ctx *ctx, long long polls);
 
+/* The second variational step for J > 0, symmetrised Radau coordinates with the bisector
+ * embedding: the reference's program ROTLEV3B (source/rotlev3b_segmented.f90). deck_text is
+ * ROTLEV3B's stdin (namelist PRT, card NVIB,NEVAL,KMIN,IBASS,NEVAL2,NPNT (12i5, insize
+ * :157-161), title, optional EZERO card, vrmain :593-596); wave_path the first step's
+ * wavefunction file (unit IVEC = 26) as dvr3d_b200_run_deck_wave writes it for k = kmin..J
+ * (ZROT, ZTRAN). The Coriolis-coupled Hamiltonian (select :306-510, solrt :1339-1620,
+ * angin1/angin2 :719-873, solofd :1682-1729) is built on the device and its lowest NEVAL levels
+ * (Eh, dgrot :1731-1800) go to levels (cap entries); *nlev receives their number; out / outlen
+ * as for dvr3d_b200_run_deck receive the printed level table. One parity per call: KMIN = 1
+ * (e, k = 0..J) or 0 (f, k = 1..J) from a file of the same KMIN (KMIN = 1 also reads a KMIN = 2
+ * file's first J + 1 blocks); the KMIN = 2 double pass returns DVR3D_ERR_UNSUPPORTED. */
+int dvr3d_b200_rotlev3b(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, double *levels, int cap,
+                        int *nlev, char *out, size_t outcap, size_t *outlen);
+
 /* The split-BF16 tensor-core product of the mixed-precision form, on host buffers:
  *     c (m x n, ldc) = a^T b,   a: k x m (lda), b: k x n (ldb), all column-major FP64.
  * Each operand is split on the device into BF16 slices (x ~= hi + lo); nslice = 1 keeps hi

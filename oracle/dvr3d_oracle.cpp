@@ -25,6 +25,7 @@
 #include <cstring>
 #include <random>
 #include <stdexcept>
+#include <string>
 #include <vector>
 
 namespace {
@@ -1591,6 +1592,437 @@ void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
     }
 }
 
+
+// ================================================================== ROTLEV3B (second step)
+// Restatement of source/rotlev3b_segmented.f90 for one parity (kmin 0 or 1) with the
+// Hamiltonian diagonalised in core (dgrot's dsyev path): insize :116-304 (the card),
+// select :306-510, radint / mkrad :665-717, angin1 :719-814, angin2 :816-873, jacobi / root /
+// recur :941-1049, asleg :1051-1157 (m < 90), solrt :1339-1620, solofd :1682-1729 (its two
+// dgemms as loops), loadh :1196-1337 (in-core branch), dgrot :1731-1800.
+
+struct RotFile {
+    std::vector<unsigned char> b;
+    size_t pos = 0;
+    bool eof() const { return pos >= b.size(); }
+    // next record's bytes
+    std::pair<const unsigned char *, int> rec() {
+        if (pos + 4 > b.size()) fail(DVR3D_ERR_ARG);
+        int32_t n;
+        std::memcpy(&n, &b[pos], 4);
+        if (n < 0 || pos + 8 + (size_t)n > b.size()) fail(DVR3D_ERR_ARG);
+        std::pair<const unsigned char *, int> r{&b[pos + 4], n};
+        pos += 8 + (size_t)n;
+        return r;
+    }
+    void skip() { rec(); }
+    std::vector<int> ints() {
+        auto r = rec();
+        std::vector<int> v(r.second / 4);
+        std::memcpy(v.data(), r.first, v.size() * 4);
+        return v;
+    }
+    // getrow: the first n doubles of the next record
+    void getrow(double *row, int n) {
+        auto r = rec();
+        if (r.second < 8 * n) fail(DVR3D_ERR_ARG);
+        std::memcpy(row, r.first, 8 * (size_t)n);
+    }
+};
+
+struct RotBlock {
+    int k1, maxleg, nang, iang, ibass, meval;
+    std::vector<double> pleg;  // pleg(ndvr, ndvr) filled with nang*ndvr values (getrow)
+    std::vector<int> iv;
+    std::vector<double> evib;
+    std::vector<double> coef;  // coef(ibass, mvib)
+};
+
+// recur :1029-1049
+void rot_recur(double &pn, double &dpn, double &pn1, double x, int nn, double alf, double bta,
+               const std::vector<double> &b, const std::vector<double> &c) {
+    double p1 = 1.0, p = x + (alf - bta) / (alf + bta + 2.0), dp1 = 0.0, dp = 1.0;
+    for (int j = 2; j <= nn; ++j) {
+        double q = (x - b[j]) * p - c[j] * p1;
+        double dq = (x - b[j]) * dp + p - c[j] * dp1;
+        p1 = p;
+        p = q;
+        dp1 = dp;
+        dp = dq;
+    }
+    pn = p;
+    dpn = dp;
+    pn1 = p1;
+}
+
+// jacobi :941-1007 (brute-force sign scan, step 1e-6) with root :1009-1027
+void rot_jacobi(int nn, int nn2, std::vector<double> &x, std::vector<double> &a, double alf, double bta,
+                double &csa, double tsa) {
+    const double eps = 1.0e-12, xstep = 1.0e-6;
+    std::vector<double> b(nn + 1, 0.0), c(nn + 1, 0.0), xt(nn + 1, 0.0);
+    x.assign(nn + 1, 0.0);
+    a.assign(nn + 1, 0.0);
+    csa = 0.0;
+    for (int i = 2; i <= nn; ++i) {
+        double xi = (double)(float)i;
+        b[i] = 0.0;
+        c[i] = 4.0 * (xi - 1.0) * (alf + xi - 1.0) * (bta + xi - 1.0) * (alf + bta + xi - 1.0) /
+               ((alf + bta + 2.0 * xi - 1.0) * (alf + bta + 2.0 * xi - 2.0) * (alf + bta + 2.0 * xi - 2.0) *
+                (alf + bta + 2.0 * xi - 3.0));
+    }
+    double cc = tsa;
+    for (int i = 2; i <= nn; ++i) cc = cc * c[i];
+    int ii = 0;
+    double pm1 = 1.0, xxx = 1.0;
+    for (;;) {
+        double p, dp, pn1;
+        rot_recur(p, dp, pn1, xxx, nn, alf, bta, b, c);
+        if (pm1 * p < 0.0) {
+            pm1 = -pm1;
+            ii = ii + 1;
+            xt[ii] = xxx - 0.5 * xstep;
+        }
+        if (ii == nn2) break;
+        xxx = xxx - xstep;
+        if (!(xxx > -1.5 * xstep)) fail(DVR3D_ERR_QUADRATURE);
+    }
+    for (int i = 1; i <= nn2; ++i) {
+        double xr = xt[i], p = 0, dp = 0, pn1 = 0, dpn = 0;
+        int iter = 0;
+        for (;;) {
+            iter = iter + 1;
+            rot_recur(p, dp, pn1, xr, nn, alf, bta, b, c);
+            double d = p / dp;
+            xr = xr - d;
+            if (std::fabs(d) <= eps) break;
+            if (iter >= 10) break;
+        }
+        dpn = dp;
+        x[i] = xr;
+        a[i] = cc / (dpn * pn1);
+        csa = csa + a[i] + a[i];
+    }
+    if (2 * nn2 != nn) csa = csa - a[nn2];
+}
+
+// asleg :1051-1157 (m < 90): pleg(0:lmax, nn2) column-major
+void rot_asleg(std::vector<double> &pleg, int lmax, const std::vector<double> &x, int nn2, int m) {
+    if (m < 0 || m >= 90) fail(DVR3D_ERR_UNSUPPORTED);
+    pleg.assign((size_t)(lmax + 1) * nn2, 0.0);
+    auto P = [&](int l, int i) -> double & { return pleg[(size_t)(i - 1) * (lmax + 1) + l]; };
+    for (int i = 1; i <= nn2; ++i) {
+        double pmm = 1.0, fact = 1.0;
+        for (int j = 1; j <= m; ++j) {
+            pmm = -pmm * fact;
+            fact = fact + 2.0;
+        }
+        P(0, i) = pmm;
+        double pmmp1 = x[i] * (m + m + 1) * pmm;
+        if (lmax >= 1) P(1, i) = pmmp1;
+        int ll = 1;
+        for (int l = 2 + m; l <= lmax + m; ++l) {
+            double r2lm1 = (double)(l + l - 1), rlpmm1 = (double)(l + m - 1), rlmm = (double)(l - m);
+            double pll = (x[i] * r2lm1 * pmmp1 - rlpmm1 * pmm) / rlmm;
+            pmm = pmmp1;
+            pmmp1 = pll;
+            ll = ll + 1;
+            P(ll, i) = pll;
+        }
+    }
+    std::vector<double> pnorm(lmax + 1);
+    int jj = -1;
+    for (int j = m; j <= lmax + m; ++j) {
+        double fact = 1.0;
+        for (int i = j - m + 1; i <= j + m; ++i) fact = fact * std::sqrt((double)i);
+        double rj = (double)j;
+        jj = jj + 1;
+        pnorm[jj] = std::sqrt((rj + rj + 1.0) / 2) / fact;
+    }
+    for (int i = 1; i <= nn2; ++i)
+        for (int j2 = 0; j2 <= lmax; ++j2) P(j2, i) = P(j2, i) * pnorm[j2];
+}
+
+struct RotQuad {
+    std::vector<double> xalf, walf;  // 1-based, npnt
+};
+
+// angin1 :719-814 / angin2 :816-873 -> angmat(iang, iang) column-major (ld iang)
+void rot_angin(int step, std::vector<double> &angmat, int iang, const RotQuad &q, int npnt, int ndvr,
+               const RotBlock &b1, const RotBlock &b2, int k1, double angfac) {
+    const int nang1 = b1.nang, nang2 = b2.nang;
+    std::vector<double> plega, plegb;
+    rot_asleg(plega, nang1 - 1, q.xalf, npnt, k1);
+    rot_asleg(plegb, nang2 - 1, q.xalf, npnt, k1 + step);
+    auto PA = [&](int j, int i) { return plega[(size_t)(i - 1) * nang1 + (j - 1)]; };
+    auto PB = [&](int k, int i) { return plegb[(size_t)(i - 1) * nang2 + (k - 1)]; };
+    std::vector<double> fbr((size_t)ndvr * ndvr, 0.0);
+    auto F = [&](int j, int k) -> double & { return fbr[(size_t)(k - 1) * ndvr + (j - 1)]; };
+    for (int i = 1; i <= npnt; ++i) {
+        double term = step == 1 ? q.walf[i] * (1.0 + q.xalf[i]) : q.walf[i] * ((1.0 + q.xalf[i]) * (1.0 + q.xalf[i]));
+        for (int j = 1; j <= nang1; ++j) {
+            double fact = term * PA(j, i);
+            for (int k = 1; k <= nang2; ++k) F(j, k) = F(j, k) + fact * PB(k, i);
+        }
+    }
+    auto P1 = [&](int j, int i) { return b1.pleg[(size_t)(i - 1) * ndvr + (j - 1)]; };
+    auto P2 = [&](int j, int i) { return b2.pleg[(size_t)(i - 1) * ndvr + (j - 1)]; };
+    angmat.assign((size_t)iang * iang, 0.0);
+    int kkp1 = k1 * (k1 + 1);
+    double xkph = (double)k1 + 0.5;
+    int i1 = 0;
+    for (int i = 1; i <= nang1; ++i) {
+        if (b1.iv[i - 1] == 0) continue;
+        i1 = i1 + 1;
+        int i2 = 0;
+        for (int ip = 1; ip <= nang2; ++ip) {
+            if (b2.iv[ip - 1] == 0) continue;
+            i2 = i2 + 1;
+            double sum1 = 0.0, sum2 = 0.0;
+            int jj = k1;
+            for (int j = 1; j <= nang1; ++j) {
+                if (step == 1 && j > 1) {
+                    jj = jj + 1;
+                    sum1 = sum1 + P1(j, i) * P2(j - 1, ip) * std::sqrt((double)(jj * (jj + 1) - kkp1));
+                }
+                for (int jp = 1; jp <= nang2; ++jp) sum2 = sum2 + P1(j, i) * P2(jp, ip) * F(j, jp);
+            }
+            angmat[(size_t)(i2 - 1) * iang + (i1 - 1)] = (step == 1 ? (sum1 + xkph * sum2) : sum2) * angfac;
+        }
+    }
+}
+
+// mkrad :698-717
+std::vector<double> rot_mkrad(int nmax, const std::vector<double> &rm2, int iq, int ip, int is) {
+    std::vector<double> radmat;
+    double symm = (double)(1 - 2 * ip), sign = (double)(1 - 2 * is);
+    for (int i1 = 1; i1 <= nmax; ++i1)
+        for (int i2 = 1; i2 <= i1 - iq; ++i2) radmat.push_back(sign * (rm2[i2 - 1] + symm * rm2[i1 - 1]));
+    return radmat;
+}
+
+// solofd :1682-1729 (the two dgemms as loops) -> offdg(mvib2, mvib1)
+void rot_solofd(std::vector<double> &offdg, const std::vector<double> &radmat, const std::vector<double> &angmat,
+                int iang11, int nmax1, int iq, int iq1, int iq2, int iang1, int iang2, int mvib1, int mvib2,
+                const RotBlock &b1, const RotBlock &b2) {
+    offdg.assign((size_t)mvib2 * mvib1, 0.0);
+    std::vector<double> pdg((size_t)iang1 * mvib2);
+    int ir1 = 0, ir2 = 0, ir = 0;
+    for (int i1 = 1; i1 <= nmax1; ++i1) {
+        for (int i2 = 1; i2 <= i1 - iq; ++i2) {
+            int i0 = ir1 * iang1;
+            ir1 = ir1 + 1;
+            int j0 = ir2 * iang2;
+            ir2 = ir2 + 1;
+            double rad = radmat[ir];
+            ir = ir + 1;
+            // pdg = radmat(ir) * angmat * coef2(j0 ...)
+            for (int v = 0; v < mvib2; ++v)
+                for (int a = 0; a < iang1; ++a) {
+                    double s = 0.0;
+                    for (int c = 0; c < iang2; ++c)
+                        s += angmat[(size_t)c * iang11 + a] * b2.coef[(size_t)v * b2.ibass + j0 + c];
+                    pdg[(size_t)v * iang1 + a] = rad * s;
+                }
+            // offdg += pdg^T coef1(i0 ...)
+            for (int v1 = 0; v1 < mvib1; ++v1)
+                for (int v2 = 0; v2 < mvib2; ++v2) {
+                    double s = 0.0;
+                    for (int a = 0; a < iang1; ++a)
+                        s += pdg[(size_t)v2 * iang1 + a] * b1.coef[(size_t)v1 * b1.ibass + i0 + a];
+                    offdg[(size_t)v1 * mvib2 + v2] += s;
+                }
+        }
+        ir1 = ir1 + iq1;
+        ir2 = ir2 + iq2;
+    }
+}
+
+int rotlev3b_run(const char *deck_text, const char *wave_path, double *levels, int cap, int *nlev) {
+    // deck: namelist, then the 12i5 card, title, optional ezero
+    std::vector<std::string> lines;
+    {
+        std::string cur;
+        for (const char *c = deck_text; *c; ++c) {
+            if (*c == '\n') {
+                lines.push_back(cur);
+                cur.clear();
+            } else if (*c != '\r') {
+                cur += *c;
+            }
+        }
+        if (!cur.empty()) lines.push_back(cur);
+    }
+    size_t li = 0;
+    while (li < lines.size() && lines[li].find('/') == std::string::npos) ++li;
+    ++li;
+    if (li >= lines.size()) fail(DVR3D_ERR_DECK);
+    auto i5 = [&](const std::string &s, int f) {
+        if ((size_t)(5 * f) >= s.size()) return 0;
+        std::string t = s.substr(5 * f, 5);
+        size_t a = t.find_first_not_of(' ');
+        return a == std::string::npos ? 0 : std::atoi(t.c_str() + a);
+    };
+    int nvib = i5(lines[li], 0), neval = i5(lines[li], 1), kmin = i5(lines[li], 2), ibass = i5(lines[li], 3);
+    int npnt = i5(lines[li], 5);
+    // file
+    RotFile f;
+    {
+        FILE *fp = std::fopen(wave_path, "rb");
+        if (!fp) fail(DVR3D_ERR_ARG);
+        std::fseek(fp, 0, SEEK_END);
+        long n = std::ftell(fp);
+        std::fseek(fp, 0, SEEK_SET);
+        f.b.resize((size_t)n);
+        if (n > 0 && std::fread(f.b.data(), 1, (size_t)n, fp) != (size_t)n) {
+            std::fclose(fp);
+            fail(DVR3D_ERR_ARG);
+        }
+        std::fclose(fp);
+    }
+    std::vector<int> h = f.ints();  // idia,ipar,ndvr,nmax,nmax,jrot,kmin0,meval,nlim (insize :155)
+    if (h.size() < 9) fail(DVR3D_ERR_ARG);
+    int idia = h[0], ipar = h[1], ndvr = h[2], nmax = h[3], jrot = h[5], kmin0 = h[6], meval = h[7];
+    if (idia != -2 || jrot <= 0) fail(DVR3D_ERR_UNSUPPORTED);
+    if (kmin != kmin0 && kmin0 != 2) fail(DVR3D_ERR_ARG);
+    if (kmin > 1 || (kmin == 0 && kmin0 != 0)) fail(DVR3D_ERR_UNSUPPORTED);
+    nvib = std::min(nvib, meval);  // insize :171-186
+    int nblk = kmin > 0 ? jrot + 1 : jrot;
+    if (neval <= 0) neval = 10;
+    npnt = std::max(ndvr, npnt);
+    f.skip();
+    f.skip();
+    std::vector<double> rm2(nmax);
+    f.getrow(rm2.data(), nmax);  // radint :686
+    f.skip();
+    // select :345-382 (blocks read sequentially) and solrt's reads
+    std::vector<RotBlock> blk(nblk);
+    std::vector<int> mvib(nblk);
+    int ipt = 0;
+    for (int ioff = 0; ioff < nblk; ++ioff) {
+        RotBlock &B = blk[ioff];
+        f.skip();  // xalf
+        std::vector<int> kk = f.ints();
+        B.k1 = kk[0];
+        B.maxleg = kk[1];
+        B.nang = kk[2];
+        B.pleg.assign((size_t)ndvr * ndvr, 0.0);
+        f.getrow(B.pleg.data(), B.nang * ndvr);
+        std::vector<int> ib = f.ints();
+        B.iang = ib[0];
+        B.ibass = ib[1];
+        std::vector<int> iv = f.ints();
+        B.iv.assign(iv.begin(), iv.begin() + B.nang);
+        B.meval = f.ints()[0];
+        mvib[ioff] = std::min(std::min(nvib, B.ibass), B.meval);
+        B.evib.resize(B.meval);
+        f.getrow(B.evib.data(), B.meval);
+        B.coef.assign((size_t)B.ibass * std::max(mvib[ioff], 1), 0.0);
+        for (int i = 0; i < B.meval; ++i) {
+            if (i < mvib[ioff]) f.getrow(&B.coef[(size_t)i * B.ibass], B.ibass);
+            else f.skip();
+        }
+        ipt += mvib[ioff];
+    }
+    int nbass = ipt;
+    if (ibass > 0 && ibass < ipt) {  // select :391-423
+        std::vector<int> iv(nblk, 1);
+        int p = 1;
+        for (int n = 1; n <= ibass; ++n) {
+            while (!(iv[p - 1] <= mvib[p - 1])) p = p + 1;
+            double evibr = blk[p - 1].evib[iv[p - 1] - 1];
+            int jpt = p;
+            for (int j = p + 1; j <= nblk; ++j) {
+                if (iv[j - 1] > mvib[j - 1]) continue;
+                if (blk[j - 1].evib[iv[j - 1] - 1] >= evibr) continue;
+                evibr = blk[j - 1].evib[iv[j - 1] - 1];
+                jpt = j;
+            }
+            iv[jpt - 1] = iv[jpt - 1] + 1;
+        }
+        for (int i = 0; i < nblk; ++i) mvib[i] = iv[i] - 1;
+        nbass = ibass;
+    }
+    neval = std::min(neval, nbass);
+    int iang = 0;
+    for (auto &B : blk) iang = std::max(iang, B.iang);
+    // radint :686-694
+    std::vector<double> radmee = rot_mkrad(nmax, rm2, 0, 0, 0), radmoo = rot_mkrad(nmax, rm2, 1, 0, 0),
+                        radmeo = rot_mkrad(nmax, rm2, 1, 1, 0), radmoe = rot_mkrad(nmax, rm2, 1, 1, 1);
+    // the Hamiltonian, in core (loadh :1296-1337)
+    std::vector<double> ham((size_t)nbass * nbass, 0.0);
+    std::vector<int> ist(nblk + 1, 0);
+    for (int i = 0; i < nblk; ++i) ist[i + 1] = ist[i] + mvib[i];
+    for (int i = 0; i < nblk; ++i)
+        for (int v = 0; v < mvib[i]; ++v) ham[(size_t)(ist[i] + v) * nbass + ist[i] + v] = blk[i].evib[v];
+    auto place = [&](int i, int j, const std::vector<double> &offdg) {
+        int p = 0;
+        for (int i1 = 0; i1 < mvib[i]; ++i1)
+            for (int i2 = 0; i2 < mvib[j]; ++i2) {
+                double x = offdg[p++];
+                ham[(size_t)(ist[j] + i2) * nbass + ist[i] + i1] = x;
+                ham[(size_t)(ist[i] + i1) * nbass + ist[j] + i2] = x;
+            }
+    };
+    double jjp1 = (double)(jrot * (jrot + 1));
+    const double sqrt2 = 1.4142135623731;
+    int ip = ipar;
+    for (int ioff = 2; ioff <= nblk; ++ioff) {  // solrt :1414-1527
+        const RotBlock &B1 = blk[ioff - 2], &B2 = blk[ioff - 1];
+        int k1 = B1.k1;
+        int mn = mvib[ioff - 2] * mvib[ioff - 1];
+        double angfac = +std::sqrt(jjp1 - (double)(k1 * (k1 + 1))) / 2.0;
+        if (k1 == 0) angfac = sqrt2 * angfac;
+        RotQuad q;
+        {
+            int npnt2 = (npnt + 1) / 2;
+            double tswalf = std::pow(2.0, k1 + k1 + 1) / (double)(k1 + 1);
+            for (int i = 1; i <= k1; ++i) tswalf = tswalf * (double)i / (double)(k1 + i + 1);
+            double cswalf;
+            rot_jacobi(npnt, npnt2, q.xalf, q.walf, (double)k1, (double)k1, cswalf, tswalf);
+            if (std::fabs((cswalf - tswalf) / tswalf) > 1.0e-8) fail(DVR3D_ERR_QUADRATURE);
+            for (int i = 1; i <= npnt2; ++i) {
+                q.xalf[npnt + 1 - i] = q.xalf[i];
+                q.xalf[i] = -q.xalf[i];
+                q.walf[npnt + 1 - i] = q.walf[i];
+            }
+        }
+        std::vector<double> angmat, offdg;
+        if (mn > 0) {
+            rot_angin(1, angmat, iang, q, npnt, ndvr, B1, B2, k1, angfac);
+            if (ip == 0)
+                rot_solofd(offdg, radmeo, angmat, iang, nmax, 1, 1, 0, B1.iang, B2.iang, mvib[ioff - 2],
+                           mvib[ioff - 1], B1, B2);
+            else
+                rot_solofd(offdg, radmoe, angmat, iang, nmax, 1, 0, 1, B1.iang, B2.iang, mvib[ioff - 2],
+                           mvib[ioff - 1], B1, B2);
+            place(ioff - 2, ioff - 1, offdg);
+        }
+        if (ioff == nblk) break;
+        const RotBlock &B3 = blk[ioff];
+        mn = mvib[ioff - 2] * mvib[ioff];
+        if (mn > 0) {
+            angfac = -std::sqrt((jjp1 - (double)((k1 + 1) * (k1 + 2))) * (jjp1 - (double)(k1 * (k1 + 1)))) / 16.0;
+            if (k1 == 0) angfac = sqrt2 * angfac;
+            rot_angin(2, angmat, iang, q, npnt, ndvr, B1, B3, k1, angfac);
+            if (ip == 0)
+                rot_solofd(offdg, radmee, angmat, iang, nmax, 0, 0, 0, B1.iang, B3.iang, mvib[ioff - 2],
+                           mvib[ioff], B1, B3);
+            else
+                rot_solofd(offdg, radmoo, angmat, iang, nmax, 1, 0, 0, B1.iang, B3.iang, mvib[ioff - 2],
+                           mvib[ioff], B1, B3);
+            place(ioff - 2, ioff, offdg);
+        }
+        ip = 1 - ip;
+    }
+    std::vector<double> ev(nbass);
+    diag(ham.data(), nbass, nbass, ev.data());
+    *nlev = neval;
+    if (levels) {
+        if (cap < neval) fail(DVR3D_ERR_BUFFER);
+        for (int i = 0; i < neval; ++i) levels[i] = ev[i];
+    }
+    return DVR3D_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1860,6 +2292,35 @@ double oracle_time_dsyev(int n, int reps, int mode) {
         tot += std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
     }
     return tot / reps;
+}
+
+int oracle_rot_quadrature(int npnt, int k, double *x, double *w, double *cswalf, double *tswalf) {
+    try {
+        int npnt2 = (npnt + 1) / 2;
+        double ts = std::pow(2.0, k + k + 1) / (double)(k + 1);
+        for (int i = 1; i <= k; ++i) ts = ts * (double)i / (double)(k + i + 1);
+        std::vector<double> xa, wa;
+        double cs = 0.0;
+        rot_jacobi(npnt, npnt2, xa, wa, (double)k, (double)k, cs, ts);
+        for (int i = 1; i <= npnt2; ++i) {
+            x[i - 1] = xa[i];
+            w[i - 1] = wa[i];
+        }
+        *cswalf = cs;
+        *tswalf = ts;
+        return DVR3D_OK;
+    } catch (Fail &f) {
+        return f.code;
+    }
+}
+
+int oracle_rotlev3b(const char *deck_text, const char *wave_path, double *levels, int cap, int *nlev) {
+    if (!deck_text || !wave_path || !nlev) return DVR3D_ERR_ARG;
+    try {
+        return rotlev3b_run(deck_text, wave_path, levels, cap, nlev);
+    } catch (Fail &f) {
+        return f.code;
+    }
 }
 
 }  // extern "C"

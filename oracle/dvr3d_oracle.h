@@ -81,6 +81,13 @@ int oracle_session_step(void *session, int units);
 int oracle_session_counts(void *session, int *iv2, int *n2d, int cap);
 int oracle_session_end(void *session, oracle_trace *trace, dvr3d_result *res);
 
+/* ROTLEV3B (source/rotlev3b_segmented.f90) for one parity on a first-step wavefunction file:
+ * lowest NEVAL levels (Eh) of the Coriolis-coupled Hamiltonian, diagonalised in core. */
+int oracle_rotlev3b(const char *deck_text, const char *wave_path, double *levels, int cap, int *nlev);
+/* ROTLEV3B's Gauss-associated Legendre rule (jacobi :941-1007): the npnt2 = (npnt+1)/2 points
+ * of the half range (descending from 1) and weights, computed and exact sums of weights. */
+int oracle_rot_quadrature(int npnt, int k, double *x, double *w, double *cswalf, double *tswalf);
+
 /* Derived sizes of insize (:171-638) for one k block (kk = loop index of ccmain :857). */
 int oracle_sizes(const dvr3d_deck *deck, int kk, int *out16);
 

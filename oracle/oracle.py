@@ -127,6 +127,9 @@ def load(build: bool = True) -> C.CDLL:
     lib.oracle_session_end.argtypes = [C.c_void_p, P(Trace), P(Result)]
     lib.oracle_time_dsyev.argtypes = [C.c_int, C.c_int, C.c_int]
     lib.oracle_time_dsyev.restype = C.c_double
+    lib.oracle_rotlev3b.argtypes = [C.c_char_p, C.c_char_p, P(C.c_double), C.c_int, P(C.c_int)]
+    lib.oracle_rot_quadrature.argtypes = [C.c_int, C.c_int, P(C.c_double), P(C.c_double), P(C.c_double),
+                                          P(C.c_double)]
     rc = lib.oracle_load_lapack(_lapack_path().encode(), b"scipy_")
     if rc != 0:
         raise RuntimeError("could not bind LAPACK dsyev for the oracle")
@@ -263,6 +266,29 @@ def solve(deck: Deck, kk: int = 0, pes=None, vgrid=None, final_mode: int = 0, wa
 def pes_morse_sum(p, r1: float, r2: float, x: float) -> float:
     pp = np.ascontiguousarray(np.asarray(p, dtype=np.float64))
     return load().oracle_pes_morse_sum(pp.ctypes.data_as(C.POINTER(C.c_double)), r1, r2, x)
+
+
+def rotlev3b(deck_text: str, wave_path: str) -> np.ndarray:
+    """ROTLEV3B's lowest levels (Eh) for one parity from a first-step wavefunction file."""
+    lv = np.zeros(20000)
+    n = C.c_int(0)
+    rc = load().oracle_rotlev3b(deck_text.encode(), str(wave_path).encode(),
+                                lv.ctypes.data_as(C.POINTER(C.c_double)), lv.size, C.byref(n))
+    if rc != 0:
+        raise RuntimeError(f"oracle_rotlev3b failed: {rc}")
+    return lv[:n.value].copy()
+
+
+def rot_quadrature(npnt: int, k: int):
+    """ROTLEV3B's Gauss-associated Legendre half-range rule: (x, w, computed sum, exact sum)."""
+    n2 = (npnt + 1) // 2
+    x, w = np.zeros(n2), np.zeros(n2)
+    cs, ts = C.c_double(0), C.c_double(0)
+    P = C.POINTER(C.c_double)
+    rc = load().oracle_rot_quadrature(npnt, k, x.ctypes.data_as(P), w.ctypes.data_as(P), C.byref(cs), C.byref(ts))
+    if rc != 0:
+        raise RuntimeError(f"oracle_rot_quadrature failed: {rc}")
+    return x, w, cs.value, ts.value
 
 
 def time_dsyev(n: int, reps: int = 1, mode: int = 0) -> float:

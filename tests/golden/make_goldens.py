@@ -4,7 +4,8 @@ Reads the job decks and printed outputs shipped with the reference (ExoMol/dvr3d
 writes ``quadrature_kat.json`` next to this script: for each example the deck text and,
 per k block, the printed Gauss-Laguerre points / r values / check sums (lagpt :1315-1361),
 Gauss-(associated) Legendre points / weights / check sums (ccmain :932-938) and, for the
-z-perpendicular embedding, Gauss-Jacobi points / weights (ccmain :956-960).
+z-perpendicular embedding, Gauss-Jacobi points / weights (ccmain :956-960); and the
+Gauss-associated Legendre rules ROTLEV3B prints (rotlev3b_segmented.f90 :752-757).
 
 The printed Laguerre "weights" column of these outputs comes from a later build of the
 program (outputs say "version of June 2010", the source "March 2002") that prints a
@@ -110,6 +111,42 @@ def parse_output(text: str) -> dict:
     return {"laguerre": lag, "legendre": leg, "gauss_jacobi": jac}
 
 
+# ROTLEV3B runs: its own Gauss-associated Legendre rule (jacobi :941-1007), printed by angin1
+# (:752-757) for each k of a Coriolis block pair.
+ROT_CASES = {
+    "water_rot_even": "water/results/result-even.water.rot",
+    "water_rot_odd": "water/results/result-odd.water.rot",
+}
+
+
+def parse_rot_output(text: str) -> list:
+    lines = text.splitlines()
+    out = []
+    i = 0
+    while i < len(lines):
+        m = re.search(r"(\d+) point gauss-associated legendre integration with k =\s*(\d+)", lines[i])
+        if m:
+            npnt, k = int(m.group(1)), int(m.group(2))
+            xs, ws = [], []
+            j = i + 1
+            while "computed sum of weights" not in lines[j]:
+                t = lines[j].split()
+                if len(t) == 2:
+                    try:
+                        xs.append(fnum(t[0]))
+                        ws.append(fnum(t[1]))
+                    except ValueError:
+                        pass
+                j += 1
+            comp = fnum(re.findall(FNUM, lines[j])[0])
+            exact = fnum(re.findall(FNUM, lines[j + 1])[0])
+            out.append({"npnt": npnt, "k": k, "x": xs, "w": ws, "computed_sum": comp, "exact_sum": exact})
+            i = j + 2
+            continue
+        i += 1
+    return out
+
+
 def main(ref: str) -> None:
     root = Path(ref)
     out = {"source": "ExoMol/dvr3d example decks and printed outputs", "cases": {}}
@@ -120,6 +157,8 @@ def main(ref: str) -> None:
         data["deck_file"] = job
         data["output_file"] = res
         out["cases"][name] = data
+    out["rot_cases"] = {name: {"output_file": res, "legendre": parse_rot_output((root / res).read_text())}
+                        for name, res in ROT_CASES.items()}
     (HERE / "quadrature_kat.json").write_text(json.dumps(out, indent=1))
     print("wrote", HERE / "quadrature_kat.json")
 

@@ -203,3 +203,25 @@ def test_zperp_product_host_grid_equals_oracle(kat, oracle_mod, name):
         r1, r2, xa = dvr3d_b200.host_grid(d, kk)
         np.testing.assert_array_equal(r1, np.array(q.r1[:len(r1)]))
         np.testing.assert_array_equal(xa, np.array(q.xalf[:len(xa)]))
+
+
+@pytest.mark.parametrize("name", ["water_rot_even", "water_rot_odd"])
+def test_rotlev3b_quadrature_matches_reference(kat, oracle_mod, name):
+    """ROTLEV3B's Gauss-associated Legendre rule (jacobi :941-1007: sign scan in steps of 1e-6,
+    Newton to 1e-12), as the water example's second step prints it (angin1 :752-757). Points
+    agree to the printed digits; the printed weights and their computed sum carry a few 1e-10
+    difference from the restated source (and from the exact rule, scipy roots_jacobi), which the
+    printing build's iteration left in them; the restatement is held to the exact rule."""
+    from scipy.special import roots_jacobi
+
+    blocks = kat["rot_cases"][name]["legendre"]
+    assert len(blocks) >= 2
+    for blk in blocks:
+        x, w, cs, ts = oracle_mod.rot_quadrature(blk["npnt"], blk["k"])
+        np.testing.assert_allclose(x, blk["x"], rtol=0, atol=1.01e-15)
+        np.testing.assert_allclose(w, blk["w"], rtol=5e-10, atol=0)
+        assert abs(ts - blk["exact_sum"]) <= 1e-14 * ts
+        assert abs(cs - blk["computed_sum"]) <= 1e-11
+        xr, wr = roots_jacobi(blk["npnt"], blk["k"], blk["k"])
+        np.testing.assert_allclose(x, xr[::-1][:len(x)], rtol=0, atol=1e-15)
+        np.testing.assert_allclose(w, wr[::-1][:len(w)], rtol=1e-10, atol=0)
