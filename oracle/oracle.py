@@ -162,8 +162,14 @@ def as_deck(deck) -> Deck:
 
 def k_blocks(deck) -> list[int]:
     """k-loop indices [kd .. ku] of ccmain (:811-819) for a deck (from oracle_sizes)."""
-    s = sizes(deck, 0)
-    return list(range(s["kd"], s["ku"] + 1))
+    deck = as_deck(deck)
+    for kk in range(0, 3):  # the loop may start at k = 1 (kmin = 1 without zbisc, or f parity)
+        try:
+            s = sizes(deck, kk)
+        except RuntimeError:
+            continue
+        return list(range(s["kd"], s["ku"] + 1))
+    raise RuntimeError("oracle_sizes failed for k = 0, 1, 2")
 
 
 def quadrature(deck, kk: int = 0) -> Quad:

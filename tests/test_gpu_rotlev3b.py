@@ -17,14 +17,16 @@ pytestmark = pytest.mark.gpu
 TOL_CM = 1e-6
 
 
-def _first_step(jrot: int, kmin: int, neval: int = 40):
+def _first_step(jrot: int, kmin: int, neval: int = 40, zlin: bool = True):
     w = configs.radau_water_like(12, 16, 30000.0, neval, title=f"rot J{jrot} kmin{kmin}")
     lines = w.deck.splitlines()
     c3 = list(lines[2])
     c3[5:10] = list(f"{jrot:5d}")
     c3[35:40] = list(f"{kmin:5d}")
     lines[2] = "".join(c3)
-    w.deck = "\n".join(lines).replace("ZPMIN=.TRUE.", "ZPMIN=.TRUE., ZROT=.TRUE., ZTRAN=.TRUE.") + "\n"
+    # ZLIN: testiv drops the functions left at theta = 0 instead of stopping (k >= 2 blocks)
+    flags = ", ZROT=.TRUE., ZTRAN=.TRUE." + (", ZLIN=.TRUE." if zlin else "")
+    w.deck = "\n".join(lines).replace("ZPMIN=.TRUE.", "ZPMIN=.TRUE." + flags) + "\n"
     return w
 
 
