@@ -157,6 +157,8 @@ void dvr3d_b200_destroy(dvr3d_ctx *ctx) {
         if (e) cudaEventDestroy(e);
     for (auto &e : ctx->panel_ev) cudaEventDestroy(e);
     for (auto &e : ctx->gemm_ev) cudaEventDestroy(e);
+    for (auto &g : ctx->graphs)
+        if (g.second.exec) cudaGraphExecDestroy(g.second.exec);
     if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
     delete ctx;
 }

@@ -61,6 +61,11 @@ struct dvr3d_ctx {
     std::vector<cudaEvent_t> gemm_ev;   // timing pool of the GEMM launches of an iterative solve
     bool lp_trained = false;            // arena "lp_w" holds a trained preconditioner network
     std::map<long long, int> tuned_split;  // autotuned split-K of the Krylov products per (N, b)
+    struct Graph {
+        cudaGraphExec_t exec = nullptr;
+        long long kernels = 0;          // kernel launches the graph replays
+    };
+    std::map<std::string, Graph> graphs;  // captured Krylov step sequences, by shape and buffers
     struct LpSet {                      // training pairs of the last training solve
         bool valid = false;
         int N = 0, nwant = 0, npair = 0;

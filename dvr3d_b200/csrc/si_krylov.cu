@@ -325,8 +325,51 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
     bool done = false, breakdown = false;
     std::vector<double> theta, rho;
     std::vector<int> perm;
+    // The block steps between two checks have no host synchronisation: outside GEMM timing they
+    // run as one CUDA graph, captured on the first solve of a shape (and buffers) in this
+    // context and replayed by later solves (DVR3D_NO_GRAPH=1 launches them one by one).
+    const char *ng = std::getenv("DVR3D_NO_GRAPH");
+    const bool use_graph = !log_gemms && !(ng && ng[0] == '1');
     while (!done) {
         tk.start(st);
+        std::string gkey;
+        bool replayed = false, capturing = false;
+        const long long kernels0 = g_kernel_launches;
+        if (use_graph && next > s) {
+            char kb[256];
+            std::snprintf(kb, sizeof(kb), "si:%d:%d:%d:%d:%d:%lld:%lld:%p:%p:%p:%p:%p:%p", N, b, s, next, trmm_s,
+                          ldq, ldT, (void *)Lb, (void *)Q, (void *)T, (void *)Y1, (void *)work, (void *)proj);
+            gkey = kb;
+            auto it = ctx->graphs.find(gkey);
+            if (it != ctx->graphs.end()) {
+                CK(cudaGraphLaunch(it->second.exec, st));
+                DVR3D_COUNT_LAUNCH(it->second.kernels);
+                replayed = true;
+            } else {
+                CK(cudaStreamBeginCapture(st, cudaStreamCaptureModeThreadLocal));
+                capturing = true;
+            }
+        }
+        // a failure while capturing ends the capture before the error propagates
+        struct CaptureGuard {
+            cudaStream_t st;
+            bool &on;
+            ~CaptureGuard() {
+                if (on) {
+                    cudaGraph_t g = nullptr;
+                    cudaStreamEndCapture(st, &g);
+                    if (g) cudaGraphDestroy(g);
+                    cudaGetLastError();
+                }
+            }
+        } guard{st, capturing};
+        const int s_first = s;
+        if (replayed) {
+            for (; s < next; ++s) {
+                const int m = (s + 1) * b;
+                flops += 2.0 * (double)N * N * b + 8.0 * (double)N * m * b + 8.0 * (double)N * b * b;
+            }
+        }
         for (; s < next; ++s) {
             const double *Qk = Q + (size_t)s * b * ldq;
             const int m = (s + 1) * b;
@@ -393,6 +436,21 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
             cholqr(W);
             flops += 2.0 * (double)N * N * b + 8.0 * (double)N * m * b + 8.0 * (double)N * b * b;
         }
+        if (capturing) {
+            cudaGraph_t graph = nullptr;
+            capturing = false;
+            CK(cudaStreamEndCapture(st, &graph));
+            cudaGraphExec_t exec = nullptr;
+            const cudaError_t ie = cudaGraphInstantiate(&exec, graph, 0);
+            cudaGraphDestroy(graph);
+            CK(ie);
+            dvr3d_ctx::Graph g;
+            g.exec = exec;
+            g.kernels = g_kernel_launches - kernels0;
+            ctx->graphs[gkey] = g;
+            CK(cudaGraphLaunch(exec, st));
+        }
+        (void)s_first;
         tk.stop(st);
         tk_ms += tk.ms();
         int qe = 0;
