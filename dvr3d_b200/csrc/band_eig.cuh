@@ -37,4 +37,18 @@ cudaError_t launch_band_chase(BandTri &t, cudaStream_t st);
 // Z (n x nev, ldz) <- Q Z with Q the product of the chase's reflectors (A = Q T Q^T).
 cudaError_t launch_band_backtransform(const BandTri &t, double *Z, long long ldz, int nev, cudaStream_t st);
 
+// Lowest eigenpairs without the reduction (band_bisect.cu): Gershgorin bounds and max |A|
+// into bounds[0..2]; Sturm-count bisection for the nev lowest eigenvalues into w (one warp
+// each, LDL^T of A - sigma I); inverse iteration per cluster of eigenvalues (clusters given by
+// cstart[0..ncl], ascending) into the columns of Z, with scratch of
+// band_bisect_scratch_doubles(n, b, ncl) doubles; *err = 1 when a vector's growth stays below
+// gmin. A: lower band of a symmetric matrix, column-major, half-bandwidth b <= kBandMaxBw.
+size_t band_bisect_scratch_doubles(int n, int b, int nclusters);
+cudaError_t launch_band_bounds(const double *A, long long lda, int n, int b, double *bounds, cudaStream_t st);
+cudaError_t launch_band_bisect(const double *A, long long lda, int n, int b, int nev, const double *bounds, double *w,
+                               cudaStream_t st);
+cudaError_t launch_band_invit(const double *A, long long lda, int n, int b, const double *w, const int *cstart, int ncl,
+                              const double *bounds, double *scratch, double *Z, long long ldz, double gmin, int *err,
+                              cudaStream_t st);
+
 }  // namespace dvr3d

@@ -756,6 +756,52 @@ bool band_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int b, int nev
     return true;
 }
 
+// Lowest eigenpairs of the band matrix by bisection and inverse iteration on LDL^T factors
+// (band_bisect.cu), with the same band check as band_lowest. Returns false (nothing usable)
+// when the band check fails or a vector's inverse iteration does not grow.
+bool band_lowest_bisect(dvr3d_ctx *ctx, double *A, long long lda, int n, int b, int nev, double *w, double *Z,
+                        long long ldz, double drop_rel, double *dropped_rel) {
+    cudaStream_t st = ctx->stream;
+    if (b < 1 || b > kBandMaxBw || n < 3 || nev > n) return false;
+    auto *mx = ctx->arena.get_t<unsigned long long>("bd_max", 2);
+    CK(launch_band_prepare(A, lda, n, b, mx, st));
+    double *bounds = ctx->arena.get_t<double>("bb_bounds", 4);
+    CK(launch_band_bounds(A, lda, n, b, bounds, st));
+    CK(launch_band_bisect(A, lda, n, b, nev, bounds, w, st));
+    unsigned long long hb[2] = {0, 0};
+    double hbd[3] = {0, 0, 0};
+    std::vector<double> wh(nev);
+    CK(cudaMemcpyAsync(hb, mx, sizeof(hb), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(hbd, bounds, sizeof(hbd), cudaMemcpyDeviceToHost, st));
+    CK(cudaMemcpyAsync(wh.data(), w, sizeof(double) * nev, cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    note_d2h(sizeof(hb) + sizeof(hbd) + sizeof(double) * nev);
+    double dropped, inside;
+    std::memcpy(&dropped, &hb[0], sizeof(double));
+    std::memcpy(&inside, &hb[1], sizeof(double));
+    const double rel = inside > 0.0 ? dropped / inside : (dropped > 0.0 ? 1.0 : 0.0);
+    if (dropped_rel) *dropped_rel = rel;
+    if (!(rel <= drop_rel)) return false;
+    // clusters: eigenvalues closer than 1e-10 ||A|| share a warp (Gram-Schmidt inside)
+    const double anorm = std::max(hbd[2], 1e-300);
+    std::vector<int> cs{0};
+    for (int j = 1; j < nev; ++j)
+        if (wh[j] - wh[j - 1] > 1.0e-10 * anorm) cs.push_back(j);
+    cs.push_back(nev);
+    const int ncl = (int)cs.size() - 1;
+    int *dcs = ctx->arena.get_t<int>("bb_cs", cs.size());
+    CK(cudaMemcpyAsync(dcs, cs.data(), sizeof(int) * cs.size(), cudaMemcpyHostToDevice, st));
+    note_h2d(sizeof(int) * cs.size());
+    double *scr = ctx->arena.get_t<double>("bb_scr", band_bisect_scratch_doubles(n, b, ncl));
+    int *err = ctx->arena.get_t<int>("bb_err", 1);
+    CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+    CK(launch_band_invit(A, lda, n, b, w, dcs, ncl, bounds, scr, Z, ldz, 1.0 / (1.0e-8 * anorm), err, st));
+    int he = 0;
+    CK(cudaMemcpyAsync(&he, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+    CK(cudaStreamSynchronize(st));
+    return he == 0;
+}
+
 // ---------------------------------------------------------------- one k block
 // ---------------------------------------------------------------- many Radau problems at once
 // The 2D stage of independent Radau problems (the repeated DVR3DRJZ runs of a fitting

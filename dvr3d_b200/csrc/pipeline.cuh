@@ -179,6 +179,11 @@ void dense_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int nev, bool
 bool band_lowest(dvr3d_ctx *ctx, double *A, long long lda, int n, int b, int nev, double *w, double *Z,
                  long long ldz, double drop_rel, double *dropped_rel);
 
+// The same eigenpairs by Sturm-count bisection and inverse iteration on LDL^T factors of the
+// band (no reduction); false when the band check fails or inverse iteration does not grow.
+bool band_lowest_bisect(dvr3d_ctx *ctx, double *A, long long lda, int n, int b, int nev, double *w, double *Z,
+                        long long ldz, double drop_rel, double *dropped_rel);
+
 // Shift-invert block Krylov solve for the lowest `nwant` levels of the assembled H3
 // (full symmetric storage, ldh even). emin_bound: a lower bound of the spectrum (min e2).
 // Returns false when it gives up (Krylov space limit, breakdown, no SPD shift found); the

@@ -24,6 +24,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <cstring>
 #include <numeric>
 #include <vector>
 
@@ -473,7 +474,16 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
         // T is block tridiagonal up to the rounding-level reorthogonalisation coefficients:
         // chase its band unless those are not small (then the dense reduction)
         double dropped = 0.0;
-        const bool banded = b <= kBandMaxBw && band_lowest(ctx, A, lda, m, b, kw, lam, Yv, m, 1.0e-11, &dropped);
+        const char *be = std::getenv("DVR3D_BAND_EIG");
+        const bool bisect = be && std::strcmp(be, "bisect") == 0;
+        bool banded = false;
+        if (b <= kBandMaxBw && bisect) banded = band_lowest_bisect(ctx, A, lda, m, b, kw, lam, Yv, m, 1.0e-11, &dropped);
+        if (!banded && bisect && b <= kBandMaxBw) {  // the factors overwrote nothing; redo the copy for the chase
+            DVR3D_COUNT_LAUNCH(1);
+            upper_sym_neg_kernel<<<nb256((long long)m * m), 256, 0, st>>>(T, ldT, m, A, lda);
+            CK(cudaGetLastError());
+        }
+        if (!banded) banded = b <= kBandMaxBw && band_lowest(ctx, A, lda, m, b, kw, lam, Yv, m, 1.0e-11, &dropped);
         if (!banded) {
             DVR3D_COUNT_LAUNCH(1);
             upper_sym_neg_kernel<<<nb256((long long)m * m), 256, 0, st>>>(T, ldT, m, A, lda);
