@@ -167,6 +167,64 @@ class Context:
                                                   None, 0, C.byref(n), buf, ln.value, None))
         return lv[:n.value].copy(), buf.value.decode()
 
+    def rotlev3b_trans(self, deck_text: str, wave_path: str, kvec_path: str) -> tuple[np.ndarray, str]:
+        """ROTLEV3B with ZTRAN (dvr3d_b200_rotlev3b_trans): the levels and the printed table; the
+        eigenvectors transformed back to the first step's basis are written to kvec_path."""
+        lv = np.zeros(20000)
+        n = C.c_int(0)
+        ln = C.c_size_t(0)
+        buf = C.create_string_buffer(1 << 20)
+        self._check(self._lib.dvr3d_b200_rotlev3b_trans(self._h, deck_text.encode(), str(wave_path).encode(),
+                                                        str(kvec_path).encode(),
+                                                        lv.ctypes.data_as(C.POINTER(C.c_double)), lv.size,
+                                                        C.byref(n), buf, len(buf), C.byref(ln)))
+        return lv[:n.value].copy(), buf.value.decode()
+
+    def dipole3(self, deck_text: str, ket_path: str, bra_path: str, dipd=None, dipsa=None,
+                tra_path: str | None = None, cap: int = 4096) -> dict:
+        """DIPOLE3 (dvr3d_b200_dipole3) on two wavefunction files with a Python dipole plug-in:
+        dipd(r1, r2, xcos, nu) -> component nu, or dipsa(q1, q2, cost) -> (dipx, dipy) for the
+        reference's own coordinate transform. Returns the energies e1, e2 (Eh), the transition
+        moments tz, tx and S(f-i) (neval1 x neval2, a.u.), the sizes and the printed table."""
+        if (dipd is None) == (dipsa is None):
+            raise ValueError("give exactly one of dipd, dipsa")
+        P = C.POINTER(C.c_double)
+        e1, e2 = np.zeros(cap), np.zeros(cap)
+        tz, tx, si = (np.zeros((cap, cap), order="F") for _ in range(3))
+        res = _abi.DipoleResult(cap1=cap, cap2=cap, e1=e1.ctypes.data_as(P), e2=e2.ctypes.data_as(P),
+                                tz=tz.ctypes.data_as(P), tx=tx.ctypes.data_as(P), sint=si.ctypes.data_as(P))
+        err = []
+
+        def _d(r1, r2, x, nu, u):
+            try:
+                return float(dipd(r1, r2, x, nu))
+            except Exception as e:  # noqa: BLE001 -- reported after the call
+                err.append(e)
+                return float("nan")
+
+        def _s(px, py, q1, q2, ct, u):
+            try:
+                dx, dy = dipsa(q1, q2, ct)
+                px[0], py[0] = float(dx), float(dy)
+            except Exception as e:  # noqa: BLE001
+                err.append(e)
+                px[0] = py[0] = float("nan")
+
+        f1 = _abi.DIPD_FN(_d) if dipd else _abi.DIPD_FN()
+        f2 = _abi.DIPSA_FN(_s) if dipsa else _abi.DIPSA_FN()
+        out = C.create_string_buffer(1 << 22)
+        ln = C.c_size_t(0)
+        rc = self._lib.dvr3d_b200_dipole3(self._h, deck_text.encode(), str(ket_path).encode(),
+                                          str(bra_path).encode(), f1, f2, None, (tra_path or "").encode(),
+                                          C.byref(res), out, len(out), C.byref(ln))
+        if err:
+            raise err[0]
+        self._check(rc)
+        n1, n2 = res.neval1, res.neval2
+        return dict(e1=e1[:n1].copy(), e2=e2[:n2].copy(), tz=tz[:n1, :n2].copy(), tx=tx[:n1, :n2].copy(),
+                    sint=si[:n1, :n2].copy(), neval1=n1, neval2=n2, j1=res.j1, j2=res.j2, kmin1=res.kmin1,
+                    kmin2=res.kmin2, nblocks=res.nblocks, text=out.value.decode())
+
     def split_gemm(self, a, b, nslice: int = 2) -> np.ndarray:
         """a^T b on the tensor cores from split-BF16 operands (dvr3d_b200_split_gemm):
         a is k x m, b is k x n (FP64); nslice 1 = one BF16 product, 2 = BF16x3."""

@@ -96,6 +96,23 @@ class Result(C.Structure):
                 ("low_iterations", C.c_int), ("low_matvecs", C.c_int)]
 
 
+class DipoleResult(C.Structure):
+    """struct dvr3d_dipole_result"""
+
+    _fields_ = [("cap1", C.c_int), ("cap2", C.c_int),
+                ("e1", C.POINTER(C.c_double)), ("e2", C.POINTER(C.c_double)),
+                ("tz", C.POINTER(C.c_double)), ("tx", C.POINTER(C.c_double)),
+                ("sint", C.POINTER(C.c_double)),
+                ("neval1", C.c_int), ("neval2", C.c_int), ("j1", C.c_int), ("j2", C.c_int),
+                ("kmin1", C.c_int), ("kmin2", C.c_int), ("nblocks", C.c_int)]
+
+
+# dvr3d_dipd_fn, dvr3d_dipsa_fn
+DIPD_FN = C.CFUNCTYPE(C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_void_p)
+DIPSA_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double, C.c_double, C.c_double,
+                       C.c_void_p)
+
+
 def header_entry_points() -> list[str]:
     """Names of the functions declared in include/dvr3d_b200.h."""
     text = HEADER.read_text()
@@ -127,6 +144,10 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "dvr3d_b200_set_wait_limit": (C.c_int, [vp, C.c_longlong]),
         "dvr3d_b200_rotlev3b": (C.c_int, [vp, C.c_char_p, C.c_char_p, P(C.c_double), C.c_int, P(C.c_int),
                                           C.c_char_p, C.c_size_t, P(C.c_size_t)]),
+        "dvr3d_b200_rotlev3b_trans": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, P(C.c_double), C.c_int,
+                                                P(C.c_int), C.c_char_p, C.c_size_t, P(C.c_size_t)]),
+        "dvr3d_b200_dipole3": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, DIPD_FN, DIPSA_FN, vp, C.c_char_p,
+                                         P(DipoleResult), C.c_char_p, C.c_size_t, P(C.c_size_t)]),
         "dvr3d_b200_split_gemm": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, P(C.c_double), C.c_longlong,
                                             P(C.c_double), C.c_longlong, C.c_int, P(C.c_double),
                                             C.c_longlong]),

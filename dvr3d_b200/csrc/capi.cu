@@ -13,6 +13,7 @@
 #include "learned_precond.cuh"
 #include "pipeline.cuh"
 #include "rotlev.cuh"
+#include "dipole.cuh"
 #include "tc_gemm.cuh"
 
 #define CK(x)                                          \
@@ -381,6 +382,38 @@ int dvr3d_b200_rotlev3b(dvr3d_ctx *ctx, const char *deck_text, const char *wave_
             std::memcpy(levels, lv.data(), sizeof(double) * lv.size());
         }
         copy_out(table, out, outcap, outlen);
+        return DVR3D_OK;
+    });
+}
+
+int dvr3d_b200_rotlev3b_trans(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, const char *kvec_path,
+                              double *levels, int cap, int *nlev, char *out, size_t outcap, size_t *outlen) {
+    if (!ctx || !deck_text || !wave_path || !kvec_path || !kvec_path[0] || !nlev) return DVR3D_ERR_ARG;
+    return guarded(ctx, [&]() -> int {
+        cudaSetDevice(ctx->device);
+        std::vector<double> lv;
+        std::string table;
+        dvr3d::RotInfo info;
+        dvr3d::rotlev3b_solve(ctx, deck_text, wave_path, lv, table, info, kvec_path);
+        *nlev = (int)lv.size();
+        if (levels) {
+            if (cap < (int)lv.size()) return fail_ctx(ctx, DVR3D_ERR_BUFFER, "levels buffer smaller than neval");
+            std::memcpy(levels, lv.data(), sizeof(double) * lv.size());
+        }
+        copy_out(table, out, outcap, outlen);
+        return DVR3D_OK;
+    });
+}
+
+int dvr3d_b200_dipole3(dvr3d_ctx *ctx, const char *deck_text, const char *ket_path, const char *bra_path,
+                       dvr3d_dipd_fn dipd, dvr3d_dipsa_fn dipsa, void *user, const char *tra_path,
+                       dvr3d_dipole_result *res, char *out, size_t outcap, size_t *outlen) {
+    if (!ctx || !deck_text || !ket_path || !bra_path || !res || (!dipd == !dipsa)) return DVR3D_ERR_ARG;
+    return guarded(ctx, [&]() -> int {
+        cudaSetDevice(ctx->device);
+        std::string text;
+        dvr3d::dipole3_run(ctx, deck_text, ket_path, bra_path, dipd, dipsa, user, tra_path, *res, text);
+        copy_out(text, out, outcap, outlen);
         return DVR3D_OK;
     });
 }

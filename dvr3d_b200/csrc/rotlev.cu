@@ -30,6 +30,7 @@
 #include "gemm64.cuh"
 #include "pipeline.cuh"
 #include "rotlev.cuh"
+#include "wavefile.cuh"
 
 #define CK(x)                                          \
     do {                                               \
@@ -42,54 +43,6 @@ namespace dvr3d {
 namespace {
 
 [[noreturn]] void bad(int code, const std::string &m) { throw HostError{code, m}; }
-
-// ---- the wavefunction file: sequential unformatted records (4-byte length before and after)
-struct Records {
-    std::vector<unsigned char> buf;
-    std::vector<std::pair<size_t, size_t>> rec;  // (offset, bytes)
-    size_t next = 0;
-
-    explicit Records(const std::string &path) {
-        std::ifstream f(path, std::ios::binary);
-        if (!f) bad(DVR3D_ERR_ARG, "cannot open the wavefunction file " + path);
-        buf.assign(std::istreambuf_iterator<char>(f), std::istreambuf_iterator<char>());
-        size_t pos = 0;
-        while (pos + 8 <= buf.size()) {
-            int32_t n = 0, m = 0;
-            std::memcpy(&n, &buf[pos], 4);
-            if (n < 0 || pos + 8 + (size_t)n > buf.size()) bad(DVR3D_ERR_ARG, "wavefunction file: broken record framing");
-            std::memcpy(&m, &buf[pos + 4 + n], 4);
-            if (m != n) bad(DVR3D_ERR_ARG, "wavefunction file: record lengths before and after differ");
-            rec.emplace_back(pos + 4, (size_t)n);
-            pos += 8 + (size_t)n;
-        }
-        if (pos != buf.size()) bad(DVR3D_ERR_ARG, "wavefunction file: trailing bytes");
-    }
-    bool more() const { return next < rec.size(); }
-    std::pair<const unsigned char *, size_t> take() {
-        if (next >= rec.size()) bad(DVR3D_ERR_ARG, "wavefunction file: ends before the expected record");
-        const auto r = rec[next++];
-        return {&buf[r.first], r.second};
-    }
-    std::vector<int> ints(size_t want_min = 0) {
-        auto r = take();
-        std::vector<int> v(r.second / 4);
-        std::memcpy(v.data(), r.first, v.size() * 4);
-        if (v.size() < want_min) bad(DVR3D_ERR_ARG, "wavefunction file: integer record too short");
-        return v;
-    }
-    std::vector<double> dbls(size_t want_min = 0) {
-        auto r = take();
-        std::vector<double> v(r.second / 8);
-        std::memcpy(v.data(), r.first, v.size() * 8);
-        if (v.size() < want_min) bad(DVR3D_ERR_ARG, "wavefunction file: real record too short");
-        return v;
-    }
-    const double *vec(size_t idx, size_t n) const {
-        if (idx >= rec.size() || rec[idx].second < n * 8) bad(DVR3D_ERR_ARG, "wavefunction file: vector record too short");
-        return reinterpret_cast<const double *>(&buf[rec[idx].first]);
-    }
-};
 
 // One k block of the file (ccmain :972-976, testiv :3446-3448, transr :3622-3641).
 struct KBlock {
@@ -375,7 +328,7 @@ std::string fmt_d(double v, int w, int d) {
 }  // namespace
 
 void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, std::vector<double> &levels,
-                    std::string &table, RotInfo &info) {
+                    std::string &table, RotInfo &info, const char *kvec_path) {
     const RotDeck rd = parse_rot_deck(deck_text);
     Records f(wave_path);
     // ---- header (setcon :1176-1184 as insize :155 reads it)
@@ -387,10 +340,11 @@ void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path
     if (kmin != kmin0 && kmin0 != 2) bad(DVR3D_ERR_ARG, "ROTLEV3B: kmin differs from the first step's kmin");
     if (kmin > 1 || (kmin == 0 && kmin0 != 0))
         bad(DVR3D_ERR_UNSUPPORTED, "ROTLEV3B: one parity per run, from a file of that parity (kmin 0 or 1)");
-    f.take();                                // logical flags, masses, g1, g2
-    f.take();                                // Morse constants
-    const std::vector<double> rm2 = f.dbls((size_t)nmax);  // r^-2 term (ccmain :824-833)
-    f.take();                                // r
+    const auto flags = f.take();                             // logical flags, masses, g1, g2
+    const std::vector<double> morse = f.dbls(6);             // Morse constants
+    const std::vector<double> rm2 = f.dbls((size_t)nmax);    // r^-2 term (ccmain :824-833)
+    const std::vector<double> rgrid = f.dbls((size_t)nmax);  // r
+    if (flags.second < 56) bad(DVR3D_ERR_ARG, "wavefunction file: short flags record");
     // ---- k blocks
     const int nblk = kmin > 0 ? jrot + 1 : jrot;
     std::vector<KBlock> kb;
@@ -559,7 +513,10 @@ void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path
     }
     // ---- lowest levels (dgrot)
     double *wv = ctx->arena.get_t<double>("rt_w_ev", neval);
-    dense_lowest(ctx, H, ldh, nbass, neval, false, wv, nullptr, 1, "rtd_", false, nullptr);
+    const bool ztran = kvec_path && kvec_path[0];
+    const long long ldz = ldh;
+    double *Z = ztran ? ctx->arena.get_t<double>("rt_z", (size_t)ldz * neval) : nullptr;
+    dense_lowest(ctx, H, ldh, nbass, neval, ztran, wv, Z, ztran ? ldz : 1, "rtd_", false, nullptr);
     levels.resize(neval);
     CK(cudaMemcpyAsync(levels.data(), wv, sizeof(double) * neval, cudaMemcpyDeviceToHost, st));
     CK(cudaStreamSynchronize(st));
@@ -567,6 +524,74 @@ void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path
     info.nblk = nblk;
     info.neval = neval;
     info.mvib = mvib;
+    // ---- ZTRAN: vectors back in the first step's basis, angular FBR (dstore :1917-2049)
+    if (ztran) {
+        std::vector<int> lmin(nblk), lbasis(nblk), nkbas(nblk);
+        int nend = 0;
+        for (int i = 0; i < nblk; ++i) {  // select :374-380
+            lmin[i] = kb[i].k;
+            lbasis[i] = kb[i].maxleg + kb[i].lincr - kb[i].k + 1;
+            nkbas[i] = (kb[i].ibass / kb[i].iang) * lbasis[i];
+            nend += nkbas[i];
+        }
+        FILE *fp = std::fopen(kvec_path, "wb");
+        if (!fp) bad(DVR3D_ERR_ARG, std::string("cannot open ") + kvec_path);
+        struct Closer {
+            FILE *f;
+            ~Closer() { std::fclose(f); }
+        } closer{fp};
+        RecordWriter w{fp};
+        for (int v : {idia, ipar0, ndvr, nmax, h[4], jrot, kmin, neval}) w.i4(v);
+        w.end();
+        w.put(flags.first, 56);  // zembed, zmors1, zmors2, xmass, g1, g2, zncor (zquad2 dropped)
+        w.end();
+        for (double v : morse) w.r8(v);
+        w.end();
+        w.i4(nend);
+        for (int v : lmin) w.i4(v);
+        for (int v : lbasis) w.i4(v);
+        for (int v : nkbas) w.i4(v);
+        w.end();
+        for (double v : rgrid) w.r8(v);
+        w.end();
+        w.i4(neval);
+        w.end();
+        for (double v : levels) w.r8(v);
+        w.end();
+        std::vector<double> dh;
+        for (int i = 0; i < nblk; ++i) {
+            const KBlock &b = kb[i];
+            const int mv = mvib[i], nang = lbasis[i], nrad = b.ibass / b.iang;
+            if (mv <= 0) continue;
+            if (nang > b.maxleg + 1) bad(DVR3D_ERR_ARG, "wavefunction file: angular basis larger than its transform");
+            // tofbr / jtran: B (nang x nrad mv) = P'' (nang x iang) V (iang x nrad mv), P''(j, kk) =
+            // pleg(j, kk-th kept angle)
+            std::vector<double> ps((size_t)nang * b.iang, 0.0);
+            int kk = 0;
+            for (int a = 0; a < b.nang; ++a) {
+                if (b.iv[a] == 0) continue;
+                if (kk >= b.iang) bad(DVR3D_ERR_ARG, "wavefunction file: more kept angles than iang");
+                for (int j = 0; j < nang; ++j) ps[(size_t)kk * nang + j] = b.pleg[(size_t)a * (b.maxleg + 1) + j];
+                ++kk;
+            }
+            if (kk != b.iang) bad(DVR3D_ERR_ARG, "wavefunction file: kept angles differ from iang");
+            double *Pd = ctx->arena.get_t<double>("rt_tp", ps.size());
+            CK(cudaMemcpyAsync(Pd, ps.data(), sizeof(double) * ps.size(), cudaMemcpyHostToDevice, st));
+            double *V = upload_vectors(b, mv, "rt_c1");
+            double *B = ctx->arena.get_t<double>("rt_tb", (size_t)nkbas[i] * mv);
+            double *D = ctx->arena.get_t<double>("rt_td", (size_t)nkbas[i] * neval);
+            launch_dgemm(false, false, nang, nrad * mv, b.iang, 1.0, Pd, nang, V, b.iang, 0.0, B, nang, st);
+            CK(cudaGetLastError());
+            // D (nkbas x nval) = B (nkbas x mv) C, C = rows off[i] .. of the eigenvectors
+            launch_dgemm(false, false, nkbas[i], neval, mv, 1.0, B, nkbas[i], Z + off[i], ldz, 0.0, D, nkbas[i], st);
+            CK(cudaGetLastError());
+            dh.resize((size_t)nkbas[i] * neval);
+            CK(cudaMemcpyAsync(dh.data(), D, sizeof(double) * dh.size(), cudaMemcpyDeviceToHost, st));
+            CK(cudaStreamSynchronize(st));
+            w.put(dh.data(), sizeof(double) * dh.size());
+            w.end();
+        }
+    }
     // ---- printed table (dgrot :1767-1769, :1795-1799)
     table.clear();
     char ln[160];

@@ -16,8 +16,9 @@ struct RotInfo {
 
 // ROTLEV3B for one parity: reads its deck (namelist PRT, nvib/neval/kmin/ibass/neval2/npnt card,
 // title, optional EZERO) and the first step's wavefunction file; returns the lowest levels (Eh)
-// and the printed level table. Throws HostError / CudaFail.
+// and the printed level table. With a kvec_path (ZTRAN) the eigenvectors are transformed back to
+// the first step's basis and written there as dstore does. Throws HostError / CudaFail.
 void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, std::vector<double> &levels,
-                    std::string &table, RotInfo &info);
+                    std::string &table, RotInfo &info, const char *kvec_path = nullptr);
 
 }  // namespace dvr3d

@@ -205,6 +205,52 @@ int dvr3d_b200_set_wait_limit(dvr3d_ctx *ctx, long long polls);
 int dvr3d_b200_rotlev3b(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, double *levels, int cap,
                         int *nlev, char *out, size_t outcap, size_t *outlen);
 
+/* The same with ROTLEV3B's ZTRAN: the eigenvectors are also transformed back to the first
+ * step's basis, the angular DVR of each k block taken to associated Legendre functions
+ * (dstore :1917-2049, tofbr :2175-2228, jtran :2230-2274), and written to kvec_path (unit
+ * KVEC = 8) in the record layout DIPOLE3 reads: the DVR3D header, (nend, lmin, lbasis, nkbas),
+ * the radial grid, nval, the levels (Eh), then one record d(nkbas(k), nval) per k block. */
+int dvr3d_b200_rotlev3b_trans(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, const char *kvec_path,
+                              double *levels, int cap, int *nlev, char *out, size_t outcap, size_t *outlen);
+
+/* ---- DIPOLE3: transition moments between two sets of vib-rot states ------------------- */
+/* The user's dipole surface, the two plug-ins of source/dipole3_segmented.f90:
+ *   DIPD(DIPC, R1, R2, XCOS, NU) (:2054): component nu (0: along the embedding z axis, 1: x)
+ *     at the scattering / Radau / bond coordinates of the wavefunction files;
+ *   DIPSA(DIPX, DIPY, Q1, Q2, COST) (:2108): the bond-frame components, called by the
+ *     reference's own DIPD, which does the coordinate transform and the rotation to the
+ *     embedding (bond-angle, scattering, general and bisector branches, :2065-2192). */
+typedef double (*dvr3d_dipd_fn)(double r1, double r2, double xcos, int nu, void *user);
+typedef void (*dvr3d_dipsa_fn)(double *dipx, double *dipy, double q1, double q2, double cost, void *user);
+
+typedef struct dvr3d_dipole_result {
+    int cap1, cap2;      /* in: capacity of e1 (cap1), e2 (cap2); tz, tx, sint hold cap1 x cap2 */
+    double *e1, *e2;     /* out: ket and bra energies (Eh) of the states taken                 */
+    double *tz, *tx;     /* out: z and x transition moments (a.u.) without the common factor
+                            sqrt((2j1+1)(2j2+1)), column-major, leading dimension cap1          */
+    double *sint;        /* out: S(f-i) in a.u. (the values written to unit ITRA)              */
+    int neval1, neval2;  /* out: ket and bra states taken (NV1, NV2, IBASE1, IBASE2)           */
+    int j1, j2, kmin1, kmin2;
+    int nblocks;         /* out: k -> k' blocks computed                                        */
+} dvr3d_dipole_result;
+
+/* DIPOLE3 (source/dipole3_segmented.f90): deck_text is its stdin (namelist PRT, title, card
+ * NPOT,NV1,NV2,IBASE1,IBASE2 (5i5), optional EZERO card (f20.0), insize :198-620, spect
+ * :1825-1954); ket_path and bra_path the two wavefunction files (units IKET = 11, IBRA = 12):
+ * a J = 0 file as dvr3d_b200_run_deck_wave writes it, or a J > 0 file as
+ * dvr3d_b200_rotlev3b_trans writes it. Exactly one of dipd / dipsa is given; it is called on
+ * the host at the radial DVR points and NPOT Gauss-Legendre points (lagpt :1141-1232). The
+ * vectors of every k block are evaluated at the angular points (dsrd :1412-1562, jtran
+ * :1564-1646) and the transition moments of each k -> k' block (trans :1648-1776) formed on the
+ * device as FP64 tensor-core (DMMA) GEMMs. Results go to res; out / outlen receive the printed
+ * table; with ZTRA (the default) and a non-empty tra_path the records of outpt (:1956-2003) are
+ * written to tra_path (appended unless ZSTART). Symmetrised Radau files (IDIA = -2, bisector
+ * embedding) and Jacobi files; both files without Coriolis coupling (ZNCOR), and restart runs
+ * (IRES), return DVR3D_ERR_UNSUPPORTED. */
+int dvr3d_b200_dipole3(dvr3d_ctx *ctx, const char *deck_text, const char *ket_path, const char *bra_path,
+                       dvr3d_dipd_fn dipd, dvr3d_dipsa_fn dipsa, void *user, const char *tra_path,
+                       dvr3d_dipole_result *res, char *out, size_t outcap, size_t *outlen);
+
 /* The split-BF16 tensor-core product of the mixed-precision form, on host buffers:
  *     c (m x n, ldc) = a^T b,   a: k x m (lda), b: k x n (ldb), all column-major FP64.
  * Each operand is split on the device into BF16 slices (x ~= hi + lo); nslice = 1 keeps hi

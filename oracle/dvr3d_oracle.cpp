@@ -1630,7 +1630,7 @@ struct RotFile {
 };
 
 struct RotBlock {
-    int k1, maxleg, nang, iang, ibass, meval;
+    int k1, maxleg, nang, lincr, iang, ibass, meval;
     std::vector<double> pleg;  // pleg(ndvr, ndvr) filled with nang*ndvr values (getrow)
     std::vector<int> iv;
     std::vector<double> evib;
@@ -1836,7 +1836,81 @@ void rot_solofd(std::vector<double> &offdg, const std::vector<double> &radmat, c
     }
 }
 
-int rotlev3b_run(const char *deck_text, const char *wave_path, double *levels, int cap, int *nlev) {
+// dstore :1917-2049 (itra = 1): the eigenvectors transformed to the first-step basis with the
+// angular DVR taken back to associated Legendre functions (tofbr :2175-2228, jtran :2230-2274),
+// one record per k block, for DIPOLE3.
+void rot_dstore(const char *kvec_path, const std::vector<int> &h, const std::vector<unsigned char> &rec2,
+                const std::vector<double> &rec3, const std::vector<double> &r, int jrot, int kmin, int ndvr,
+                const std::vector<RotBlock> &blk, const std::vector<int> &mvib, const std::vector<double> &vec,
+                int nbass, const std::vector<double> &ev, int nval) {
+    const int nblk = (int)blk.size();
+    std::vector<int> lmin(nblk), lbasis(nblk), nkbas(nblk);
+    int nend = 0;
+    for (int k = 0; k < nblk; ++k) {  // select :374-380
+        lmin[k] = blk[k].k1;
+        lbasis[k] = blk[k].maxleg + blk[k].lincr - blk[k].k1 + 1;
+        nkbas[k] = (blk[k].ibass / blk[k].iang) * lbasis[k];
+        nend += nkbas[k];
+    }
+    FILE *fp = std::fopen(kvec_path, "wb");
+    if (!fp) fail(DVR3D_ERR_ARG);
+    auto put = [&](const void *p, size_t n) {
+        const int32_t m = (int32_t)n;
+        std::fwrite(&m, 4, 1, fp);
+        if (n) std::fwrite(p, 1, n, fp);
+        std::fwrite(&m, 4, 1, fp);
+    };
+    const int hdr[8] = {h[0], h[1], h[2], h[3], h[4], jrot, kmin, nval};
+    put(hdr, sizeof(hdr));
+    put(rec2.data(), std::min<size_t>(rec2.size(), 56));  // zembed .. zncor (no zquad2)
+    put(rec3.data(), 8 * rec3.size());
+    std::vector<int> r4;
+    r4.push_back(nend);
+    r4.insert(r4.end(), lmin.begin(), lmin.end());
+    r4.insert(r4.end(), lbasis.begin(), lbasis.end());
+    r4.insert(r4.end(), nkbas.begin(), nkbas.end());
+    put(r4.data(), 4 * r4.size());
+    put(r.data(), 8 * r.size());
+    put(&nval, 4);
+    put(ev.data(), 8 * (size_t)nval);
+    int mend = 0;
+    for (int k = 0; k < nblk; ++k) {
+        const RotBlock &B = blk[k];
+        const int nang = lbasis[k], nrad = B.ibass / B.iang, mv = mvib[k];
+        const int mbeg = mend;
+        mend += mv;
+        if (mv <= 0) continue;
+        // jtran: b(j + mn*nang, l) = sum over kept angles of dvrvec(kk, mn) pleg(j, k)
+        std::vector<double> b((size_t)nkbas[k] * mv, 0.0);
+        for (int l = 0; l < mv; ++l) {
+            const double *dv = &B.coef[(size_t)l * B.ibass];
+            for (int j = 0; j < nang; ++j) {
+                for (int mn = 0; mn < nrad; ++mn) {
+                    double sumk = 0.0;
+                    int kk = 0;
+                    for (int a = 0; a < B.nang; ++a) {
+                        if (B.iv[a] == 0) continue;
+                        sumk += dv[kk + (size_t)mn * B.iang] * B.pleg[j + (size_t)a * ndvr];
+                        ++kk;
+                    }
+                    b[(size_t)l * nkbas[k] + j + (size_t)mn * nang] = sumk;
+                }
+            }
+        }
+        // d = b c, c(mvib(k), nval): rows mbeg.. of the eigenvectors
+        std::vector<double> d((size_t)nkbas[k] * nval, 0.0);
+        for (int i = 0; i < nval; ++i)
+            for (int l = 0; l < mv; ++l) {
+                const double c = vec[(size_t)i * nbass + mbeg + l];
+                for (int j = 0; j < nkbas[k]; ++j) d[(size_t)i * nkbas[k] + j] += b[(size_t)l * nkbas[k] + j] * c;
+            }
+        put(d.data(), 8 * d.size());
+    }
+    std::fclose(fp);
+}
+
+int rotlev3b_run(const char *deck_text, const char *wave_path, double *levels, int cap, int *nlev,
+                 const char *kvec_path = nullptr) {
     // deck: namelist, then the 12i5 card, title, optional ezero
     std::vector<std::string> lines;
     {
@@ -1888,11 +1962,17 @@ int rotlev3b_run(const char *deck_text, const char *wave_path, double *levels, i
     int nblk = kmin > 0 ? jrot + 1 : jrot;
     if (neval <= 0) neval = 10;
     npnt = std::max(ndvr, npnt);
-    f.skip();
-    f.skip();
+    std::vector<unsigned char> rec2;
+    {
+        auto r = f.rec();
+        rec2.assign(r.first, r.first + r.second);
+    }
+    std::vector<double> rec3(6);
+    f.getrow(rec3.data(), 6);
     std::vector<double> rm2(nmax);
     f.getrow(rm2.data(), nmax);  // radint :686
-    f.skip();
+    std::vector<double> rgrid(nmax);
+    f.getrow(rgrid.data(), nmax);
     // select :345-382 (blocks read sequentially) and solrt's reads
     std::vector<RotBlock> blk(nblk);
     std::vector<int> mvib(nblk);
@@ -1904,6 +1984,7 @@ int rotlev3b_run(const char *deck_text, const char *wave_path, double *levels, i
         B.k1 = kk[0];
         B.maxleg = kk[1];
         B.nang = kk[2];
+        B.lincr = kk.size() > 3 ? kk[3] : 0;
         B.pleg.assign((size_t)ndvr * ndvr, 0.0);
         f.getrow(B.pleg.data(), B.nang * ndvr);
         std::vector<int> ib = f.ints();
@@ -2015,6 +2096,7 @@ int rotlev3b_run(const char *deck_text, const char *wave_path, double *levels, i
     }
     std::vector<double> ev(nbass);
     diag(ham.data(), nbass, nbass, ev.data());
+    if (kvec_path) rot_dstore(kvec_path, h, rec2, rec3, rgrid, jrot, kmin, ndvr, blk, mvib, ham, nbass, ev, neval);
     *nlev = neval;
     if (levels) {
         if (cap < neval) fail(DVR3D_ERR_BUFFER);
@@ -2318,6 +2400,16 @@ int oracle_rotlev3b(const char *deck_text, const char *wave_path, double *levels
     if (!deck_text || !wave_path || !nlev) return DVR3D_ERR_ARG;
     try {
         return rotlev3b_run(deck_text, wave_path, levels, cap, nlev);
+    } catch (Fail &f) {
+        return f.code;
+    }
+}
+
+int oracle_rotlev3b_trans(const char *deck_text, const char *wave_path, const char *kvec_path, double *levels,
+                          int cap, int *nlev) {
+    if (!deck_text || !wave_path || !kvec_path || !nlev) return DVR3D_ERR_ARG;
+    try {
+        return rotlev3b_run(deck_text, wave_path, levels, cap, nlev, kvec_path);
     } catch (Fail &f) {
         return f.code;
     }

@@ -84,6 +84,19 @@ int oracle_session_end(void *session, oracle_trace *trace, dvr3d_result *res);
 /* ROTLEV3B (source/rotlev3b_segmented.f90) for one parity on a first-step wavefunction file:
  * lowest NEVAL levels (Eh) of the Coriolis-coupled Hamiltonian, diagonalised in core. */
 int oracle_rotlev3b(const char *deck_text, const char *wave_path, double *levels, int cap, int *nlev);
+/* DIPOLE3 (source/dipole3_segmented.f90) on two wavefunction files, arguments as
+ * dvr3d_b200_dipole3 (without the context). */
+int oracle_dipole3(const char *deck_text, const char *ket_path, const char *bra_path, dvr3d_dipd_fn dipd,
+                   dvr3d_dipsa_fn dipsa, void *user, const char *tra_path, dvr3d_dipole_result *res, char *out,
+                   size_t outcap, size_t *outlen);
+/* lagpt's angular rule (jacobi :1311-1368, alf = bta = 0): the npot/2 largest points, weights,
+ * computed and exact half sums of the weights. */
+int oracle_dipole_quadrature(int npot, double *x, double *w, double *csa, double *tsa);
+/* threej :1778-1823 */
+double oracle_threej(int j1, int j2, int j3, int m1, int m2, int m3);
+/* The same with ZTRAN: the transformed vectors (dstore :1917-2049) written to kvec_path. */
+int oracle_rotlev3b_trans(const char *deck_text, const char *wave_path, const char *kvec_path, double *levels,
+                          int cap, int *nlev);
 /* ROTLEV3B's Gauss-associated Legendre rule (jacobi :941-1007): the npnt2 = (npnt+1)/2 points
  * of the half range (descending from 1) and weights, computed and exact sums of weights. */
 int oracle_rot_quadrature(int npnt, int k, double *x, double *w, double *cswalf, double *tswalf);

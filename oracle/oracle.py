@@ -58,6 +58,22 @@ class Result(C.Structure):
                 ("lp_loss_first", C.c_double), ("lp_loss_last", C.c_double)]
 
 
+class DipoleResult(C.Structure):
+    """struct dvr3d_dipole_result (include/dvr3d_b200.h)."""
+
+    _fields_ = [("cap1", C.c_int), ("cap2", C.c_int),
+                ("e1", C.POINTER(C.c_double)), ("e2", C.POINTER(C.c_double)),
+                ("tz", C.POINTER(C.c_double)), ("tx", C.POINTER(C.c_double)),
+                ("sint", C.POINTER(C.c_double)),
+                ("neval1", C.c_int), ("neval2", C.c_int), ("j1", C.c_int), ("j2", C.c_int),
+                ("kmin1", C.c_int), ("kmin2", C.c_int), ("nblocks", C.c_int)]
+
+
+DIPD_FN = C.CFUNCTYPE(C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_void_p)
+DIPSA_FN = C.CFUNCTYPE(None, C.POINTER(C.c_double), C.POINTER(C.c_double), C.c_double, C.c_double, C.c_double,
+                       C.c_void_p)
+
+
 class Quad(C.Structure):
     _fields_ = [("npnt1", C.c_int), ("npnt2", C.c_int), ("nang2", C.c_int), ("nidvr", C.c_int),
                 ("y1", C.c_double * 128), ("wt1", C.c_double * 128), ("r1", C.c_double * 128),
@@ -128,6 +144,12 @@ def load(build: bool = True) -> C.CDLL:
     lib.oracle_time_dsyev.argtypes = [C.c_int, C.c_int, C.c_int]
     lib.oracle_time_dsyev.restype = C.c_double
     lib.oracle_rotlev3b.argtypes = [C.c_char_p, C.c_char_p, P(C.c_double), C.c_int, P(C.c_int)]
+    lib.oracle_rotlev3b_trans.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, P(C.c_double), C.c_int, P(C.c_int)]
+    lib.oracle_dipole3.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, DIPD_FN, DIPSA_FN, C.c_void_p, C.c_char_p,
+                                   P(DipoleResult), C.c_char_p, C.c_size_t, P(C.c_size_t)]
+    lib.oracle_dipole_quadrature.argtypes = [C.c_int, P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double)]
+    lib.oracle_threej.argtypes = [C.c_int] * 6
+    lib.oracle_threej.restype = C.c_double
     lib.oracle_rot_quadrature.argtypes = [C.c_int, C.c_int, P(C.c_double), P(C.c_double), P(C.c_double),
                                           P(C.c_double)]
     rc = lib.oracle_load_lapack(_lapack_path().encode(), b"scipy_")
@@ -283,6 +305,65 @@ def rotlev3b(deck_text: str, wave_path: str) -> np.ndarray:
     if rc != 0:
         raise RuntimeError(f"oracle_rotlev3b failed: {rc}")
     return lv[:n.value].copy()
+
+
+def rotlev3b_trans(deck_text: str, wave_path: str, kvec_path: str) -> np.ndarray:
+    """ROTLEV3B with ZTRAN: the levels, and the transformed vectors written to kvec_path."""
+    lv = np.zeros(20000)
+    n = C.c_int(0)
+    rc = load().oracle_rotlev3b_trans(deck_text.encode(), str(wave_path).encode(), str(kvec_path).encode(),
+                                      lv.ctypes.data_as(C.POINTER(C.c_double)), lv.size, C.byref(n))
+    if rc != 0:
+        raise RuntimeError(f"oracle_rotlev3b_trans failed: {rc}")
+    return lv[:n.value].copy()
+
+
+def dipole3(deck_text: str, ket_path: str, bra_path: str, dipd=None, dipsa=None, tra_path: str | None = None,
+            cap: int = 4096) -> dict:
+    """DIPOLE3 on two wavefunction files with a Python dipole plug-in: dipd(r1, r2, xcos, nu) -> float
+    or dipsa(q1, q2, cost) -> (dipx, dipy). Returns e1, e2, tz, tx, sint (neval1 x neval2), the
+    sizes and the printed text."""
+    if (dipd is None) == (dipsa is None):
+        raise ValueError("give exactly one of dipd, dipsa")
+    e1, e2 = np.zeros(cap), np.zeros(cap)
+    tz, tx, si = (np.zeros((cap, cap), order="F") for _ in range(3))
+    P = C.POINTER(C.c_double)
+    res = DipoleResult(cap1=cap, cap2=cap, e1=e1.ctypes.data_as(P), e2=e2.ctypes.data_as(P),
+                       tz=tz.ctypes.data_as(P), tx=tx.ctypes.data_as(P), sint=si.ctypes.data_as(P))
+    f1 = DIPD_FN(lambda r1, r2, x, nu, u: float(dipd(r1, r2, x, nu))) if dipd else DIPD_FN()
+
+    def _sa(px, py, q1, q2, ct, u):
+        dx, dy = dipsa(q1, q2, ct)
+        px[0] = dx
+        py[0] = dy
+
+    f2 = DIPSA_FN(_sa) if dipsa else DIPSA_FN()
+    out = C.create_string_buffer(1 << 22)
+    olen = C.c_size_t(0)
+    rc = load().oracle_dipole3(deck_text.encode(), str(ket_path).encode(), str(bra_path).encode(), f1, f2, None,
+                               (tra_path or "").encode(), C.byref(res), out, len(out), C.byref(olen))
+    if rc != 0:
+        raise RuntimeError(f"oracle_dipole3 failed: {rc}")
+    n1, n2 = res.neval1, res.neval2
+    return dict(e1=e1[:n1].copy(), e2=e2[:n2].copy(), tz=tz[:n1, :n2].copy(), tx=tx[:n1, :n2].copy(),
+                sint=si[:n1, :n2].copy(), neval1=n1, neval2=n2, j1=res.j1, j2=res.j2, kmin1=res.kmin1,
+                kmin2=res.kmin2, nblocks=res.nblocks, text=out.value.decode())
+
+
+def dipole_quadrature(npot: int):
+    """DIPOLE3's angular rule: the npot/2 largest Gauss-Legendre points, weights, and the
+    computed and exact half sums."""
+    x, w = np.zeros(npot // 2), np.zeros(npot // 2)
+    cs, ts = C.c_double(0), C.c_double(0)
+    P = C.POINTER(C.c_double)
+    rc = load().oracle_dipole_quadrature(npot, x.ctypes.data_as(P), w.ctypes.data_as(P), C.byref(cs), C.byref(ts))
+    if rc != 0:
+        raise RuntimeError(f"oracle_dipole_quadrature failed: {rc}")
+    return x, w, cs.value, ts.value
+
+
+def threej(j1: int, j2: int, j3: int, m1: int, m2: int, m3: int) -> float:
+    return load().oracle_threej(j1, j2, j3, m1, m2, m3)
 
 
 def rot_quadrature(npnt: int, k: int):

@@ -6,6 +6,9 @@ per k block, the printed Gauss-Laguerre points / r values / check sums (lagpt :1
 Gauss-(associated) Legendre points / weights / check sums (ccmain :932-938) and, for the
 z-perpendicular embedding, Gauss-Jacobi points / weights (ccmain :956-960); and the
 Gauss-associated Legendre rules ROTLEV3B prints (rotlev3b_segmented.f90 :752-757).
+It also writes ``dipole3_kat.json``: for each DIPOLE3 example (dipole3_segmented.f90) the
+deck, the printed angular rule, the ket / bra energies, spect's header and every printed
+row of its transition table.
 
 The printed Laguerre "weights" column of these outputs comes from a later build of the
 program (outputs say "version of June 2010", the source "March 2002") that prints a
@@ -147,6 +150,47 @@ def parse_rot_output(text: str) -> list:
     return out
 
 
+# DIPOLE3 runs: lagpt's Gauss-Legendre rule (jacobi :1311-1368, printed :1199-1206), spect's
+# header (:1881-1890) and its table of transitions (:1929-1948), with the ket and bra energies
+# dmain prints (:802-815).
+DIP_CASES = {
+    "water_dip": ("water/jobs/dip.job", "water/results/result.water.dip"),
+    "h3p_jacobi_dip": ("H3+Jacobi/jobs/dip.job", "H3+Jacobi/results/result.H3p.dip"),
+    "hcn_dip": ("HCN/jobs/dip.job", "HCN/results/result.HCN.dip"),
+}
+
+
+def parse_dip_output(text: str) -> dict:
+    lines = text.splitlines()
+    out = {"quadrature": parse_rot_output(text)[0]}
+    for ln in lines:
+        m = re.search(r"j1=\s*(-?\d+)\s+kmin1=\s*(-?\d+)\s+j2=\s*(-?\d+)\s+kmin2=\s*(-?\d+)\s+idia=\s*(-?\d+)"
+                      r"\s+ipar1=\s*(-?\d+)\s+ipar2=\s*(-?\d+)", ln)
+        if m:
+            out.update(zip(("j1", "kmin1", "j2", "kmin2", "idia", "ipar1", "ipar2"), map(int, m.groups())))
+        m = re.search(r"ground zero =\s*(\S+) cm-1", ln)
+        if m:
+            out["ezero"] = fnum(m.group(1))
+    for side in ("ket", "bra"):
+        i = next(k for k, ln in enumerate(lines) if f"First 10 energies for the {side} in a.u." in ln)
+        vals, j = [], i + 1
+        while len(vals) < 10 and j < len(lines):
+            toks = lines[j].split()
+            if toks and not all(re.fullmatch(FNUM, t) for t in toks):
+                break
+            vals += [fnum(t) for t in toks]
+            j += 1
+        out[f"e_{side}"] = vals
+    rows = []
+    head = next(k for k, ln in enumerate(lines) if ln.lstrip().startswith("ie1 ie2"))
+    for ln in lines[head + 1:]:
+        toks = ln.split()
+        if len(toks) == 10 and toks[0].isdigit() and toks[1].isdigit():
+            rows.append([int(toks[0]), int(toks[1])] + [float(t) for t in toks[2:]])
+    out["rows"] = rows
+    return out
+
+
 def main(ref: str) -> None:
     root = Path(ref)
     out = {"source": "ExoMol/dvr3d example decks and printed outputs", "cases": {}}
@@ -161,6 +205,15 @@ def main(ref: str) -> None:
                         for name, res in ROT_CASES.items()}
     (HERE / "quadrature_kat.json").write_text(json.dumps(out, indent=1))
     print("wrote", HERE / "quadrature_kat.json")
+    dip = {"source": "ExoMol/dvr3d DIPOLE3 example decks and printed outputs", "cases": {}}
+    for name, (job, res) in DIP_CASES.items():
+        data = parse_dip_output((root / res).read_text())
+        data["deck"] = (root / job).read_text()
+        data["deck_file"] = job
+        data["output_file"] = res
+        dip["cases"][name] = data
+    (HERE / "dipole3_kat.json").write_text(json.dumps(dip, indent=1))
+    print("wrote", HERE / "dipole3_kat.json")
 
 
 if __name__ == "__main__":
