@@ -1,7 +1,8 @@
 """Transition moments (the reference's DIPOLE3, dvr3d_b200_dipole3) and the ROTLEV3B vectors they
-read (ZTRAN, dvr3d_b200_rotlev3b_trans), on a chain built by the product: a J = 0 first-step
-wavefunction file (Radau, even radial parity) and a J = 1 e-parity set (first step with ZROT,
-odd radial parity, then ROTLEV3B with ZTRAN).
+read (ZTRAN, dvr3d_b200_rotlev3b_trans), on chains built by the product: a J = 0 first-step
+wavefunction file (Radau, even radial parity); J = 1 e-parity (first step with ZROT, odd radial
+parity, then ROTLEV3B with ZTRAN) and f-parity (the first-step file of its one k block) sets;
+J = 2 e and f sets from ROTLEV3B.
 
 * the ROTLEV3B vector file against the oracle's restatement of dstore on the same first-step
   file: identical header records, levels to 1e-12 Eh, every transformed vector to 1e-9 (each
@@ -78,14 +79,20 @@ def model_dipd(r1: float, r2: float, xcos: float, nu: int) -> float:
 
 @pytest.fixture(scope="module")
 def chain(ctx, tmp_path_factory):
+    """First-step files and ROTLEV3B vector files: J = 0 (even); J = 1 e (odd, k = 0, 1); J = 1
+    e (even) and f (even, k = 1: the first-step file itself; an odd J = 1 f run has no room in
+    MAX3D2, insize :335-342); J = 2 e (even, k = 0..2) and f (k = 1, 2)."""
     d = tmp_path_factory.mktemp("dip")
-    w0 = _deck(0, 0, 0)
-    ctx.set_pes(w0.pes)
-    ctx.run_deck(w0.deck, wave_path=str(d / "j0.26"))
-    w1 = _deck(1, 1, 1)
-    ctx.set_pes(w1.pes)
-    ctx.run_deck(w1.deck, wave_path=str(d / "j1.26"))
+    runs = {"j0.26": (0, 0, 0), "j1.26": (1, 1, 1), "j1e0.26": (1, 1, 0), "j1f.26": (1, 0, 0), "j2e.26": (2, 1, 0),
+            "j2f.26": (2, 0, 0)}
+    for name, (j, kmin, ipar) in runs.items():
+        w = _deck(j, kmin, ipar)
+        ctx.set_pes(w.pes)
+        ctx.run_deck(w.deck, wave_path=str(d / name))
     lv, table = ctx.rotlev3b_trans(_rot_deck(30, 20, 1), str(d / "j1.26"), str(d / "j1.8"))
+    ctx.rotlev3b_trans(_rot_deck(30, 20, 1), str(d / "j1e0.26"), str(d / "j1e0.8"))
+    ctx.rotlev3b_trans(_rot_deck(30, 20, 1), str(d / "j2e.26"), str(d / "j2e.8"))
+    ctx.rotlev3b_trans(_rot_deck(30, 20, 0), str(d / "j2f.26"), str(d / "j2f.8"))
     return d, lv, table
 
 
@@ -121,24 +128,30 @@ def test_rotlev3b_vectors_match_oracle(chain, oracle_mod):
     np.testing.assert_allclose(np.einsum("ij,ij->j", G, G), 1.0, atol=1e-9)
 
 
+# (ket, bra, plug-in, k -> k' blocks): J = 0 <-> 1 both ways, J = 1 e <-> f (the f set is a
+# single first-step block: DIPOLE3 skips the nu = +1 blocks of a one-block bra, :928) and
+# J = 2 e <-> f, the five blocks of the reference's water example.
 CASES = [
-    dict(order="j0-j1", plugin="dipsa"),
-    dict(order="j1-j0", plugin="dipsa"),
-    dict(order="j0-j1", plugin="dipd"),
+    ("j0.26", "j1.8", "dipsa", 2),
+    ("j1.8", "j0.26", "dipsa", 2),
+    ("j0.26", "j1.8", "dipd", 2),
+    ("j1e0.8", "j1f.26", "dipsa", 1),
+    ("j2e.8", "j2f.8", "dipsa", 5),
+    ("j2f.8", "j2e.8", "dipd", 5),
 ]
 
 
-@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c['order']}-{c['plugin']}")
+@pytest.mark.parametrize("case", CASES, ids=lambda c: f"{c[0]}-{c[1]}-{c[2]}")
 def test_dipole3_matches_oracle(ctx, oracle_mod, chain, case, tmp_path):
     d, _, _ = chain
-    ket, bra = (d / "j0.26", d / "j1.8") if case["order"] == "j0-j1" else (d / "j1.8", d / "j0.26")
-    kw = dict(dipsa=model_dipsa) if case["plugin"] == "dipsa" else dict(dipd=model_dipd)
+    ket, bra = d / case[0], d / case[1]
+    kw = dict(dipsa=model_dipsa) if case[2] == "dipsa" else dict(dipd=model_dipd)
     deck = _dip_deck(24, 10, 8, extra=", zstart=.true.")
     got = ctx.dipole3(deck, str(ket), str(bra), tra_path=str(tmp_path / "g.13"), **kw)
     ref = oracle_mod.dipole3(deck, str(ket), str(bra), tra_path=str(tmp_path / "r.13"), **kw)
     assert (got["neval1"], got["neval2"]) == (ref["neval1"], ref["neval2"]) == (10, 8)
     assert (got["j1"], got["j2"]) == (ref["j1"], ref["j2"])
-    assert got["nblocks"] == ref["nblocks"] > 0
+    assert got["nblocks"] == ref["nblocks"] == case[3]
     np.testing.assert_array_equal(got["e1"], ref["e1"])
     np.testing.assert_array_equal(got["e2"], ref["e2"])
     scale = max(np.abs(ref["tz"]).max(), np.abs(ref["tx"]).max())
