@@ -322,6 +322,102 @@ def run_batch64(args) -> int:
     return 0
 
 
+def _dipole_model(q1: float, q2: float, cost: float):
+    """Bond-frame dipole of an AB2 molecule (a.u.) for the DIPOLE3 workload: bisector component
+    symmetric in the two bonds, perpendicular one antisymmetric."""
+    import math
+
+    th = math.acos(max(-1.0, min(1.0, cost)))
+    c, s = math.cos(th / 2), math.sin(th / 2)
+    dy = (0.73 + 0.21 * (q1 + q2 - 3.62) - 0.05 * (q1 - q2) ** 2) * c * (1.0 + 0.1 * cost)
+    dx = (0.38 - 0.04 * (q1 + q2 - 3.62)) * (q1 - q2) * s
+    return dx, dy
+
+
+def run_dipole(args) -> int:
+    """Transition moments J = 2 e <-> J = 2 f (the reference's water example chain, at its sizes
+    and with all states): first steps (Radau, NPNT = 21, NALF = 40, EMAX2 = 40000 cm-1, ZROT,
+    ZTRAN), ROTLEV3B with ZTRAN (NVIB = 150, NEVAL = 200) for each parity -- not timed -- then
+    per step one DIPOLE3 run (NPOT = 60, all 200 x 200 states, five k -> k' blocks) through
+    dvr3d_b200_dipole3 with the files on disk and a Python DIPSA plug-in. Reported: runs/s end
+    to end, the device time and flop rate of its GEMMs, and the oracle's restatement of DIPOLE3
+    (the reference's rank-1 updates) on the same files on the host's cores."""
+    import tempfile
+
+    import torch
+
+    import dvr3d_b200
+    from dvr3d_b200 import configs
+
+    dev = 0
+    torch.cuda.set_device(dev)
+    ctx = dvr3d_b200.Context(dev)
+    tmp = tempfile.TemporaryDirectory()
+    d = Path(tmp.name)
+
+    def first_step(jrot, kmin, ipar, name):
+        w = configs.radau_water_like(21, 40, 40000.0, 200, title=f"dipole bench J{jrot} kmin{kmin}")
+        lines = w.deck.splitlines()
+        c3 = list(lines[2])
+        c3[5:10] = list(f"{jrot:5d}")
+        c3[35:40] = list(f"{kmin:5d}")
+        c3[45:50] = list(f"{ipar:5d}")
+        lines[2] = "".join(c3)
+        w.deck = "\n".join(lines).replace("ZPMIN=.TRUE.", "ZPMIN=.TRUE., ZROT=.TRUE., ZTRAN=.TRUE., ZLIN=.TRUE.") + "\n"
+        ctx.set_pes(w.pes)
+        ctx.run_deck(w.deck, wave_path=str(d / name))
+
+    def rot_deck(kmin):
+        return (" &PRT zdcore=.true., ztran=.true. /\n" + "".join(f"{v:5d}" for v in (150, 200, kmin, 0, 0, 0))
+                + "\n ROTLEV3B for DIPOLE3\n" + f"{4500.0:20.6f}\n")
+
+    first_step(2, 1, 0, "e.26")
+    first_step(2, 0, 0, "f.26")
+    ctx.rotlev3b_trans(rot_deck(1), str(d / "e.26"), str(d / "e.8"))
+    ctx.rotlev3b_trans(rot_deck(0), str(d / "f.26"), str(d / "f.8"))
+    deck = " &PRT zstart=.true. /\n DIPOLE3 bench\n" + "".join(f"{v:5d}" for v in (60, 200, 200, 0, 0)) + f"\n{4500.0:20.6f}\n"
+    ket, bra = str(d / "e.8"), str(d / "f.8")
+    run = lambda: ctx.dipole3(deck, ket, bra, dipsa=_dipole_model, tra_path=str(d / "g.13"), cap=256)  # noqa: E731
+    for _ in range(max(1, args.warmup)):
+        got = run()
+    walls, devs = [], []
+    with ClockSampler(dev) as clk:
+        for _ in range(args.steps):
+            t0 = time.perf_counter()
+            got = run()
+            walls.append(time.perf_counter() - t0)
+            devs.append(got["dev_ms"])
+    wall = float(np.median(walls))
+    dev_ms = float(np.median(devs))
+    # the oracle on the same files: parity and the host baseline
+    from oracle import oracle as O
+
+    t0 = time.perf_counter()
+    ref = O.dipole3(deck, ket, bra, dipsa=_dipole_model, tra_path=str(d / "r.13"), cap=256)
+    cpu_s = time.perf_counter() - t0
+    scale = max(np.abs(ref["tz"]).max(), np.abs(ref["tx"]).max())
+    err = max(np.abs(got["tz"] - ref["tz"]).max(), np.abs(got["tx"] - ref["tx"]).max()) / scale
+    peak = _fp64_peak(dev)
+    achieved = got["flops"] / (dev_ms * 1e-3) / 1e12
+    line = {"metric": "DIPOLE3 runs/s, J=2 e<->f, 200 x 200 states, NPOT=60", "value": 1.0 / wall, "unit": "runs/s",
+            "n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "ms_per_step": wall * 1e3,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic (seeded Morse + bend surface, model bond dipole)",
+            "config": {"workload": "Radau J=2 e/f first steps NPNT=21 NALF=40 EMAX2=40000, ROTLEV3B NVIB=150 NEVAL=200, "
+                                   "DIPOLE3 NPOT=60 NV1=NV2=200 (5 k->k' blocks)",
+                       "device_ms": dev_ms, "gflop": got["flops"] / 1e9, "blocks": got["nblocks"],
+                       "max_rel_err_vs_oracle": float(err)},
+            "roofline": {"bound": "fp64 tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                         "frac": achieved / peak},
+            "cpu_baseline": {"value": 1.0 / cpu_s, "unit": "runs/s", "cores": 1, "kind": "port",
+                             "sample": "the oracle's DIPOLE3 restatement (rank-1 updates as loops) on the same files, one run"},
+            "clocks": clk.summary()}
+    print(json.dumps(line), flush=True)
+    ctx.close()
+    tmp.cleanup()
+    return 0 if err < 1e-9 else 1
+
+
 def main() -> int:
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -335,14 +431,17 @@ def main() -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-solve", action="store_true",
                     help="one solve of the workload and nothing else (for ncu captures of its kernels)")
-    ap.add_argument("--workload", default="cfg4", choices=["cfg4", "batch64"],
-                    help="cfg4: the headline solve; batch64: 64 independent Radau problems per step")
+    ap.add_argument("--workload", default="cfg4", choices=["cfg4", "batch64", "dipole"],
+                    help="cfg4: the headline solve; batch64: 64 independent Radau problems per step; "
+                         "dipole: DIPOLE3 transition moments J=2 e<->f")
     args = ap.parse_args()
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if args.workload == "batch64" and args.impl == "ours":
         return run_batch64(args)
+    if args.workload == "dipole" and args.impl == "ours":
+        return run_dipole(args)
     if args.profile_solve:
         # one solve of the workload and nothing else. The chosen form: the 1D/2D stage,
         # assembly, the Cholesky-inverse (764 GEMM launches at this size, counting the start

@@ -223,7 +223,8 @@ class Context:
         n1, n2 = res.neval1, res.neval2
         return dict(e1=e1[:n1].copy(), e2=e2[:n2].copy(), tz=tz[:n1, :n2].copy(), tx=tx[:n1, :n2].copy(),
                     sint=si[:n1, :n2].copy(), neval1=n1, neval2=n2, j1=res.j1, j2=res.j2, kmin1=res.kmin1,
-                    kmin2=res.kmin2, nblocks=res.nblocks, text=out.value.decode())
+                    kmin2=res.kmin2, nblocks=res.nblocks, dev_ms=res.dev_ms, flops=res.flops,
+                    text=out.value.decode())
 
     def split_gemm(self, a, b, nslice: int = 2) -> np.ndarray:
         """a^T b on the tensor cores from split-BF16 operands (dvr3d_b200_split_gemm):

@@ -416,7 +416,28 @@ struct Dip {
     std::vector<int> nbass[2];
     std::vector<double> r1, r2, xd, wtd, dipol;
     DipoleFn fn{};
-    long long flops = 0;
+    double flops = 0.0;
+    double dev_ms = 0.0;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    ~Dip() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+    }
+    // device work between begin() and end() is timed with events on the context's stream
+    void begin() {
+        if (!ev0) {
+            CK(cudaEventCreate(&ev0));
+            CK(cudaEventCreate(&ev1));
+        }
+        CK(cudaEventRecord(ev0, st));
+    }
+    void end() {
+        CK(cudaEventRecord(ev1, st));
+        CK(cudaEventSynchronize(ev1));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ev0, ev1));
+        dev_ms += ms;
+    }
 
     // lagpt: points, weights and the weighted dipole at (r1(i1), r2(i2), xd(j)) in the order
     // trans reads it (i2 outer; symmetric Radau: i1 <= i2 - (1 - |nu|)).
@@ -558,6 +579,7 @@ struct Dip {
             for (int i = 0; i < ipot; ++i) pd[(size_t)l * ipot + i] = P[(size_t)(jfirst + step * l) * ipot + i];
         double *dv = ctx->arena.get_t<double>("dp_v" + tg, v.size());
         double *dpd = ctx->arena.get_t<double>("dp_pd" + tg, pd.size());
+        begin();
         CK(cudaMemcpyAsync(dv, v.data(), 8 * v.size(), cudaMemcpyHostToDevice, st));
         CK(cudaMemcpyAsync(dpd, pd.data(), 8 * pd.size(), cudaMemcpyHostToDevice, st));
         const double *fb = dv;
@@ -569,7 +591,7 @@ struct Dip {
             if (nkept > 0) {
                 launch_dgemm(false, false, nang, nrad * n, nkept, 1.0, dpk, nang, dv, iang, 0.0, df, nang, st);
                 CK(cudaGetLastError());
-                flops += 2LL * nang * nkept * (long long)nrad * n;
+                flops += 2.0 * nang * nkept * (double)nrad * n;
             } else {
                 CK(cudaMemsetAsync(df, 0, 8 * (size_t)nang * nrad * n, st));
             }
@@ -578,8 +600,8 @@ struct Dip {
         // A (ipot x nrad n) = Pd (ipot x nang) FBR (nang x nrad n)
         launch_dgemm(false, false, ipot, nrad * n, nang, 1.0, dpd, ipot, fb, nang, 0.0, A, ipot, st);
         CK(cudaGetLastError());
-        flops += 2LL * ipot * nang * (long long)nrad * n;
-        CK(cudaStreamSynchronize(st));  // host buffers v, pd, pk go out of scope
+        flops += 2.0 * ipot * nang * (double)nrad * n;
+        end();  // also the host buffers v, pd, pk may go out of scope now
         return nrad;
     }
 
@@ -605,14 +627,15 @@ struct Dip {
         if (K == 0) return;
         double *dw = ctx->arena.get_t<double>("dp_w", (size_t)K);
         double *S = ctx->arena.get_t<double>("dp_s", (size_t)K * ne[1]);
+        begin();
         CK(cudaMemcpyAsync(dw, wv.data(), 8 * (size_t)K, cudaMemcpyHostToDevice, st));
         DVR3D_COUNT_LAUNCH(1);
         scale_rows_kernel<<<grid_for((long long)K * ne[1]), 256, 0, st>>>(A1, (long long)nrad1 * ipot, dw, K, ne[1], S);
         CK(cudaGetLastError());
         launch_dgemm(true, false, ne[0], ne[1], K, 1.0, A0, (long long)nrad0 * ipot, S, K, 1.0, T, ne[0], st);
         CK(cudaGetLastError());
-        flops += 2LL * ne[0] * ne[1] * (long long)K;
-        CK(cudaStreamSynchronize(st));
+        flops += 2.0 * ne[0] * ne[1] * (double)K;
+        end();
     }
 };
 
@@ -904,6 +927,8 @@ void dipole3_run(dvr3d_ctx *ctx, const char *deck_text, const char *ket_path, co
     res.kmin1 = D.kmin[0];
     res.kmin2 = D.kmin[1];
     res.nblocks = iblock;
+    res.dev_ms = D.dev_ms;
+    res.flops = D.flops;
     auto put = [&](double *dst, const std::vector<double> &src) {
         if (!dst) return;
         for (int b = 0; b < n1; ++b)

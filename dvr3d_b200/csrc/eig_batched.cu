@@ -302,6 +302,10 @@ __global__ void __launch_bounds__(kVecThreads) eigvecs_kernel(BatchDesc bd, cons
 //     W = V^T z, W2 = Tm W and z -= V W2 in registers.
 constexpr int kFastPanel = 16;
 
+// The first vector of eigvecs_fast_kernel that failed its growth test since the last clear:
+// {failed, block, eigenvalue index, block order}, for the host's error message.
+__device__ int g_invit_fail[4];
+
 __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double *dg, const double *eo,
                                     const double *tauo, const double *wo, const int *sel, const long long *zoff,
                                     const int *zld, double *Z, int *err) {
@@ -385,6 +389,10 @@ __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double 
                     }
                     if (fabs(av) < tiny) av = (av < 0.0) ? -tiny : tiny;
                     D[n - 1] = av;
+                    // no superdiagonals in the last row of U; the back substitution reads them
+                    // (times zero), so stale shared memory must not leave a NaN there
+                    E1[n - 1] = 0.0;
+                    E2[n - 1] = 0.0;
                 }
                 __syncwarp();
                 for (int i = lane; i < n - 1; i += 32)
@@ -449,7 +457,14 @@ __global__ void eigvecs_fast_kernel(BatchDesc bd, const double *A, const double 
                     for (int i = lane; i < n; i += 32) x[i] *= inv;
                     __syncwarp();
                 }
-                if (grown < kInvitGrowPasses && lane == 0 && err) *err = 1;
+                if (grown < kInvitGrowPasses && lane == 0 && err) {
+                    *err = kDevNoConv;
+                    if (atomicCAS(&g_invit_fail[0], 0, 1) == 0) {
+                        g_invit_fail[1] = b;
+                        g_invit_fail[2] = j;
+                        g_invit_fail[3] = n;
+                    }
+                }
                 // sign convention: the first largest component positive
                 double big = 0.0;
                 int bi = n;
@@ -652,6 +667,20 @@ void launch_eigvecs_batched_fast(const BatchDesc &bd, const double *A, const dou
     const int parts = (bd.nblk < nsm) ? 2 : 1;
     DVR3D_COUNT_LAUNCH(1);
     eigvecs_fast_kernel<<<dim3(bd.nblk, parts), 32 * nwarp, smem, st>>>(bd, A, d, e, tau, w, sel, zoff, zld, Z, err);
+}
+
+void invit_fail_clear(cudaStream_t st) {
+    void *p = nullptr;
+    if (cudaGetSymbolAddress(&p, g_invit_fail) == cudaSuccess) cudaMemsetAsync(p, 0, sizeof(int) * 4, st);
+}
+
+void invit_fail_info(cudaStream_t st, int out[4]) {
+    void *p = nullptr;
+    out[0] = out[1] = out[2] = out[3] = 0;
+    if (cudaGetSymbolAddress(&p, g_invit_fail) == cudaSuccess) {
+        cudaMemcpyAsync(out, p, sizeof(int) * 4, cudaMemcpyDeviceToHost, st);
+        cudaStreamSynchronize(st);
+    }
 }
 
 }  // namespace dvr3d

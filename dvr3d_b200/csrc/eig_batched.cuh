@@ -50,6 +50,10 @@ void launch_eigvecs_batched(const BatchDesc &bd, const double *A, const double *
 // with the factors in shared memory (one warp per cluster) and a blocked back-transformation.
 // Both set *err = 1 (err may be null) when inverse iteration fails its growth test for some
 // vector (dstein's convergence criterion); the flag is never cleared by the kernels.
+// Diagnostics of the fast batched inverse iteration: the first vector that failed its growth
+// test since the last clear ({failed, block, eigenvalue index, block order}).
+void invit_fail_clear(cudaStream_t st);
+void invit_fail_info(cudaStream_t st, int out[4]);
 void launch_eigvecs_batched_fast(const BatchDesc &bd, const double *A, const double *d, const double *e,
                                  const double *tau, const double *w, const int *sel, const long long *zoff,
                                  const int *zld, double *Z, int nmax, int *err, cudaStream_t st);

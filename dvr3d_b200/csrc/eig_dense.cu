@@ -746,8 +746,12 @@ __global__ void __launch_bounds__(32) invit_smem_kernel(const double *d, const d
                         bv = -mlt * bn;
                     }
                 }
-                if (fabs(av) < tiny) av = (av < 0.0) ? -tiny : tiny;
+                    if (fabs(av) < tiny) av = (av < 0.0) ? -tiny : tiny;
                 D[n - 1] = av;
+                // no superdiagonals in the last row of U; the back substitution reads them
+                // (times zero), so stale shared memory must not leave a NaN there
+                E1[n - 1] = 0.0;
+                E2[n - 1] = 0.0;
             }
             __syncwarp();
             for (int i = lane; i < n - 1; i += 32)

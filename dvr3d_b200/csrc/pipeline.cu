@@ -99,6 +99,14 @@ void check_dev_err(dvr3d_ctx *ctx, const int *err_dev, const char *stage) {
     t_d2h += sizeof(int);
     CK(cudaStreamSynchronize(ctx->stream));
     if (e == kDevBarrierTimeout) throw HostError{DVR3D_ERR_NOCONV, std::string(stage) + ": grid barrier wait exceeded its limit"};
+    if (e == kDevNoConv) {
+        int f[4];
+        invit_fail_info(ctx->stream, f);
+        std::string where;
+        if (f[0]) where = " (block " + std::to_string(f[1] + 1) + ", vector " + std::to_string(f[2] + 1) + " of order " +
+                          std::to_string(f[3]) + ")";
+        throw HostError{DVR3D_ERR_NOCONV, std::string(stage) + ": did not converge" + where};
+    }
     if (e != 0) throw HostError{DVR3D_ERR_NOCONV, std::string(stage) + ": device error flag " + std::to_string(e)};
 }
 
@@ -1258,12 +1266,13 @@ void solve_block(dvr3d_ctx *ctx, const dvr3d_deck &deck, int kk, const dvr3d_opt
     std::memset(res.dom_kernel, 0, sizeof(res.dom_kernel));
     cudaStream_t st = ctx->stream;
     CK(cudaMemsetAsync(ev_err(ctx), 0, sizeof(int), st));
+    invit_fail_clear(st);
     CK(cudaEventRecord(ctx->ev[0], st));
     Contracted C;
     if (p.radau) radau_stage(ctx, p, C);
     else jacobi_stage(ctx, p, C);
     CK(cudaEventRecord(ctx->ev[1], st));
-    check_dev_err(ctx, ev_err(ctx), "batched inverse iteration (1D/2D eigenvectors)");
+    check_dev_err(ctx, ev_err(ctx), ("batched inverse iteration (1D/2D eigenvectors, k = " + std::to_string(p.kz) + ")").c_str());
     solve_contracted(ctx, p, C, opt, res, wave, th0, th1, launches0);
 }
 

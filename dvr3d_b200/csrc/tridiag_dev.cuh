@@ -57,7 +57,7 @@ static __device__ __forceinline__ double invit_growth_limit(int n) { return sqrt
 
 // One thread: eigenvectors of the cluster [j0, j1) of T. Factor arrays interleaved with
 // stride T (thread slots), vectors interleaved with stride nsel (eigenvalue slots). A vector
-// that fails the growth test sets *err = 1 (when err is not null).
+// that fails the growth test sets *err = kDevNoConv (when err is not null).
 static __device__ __noinline__ void invit_cluster(const double *d, const double *e, int n, const double *w, int j0,
                               int j1, double onenrm, double *fac, int T, int t, double *X,
                               int nsel, int *err) {
@@ -101,6 +101,10 @@ static __device__ __noinline__ void invit_cluster(const double *d, const double 
         }
         if (fabs(av) < tiny) av = (av < 0.0) ? -tiny : tiny;
         F(D, n - 1) = av;
+        // the last row of U has no superdiagonals; the back substitution reads them (times
+        // zero), so they must not hold stale non-finite values
+        F(E1, n - 1) = 0.0;
+        F(E2, n - 1) = 0.0;
         for (int i = 0; i < n - 1; ++i)
             if (fabs(F(D, i)) < tiny) F(D, i) = (F(D, i) < 0.0) ? -tiny : tiny;
         // deterministic start vector in (-1, 1)
@@ -151,7 +155,7 @@ static __device__ __noinline__ void invit_cluster(const double *d, const double 
             const double inv = (nrm > 0.0) ? 1.0 / nrm : 0.0;
             for (int i = 0; i < n; ++i) XV(i, j) *= inv;
         }
-        if (grown < kInvitGrowPasses && err) *err = 1;
+        if (grown < kInvitGrowPasses && err) *err = kDevNoConv;
         // sign convention: largest component positive
         double big = 0.0;
         for (int i = 0; i < n; ++i)

@@ -232,6 +232,9 @@ typedef struct dvr3d_dipole_result {
     int neval1, neval2;  /* out: ket and bra states taken (NV1, NV2, IBASE1, IBASE2)           */
     int j1, j2, kmin1, kmin2;
     int nblocks;         /* out: k -> k' blocks computed                                        */
+    double dev_ms;       /* out: device time (CUDA events) of the vector uploads, the angular
+                            transforms and the moment products                                */
+    double flops;        /* out: their algorithmic floating-point operations                   */
 } dvr3d_dipole_result;
 
 /* DIPOLE3 (source/dipole3_segmented.f90): deck_text is its stdin (namelist PRT, title, card

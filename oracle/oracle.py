@@ -66,7 +66,8 @@ class DipoleResult(C.Structure):
                 ("tz", C.POINTER(C.c_double)), ("tx", C.POINTER(C.c_double)),
                 ("sint", C.POINTER(C.c_double)),
                 ("neval1", C.c_int), ("neval2", C.c_int), ("j1", C.c_int), ("j2", C.c_int),
-                ("kmin1", C.c_int), ("kmin2", C.c_int), ("nblocks", C.c_int)]
+                ("kmin1", C.c_int), ("kmin2", C.c_int), ("nblocks", C.c_int),
+                ("dev_ms", C.c_double), ("flops", C.c_double)]
 
 
 DIPD_FN = C.CFUNCTYPE(C.c_double, C.c_double, C.c_double, C.c_double, C.c_int, C.c_void_p)

@@ -173,3 +173,25 @@ def test_jacobi_j1_wavefunction_file_two_k_blocks(ctx, oracle_mod, tmp_path):
     for k in ks:
         i = _check_block(recs, i, oracle_mod, w, k, radau=False)
     assert i == len(recs)
+
+
+def test_j2_wave_run_after_back_transforms(ctx, tmp_path):
+    """A J = 2 Radau job (k = 0, 1, 2; NPNT = 21, NALF = 40, 2D blocks of 231 and 210) with the
+    wavefunction file, run repeatedly: each k block follows the previous block's back-transform
+    GEMMs. The batched inverse iteration must not read stale shared memory: its LU leaves the
+    last row's superdiagonals to be set explicitly (the back substitution multiplies them by
+    zero, and a NaN left there by an earlier kernel poisoned a vector)."""
+    w = configs.radau_water_like(21, 40, 40000.0, 200, title="J2 wave")
+    lines = w.deck.splitlines()
+    c3 = list(lines[2])
+    c3[5:10] = list(f"{2:5d}")
+    c3[35:40] = list(f"{1:5d}")
+    lines[2] = "".join(c3)
+    w.deck = "\n".join(lines).replace("ZPMIN=.TRUE.", "ZPMIN=.TRUE., ZROT=.TRUE., ZTRAN=.TRUE., ZLIN=.TRUE.") + "\n"
+    ctx.set_pes(w.pes)
+    texts = [ctx.run_deck(w.deck, wave_path=str(tmp_path / f"w{t}.26"))[0] for t in range(3)]
+    assert texts[0] == texts[1] == texts[2]
+    assert "lowest 200 eigenvalues" in texts[0].lower()
+    recs = [read_records(tmp_path / f"w{t}.26") for t in range(3)]
+    assert [len(r) for r in recs] == [len(recs[0])] * 3
+    assert [len(x) for x in recs[2]] == [len(x) for x in recs[0]]
