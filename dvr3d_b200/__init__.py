@@ -180,6 +180,22 @@ class Context:
                                                         C.byref(n), buf, len(buf), C.byref(ln)))
         return lv[:n.value].copy(), buf.value.decode()
 
+    def rotlev3b_pair(self, deck_text: str, wave_path: str, kvec_path: str | None = None,
+                      kvec2_path: str | None = None) -> tuple[np.ndarray, np.ndarray, str]:
+        """ROTLEV3B with KMIN = 2 (dvr3d_b200_rotlev3b_pair): the e levels, the f levels of the
+        second pass and both printed tables; with paths, the e and f vector files (ZTRAN)."""
+        le, lf = np.zeros(20000), np.zeros(20000)
+        ne, nf = C.c_int(0), C.c_int(0)
+        ln = C.c_size_t(0)
+        buf = C.create_string_buffer(1 << 21)
+        P = C.POINTER(C.c_double)
+        self._check(self._lib.dvr3d_b200_rotlev3b_pair(self._h, deck_text.encode(), str(wave_path).encode(),
+                                                       (kvec_path or "").encode(), (kvec2_path or "").encode(),
+                                                       le.ctypes.data_as(P), le.size, C.byref(ne),
+                                                       lf.ctypes.data_as(P), lf.size, C.byref(nf), buf, len(buf),
+                                                       C.byref(ln)))
+        return le[:ne.value].copy(), lf[:nf.value].copy(), buf.value.decode()
+
     def dipole3(self, deck_text: str, ket_path: str, bra_path: str, dipd=None, dipsa=None,
                 tra_path: str | None = None, cap: int = 4096) -> dict:
         """DIPOLE3 (dvr3d_b200_dipole3) on two wavefunction files with a Python dipole plug-in:

@@ -147,6 +147,9 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
                                           C.c_char_p, C.c_size_t, P(C.c_size_t)]),
         "dvr3d_b200_rotlev3b_trans": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, P(C.c_double), C.c_int,
                                                 P(C.c_int), C.c_char_p, C.c_size_t, P(C.c_size_t)]),
+        "dvr3d_b200_rotlev3b_pair": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, P(C.c_double),
+                                               C.c_int, P(C.c_int), P(C.c_double), C.c_int, P(C.c_int), C.c_char_p,
+                                               C.c_size_t, P(C.c_size_t)]),
         "dvr3d_b200_dipole3": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, DIPD_FN, DIPSA_FN, vp, C.c_char_p,
                                          P(DipoleResult), C.c_char_p, C.c_size_t, P(C.c_size_t)]),
         "dvr3d_b200_split_gemm": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, P(C.c_double), C.c_longlong,

@@ -405,6 +405,31 @@ int dvr3d_b200_rotlev3b_trans(dvr3d_ctx *ctx, const char *deck_text, const char 
     });
 }
 
+int dvr3d_b200_rotlev3b_pair(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, const char *kvec_path,
+                             const char *kvec2_path, double *levels_e, int cap_e, int *nlev_e, double *levels_f,
+                             int cap_f, int *nlev_f, char *out, size_t outcap, size_t *outlen) {
+    if (!ctx || !deck_text || !wave_path || !nlev_e || !nlev_f) return DVR3D_ERR_ARG;
+    return guarded(ctx, [&]() -> int {
+        cudaSetDevice(ctx->device);
+        std::vector<double> le, lf;
+        std::string table;
+        dvr3d::RotInfo info;
+        dvr3d::rotlev3b_solve(ctx, deck_text, wave_path, le, table, info, kvec_path, &lf, kvec2_path);
+        *nlev_e = (int)le.size();
+        *nlev_f = (int)lf.size();
+        if (levels_e) {
+            if (cap_e < (int)le.size()) return fail_ctx(ctx, DVR3D_ERR_BUFFER, "e levels buffer smaller than neval");
+            std::memcpy(levels_e, le.data(), sizeof(double) * le.size());
+        }
+        if (levels_f) {
+            if (cap_f < (int)lf.size()) return fail_ctx(ctx, DVR3D_ERR_BUFFER, "f levels buffer smaller than neval2");
+            std::memcpy(levels_f, lf.data(), sizeof(double) * lf.size());
+        }
+        copy_out(table, out, outcap, outlen);
+        return DVR3D_OK;
+    });
+}
+
 int dvr3d_b200_dipole3(dvr3d_ctx *ctx, const char *deck_text, const char *ket_path, const char *bra_path,
                        dvr3d_dipd_fn dipd, dvr3d_dipsa_fn dipsa, void *user, const char *tra_path,
                        dvr3d_dipole_result *res, char *out, size_t outcap, size_t *outlen) {

@@ -51,6 +51,7 @@ struct KBlock {
     std::vector<int> iv;       // kept 2D states per angle
     std::vector<double> ev;    // levels (Eh)
     size_t vec0 = 0;           // record index of the first vector
+    size_t xalf_rec = 0;       // record index of the block's angular points
 };
 
 // ROTLEV3B's cards after the namelist (insize :157-161): nvib, neval, kmin, ibass, neval2,
@@ -328,7 +329,8 @@ std::string fmt_d(double v, int w, int d) {
 }  // namespace
 
 void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, std::vector<double> &levels,
-                    std::string &table, RotInfo &info, const char *kvec_path) {
+                    std::string &table, RotInfo &info, const char *kvec_path, std::vector<double> *levels_f,
+                    const char *kvec2_path) {
     const RotDeck rd = parse_rot_deck(deck_text);
     Records f(wave_path);
     // ---- header (setcon :1176-1184 as insize :155 reads it)
@@ -338,8 +340,9 @@ void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path
     if (jrot <= 0) bad(DVR3D_ERR_ARG, "ROTLEV3B needs a J > 0 wavefunction file");
     const int kmin = rd.kmin;
     if (kmin != kmin0 && kmin0 != 2) bad(DVR3D_ERR_ARG, "ROTLEV3B: kmin differs from the first step's kmin");
-    if (kmin > 1 || (kmin == 0 && kmin0 != 0))
-        bad(DVR3D_ERR_UNSUPPORTED, "ROTLEV3B: one parity per run, from a file of that parity (kmin 0 or 1)");
+    if (kmin > 2 || (kmin == 0 && kmin0 != 0))
+        bad(DVR3D_ERR_UNSUPPORTED, "ROTLEV3B: kmin 0 needs a file of kmin 0; kmin 1 a file of kmin 1 or 2; kmin 2 both");
+    if (kmin == 2 && !levels_f) bad(DVR3D_ERR_ARG, "ROTLEV3B with KMIN = 2 returns two sets: use the pair entry point");
     const auto flags = f.take();                             // logical flags, masses, g1, g2
     const std::vector<double> morse = f.dbls(6);             // Morse constants
     const std::vector<double> rm2 = f.dbls((size_t)nmax);    // r^-2 term (ccmain :824-833)
@@ -347,9 +350,9 @@ void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path
     if (flags.second < 56) bad(DVR3D_ERR_ARG, "wavefunction file: short flags record");
     // ---- k blocks
     const int nblk = kmin > 0 ? jrot + 1 : jrot;
-    std::vector<KBlock> kb;
-    while ((int)kb.size() < nblk && f.more()) {
+    auto read_block = [&]() {
         KBlock b;
+        b.xalf_rec = f.next;
         f.take();  // xalf
         const std::vector<int> hk = f.ints(4);
         b.k = hk[0];
@@ -367,11 +370,20 @@ void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path
         f.next += (size_t)b.meval;
         if (f.next > f.rec.size()) bad(DVR3D_ERR_ARG, "wavefunction file: ends inside the vectors of a k block");
         if (b.iang <= 0 || b.ibass % b.iang != 0) bad(DVR3D_ERR_ARG, "wavefunction file: inconsistent basis sizes");
-        kb.push_back(std::move(b));
-    }
+        return b;
+    };
+    std::vector<KBlock> kb;
+    while ((int)kb.size() < nblk && f.more()) kb.push_back(read_block());
     if ((int)kb.size() < nblk) bad(DVR3D_ERR_ARG, "wavefunction file holds fewer k blocks than J + 1 - kmin");
     for (int i = 0; i < nblk; ++i)
         if (kb[i].k != (kmin > 0 ? i : i + 1)) bad(DVR3D_ERR_ARG, "wavefunction file: unexpected k block order");
+    // KMIN = 2: the f-type k = 1 block follows the J + 1 e-type blocks (endiv :1635-1658)
+    KBlock kf1;
+    if (kmin == 2) {
+        if (!f.more()) bad(DVR3D_ERR_ARG, "wavefunction file: no f-type k = 1 block after the e blocks (KMIN = 2)");
+        kf1 = read_block();
+        if (kf1.k != 1) bad(DVR3D_ERR_ARG, "wavefunction file: the block after the e blocks is not k = 1");
+    }
     // ---- basis selection (select :306-510)
     const int nvib = std::min(rd.nvib, meval);
     std::vector<int> mvib(nblk);
@@ -399,6 +411,7 @@ void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path
         nbass = rd.ibass;
     }
     int neval = rd.neval <= 0 ? 10 : rd.neval;
+    const int neval2 = rd.neval2 <= 0 ? neval : rd.neval2;
     neval = std::min(neval, nbass);
     const int npnt = std::max(ndvr, rd.npnt);
     // ---- symmetrised radial r^-2 matrix elements (mkrad :698-717)
@@ -411,25 +424,8 @@ void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path
     };
     const std::vector<double> radmee = mkrad(0, 0, 0), radmoo = mkrad(1, 0, 0), radmeo = mkrad(1, 1, 0),
                               radmoe = mkrad(1, 1, 1);
-    // ---- device Hamiltonian
     cudaStream_t st = ctx->stream;
-    std::vector<int> off(nblk + 1, 0);
-    for (int i = 0; i < nblk; ++i) off[i + 1] = off[i] + mvib[i];
-    const long long ldh = (nbass + 7) / 8 * 8;
-    double *H = ctx->arena.get_t<double>("rt_h", (size_t)ldh * nbass);
-    CK(cudaMemsetAsync(H, 0, sizeof(double) * ldh * nbass, st));
-    {
-        std::vector<double> dg(nbass);
-        for (int i = 0; i < nblk; ++i)
-            for (int v = 0; v < mvib[i]; ++v) dg[off[i] + v] = kb[i].ev[v];
-        double *dd = ctx->arena.get_t<double>("rt_dg", nbass);
-        CK(cudaMemcpyAsync(dd, dg.data(), sizeof(double) * nbass, cudaMemcpyHostToDevice, st));
-        DVR3D_COUNT_LAUNCH(1);
-        rot_diag_kernel<<<nblocks256(nbass), 256, 0, st>>>(dd, nbass, H, ldh);
-        CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(st));
-    }
-    // first-step vectors of a block, on the device (ibass x mvib)
+    // first-step vectors of a block, on the device (ibass x nv)
     auto upload_vectors = [&](const KBlock &b, int nv, const char *name) {
         double *d = ctx->arena.get_t<double>(name, (size_t)b.ibass * std::max(nv, 1));
         for (int v = 0; v < nv; ++v)
@@ -440,108 +436,142 @@ void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path
     };
     const double jjp1 = (double)jrot * (jrot + 1);
     info.offdiag_flops = 0.0;
-    // one Coriolis block (solofd): off (mvib2 x mvib1), placed at rows of block i, columns of block j
-    auto coriolis = [&](int i, int j, const std::vector<double> &ang, const std::vector<double> &rad, int iq, int iq1,
-                        int iq2) {
-        const KBlock &b1 = kb[i], &b2 = kb[j];
-        const int n1 = mvib[i], n2 = mvib[j];
-        if (n1 == 0 || n2 == 0) return;
-        const int nrad2 = b2.ibass / b2.iang;
-        std::vector<int> m1, m2;
-        int ir1 = 0, ir2 = 0;
-        for (int a1 = 0; a1 < nmax; ++a1) {
-            for (int a2 = 0; a2 < a1 + 1 - iq; ++a2) {
-                m1.push_back(ir1++);
-                m2.push_back(ir2++);
-            }
-            ir1 += iq1;
-            ir2 += iq2;
-        }
-        const int npair = (int)m1.size();
-        if (ir1 > b1.ibass / b1.iang || ir2 > nrad2 || (int)rad.size() != npair)
-            bad(DVR3D_ERR_ARG, "wavefunction file: radial basis does not match the block parities");
-        double *C1 = upload_vectors(b1, n1, "rt_c1");
-        double *C2 = upload_vectors(b2, n2, "rt_c2");
-        double *A = ctx->arena.get_t<double>("rt_ang", ang.size());
-        CK(cudaMemcpyAsync(A, ang.data(), sizeof(double) * ang.size(), cudaMemcpyHostToDevice, st));
-        const long long K = (long long)npair * b1.iang;
-        double *W = ctx->arena.get_t<double>("rt_w", (size_t)b1.iang * nrad2 * n2);
-        double *Wg = ctx->arena.get_t<double>("rt_wg", (size_t)K * n2);
-        double *Cg = ctx->arena.get_t<double>("rt_cg", (size_t)K * n1);
-        double *O = ctx->arena.get_t<double>("rt_off", (size_t)n1 * n2);
-        int *dm1 = ctx->arena.get_t<int>("rt_m1", npair), *dm2 = ctx->arena.get_t<int>("rt_m2", npair);
-        double *dr = ctx->arena.get_t<double>("rt_rad", npair);
-        CK(cudaMemcpyAsync(dm1, m1.data(), sizeof(int) * npair, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(dm2, m2.data(), sizeof(int) * npair, cudaMemcpyHostToDevice, st));
-        CK(cudaMemcpyAsync(dr, rad.data(), sizeof(double) * npair, cudaMemcpyHostToDevice, st));
-        // W (iang1 x nrad2 n2) = A (iang1 x iang2) C2 (iang2 x nrad2 n2)
-        launch_dgemm(false, false, b1.iang, nrad2 * n2, b2.iang, 1.0, A, b1.iang, C2, b2.iang, 0.0, W, b1.iang, st);
-        CK(cudaGetLastError());
-        DVR3D_COUNT_LAUNCH(1);
-        rot_gather_kernel<<<nblocks256(K * std::max(n1, n2)), 256, 0, st>>>(W, b1.iang, nrad2, n2, C1, b1.ibass, n1,
-                                                                             dm1, dm2, dr, npair, Wg, Cg);
-        CK(cudaGetLastError());
-        // off (n2 x n1) = W''^T C1''
-        launch_dgemm(true, false, n2, n1, (int)K, 1.0, Wg, K, Cg, K, 0.0, O, n2, st);
-        CK(cudaGetLastError());
-        DVR3D_COUNT_LAUNCH(1);
-        rot_place_kernel<<<nblocks256((long long)n1 * n2), 256, 0, st>>>(O, n2, n1, H, ldh, off[i], off[j]);
-        CK(cudaGetLastError());
-        CK(cudaStreamSynchronize(st));
-        info.offdiag_flops += 2.0 * b1.iang * b2.iang * (double)nrad2 * n2 + 2.0 * (double)K * n1 * n2;
+    // The Hamiltonian of a chain of k blocks on the device (solrt :1414-1527, loadh): each block's
+    // levels on the diagonal, the Coriolis blocks of neighbours k, k+1 and k, k+2 (solofd); ip0
+    // is the radial parity label of the first pair, alternating along the chain. Returns the
+    // lowest nev levels, and the eigenvectors in Z (ldz) when asked.
+    struct Pass {
+        std::vector<int> off;
+        int nb = 0;
+        long long ldz = 0;
+        double *Z = nullptr;
     };
-    int ip = ipar0;
-    for (int i = 1; i < nblk; ++i) {
-        const int k1 = kb[i - 1].k;
-        // k and k + 1 (solrt :1468-1486)
-        double angfac = std::sqrt(jjp1 - (double)k1 * (k1 + 1)) / 2.0;
-        if (k1 == 0) angfac = 1.4142135623731 * angfac;
-        if (mvib[i - 1] * mvib[i] > 0) {
-            const std::vector<double> ang = angular_block(1, k1, kb[i - 1], kb[i], npnt, angfac);
-            if (ip == 0) coriolis(i - 1, i, ang, radmeo, 1, 1, 0);
-            else coriolis(i - 1, i, ang, radmoe, 1, 0, 1);
+    auto solve_chain = [&](const std::vector<const KBlock *> &B, const std::vector<int> &mv, int ip0, int nev,
+                           bool vecs, std::vector<double> &lv, const char *tag) {
+        Pass ps;
+        const int nk = (int)B.size();
+        ps.off.assign(nk + 1, 0);
+        for (int i = 0; i < nk; ++i) ps.off[i + 1] = ps.off[i] + mv[i];
+        const int nb = ps.off[nk];
+        ps.nb = nb;
+        const long long ldh = (nb + 7) / 8 * 8;
+        double *H = ctx->arena.get_t<double>("rt_h", (size_t)ldh * nb);
+        CK(cudaMemsetAsync(H, 0, sizeof(double) * ldh * nb, st));
+        {
+            std::vector<double> dg(nb);
+            for (int i = 0; i < nk; ++i)
+                for (int v = 0; v < mv[i]; ++v) dg[ps.off[i] + v] = B[i]->ev[v];
+            double *dd = ctx->arena.get_t<double>("rt_dg", nb);
+            CK(cudaMemcpyAsync(dd, dg.data(), sizeof(double) * nb, cudaMemcpyHostToDevice, st));
+            DVR3D_COUNT_LAUNCH(1);
+            rot_diag_kernel<<<nblocks256(nb), 256, 0, st>>>(dd, nb, H, ldh);
+            CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(st));
         }
-        // k and k + 2 (:1488-1520)
-        if (i + 1 < nblk && mvib[i - 1] * mvib[i + 1] > 0) {
-            double af = -std::sqrt((jjp1 - (double)(k1 + 1) * (k1 + 2)) * (jjp1 - (double)k1 * (k1 + 1))) / 16.0;
-            if (k1 == 0) af = 1.4142135623731 * af;
-            const std::vector<double> ang = angular_block(2, k1, kb[i - 1], kb[i + 1], npnt, af);
-            if (ip == 0) coriolis(i - 1, i + 1, ang, radmee, 0, 0, 0);
-            else coriolis(i - 1, i + 1, ang, radmoo, 1, 0, 0);
+        // one Coriolis block (solofd): off (n2 x n1), placed at rows of block i, columns of block j
+        auto coriolis = [&](int i, int j, const std::vector<double> &ang, const std::vector<double> &rad, int iq,
+                            int iq1, int iq2) {
+            const KBlock &b1 = *B[i], &b2 = *B[j];
+            const int n1 = mv[i], n2 = mv[j];
+            if (n1 == 0 || n2 == 0) return;
+            const int nrad2 = b2.ibass / b2.iang;
+            std::vector<int> m1, m2;
+            int ir1 = 0, ir2 = 0;
+            for (int a1 = 0; a1 < nmax; ++a1) {
+                for (int a2 = 0; a2 < a1 + 1 - iq; ++a2) {
+                    m1.push_back(ir1++);
+                    m2.push_back(ir2++);
+                }
+                ir1 += iq1;
+                ir2 += iq2;
+            }
+            const int npair = (int)m1.size();
+            if (ir1 > b1.ibass / b1.iang || ir2 > nrad2 || (int)rad.size() != npair)
+                bad(DVR3D_ERR_ARG, "wavefunction file: radial basis does not match the block parities");
+            double *C1 = upload_vectors(b1, n1, "rt_c1");
+            double *C2 = upload_vectors(b2, n2, "rt_c2");
+            double *A = ctx->arena.get_t<double>("rt_ang", ang.size());
+            CK(cudaMemcpyAsync(A, ang.data(), sizeof(double) * ang.size(), cudaMemcpyHostToDevice, st));
+            const long long K = (long long)npair * b1.iang;
+            double *W = ctx->arena.get_t<double>("rt_w", (size_t)b1.iang * nrad2 * n2);
+            double *Wg = ctx->arena.get_t<double>("rt_wg", (size_t)K * n2);
+            double *Cg = ctx->arena.get_t<double>("rt_cg", (size_t)K * n1);
+            double *O = ctx->arena.get_t<double>("rt_off", (size_t)n1 * n2);
+            int *dm1 = ctx->arena.get_t<int>("rt_m1", npair), *dm2 = ctx->arena.get_t<int>("rt_m2", npair);
+            double *dr = ctx->arena.get_t<double>("rt_rad", npair);
+            CK(cudaMemcpyAsync(dm1, m1.data(), sizeof(int) * npair, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(dm2, m2.data(), sizeof(int) * npair, cudaMemcpyHostToDevice, st));
+            CK(cudaMemcpyAsync(dr, rad.data(), sizeof(double) * npair, cudaMemcpyHostToDevice, st));
+            // W (iang1 x nrad2 n2) = A (iang1 x iang2) C2 (iang2 x nrad2 n2)
+            launch_dgemm(false, false, b1.iang, nrad2 * n2, b2.iang, 1.0, A, b1.iang, C2, b2.iang, 0.0, W, b1.iang, st);
+            CK(cudaGetLastError());
+            DVR3D_COUNT_LAUNCH(1);
+            rot_gather_kernel<<<nblocks256(K * std::max(n1, n2)), 256, 0, st>>>(W, b1.iang, nrad2, n2, C1, b1.ibass, n1,
+                                                                                 dm1, dm2, dr, npair, Wg, Cg);
+            CK(cudaGetLastError());
+            // off (n2 x n1) = W''^T C1''
+            launch_dgemm(true, false, n2, n1, (int)K, 1.0, Wg, K, Cg, K, 0.0, O, n2, st);
+            CK(cudaGetLastError());
+            DVR3D_COUNT_LAUNCH(1);
+            rot_place_kernel<<<nblocks256((long long)n1 * n2), 256, 0, st>>>(O, n2, n1, H, ldh, ps.off[i], ps.off[j]);
+            CK(cudaGetLastError());
+            CK(cudaStreamSynchronize(st));
+            info.offdiag_flops += 2.0 * b1.iang * b2.iang * (double)nrad2 * n2 + 2.0 * (double)K * n1 * n2;
+        };
+        int ip = ip0;
+        for (int i = 1; i < nk; ++i) {
+            const int k1 = B[i - 1]->k;
+            // k and k + 1 (solrt :1468-1486)
+            double angfac = std::sqrt(jjp1 - (double)k1 * (k1 + 1)) / 2.0;
+            if (k1 == 0) angfac = 1.4142135623731 * angfac;
+            if (mv[i - 1] * mv[i] > 0) {
+                const std::vector<double> ang = angular_block(1, k1, *B[i - 1], *B[i], npnt, angfac);
+                if (ip == 0) coriolis(i - 1, i, ang, radmeo, 1, 1, 0);
+                else coriolis(i - 1, i, ang, radmoe, 1, 0, 1);
+            }
+            // k and k + 2 (:1488-1520)
+            if (i + 1 < nk && mv[i - 1] * mv[i + 1] > 0) {
+                double af = -std::sqrt((jjp1 - (double)(k1 + 1) * (k1 + 2)) * (jjp1 - (double)k1 * (k1 + 1))) / 16.0;
+                if (k1 == 0) af = 1.4142135623731 * af;
+                const std::vector<double> ang = angular_block(2, k1, *B[i - 1], *B[i + 1], npnt, af);
+                if (ip == 0) coriolis(i - 1, i + 1, ang, radmee, 0, 0, 0);
+                else coriolis(i - 1, i + 1, ang, radmoo, 1, 0, 0);
+            }
+            ip = 1 - ip;
         }
-        ip = 1 - ip;
-    }
-    // ---- lowest levels (dgrot)
-    double *wv = ctx->arena.get_t<double>("rt_w_ev", neval);
-    const bool ztran = kvec_path && kvec_path[0];
-    const long long ldz = ldh;
-    double *Z = ztran ? ctx->arena.get_t<double>("rt_z", (size_t)ldz * neval) : nullptr;
-    dense_lowest(ctx, H, ldh, nbass, neval, ztran, wv, Z, ztran ? ldz : 1, "rtd_", false, nullptr);
-    levels.resize(neval);
-    CK(cudaMemcpyAsync(levels.data(), wv, sizeof(double) * neval, cudaMemcpyDeviceToHost, st));
-    CK(cudaStreamSynchronize(st));
-    info.nbass = nbass;
-    info.nblk = nblk;
-    info.neval = neval;
-    info.mvib = mvib;
-    // ---- ZTRAN: vectors back in the first step's basis, angular FBR (dstore :1917-2049)
-    if (ztran) {
-        std::vector<int> lmin(nblk), lbasis(nblk), nkbas(nblk);
+        // ---- lowest levels (dgrot)
+        double *wv = ctx->arena.get_t<double>("rt_w_ev", nev);
+        ps.ldz = ldh;
+        ps.Z = vecs ? ctx->arena.get_t<double>(std::string("rt_z") + tag, (size_t)ps.ldz * nev) : nullptr;
+        dense_lowest(ctx, H, ldh, nb, nev, vecs, wv, ps.Z, vecs ? ps.ldz : 1, "rtd_", false, nullptr);
+        lv.resize(nev);
+        CK(cudaMemcpyAsync(lv.data(), wv, sizeof(double) * nev, cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        return ps;
+    };
+    // ZTRAN: the vectors back in the first step's basis, angular FBR (dstore :1917-2049)
+    auto write_kvec = [&](const char *path, const std::vector<const KBlock *> &B, const std::vector<int> &mv,
+                          const std::vector<int> &nkbas_in, int ipar_out, int kmin_out, const std::vector<double> &lv,
+                          const Pass &ps) {
+        const int nk = (int)B.size(), nval = (int)lv.size();
+        std::vector<int> lmin(nk), lbasis(nk), nkbas(nk);
         int nend = 0;
-        for (int i = 0; i < nblk; ++i) {  // select :374-380
-            lmin[i] = kb[i].k;
-            lbasis[i] = kb[i].maxleg + kb[i].lincr - kb[i].k + 1;
-            nkbas[i] = (kb[i].ibass / kb[i].iang) * lbasis[i];
+        for (int i = 0; i < nk; ++i) {  // select :374-380
+            lmin[i] = B[i]->k;
+            lbasis[i] = B[i]->maxleg + B[i]->lincr - B[i]->k + 1;
+            nkbas[i] = (B[i]->ibass / B[i]->iang) * lbasis[i];
+            if (!nkbas_in.empty() && nkbas_in[i] != nkbas[i])
+                bad(DVR3D_ERR_UNSUPPORTED, "ROTLEV3B: the f-type k = 1 block differs in size from the e-type one");
             nend += nkbas[i];
         }
-        FILE *fp = std::fopen(kvec_path, "wb");
-        if (!fp) bad(DVR3D_ERR_ARG, std::string("cannot open ") + kvec_path);
+        FILE *fp = std::fopen(path, "wb");
+        if (!fp) bad(DVR3D_ERR_ARG, std::string("cannot open ") + path);
         struct Closer {
             FILE *f;
             ~Closer() { std::fclose(f); }
         } closer{fp};
         RecordWriter w{fp};
-        for (int v : {idia, ipar0, ndvr, nmax, h[4], jrot, kmin, neval}) w.i4(v);
+        for (int v : {idia, ipar_out, ndvr, nmax, h[4], jrot, kmin_out, nval}) w.i4(v);
         w.end();
         w.put(flags.first, 56);  // zembed, zmors1, zmors2, xmass, g1, g2, zncor (zquad2 dropped)
         w.end();
@@ -554,66 +584,149 @@ void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path
         w.end();
         for (double v : rgrid) w.r8(v);
         w.end();
-        w.i4(neval);
+        w.i4(nval);
         w.end();
-        for (double v : levels) w.r8(v);
+        for (double v : lv) w.r8(v);
         w.end();
         std::vector<double> dh;
-        for (int i = 0; i < nblk; ++i) {
-            const KBlock &b = kb[i];
-            const int mv = mvib[i], nang = lbasis[i], nrad = b.ibass / b.iang;
-            if (mv <= 0) continue;
+        for (int i = 0; i < nk; ++i) {
+            const KBlock &b = *B[i];
+            const int mvi = mv[i], nang = lbasis[i], nrad = b.ibass / b.iang;
+            if (mvi <= 0) continue;
             if (nang > b.maxleg + 1) bad(DVR3D_ERR_ARG, "wavefunction file: angular basis larger than its transform");
             // tofbr / jtran: B (nang x nrad mv) = P'' (nang x iang) V (iang x nrad mv), P''(j, kk) =
             // pleg(j, kk-th kept angle)
-            std::vector<double> ps((size_t)nang * b.iang, 0.0);
+            std::vector<double> pk((size_t)nang * b.iang, 0.0);
             int kk = 0;
             for (int a = 0; a < b.nang; ++a) {
                 if (b.iv[a] == 0) continue;
                 if (kk >= b.iang) bad(DVR3D_ERR_ARG, "wavefunction file: more kept angles than iang");
-                for (int j = 0; j < nang; ++j) ps[(size_t)kk * nang + j] = b.pleg[(size_t)a * (b.maxleg + 1) + j];
+                for (int j = 0; j < nang; ++j) pk[(size_t)kk * nang + j] = b.pleg[(size_t)a * (b.maxleg + 1) + j];
                 ++kk;
             }
             if (kk != b.iang) bad(DVR3D_ERR_ARG, "wavefunction file: kept angles differ from iang");
-            double *Pd = ctx->arena.get_t<double>("rt_tp", ps.size());
-            CK(cudaMemcpyAsync(Pd, ps.data(), sizeof(double) * ps.size(), cudaMemcpyHostToDevice, st));
-            double *V = upload_vectors(b, mv, "rt_c1");
-            double *B = ctx->arena.get_t<double>("rt_tb", (size_t)nkbas[i] * mv);
-            double *D = ctx->arena.get_t<double>("rt_td", (size_t)nkbas[i] * neval);
-            launch_dgemm(false, false, nang, nrad * mv, b.iang, 1.0, Pd, nang, V, b.iang, 0.0, B, nang, st);
+            double *Pd = ctx->arena.get_t<double>("rt_tp", pk.size());
+            CK(cudaMemcpyAsync(Pd, pk.data(), sizeof(double) * pk.size(), cudaMemcpyHostToDevice, st));
+            double *V = upload_vectors(b, mvi, "rt_c1");
+            double *Bm = ctx->arena.get_t<double>("rt_tb", (size_t)nkbas[i] * mvi);
+            double *D = ctx->arena.get_t<double>("rt_td", (size_t)nkbas[i] * nval);
+            launch_dgemm(false, false, nang, nrad * mvi, b.iang, 1.0, Pd, nang, V, b.iang, 0.0, Bm, nang, st);
             CK(cudaGetLastError());
             // D (nkbas x nval) = B (nkbas x mv) C, C = rows off[i] .. of the eigenvectors
-            launch_dgemm(false, false, nkbas[i], neval, mv, 1.0, B, nkbas[i], Z + off[i], ldz, 0.0, D, nkbas[i], st);
+            launch_dgemm(false, false, nkbas[i], nval, mvi, 1.0, Bm, nkbas[i], ps.Z + ps.off[i], ps.ldz, 0.0, D, nkbas[i],
+                         st);
             CK(cudaGetLastError());
-            dh.resize((size_t)nkbas[i] * neval);
+            dh.resize((size_t)nkbas[i] * nval);
             CK(cudaMemcpyAsync(dh.data(), D, sizeof(double) * dh.size(), cudaMemcpyDeviceToHost, st));
             CK(cudaStreamSynchronize(st));
             w.put(dh.data(), sizeof(double) * dh.size());
             w.end();
         }
-    }
-    // ---- printed table (dgrot :1767-1769, :1795-1799)
+    };
+    // ---- first (or only) pass: e parity for KMIN >= 1, f parity for KMIN = 0
+    std::vector<const KBlock *> chain;
+    for (auto &b : kb) chain.push_back(&b);
+    const bool ztran = kvec_path && kvec_path[0];
+    const Pass pe = solve_chain(chain, mvib, ipar0, neval, ztran, levels, "e");
+    info.nbass = nbass;
+    info.nblk = nblk;
+    info.neval = neval;
+    info.mvib = mvib;
+    if (ztran) write_kvec(kvec_path, chain, mvib, {}, ipar0, kmin == 2 ? 1 : kmin, levels, pe);
+    // ---- printed tables (dgrot :1767-1769, :1795-1799)
     table.clear();
     char ln[160];
-    std::snprintf(ln, sizeof(ln), "\n     J =%3d rotational state,%7d basis functions\n", jrot, nbass);
-    table += ln;
-    table += kmin >= 1 ? "            e parity, symmetric |jk> + |j-k> functions in basis\n"
-                       : "            f parity, anti-symmetric |jk> - |j-k> functions in basis\n";
-    std::snprintf(ln, sizeof(ln), "\n\n     lowest%4d eigenvalues in Hartrees\n\n", neval);
-    table += ln;
-    auto rows = [&](const std::vector<double> &v) {
-        for (size_t i = 0; i < v.size(); ++i) {
-            table += fmt_d(v[i], 24, 12);
-            if (i % 5 == 4 || i + 1 == v.size()) table += "\n\n";
-        }
+    auto print_pass = [&](const std::vector<double> &lv, int nb, bool epar) {
+        std::snprintf(ln, sizeof(ln), "\n     J =%3d rotational state,%7d basis functions\n", jrot, nb);
+        table += ln;
+        table += epar ? "            e parity, symmetric |jk> + |j-k> functions in basis\n"
+                      : "            f parity, anti-symmetric |jk> - |j-k> functions in basis\n";
+        std::snprintf(ln, sizeof(ln), "\n\n     lowest%4d eigenvalues in Hartrees\n\n", (int)lv.size());
+        table += ln;
+        auto rows = [&](const std::vector<double> &v) {
+            for (size_t i = 0; i < v.size(); ++i) {
+                table += fmt_d(v[i], 24, 12);
+                if (i % 5 == 4 || i + 1 == v.size()) table += "\n\n";
+            }
+        };
+        rows(lv);
+        std::vector<double> cm(lv.size());
+        for (size_t i = 0; i < lv.size(); ++i) cm[i] = lv[i] * 2.19474624e5 - rd.ezero;
+        std::snprintf(ln, sizeof(ln), "\n\n     lowest%4d eigenvalues in wavenumbers relative to ezero =", (int)lv.size());
+        table += ln;
+        table += fmt_d(rd.ezero, 24, 12) + "\n\n";
+        rows(cm);
     };
-    rows(levels);
-    std::vector<double> cm(neval);
-    for (int i = 0; i < neval; ++i) cm[i] = levels[i] * 2.19474624e5 - rd.ezero;
-    std::snprintf(ln, sizeof(ln), "\n\n     lowest%4d eigenvalues in wavenumbers relative to ezero =", neval);
-    table += ln;
-    table += fmt_d(rd.ezero, 24, 12) + "\n\n";
-    rows(cm);
+    print_pass(levels, nbass, kmin >= 1);
+    if (kmin != 2) return;
+    // ---- KMIN = 2, second pass (vrmain :600-660): f parity, k = 1..J, with the f-type k = 1
+    // block in place of the e-type one; its Coriolis blocks with k = 2, 3 are formed anew
+    // (solrt :1529-1617, ip = 1 - ipar), those among k >= 2 are the same as in the first pass
+    const int nbf = nbass - mvib[0];
+    const int nevf = std::min(neval2, nbf);
+    const bool ztran2 = kvec2_path && kvec2_path[0];
+    if (jrot == 1) {
+        // J = 1 f: the k = 1 f block alone, its levels and vectors as they are (dstore1 :2051-2173)
+        const int nv = std::min(nevf, kf1.meval);
+        levels_f->assign(kf1.ev.begin(), kf1.ev.begin() + nv);
+        if (ztran2) {
+            FILE *fp = std::fopen(kvec2_path, "wb");
+            if (!fp) bad(DVR3D_ERR_ARG, std::string("cannot open ") + kvec2_path);
+            struct Closer {
+                FILE *f;
+                ~Closer() { std::fclose(f); }
+            } closer{fp};
+            RecordWriter w{fp};
+            const int ipf = 1 - ipar0, idvr = kb[nblk - 1].nang;
+            for (int v : {idia, ipf, idvr, nmax, h[4], jrot, 0, nv}) w.i4(v);
+            w.end();
+            w.put(flags.first, 56);
+            w.end();
+            for (double v : morse) w.r8(v);
+            w.end();
+            const int max2d = nmax * (nmax + 1 - 2 * ipf) / 2, mbass = idvr * max2d;
+            for (int v : {mbass, 0, idvr, mbass}) w.i4(v);
+            w.end();
+            for (double v : rgrid) w.r8(v);
+            w.end();
+            const double *xa = f.vec(kf1.xalf_rec, 0);
+            const size_t nxa = std::min<size_t>((size_t)idvr, f.rec[kf1.xalf_rec].second / 8);
+            w.put(xa, 8 * nxa);
+            w.end();
+            for (int v : {kf1.k, kf1.maxleg, kf1.nang}) w.i4(v);
+            w.end();
+            w.put(kf1.pleg.data(), 8 * (size_t)kf1.nang * ndvr > 8 * kf1.pleg.size() ? 8 * kf1.pleg.size()
+                                                                                       : 8 * (size_t)kf1.nang * ndvr);
+            w.end();
+            w.i4(kf1.iang);
+            w.i4(kf1.ibass);
+            w.end();
+            for (int v : kf1.iv) w.i4(v);
+            w.end();
+            w.i4(nv);
+            w.end();
+            w.put(kf1.ev.data(), 8 * (size_t)nv);
+            w.end();
+            for (int l = 0; l < nv; ++l) {
+                w.put(f.vec(kf1.vec0 + l, (size_t)kf1.ibass), 8 * (size_t)kf1.ibass);
+                w.end();
+            }
+        }
+    } else {
+        std::vector<const KBlock *> fchain{&kf1};
+        std::vector<int> mvf{std::min(mvib[1], std::min(kf1.ibass, kf1.meval))};
+        if (mvf[0] != mvib[1]) bad(DVR3D_ERR_ARG, "wavefunction file: the f-type k = 1 block holds too few vectors");
+        std::vector<int> nkb_ref{(kb[1].ibass / kb[1].iang) * (kb[1].maxleg + kb[1].lincr - kb[1].k + 1)};
+        for (int i = 2; i < nblk; ++i) {
+            fchain.push_back(&kb[i]);
+            mvf.push_back(mvib[i]);
+            nkb_ref.push_back((kb[i].ibass / kb[i].iang) * (kb[i].maxleg + kb[i].lincr - kb[i].k + 1));
+        }
+        const Pass pf = solve_chain(fchain, mvf, 1 - ipar0, nevf, ztran2, *levels_f, "f");
+        if (pf.nb != nbf) bad(DVR3D_ERR_ARG, "ROTLEV3B: f basis size mismatch");
+        if (ztran2) write_kvec(kvec2_path, fchain, mvf, nkb_ref, 1 - ipar0, 0, *levels_f, pf);
+    }
+    print_pass(*levels_f, nbf, false);
 }
 
 }  // namespace dvr3d

@@ -18,7 +18,10 @@ struct RotInfo {
 // title, optional EZERO) and the first step's wavefunction file; returns the lowest levels (Eh)
 // and the printed level table. With a kvec_path (ZTRAN) the eigenvectors are transformed back to
 // the first step's basis and written there as dstore does. Throws HostError / CudaFail.
+// KMIN = 2 (both sets from a KMIN = 2 file) needs levels_f: the e levels go to levels, the f
+// levels of the second pass to levels_f, their vectors (ZTRAN) to kvec_path and kvec2_path.
 void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, std::vector<double> &levels,
-                    std::string &table, RotInfo &info, const char *kvec_path = nullptr);
+                    std::string &table, RotInfo &info, const char *kvec_path = nullptr,
+                    std::vector<double> *levels_f = nullptr, const char *kvec2_path = nullptr);
 
 }  // namespace dvr3d

@@ -201,7 +201,8 @@ int dvr3d_b200_set_wait_limit(dvr3d_ctx *ctx, long long polls);
  * (Eh, dgrot :1731-1800) go to levels (cap entries); *nlev receives their number; out / outlen
  * as for dvr3d_b200_run_deck receive the printed level table. One parity per call: KMIN = 1
  * (e, k = 0..J) or 0 (f, k = 1..J) from a file of the same KMIN (KMIN = 1 also reads a KMIN = 2
- * file's first J + 1 blocks); the KMIN = 2 double pass returns DVR3D_ERR_UNSUPPORTED. */
+ * file's first J + 1 blocks); KMIN = 2 (both sets) returns DVR3D_ERR_ARG here and is run by
+ * dvr3d_b200_rotlev3b_pair. */
 int dvr3d_b200_rotlev3b(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, double *levels, int cap,
                         int *nlev, char *out, size_t outcap, size_t *outlen);
 
@@ -212,6 +213,17 @@ int dvr3d_b200_rotlev3b(dvr3d_ctx *ctx, const char *deck_text, const char *wave_
  * the radial grid, nval, the levels (Eh), then one record d(nkbas(k), nval) per k block. */
 int dvr3d_b200_rotlev3b_trans(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, const char *kvec_path,
                               double *levels, int cap, int *nlev, char *out, size_t outcap, size_t *outlen);
+
+/* ROTLEV3B with KMIN = 2 on a KMIN = 2 first-step file: the e set (k = 0..J), then the second
+ * pass (vrmain :600-660), the f set (k = 1..J) with the file's f-type k = 1 block (stored after
+ * the e blocks) in place of the e-type one; its Coriolis blocks with k = 2 and 3 formed anew
+ * (solrt :1529-1617), those among k >= 2 as in the first pass; NEVAL2 f levels. With ZTRAN
+ * (non-empty paths) the e vectors go to kvec_path (unit KVEC = 8) and the f vectors to
+ * kvec2_path (KVEC2 = 9); for J = 1 the f set is the f-type k = 1 block itself, copied in the
+ * layout of a one-block file (dstore1 :2051-2173). out receives both printed tables. */
+int dvr3d_b200_rotlev3b_pair(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, const char *kvec_path,
+                             const char *kvec2_path, double *levels_e, int cap_e, int *nlev_e, double *levels_f,
+                             int cap_f, int *nlev_f, char *out, size_t outcap, size_t *outlen);
 
 /* ---- DIPOLE3: transition moments between two sets of vib-rot states ------------------- */
 /* The user's dipole surface, the two plug-ins of source/dipole3_segmented.f90:

@@ -1839,11 +1839,13 @@ void rot_solofd(std::vector<double> &offdg, const std::vector<double> &radmat, c
 // dstore :1917-2049 (itra = 1): the eigenvectors transformed to the first-step basis with the
 // angular DVR taken back to associated Legendre functions (tofbr :2175-2228, jtran :2230-2274),
 // one record per k block, for DIPOLE3.
-void rot_dstore(const char *kvec_path, const std::vector<int> &h, const std::vector<unsigned char> &rec2,
+void rot_dstore(const char *kvec_path, const std::vector<int> &h, int ipar_out, const std::vector<unsigned char> &rec2,
                 const std::vector<double> &rec3, const std::vector<double> &r, int jrot, int kmin, int ndvr,
-                const std::vector<RotBlock> &blk, const std::vector<int> &mvib, const std::vector<double> &vec,
+                const std::vector<const RotBlock *> &bp, const std::vector<int> &mvib, const std::vector<double> &vec,
                 int nbass, const std::vector<double> &ev, int nval) {
-    const int nblk = (int)blk.size();
+    const int nblk = (int)bp.size();
+    std::vector<RotBlock> blk;
+    for (auto *b : bp) blk.push_back(*b);
     std::vector<int> lmin(nblk), lbasis(nblk), nkbas(nblk);
     int nend = 0;
     for (int k = 0; k < nblk; ++k) {  // select :374-380
@@ -1860,7 +1862,7 @@ void rot_dstore(const char *kvec_path, const std::vector<int> &h, const std::vec
         if (n) std::fwrite(p, 1, n, fp);
         std::fwrite(&m, 4, 1, fp);
     };
-    const int hdr[8] = {h[0], h[1], h[2], h[3], h[4], jrot, kmin, nval};
+    const int hdr[8] = {h[0], ipar_out, h[2], h[3], h[4], jrot, kmin, nval};
     put(hdr, sizeof(hdr));
     put(rec2.data(), std::min<size_t>(rec2.size(), 56));  // zembed .. zncor (no zquad2)
     put(rec3.data(), 8 * rec3.size());
@@ -1909,8 +1911,44 @@ void rot_dstore(const char *kvec_path, const std::vector<int> &h, const std::vec
     std::fclose(fp);
 }
 
+// dstore1 :2051-2173: the J = 1 f set is the first step's k = 1 f block itself; its records are
+// copied in the layout of a J = 0 first-step file (read by DIPOLE3 as a one-block set).
+// idvr: the angular point count of the last e-type block select read (vrmain's argument).
+void rot_dstore1(const char *kvec_path, const std::vector<int> &h, int ipar_out, const std::vector<unsigned char> &rec2,
+                 const std::vector<double> &rec3, const std::vector<double> &r, int idvr, int ndvr, int nmax,
+                 const std::vector<double> &xalf, const RotBlock &B, const std::vector<double> &vecs, int nval) {
+    FILE *fp = std::fopen(kvec_path, "wb");
+    if (!fp) fail(DVR3D_ERR_ARG);
+    auto put = [&](const void *p, size_t n) {
+        const int32_t m = (int32_t)n;
+        std::fwrite(&m, 4, 1, fp);
+        if (n) std::fwrite(p, 1, n, fp);
+        std::fwrite(&m, 4, 1, fp);
+    };
+    const int hdr[8] = {h[0], ipar_out, idvr, h[3], h[4], h[5], 0, nval};
+    put(hdr, sizeof(hdr));
+    put(rec2.data(), std::min<size_t>(rec2.size(), 56));
+    put(rec3.data(), 8 * rec3.size());
+    const int max2d = nmax * (nmax + 1 - 2 * ipar_out) / 2, mbass = idvr * max2d;
+    const int r4[4] = {mbass, 0, idvr, mbass};
+    put(r4, sizeof(r4));
+    put(r.data(), 8 * r.size());
+    put(xalf.data(), 8 * (size_t)std::min(idvr, (int)xalf.size()));
+    const int kh[3] = {B.k1, B.maxleg, B.nang};
+    put(kh, sizeof(kh));
+    put(B.pleg.data(), 8 * (size_t)B.nang * ndvr);
+    const int ib[2] = {B.iang, B.ibass};
+    put(ib, sizeof(ib));
+    put(B.iv.data(), 4 * (size_t)B.nang);
+    put(&nval, 4);
+    put(B.evib.data(), 8 * (size_t)nval);
+    for (int l = 0; l < nval; ++l) put(&vecs[(size_t)l * B.ibass], 8 * (size_t)B.ibass);
+    std::fclose(fp);
+}
+
 int rotlev3b_run(const char *deck_text, const char *wave_path, double *levels, int cap, int *nlev,
-                 const char *kvec_path = nullptr) {
+                 const char *kvec_path = nullptr, std::vector<double> *f_out = nullptr,
+                 const char *kvec2_path = nullptr) {
     // deck: namelist, then the 12i5 card, title, optional ezero
     std::vector<std::string> lines;
     {
@@ -1936,6 +1974,7 @@ int rotlev3b_run(const char *deck_text, const char *wave_path, double *levels, i
         return a == std::string::npos ? 0 : std::atoi(t.c_str() + a);
     };
     int nvib = i5(lines[li], 0), neval = i5(lines[li], 1), kmin = i5(lines[li], 2), ibass = i5(lines[li], 3);
+    int neval2 = i5(lines[li], 4);
     int npnt = i5(lines[li], 5);
     // file
     RotFile f;
@@ -1957,10 +1996,11 @@ int rotlev3b_run(const char *deck_text, const char *wave_path, double *levels, i
     int idia = h[0], ipar = h[1], ndvr = h[2], nmax = h[3], jrot = h[5], kmin0 = h[6], meval = h[7];
     if (idia != -2 || jrot <= 0) fail(DVR3D_ERR_UNSUPPORTED);
     if (kmin != kmin0 && kmin0 != 2) fail(DVR3D_ERR_ARG);
-    if (kmin > 1 || (kmin == 0 && kmin0 != 0)) fail(DVR3D_ERR_UNSUPPORTED);
+    if (kmin > 2 || (kmin == 0 && kmin0 != 0)) fail(DVR3D_ERR_UNSUPPORTED);
     nvib = std::min(nvib, meval);  // insize :171-186
     int nblk = kmin > 0 ? jrot + 1 : jrot;
     if (neval <= 0) neval = 10;
+    if (neval2 <= 0) neval2 = neval;
     npnt = std::max(ndvr, npnt);
     std::vector<unsigned char> rec2;
     {
@@ -1977,8 +2017,9 @@ int rotlev3b_run(const char *deck_text, const char *wave_path, double *levels, i
     std::vector<RotBlock> blk(nblk);
     std::vector<int> mvib(nblk);
     int ipt = 0;
-    for (int ioff = 0; ioff < nblk; ++ioff) {
-        RotBlock &B = blk[ioff];
+    // one k block of the file (ccmain :972-976, testiv :3446-3448, transr :3622-3641), with its
+    // first `keep` vectors (at most)
+    auto read_block = [&](RotBlock &B, int keep) {
         f.skip();  // xalf
         std::vector<int> kk = f.ints();
         B.k1 = kk[0];
@@ -1993,15 +2034,34 @@ int rotlev3b_run(const char *deck_text, const char *wave_path, double *levels, i
         std::vector<int> iv = f.ints();
         B.iv.assign(iv.begin(), iv.begin() + B.nang);
         B.meval = f.ints()[0];
-        mvib[ioff] = std::min(std::min(nvib, B.ibass), B.meval);
+        const int m = std::min(std::min(keep, B.ibass), B.meval);
         B.evib.resize(B.meval);
         f.getrow(B.evib.data(), B.meval);
-        B.coef.assign((size_t)B.ibass * std::max(mvib[ioff], 1), 0.0);
+        B.coef.assign((size_t)B.ibass * std::max(m, 1), 0.0);
         for (int i = 0; i < B.meval; ++i) {
-            if (i < mvib[ioff]) f.getrow(&B.coef[(size_t)i * B.ibass], B.ibass);
+            if (i < m) f.getrow(&B.coef[(size_t)i * B.ibass], B.ibass);
             else f.skip();
         }
+        return m;
+    };
+    for (int ioff = 0; ioff < nblk; ++ioff) {
+        mvib[ioff] = read_block(blk[ioff], nvib);
         ipt += mvib[ioff];
+    }
+    // KMIN = 2: the f-type k = 1 block follows the J + 1 e-type blocks (endiv :1635-1658)
+    RotBlock endblk{};
+    size_t endpos = 0;
+    std::vector<double> endxalf(ndvr, 0.0);
+    if (kmin == 2) {
+        endpos = f.pos;
+        {
+            RotFile g;
+            g.b = f.b;
+            g.pos = endpos;
+            g.getrow(endxalf.data(), ndvr);
+        }
+        read_block(endblk, nvib);
+        if (endblk.k1 != 1) fail(DVR3D_ERR_ARG);
     }
     int nbass = ipt;
     if (ibass > 0 && ibass < ipt) {  // select :391-423
@@ -2028,79 +2088,149 @@ int rotlev3b_run(const char *deck_text, const char *wave_path, double *levels, i
     // radint :686-694
     std::vector<double> radmee = rot_mkrad(nmax, rm2, 0, 0, 0), radmoo = rot_mkrad(nmax, rm2, 1, 0, 0),
                         radmeo = rot_mkrad(nmax, rm2, 1, 1, 0), radmoe = rot_mkrad(nmax, rm2, 1, 1, 1);
-    // the Hamiltonian, in core (loadh :1296-1337)
-    std::vector<double> ham((size_t)nbass * nbass, 0.0);
-    std::vector<int> ist(nblk + 1, 0);
-    for (int i = 0; i < nblk; ++i) ist[i + 1] = ist[i] + mvib[i];
-    for (int i = 0; i < nblk; ++i)
-        for (int v = 0; v < mvib[i]; ++v) ham[(size_t)(ist[i] + v) * nbass + ist[i] + v] = blk[i].evib[v];
-    auto place = [&](int i, int j, const std::vector<double> &offdg) {
-        int p = 0;
-        for (int i1 = 0; i1 < mvib[i]; ++i1)
-            for (int i2 = 0; i2 < mvib[j]; ++i2) {
-                double x = offdg[p++];
-                ham[(size_t)(ist[j] + i2) * nbass + ist[i] + i1] = x;
-                ham[(size_t)(ist[i] + i1) * nbass + ist[j] + i2] = x;
-            }
-    };
     double jjp1 = (double)(jrot * (jrot + 1));
     const double sqrt2 = 1.4142135623731;
-    int ip = ipar;
-    for (int ioff = 2; ioff <= nblk; ++ioff) {  // solrt :1414-1527
-        const RotBlock &B1 = blk[ioff - 2], &B2 = blk[ioff - 1];
-        int k1 = B1.k1;
-        int mn = mvib[ioff - 2] * mvib[ioff - 1];
-        double angfac = +std::sqrt(jjp1 - (double)(k1 * (k1 + 1))) / 2.0;
-        if (k1 == 0) angfac = sqrt2 * angfac;
-        RotQuad q;
-        {
-            int npnt2 = (npnt + 1) / 2;
-            double tswalf = std::pow(2.0, k1 + k1 + 1) / (double)(k1 + 1);
-            for (int i = 1; i <= k1; ++i) tswalf = tswalf * (double)i / (double)(k1 + i + 1);
-            double cswalf;
-            rot_jacobi(npnt, npnt2, q.xalf, q.walf, (double)k1, (double)k1, cswalf, tswalf);
-            if (std::fabs((cswalf - tswalf) / tswalf) > 1.0e-8) fail(DVR3D_ERR_QUADRATURE);
-            for (int i = 1; i <= npnt2; ++i) {
-                q.xalf[npnt + 1 - i] = q.xalf[i];
-                q.xalf[i] = -q.xalf[i];
-                q.walf[npnt + 1 - i] = q.walf[i];
-            }
-        }
-        std::vector<double> angmat, offdg;
-        if (mn > 0) {
-            rot_angin(1, angmat, iang, q, npnt, ndvr, B1, B2, k1, angfac);
-            if (ip == 0)
-                rot_solofd(offdg, radmeo, angmat, iang, nmax, 1, 1, 0, B1.iang, B2.iang, mvib[ioff - 2],
-                           mvib[ioff - 1], B1, B2);
-            else
-                rot_solofd(offdg, radmoe, angmat, iang, nmax, 1, 0, 1, B1.iang, B2.iang, mvib[ioff - 2],
-                           mvib[ioff - 1], B1, B2);
-            place(ioff - 2, ioff - 1, offdg);
-        }
-        if (ioff == nblk) break;
-        const RotBlock &B3 = blk[ioff];
-        mn = mvib[ioff - 2] * mvib[ioff];
-        if (mn > 0) {
-            angfac = -std::sqrt((jjp1 - (double)((k1 + 1) * (k1 + 2))) * (jjp1 - (double)(k1 * (k1 + 1)))) / 16.0;
+    // The Hamiltonian of a chain of k blocks, in core (solrt :1414-1527, loadh :1296-1337): the
+    // levels of each block on the diagonal, the Coriolis blocks of neighbours k, k+1 and k, k+2;
+    // ip0 is the radial parity label of the first pair and alternates along the chain.
+    auto build = [&](const std::vector<const RotBlock *> &B, const std::vector<int> &mv, int ip0,
+                     std::vector<double> &ham, int &nb) {
+        const int nk = (int)B.size();
+        nb = 0;
+        for (int v : mv) nb += v;
+        ham.assign((size_t)nb * nb, 0.0);
+        std::vector<int> ist(nk + 1, 0);
+        for (int i = 0; i < nk; ++i) ist[i + 1] = ist[i] + mv[i];
+        for (int i = 0; i < nk; ++i)
+            for (int v = 0; v < mv[i]; ++v) ham[(size_t)(ist[i] + v) * nb + ist[i] + v] = B[i]->evib[v];
+        auto place = [&](int i, int j, const std::vector<double> &offdg) {
+            int p = 0;
+            for (int i1 = 0; i1 < mv[i]; ++i1)
+                for (int i2 = 0; i2 < mv[j]; ++i2) {
+                    double x = offdg[p++];
+                    ham[(size_t)(ist[j] + i2) * nb + ist[i] + i1] = x;
+                    ham[(size_t)(ist[i] + i1) * nb + ist[j] + i2] = x;
+                }
+        };
+        int ip = ip0;
+        for (int ioff = 2; ioff <= nk; ++ioff) {
+            const RotBlock &B1 = *B[ioff - 2], &B2 = *B[ioff - 1];
+            int k1 = B1.k1;
+            int mn = mv[ioff - 2] * mv[ioff - 1];
+            double angfac = +std::sqrt(jjp1 - (double)(k1 * (k1 + 1))) / 2.0;
             if (k1 == 0) angfac = sqrt2 * angfac;
-            rot_angin(2, angmat, iang, q, npnt, ndvr, B1, B3, k1, angfac);
-            if (ip == 0)
-                rot_solofd(offdg, radmee, angmat, iang, nmax, 0, 0, 0, B1.iang, B3.iang, mvib[ioff - 2],
-                           mvib[ioff], B1, B3);
-            else
-                rot_solofd(offdg, radmoo, angmat, iang, nmax, 1, 0, 0, B1.iang, B3.iang, mvib[ioff - 2],
-                           mvib[ioff], B1, B3);
-            place(ioff - 2, ioff, offdg);
+            RotQuad q;
+            {
+                int npnt2 = (npnt + 1) / 2;
+                double tswalf = std::pow(2.0, k1 + k1 + 1) / (double)(k1 + 1);
+                for (int i = 1; i <= k1; ++i) tswalf = tswalf * (double)i / (double)(k1 + i + 1);
+                double cswalf;
+                rot_jacobi(npnt, npnt2, q.xalf, q.walf, (double)k1, (double)k1, cswalf, tswalf);
+                if (std::fabs((cswalf - tswalf) / tswalf) > 1.0e-8) fail(DVR3D_ERR_QUADRATURE);
+                for (int i = 1; i <= npnt2; ++i) {
+                    q.xalf[npnt + 1 - i] = q.xalf[i];
+                    q.xalf[i] = -q.xalf[i];
+                    q.walf[npnt + 1 - i] = q.walf[i];
+                }
+            }
+            std::vector<double> angmat, offdg;
+            if (mn > 0) {
+                rot_angin(1, angmat, iang, q, npnt, ndvr, B1, B2, k1, angfac);
+                if (ip == 0)
+                    rot_solofd(offdg, radmeo, angmat, iang, nmax, 1, 1, 0, B1.iang, B2.iang, mv[ioff - 2],
+                               mv[ioff - 1], B1, B2);
+                else
+                    rot_solofd(offdg, radmoe, angmat, iang, nmax, 1, 0, 1, B1.iang, B2.iang, mv[ioff - 2],
+                               mv[ioff - 1], B1, B2);
+                place(ioff - 2, ioff - 1, offdg);
+            }
+            if (ioff == nk) break;
+            const RotBlock &B3 = *B[ioff];
+            mn = mv[ioff - 2] * mv[ioff];
+            if (mn > 0) {
+                angfac = -std::sqrt((jjp1 - (double)((k1 + 1) * (k1 + 2))) * (jjp1 - (double)(k1 * (k1 + 1)))) / 16.0;
+                if (k1 == 0) angfac = sqrt2 * angfac;
+                rot_angin(2, angmat, iang, q, npnt, ndvr, B1, B3, k1, angfac);
+                if (ip == 0)
+                    rot_solofd(offdg, radmee, angmat, iang, nmax, 0, 0, 0, B1.iang, B3.iang, mv[ioff - 2],
+                               mv[ioff], B1, B3);
+                else
+                    rot_solofd(offdg, radmoo, angmat, iang, nmax, 1, 0, 0, B1.iang, B3.iang, mv[ioff - 2],
+                               mv[ioff], B1, B3);
+                place(ioff - 2, ioff, offdg);
+            }
+            ip = 1 - ip;
         }
-        ip = 1 - ip;
-    }
+    };
+    std::vector<const RotBlock *> chain;
+    for (auto &B : blk) chain.push_back(&B);
+    std::vector<double> ham;
+    int nb = 0;
+    build(chain, mvib, ipar, ham, nb);
     std::vector<double> ev(nbass);
     diag(ham.data(), nbass, nbass, ev.data());
-    if (kvec_path) rot_dstore(kvec_path, h, rec2, rec3, rgrid, jrot, kmin, ndvr, blk, mvib, ham, nbass, ev, neval);
+    const int kmin_e = kmin == 2 ? 1 : kmin;
+    if (kvec_path) rot_dstore(kvec_path, h, ipar, rec2, rec3, rgrid, jrot, kmin_e, ndvr, chain, mvib, ham, nbass, ev, neval);
     *nlev = neval;
     if (levels) {
         if (cap < neval) fail(DVR3D_ERR_BUFFER);
         for (int i = 0; i < neval; ++i) levels[i] = ev[i];
+    }
+    if (kmin == 2 && f_out) {
+        // the second pass, f parity (vrmain :600-660): k = 1..J with the f-type k = 1 block stored
+        // at the end of the first-step file; the Coriolis blocks among k >= 2 are the first
+        // pass's, those of the k = 1 f block are formed anew (solrt :1529-1617), ip = 1 - ipar
+        const int nbf = nbass - mvib[0];
+        int nevf = std::min(neval2, nbf);
+        std::vector<double> evf;
+        if (jrot == 1) {
+            // J = 1 f: the k = 1 f block alone (dstore1 :2051-2173)
+            nevf = std::min(nevf, endblk.meval);
+            evf.assign(endblk.evib.begin(), endblk.evib.begin() + nevf);
+            if (kvec2_path) {
+                RotBlock e1 = endblk;
+                std::vector<double> vecs;
+                // all nevf vectors of the block, re-read (the e pass kept at most nvib)
+                RotFile g;
+                g.b = f.b;
+                g.pos = endpos;
+                g.skip();
+                g.skip();
+                g.skip();
+                g.skip();
+                g.skip();
+                g.skip();
+                g.skip();
+                vecs.assign((size_t)e1.ibass * nevf, 0.0);
+                for (int l = 0; l < nevf; ++l) g.getrow(&vecs[(size_t)l * e1.ibass], e1.ibass);
+                rot_dstore1(kvec2_path, h, 1 - ipar, rec2, rec3, rgrid, blk[nblk - 1].nang, ndvr, nmax, endxalf, e1, vecs,
+                            nevf);
+            }
+        } else {
+            std::vector<const RotBlock *> fchain{&endblk};
+            std::vector<int> mvf{mvib[1]};
+            for (int i = 2; i < nblk; ++i) {
+                fchain.push_back(&blk[i]);
+                mvf.push_back(mvib[i]);
+            }
+            if (mvf[0] > (int)endblk.evib.size() || (size_t)mvf[0] * endblk.ibass > endblk.coef.size())
+                fail(DVR3D_ERR_ARG);
+            std::vector<double> hf;
+            int nbf2 = 0;
+            build(fchain, mvf, 1 - ipar, hf, nbf2);
+            if (nbf2 != nbf) fail(DVR3D_ERR_ARG);
+            evf.assign(nbf, 0.0);
+            diag(hf.data(), nbf, nbf, evf.data());
+            // the f k = 1 block takes the e-type k = 1 block's place in the labels (select
+            // :374-380 ran on the e blocks); the two must agree in size
+            const int nk1e = (blk[1].ibass / blk[1].iang) * (blk[1].maxleg + blk[1].lincr - blk[1].k1 + 1);
+            const int nk1f = (endblk.ibass / endblk.iang) * (endblk.maxleg + endblk.lincr - endblk.k1 + 1);
+            if (kvec2_path && nk1e != nk1f) fail(DVR3D_ERR_UNSUPPORTED);
+            if (kvec2_path)
+                rot_dstore(kvec2_path, h, 1 - ipar, rec2, rec3, rgrid, jrot, 0, ndvr, fchain, mvf, hf, nbf, evf, nevf);
+            evf.resize(nevf);
+        }
+        *f_out = evf;
     }
     return DVR3D_OK;
 }
@@ -2402,6 +2532,25 @@ int oracle_rotlev3b(const char *deck_text, const char *wave_path, double *levels
         return rotlev3b_run(deck_text, wave_path, levels, cap, nlev);
     } catch (Fail &f) {
         return f.code;
+    }
+}
+
+int oracle_rotlev3b_pair(const char *deck_text, const char *wave_path, const char *kvec_path, const char *kvec2_path,
+                         double *levels, int cap, int *nlev, double *levels2, int cap2, int *nlev2) {
+    if (!deck_text || !wave_path || !nlev || !nlev2) return DVR3D_ERR_ARG;
+    try {
+        std::vector<double> f;
+        int rc = rotlev3b_run(deck_text, wave_path, levels, cap, nlev, (kvec_path && kvec_path[0]) ? kvec_path : nullptr,
+                              &f, (kvec2_path && kvec2_path[0]) ? kvec2_path : nullptr);
+        if (rc != DVR3D_OK) return rc;
+        *nlev2 = (int)f.size();
+        if (levels2) {
+            if (cap2 < (int)f.size()) return DVR3D_ERR_BUFFER;
+            for (size_t i = 0; i < f.size(); ++i) levels2[i] = f[i];
+        }
+        return DVR3D_OK;
+    } catch (Fail &e) {
+        return e.code;
     }
 }
 

@@ -94,6 +94,10 @@ int oracle_dipole3(const char *deck_text, const char *ket_path, const char *bra_
 int oracle_dipole_quadrature(int npot, double *x, double *w, double *csa, double *tsa);
 /* threej :1778-1823 */
 double oracle_threej(int j1, int j2, int j3, int m1, int m2, int m3);
+/* KMIN = 2: both passes (e levels, then the f levels of the second pass, vrmain :600-660),
+ * with ZTRAN the e vectors to kvec_path and the f vectors to kvec2_path (either may be empty). */
+int oracle_rotlev3b_pair(const char *deck_text, const char *wave_path, const char *kvec_path, const char *kvec2_path,
+                         double *levels, int cap, int *nlev, double *levels2, int cap2, int *nlev2);
 /* The same with ZTRAN: the transformed vectors (dstore :1917-2049) written to kvec_path. */
 int oracle_rotlev3b_trans(const char *deck_text, const char *wave_path, const char *kvec_path, double *levels,
                           int cap, int *nlev);

@@ -146,6 +146,8 @@ def load(build: bool = True) -> C.CDLL:
     lib.oracle_time_dsyev.restype = C.c_double
     lib.oracle_rotlev3b.argtypes = [C.c_char_p, C.c_char_p, P(C.c_double), C.c_int, P(C.c_int)]
     lib.oracle_rotlev3b_trans.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, P(C.c_double), C.c_int, P(C.c_int)]
+    lib.oracle_rotlev3b_pair.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, P(C.c_double), C.c_int,
+                                         P(C.c_int), P(C.c_double), C.c_int, P(C.c_int)]
     lib.oracle_dipole3.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, DIPD_FN, DIPSA_FN, C.c_void_p, C.c_char_p,
                                    P(DipoleResult), C.c_char_p, C.c_size_t, P(C.c_size_t)]
     lib.oracle_dipole_quadrature.argtypes = [C.c_int, P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double)]
@@ -317,6 +319,19 @@ def rotlev3b_trans(deck_text: str, wave_path: str, kvec_path: str) -> np.ndarray
     if rc != 0:
         raise RuntimeError(f"oracle_rotlev3b_trans failed: {rc}")
     return lv[:n.value].copy()
+
+
+def rotlev3b_pair(deck_text: str, wave_path: str, kvec_path: str | None = None, kvec2_path: str | None = None):
+    """ROTLEV3B with KMIN = 2: (e levels, f levels) in Eh; with paths, the two vector files."""
+    lv, lv2 = np.zeros(20000), np.zeros(20000)
+    n, n2 = C.c_int(0), C.c_int(0)
+    P = C.POINTER(C.c_double)
+    rc = load().oracle_rotlev3b_pair(deck_text.encode(), str(wave_path).encode(), (kvec_path or "").encode(),
+                                     (kvec2_path or "").encode(), lv.ctypes.data_as(P), lv.size, C.byref(n),
+                                     lv2.ctypes.data_as(P), lv2.size, C.byref(n2))
+    if rc != 0:
+        raise RuntimeError(f"oracle_rotlev3b_pair failed: {rc}")
+    return lv[:n.value].copy(), lv2[:n2.value].copy()
 
 
 def dipole3(deck_text: str, ket_path: str, bra_path: str, dipd=None, dipsa=None, tra_path: str | None = None,
