@@ -196,6 +196,23 @@ class Context:
                                                        C.byref(ln)))
         return le[:ne.value].copy(), lf[:nf.value].copy(), buf.value.decode()
 
+    def rotlev3(self, deck_text: str, wave_path: str, kvec_path: str | None = None,
+                kvec2_path: str | None = None) -> tuple[np.ndarray, np.ndarray, str]:
+        """ROTLEV3, z along r1 or r2 (dvr3d_b200_rotlev3): the first set of levels (e for KMIN =
+        1, 2; f for KMIN = 0), the f set of KMIN = 2 (empty otherwise) and the printed lists; with
+        paths, the vector files (ZTRAN; J = 1 f with KMIN = 0 writes kvec2_path)."""
+        le, lf = np.zeros(20000), np.zeros(20000)
+        ne, nf = C.c_int(0), C.c_int(0)
+        ln = C.c_size_t(0)
+        buf = C.create_string_buffer(1 << 21)
+        P = C.POINTER(C.c_double)
+        self._check(self._lib.dvr3d_b200_rotlev3(self._h, deck_text.encode(), str(wave_path).encode(),
+                                                 (kvec_path or "").encode(), (kvec2_path or "").encode(),
+                                                 le.ctypes.data_as(P), le.size, C.byref(ne),
+                                                 lf.ctypes.data_as(P), lf.size, C.byref(nf), buf, len(buf),
+                                                 C.byref(ln)))
+        return le[:ne.value].copy(), lf[:nf.value].copy(), buf.value.decode()
+
     def dipole3(self, deck_text: str, ket_path: str, bra_path: str, dipd=None, dipsa=None,
                 tra_path: str | None = None, cap: int = 4096) -> dict:
         """DIPOLE3 (dvr3d_b200_dipole3) on two wavefunction files with a Python dipole plug-in:
@@ -269,6 +286,13 @@ class Context:
         t = np.ascontiguousarray(np.asarray(table, dtype=np.float64).ravel())
         self._check(self._lib.dvr3d_b200_set_pes_grid(
             self._h, t.ctypes.data_as(C.POINTER(C.c_double)), t.size))
+
+    def set_pes_grid_k(self, kz: int, table) -> None:
+        """The PES table of k block kz alone, on that block's grid (dvr3d_b200_set_pes_grid_k);
+        an empty table removes it."""
+        t = np.ascontiguousarray(np.asarray(table, dtype=np.float64).ravel())
+        self._check(self._lib.dvr3d_b200_set_pes_grid_k(
+            self._h, int(kz), t.ctypes.data_as(C.POINTER(C.c_double)), t.size))
 
     def grid(self, deck: Deck, kk: int = 0):
         r1 = np.zeros(256)

@@ -150,6 +150,9 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "dvr3d_b200_rotlev3b_pair": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, P(C.c_double),
                                                C.c_int, P(C.c_int), P(C.c_double), C.c_int, P(C.c_int), C.c_char_p,
                                                C.c_size_t, P(C.c_size_t)]),
+        "dvr3d_b200_rotlev3": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, P(C.c_double),
+                                         C.c_int, P(C.c_int), P(C.c_double), C.c_int, P(C.c_int), C.c_char_p,
+                                         C.c_size_t, P(C.c_size_t)]),
         "dvr3d_b200_dipole3": (C.c_int, [vp, C.c_char_p, C.c_char_p, C.c_char_p, DIPD_FN, DIPSA_FN, vp, C.c_char_p,
                                          P(DipoleResult), C.c_char_p, C.c_size_t, P(C.c_size_t)]),
         "dvr3d_b200_split_gemm": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, P(C.c_double), C.c_longlong,
@@ -158,6 +161,7 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "dvr3d_b200_parse_deck": (C.c_int, [C.c_char_p, P(Deck)]),
         "dvr3d_b200_set_pes": (C.c_int, [vp, C.c_int, P(C.c_double), C.c_int]),
         "dvr3d_b200_set_pes_grid": (C.c_int, [vp, P(C.c_double), C.c_size_t]),
+        "dvr3d_b200_set_pes_grid_k": (C.c_int, [vp, C.c_int, P(C.c_double), C.c_size_t]),
         "dvr3d_b200_grid": (C.c_int, [vp, P(Deck), C.c_int, P(C.c_double), C.c_int,
                                       P(C.c_double), C.c_int, P(C.c_double), C.c_int]),
         "dvr3d_b200_solve_block": (C.c_int, [vp, P(Deck), C.c_int, P(Options), P(Result)]),

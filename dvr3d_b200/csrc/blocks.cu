@@ -40,7 +40,7 @@ __global__ void radau_build_kernel(RadauBuild rb, double *H) {
         double fact = rb.term + rb.term2 / (1.0 - x);
         if (rb.kz == 1) fact += rb.term3 * (1.0 + x) / (1.0 - x);
         const double wa = 0.5 / (rb.r[a] * rb.r[a]), wb = 0.5 / (rb.r[b] * rb.r[b]);
-        const double ws = (wa + wb) * fact / rb.urr1;
+        const double ws = (wa + wb) * fact / rb.urr1 - (wa + wb) * rb.xterm / (1.0 - x * x);
         h += (a == b && rb.ipar == 0) ? 2.0 * ws : ws;
     }
     if (b == bp) h += hr(ap, a);
@@ -73,7 +73,12 @@ __global__ void jacobi_build1d_kernel(Jacobi1D jb, double *H) {
         if (i == j) {
             double wterm = 0.0;
             if (jb.jrot > 0) wterm = jb.zembed ? jb.term * w2 * jb.ur2 / jb.urr2 : jb.term * w1 * jb.ur1 / jb.urr1;
-            h += pes_eval(jb.pes, jb.r1[i1], jb.r2[i2], jb.xalf[i], i1, i2, i) + wterm;
+            double v = pes_eval(jb.pes, jb.r1[i1], jb.r2[i2], jb.xalf[i], i1, i2, i);
+            if (jb.w3k != 0.0) {  // the extra term when the vibrational and rotational masses differ
+                const double w3 = jb.w3k * ((jb.ur1 / jb.urr1 - 1.0) * w1 + (jb.ur2 / jb.urr2 - 1.0) * w2);
+                v = v + w3 / (1.0 - jb.xalf[i] * jb.xalf[i]);
+            }
+            h += v + wterm;
         }
     } else {
         h = jb.ta[(size_t)j * jb.lda + i];

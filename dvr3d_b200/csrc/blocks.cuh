@@ -16,6 +16,7 @@ struct RadauBuild {
     const double *hr;         // DVR kinetic matrix xk1 (npnt x npnt)
     const double *xalf;       // cos theta of each angle
     double term, term2, term3, urr1;
+    double xterm;             // ZX: k^2 (1/ur1 - 1/urr1), subtracted over (1 - x^2) (blc2d1 :3169)
     PesParams pes;
 };
 
@@ -26,6 +27,7 @@ struct Jacobi1D {
     const double *ta;         // kinetic matrix of coordinate a (xk1, xk2 or L), lda
     int lda;
     double ur1, ur2, urr1, urr2, term;
+    double w3k;               // ZX, theta first: k^2 of mkham1's extra term (:2166-2171), else 0
     PesParams pes;
 };
 

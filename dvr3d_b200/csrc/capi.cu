@@ -192,7 +192,8 @@ int dvr3d_b200_set_pes(dvr3d_ctx *ctx, int kind, const double *params, int npara
         return DVR3D_OK;
     }
     if (kind == DVR3D_PES_GRID) {
-        if (ctx->pes_grid.empty()) return fail_ctx(ctx, DVR3D_ERR_ARG, "call dvr3d_b200_set_pes_grid first");
+        if (ctx->pes_grid.empty() && ctx->pes_grid_k.empty())
+            return fail_ctx(ctx, DVR3D_ERR_ARG, "call dvr3d_b200_set_pes_grid first");
         ctx->pes.kind = kind;
         return DVR3D_OK;
     }
@@ -204,6 +205,19 @@ int dvr3d_b200_set_pes_grid(dvr3d_ctx *ctx, const double *v, size_t n) {
     for (size_t i = 0; i < n; ++i)
         if (!std::isfinite(v[i])) return fail_ctx(ctx, DVR3D_ERR_PES, "non-finite value in the PES table");
     ctx->pes_grid.assign(v, v + n);
+    ctx->pes.kind = DVR3D_PES_GRID;
+    return DVR3D_OK;
+}
+
+int dvr3d_b200_set_pes_grid_k(dvr3d_ctx *ctx, int kz, const double *v, size_t n) {
+    if (!ctx || kz < 0 || (n > 0 && !v)) return DVR3D_ERR_ARG;
+    if (n == 0) {
+        ctx->pes_grid_k.erase(kz);
+        return DVR3D_OK;
+    }
+    for (size_t i = 0; i < n; ++i)
+        if (!std::isfinite(v[i])) return fail_ctx(ctx, DVR3D_ERR_PES, "non-finite value in the PES table");
+    ctx->pes_grid_k[kz].assign(v, v + n);
     ctx->pes.kind = DVR3D_PES_GRID;
     return DVR3D_OK;
 }
@@ -426,6 +440,31 @@ int dvr3d_b200_rotlev3b_pair(dvr3d_ctx *ctx, const char *deck_text, const char *
             std::memcpy(levels_f, lf.data(), sizeof(double) * lf.size());
         }
         copy_out(table, out, outcap, outlen);
+        return DVR3D_OK;
+    });
+}
+
+int dvr3d_b200_rotlev3(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, const char *kvec_path,
+                       const char *kvec2_path, double *levels, int cap, int *nlev, double *levels_f, int cap_f,
+                       int *nlev_f, char *out, size_t outcap, size_t *outlen) {
+    if (!ctx || !deck_text || !wave_path || !nlev) return DVR3D_ERR_ARG;
+    return guarded(ctx, [&]() -> int {
+        cudaSetDevice(ctx->device);
+        std::vector<double> le, lf;
+        std::string text;
+        dvr3d::RotInfo info;
+        dvr3d::rotlev3_solve(ctx, deck_text, wave_path, le, lf, text, info, kvec_path, kvec2_path);
+        *nlev = (int)le.size();
+        if (nlev_f) *nlev_f = (int)lf.size();
+        if (levels) {
+            if (cap < (int)le.size()) return fail_ctx(ctx, DVR3D_ERR_BUFFER, "levels buffer smaller than neval");
+            std::memcpy(levels, le.data(), sizeof(double) * le.size());
+        }
+        if (levels_f && !lf.empty()) {
+            if (cap_f < (int)lf.size()) return fail_ctx(ctx, DVR3D_ERR_BUFFER, "f levels buffer smaller than neval2");
+            std::memcpy(levels_f, lf.data(), sizeof(double) * lf.size());
+        }
+        copy_out(text, out, outcap, outlen);
         return DVR3D_OK;
     });
 }

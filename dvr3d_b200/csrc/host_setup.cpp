@@ -590,7 +590,7 @@ void plan_block(const dvr3d_deck &d, int kk, BlockPlan &p) {
     if (d.ncoord == 2) raise(DVR3D_ERR_UNSUPPORTED, "ncoord=2 (rigid diatom) is not on this path");
     if (!d.zquad2) raise(DVR3D_ERR_UNSUPPORTED, "zquad2=F is not on this path");
     if (!d.zmors1 || !d.zmors2) raise(DVR3D_ERR_UNSUPPORTED, "spherical oscillators (zmors=F) are not on this path");
-    if (d.zx || d.zs0 || d.zs1) raise(DVR3D_ERR_UNSUPPORTED, "zx/zs0/zs1 corrections are not on this path");
+    if (d.zs0 || d.zs1) raise(DVR3D_ERR_UNSUPPORTED, "zs0/zs1 NBO corrections are not on this path");
     int npnt1 = d.npnt1, npnt2 = d.npnt2, nalf = d.nalf, jrot = d.jrot, kmin = d.kmin;
     int idia = d.idia, ipar = d.ipar, max2d = d.max2d, max3d = d.max3d, max3d2 = d.max3d2;
     int neval = d.neval;
@@ -887,6 +887,7 @@ void plan_block(const dvr3d_deck &d, int kk, BlockPlan &p) {
     }
     // J > 0 angular-momentum terms
     p.term = (double)(jrot * jrot + jrot - 2 * kz * kz);  // jhmain :1970
+    p.xp0 = d.zx ? 1.0 : 0.0;
     if (jrot != 0 && zperp) {  // z_blc2d1 :4059-4073
         const double rj = jrot, rk = kz;
         p.nf_term = rk * rk / 4.0;                                           // k^2 / 4

@@ -52,6 +52,7 @@ struct BlockPlan {
     std::vector<double> pleg_walf;
     // J > 0 terms
     double term = 0;                   // jhmain :1970
+    double xp0 = 0;                    // the rotational x-term (ZX, :571-577): mkham1 :2166-2171, blc2d1 :3169
     double nf_term = 0, nf_term2 = 0, nf_term3 = 0;  // nfmain :3055-3064; z-perp: z_blc2d1 :4059-4073
                                                      // (k^2/4, s (J(J+1)-k^2)/4, -+J(J+1)/4)
 };

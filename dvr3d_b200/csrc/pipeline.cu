@@ -149,11 +149,13 @@ void radau_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
     rb.term3 = p.nf_term3;
     rb.zperp = p.zperp ? 1 : 0;
     rb.urr1 = p.urr1;
+    rb.xterm = p.zperp ? 0.0 : (double)(p.kz * p.kz) * (1.0 / p.ur1 - 1.0 / p.urr1) * p.xp0;
     rb.pes = ctx->pes;
     if (rb.pes.kind == DVR3D_PES_GRID) {
-        if (ctx->pes_grid.size() < (size_t)nalf * p.npnt1 * p.npnt1)
+        const std::vector<double> &tab = ctx->pes_table(p.kz);
+        if (tab.size() < (size_t)nalf * p.npnt1 * p.npnt1)
             throw HostError{DVR3D_ERR_ARG, "tabulated PES smaller than the DVR grid"};
-        rb.pes.grid = upload(ctx, "pesgrid", ctx->pes_grid);
+        rb.pes.grid = upload(ctx, "pesgrid", tab);
         rb.pes.npnt1 = p.npnt1;
         rb.pes.npnt2 = p.npnt1;
     }
@@ -283,11 +285,13 @@ void jacobi_stage(dvr3d_ctx *ctx, const BlockPlan &p, Contracted &out) {
     j1.urr1 = p.urr1;
     j1.urr2 = p.urr2;
     j1.term = p.term;
+    j1.w3k = (p.ztheta && p.jrot > 0 && p.kz > 0) ? (double)(p.kz * p.kz) * p.xp0 : 0.0;
     j1.pes = ctx->pes;
     if (j1.pes.kind == DVR3D_PES_GRID) {
-        if (ctx->pes_grid.size() < (size_t)p.idvr * p.npnt1 * p.npnt2)
+        const std::vector<double> &tab = ctx->pes_table(p.kz);
+        if (tab.size() < (size_t)p.idvr * p.npnt1 * p.npnt2)
             throw HostError{DVR3D_ERR_ARG, "tabulated PES smaller than the DVR grid"};
-        j1.pes.grid = upload(ctx, "pesgrid", ctx->pes_grid);
+        j1.pes.grid = upload(ctx, "pesgrid", tab);
         j1.pes.npnt1 = p.npnt1;
         j1.pes.npnt2 = p.npnt2;
     }
@@ -872,6 +876,7 @@ void radau_stage_batch(dvr3d_ctx *ctx, const std::vector<BlockPlan> &plans, cons
         rb.term3 = p.nf_term3;
         rb.zperp = p.zperp ? 1 : 0;
         rb.urr1 = p.urr1;
+        rb.xterm = p.zperp ? 0.0 : (double)(p.kz * p.kz) * (1.0 / p.ur1 - 1.0 / p.urr1) * p.xp0;
         rb.pes = pes[i];
         if (rb.pes.kind != DVR3D_PES_MORSE_SUM)
             throw HostError{DVR3D_ERR_ARG, "batched problems take DVR3D_PES_MORSE_SUM surfaces"};

@@ -52,6 +52,12 @@ struct dvr3d_ctx {
     std::string last_error;
     dvr3d::PesParams pes{};
     std::vector<double> pes_grid;  // host copy of a tabulated PES
+    std::map<int, std::vector<double>> pes_grid_k;  // tables of single k blocks (their own grids)
+    // the table of k block kz: its own, else the common one
+    const std::vector<double> &pes_table(int kz) const {
+        const auto it = pes_grid_k.find(kz);
+        return it == pes_grid_k.end() ? pes_grid : it->second;
+    }
     dvr3d::DeviceArena arena;
     cudaEvent_t ev[8] = {};
     int sm_count = 0;

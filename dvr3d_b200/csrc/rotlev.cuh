@@ -24,4 +24,14 @@ void rotlev3b_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path
                     std::string &table, RotInfo &info, const char *kvec_path = nullptr,
                     std::vector<double> *levels_f = nullptr, const char *kvec2_path = nullptr);
 
+// ROTLEV3 (z along r1 or r2; Jacobi and unsymmetrised Radau files): reads its deck (namelist
+// PRT, NVIB/NEVAL/KMIN/IBASS/NEVAL2 card, title, optional EZERO) and the first step's file.
+// levels: the e set (KMIN = 1, 2) or the f set (KMIN = 0); levels_f: the f set of KMIN = 2;
+// text: the printed level lists. With kvec_path / kvec2_path (ZTRAN) the vectors of the first /
+// second set are written as dstore does; J = 1 f (KMIN = 0) writes its set to kvec2_path, as the
+// reference does. Throws HostError / CudaFail.
+void rotlev3_solve(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, std::vector<double> &levels,
+                   std::vector<double> &levels_f, std::string &text, RotInfo &info, const char *kvec_path,
+                   const char *kvec2_path);
+
 }  // namespace dvr3d

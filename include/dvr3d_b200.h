@@ -225,6 +225,25 @@ int dvr3d_b200_rotlev3b_pair(dvr3d_ctx *ctx, const char *deck_text, const char *
                              const char *kvec2_path, double *levels_e, int cap_e, int *nlev_e, double *levels_f,
                              int cap_f, int *nlev_f, char *out, size_t outcap, size_t *outlen);
 
+/* The second variational step for J > 0 with the z axis along r1 or r2 (Jacobi coordinates,
+ * IDIA = 1 or 2, and unsymmetrised Radau): the reference's program ROTLEV3 (source/rotlev3.f90).
+ * deck_text is ROTLEV3's stdin (namelist PRT, card NVIB,NEVAL,KMIN,IBASS,NEVAL2 (12i5, insize
+ * :150-151), title, optional EZERO card, vrmain :519-522); wave_path the first step's ZTRAN file
+ * (unit IWAVE = 26; KMIN = 1 or 2 need a file of KMIN = 1, :287). The Hamiltonian in the lowest
+ * first-step functions of each k block (select :301-480) with the Coriolis blocks of k-1, k
+ * (solrt :671-837 on the vectors taken to associated Legendre functions, jtran :839-905) is built
+ * on the device; its lowest NEVAL levels (Eh, dgrot :1046-1199) go to levels (cap), their number
+ * to *nlev: the e set for KMIN = 1, the f set for KMIN = 0; KMIN = 2 also gives the f set (the
+ * Hamiltonian without its k = 0 block, NEVAL2 levels, vrmain :600-660) in levels_f (cap_f,
+ * *nlev_f; may be NULL otherwise). Non-empty kvec_path / kvec2_path (ZTRAN) receive the first /
+ * second set's vectors in the first step's basis (dstore :1201-1342, units KVEC = 8 and
+ * KVEC2 = 9); the J = 1 f set is the file's second k block copied as a one-block file (dstore1
+ * :1344-1476), written to kvec2_path also when KMIN = 0, as the reference writes it to KVEC2.
+ * out / outlen receive the printed level lists. */
+int dvr3d_b200_rotlev3(dvr3d_ctx *ctx, const char *deck_text, const char *wave_path, const char *kvec_path,
+                       const char *kvec2_path, double *levels, int cap, int *nlev, double *levels_f, int cap_f,
+                       int *nlev_f, char *out, size_t outcap, size_t *outlen);
+
 /* ---- DIPOLE3: transition moments between two sets of vib-rot states ------------------- */
 /* The user's dipole surface, the two plug-ins of source/dipole3_segmented.f90:
  *   DIPD(DIPC, R1, R2, XCOS, NU) (:2054): component nu (0: along the embedding z axis, 1: x)
@@ -287,6 +306,11 @@ int dvr3d_b200_parse_deck(const char *text, dvr3d_deck *out);
 int dvr3d_b200_set_pes(dvr3d_ctx *ctx, int kind, const double *params, int nparams);
 /* Table of V for DVR3D_PES_GRID (layout documented at DVR3D_PES_GRID). */
 int dvr3d_b200_set_pes_grid(dvr3d_ctx *ctx, const double *v, size_t n);
+/* The table of k block kz alone, in the same layout on that block's own grid (the angular
+ * points of block k are those of its associated Legendre quadrature, dvr3d_b200_grid(kz)):
+ * with ZROT every k block of a run calls the reference's POTV at its own points. Takes
+ * precedence over the common table for that block; n = 0 removes it. */
+int dvr3d_b200_set_pes_grid_k(dvr3d_ctx *ctx, int kz, const double *v, size_t n);
 
 /* DVR grid of one k block, so a host can evaluate its own POTV there: r1[npnt1],
  * r2[npnt2] (bohr; r2 = r1 for Radau idia=-2) and xalf[nalf] (cos theta, full range),

@@ -12,7 +12,7 @@ from pathlib import Path
 
 HERE = Path(__file__).resolve().parent
 ROOT = HERE.parent
-SOURCES = [HERE / "dvr3d_oracle.cpp", HERE / "deck_reader.cpp", HERE / "dipole3_oracle.cpp"]
+SOURCES = [HERE / "dvr3d_oracle.cpp", HERE / "deck_reader.cpp", HERE / "dipole3_oracle.cpp", HERE / "rotlev3_oracle.cpp"]
 DEPS = SOURCES + [HERE / "dvr3d_oracle.h", ROOT / "include" / "dvr3d_b200.h"]
 LIB = HERE / "libdvr3d_oracle.so"
 

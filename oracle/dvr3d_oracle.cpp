@@ -644,6 +644,19 @@ void asleg(Run &R) {
     }
 }
 
+// the block's angular record of a ZTRAN file (ccmain :972-976) into the trace
+void trace_pleg(const Run &R, oracle_trace *tr) {
+    if (!tr) return;
+    tr->maxleg = R.maxleg;
+    tr->nidvr = R.nidvr;
+    tr->lincr = R.lincr;
+    const size_t n = (size_t)(R.maxleg + 1) * R.nidvr;
+    if (!tr->pleg_walf || tr->pleg_cap < n || R.pleg.size() < n) return;
+    for (int j = 0; j < R.nidvr; ++j)
+        for (int i = 0; i <= R.maxleg; ++i)
+            tr->pleg_walf[(size_t)j * (R.maxleg + 1) + i] = R.pleg[(size_t)j * (R.maxleg + 1) + i] * R.walf[j];
+}
+
 // lmatrx :1846-1911 -> xlmatr(idvr,idvr) column-major (z-perp: j from 0 with the weights
 // (j+1+alf)(j+alf) of the Jacobi polynomials)
 void lmatrx(Run &R, int ipar0) {
@@ -1199,6 +1212,7 @@ void nfmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
         tr->stage_s[1] = std::chrono::duration<double>(t2 - t1).count();
         tr->stage_s[2] = std::chrono::duration<double>(t3 - t2).count();
         tr->stage_s[3] = std::chrono::duration<double>(t3 - t0).count();
+        trace_pleg(R, tr);
     }
     if (tr && tr->psi && final_mode != 2) {
         // transr (:3622-3641): wvfunc(nbass), index over the pairs irs (outer) and the angles
@@ -1549,6 +1563,7 @@ void jhmain(Run &R, int final_mode, oracle_trace *tr, dvr3d_result *res) {
         tr->stage_s[1] = std::chrono::duration<double>(t2 - t1).count();
         tr->stage_s[2] = std::chrono::duration<double>(t3 - t2).count();
         tr->stage_s[3] = std::chrono::duration<double>(t3 - t0).count();
+        trace_pleg(R, tr);
     }
     if (want_psi && final_mode != 2) {
         // trans (:3733-3841): psi(idvr, npnt1, npnt2) for each level, summed block by block
@@ -2238,6 +2253,15 @@ int rotlev3b_run(const char *deck_text, const char *wave_path, double *levels, i
 }  // namespace
 
 extern "C" {
+
+int oracle_dsyev_lower(double *a, int n, double *w) {
+    try {
+        diag(a, n, n, w);
+        return DVR3D_OK;
+    } catch (const Fail &f) {
+        return f.code;
+    }
+}
 
 int oracle_load_lapack(const char *path, const char *prefix) {
     void *h = dlopen(path, RTLD_NOW | RTLD_LOCAL);

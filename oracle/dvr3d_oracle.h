@@ -19,6 +19,10 @@ extern "C" {
  * as scipy_dsyev_ ...). `prefix` is the symbol prefix ("scipy_" or ""). */
 int oracle_load_lapack(const char *path, const char *prefix);
 
+/* All eigenpairs of the symmetric n x n matrix a (lower triangle read, column-major) by the
+ * loaded dsyev('V','L'): ascending w, vectors over a. */
+int oracle_dsyev_lower(double *a, int n, double *w);
+
 /* The oracle's own reader of a job deck (deck_reader.cpp), independent of the product's
  * dvr3d_b200_parse_deck: namelist PRT, cards 2-10 and the optional EZERO card. */
 int oracle_parse_deck(const char *text, dvr3d_deck *out);
@@ -56,6 +60,10 @@ typedef struct oracle_trace {
      * transr :3596-3643): psi_nlev records of psi_len doubles, as the reference writes them */
     double *psi; size_t psi_cap;
     long long psi_len; int psi_nlev;
+    /* the angular record of the block as a ZTRAN file holds it (ccmain :972-976): pleg(l, i)
+     * walf(i), (maxleg + 1) x nidvr, with the kz line's maxleg, nidvr and lincr */
+    double *pleg_walf; size_t pleg_cap;
+    int maxleg, nidvr, lincr;
 } oracle_trace;
 
 /* final_mode: 0 = dsyev('V','L') with lwork = 3*N as diag() does (:2650-2654);
@@ -101,6 +109,12 @@ int oracle_rotlev3b_pair(const char *deck_text, const char *wave_path, const cha
 /* The same with ZTRAN: the transformed vectors (dstore :1917-2049) written to kvec_path. */
 int oracle_rotlev3b_trans(const char *deck_text, const char *wave_path, const char *kvec_path, double *levels,
                           int cap, int *nlev);
+/* ROTLEV3 (rotlev3_oracle.cpp): the second step for z along r1 or r2 on a first-step ZTRAN
+ * file. levels: the e set (KMIN = 1, 2) or the f set (KMIN = 0); levels_f: the f set of
+ * KMIN = 2. With ZTRAN the first set's vectors go to kvec_path and the KMIN = 2 f set's to
+ * kvec2_path; J = 1 f (KMIN = 0) writes its single block to kvec2_path as the reference does. */
+int oracle_rotlev3(const char *deck_text, const char *wave_path, const char *kvec_path, const char *kvec2_path,
+                   double *levels, int cap, int *nlev, double *levels_f, int cap_f, int *nlev_f);
 /* ROTLEV3B's Gauss-associated Legendre rule (jacobi :941-1007): the npnt2 = (npnt+1)/2 points
  * of the half range (descending from 1) and weights, computed and exact sums of weights. */
 int oracle_rot_quadrature(int npnt, int k, double *x, double *w, double *cswalf, double *tswalf);

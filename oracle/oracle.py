@@ -101,7 +101,9 @@ class Trace(C.Structure):
                 ("h3", C.POINTER(C.c_double)), ("h3_cap", C.c_size_t),
                 ("stage_s", C.c_double * 4), ("nham3", C.c_int),
                 ("psi", C.POINTER(C.c_double)), ("psi_cap", C.c_size_t),
-                ("psi_len", C.c_longlong), ("psi_nlev", C.c_int)]
+                ("psi_len", C.c_longlong), ("psi_nlev", C.c_int),
+                ("pleg_walf", C.POINTER(C.c_double)), ("pleg_cap", C.c_size_t),
+                ("maxleg", C.c_int), ("nidvr", C.c_int), ("lincr", C.c_int)]
 
 
 def _lapack_path() -> str:
@@ -148,6 +150,8 @@ def load(build: bool = True) -> C.CDLL:
     lib.oracle_rotlev3b_trans.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, P(C.c_double), C.c_int, P(C.c_int)]
     lib.oracle_rotlev3b_pair.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, P(C.c_double), C.c_int,
                                          P(C.c_int), P(C.c_double), C.c_int, P(C.c_int)]
+    lib.oracle_rotlev3.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_char_p, P(C.c_double), C.c_int,
+                                   P(C.c_int), P(C.c_double), C.c_int, P(C.c_int)]
     lib.oracle_dipole3.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, DIPD_FN, DIPSA_FN, C.c_void_p, C.c_char_p,
                                    P(DipoleResult), C.c_char_p, C.c_size_t, P(C.c_size_t)]
     lib.oracle_dipole_quadrature.argtypes = [C.c_int, P(C.c_double), P(C.c_double), P(C.c_double), P(C.c_double)]
@@ -228,6 +232,10 @@ class OracleResult:
     kz: int
     ipar: int
     psi: np.ndarray | None = None  # (levels, record length): amplitudes as trans / transr write them
+    pleg_walf: np.ndarray | None = None  # ((maxleg + 1) x nidvr, column-major) the block's angular record
+    maxleg: int = 0
+    nidvr: int = 0
+    lincr: int = 0
 
 
 def solve(deck: Deck, kk: int = 0, pes=None, vgrid=None, final_mode: int = 0, want_h3: bool = False,
@@ -273,6 +281,9 @@ def solve(deck: Deck, kk: int = 0, pes=None, vgrid=None, final_mode: int = 0, wa
         psi = np.zeros(cap)
         t.psi = psi.ctypes.data_as(C.POINTER(C.c_double))
         t.psi_cap = psi.size
+        pleg = np.zeros(256 * 256)
+        t.pleg_walf = pleg.ctypes.data_as(C.POINTER(C.c_double))
+        t.pleg_cap = pleg.size
     kind, pp, npes, vg, nvg = 0, None, 0, None, 0
     if pes is not None:
         p = np.ascontiguousarray(np.asarray(pes, dtype=np.float64))
@@ -291,7 +302,9 @@ def solve(deck: Deck, kk: int = 0, pes=None, vgrid=None, final_mode: int = 0, wa
                         h3=None if h3 is None or n == 0 else h3[:n * n].reshape(n, n, order="F").copy(),
                         stage_s=np.array(t.stage_s[:]), kz=t.kz, ipar=t.ipar,
                         psi=None if psi is None or t.psi_nlev == 0 else
-                        psi[:t.psi_len * t.psi_nlev].reshape(t.psi_nlev, t.psi_len).copy())
+                        psi[:t.psi_len * t.psi_nlev].reshape(t.psi_nlev, t.psi_len).copy(),
+                        pleg_walf=None if psi is None else pleg[:(t.maxleg + 1) * t.nidvr].copy(),
+                        maxleg=t.maxleg, nidvr=t.nidvr, lincr=t.lincr)
 
 
 def pes_morse_sum(p, r1: float, r2: float, x: float) -> float:
@@ -331,6 +344,20 @@ def rotlev3b_pair(deck_text: str, wave_path: str, kvec_path: str | None = None, 
                                      lv2.ctypes.data_as(P), lv2.size, C.byref(n2))
     if rc != 0:
         raise RuntimeError(f"oracle_rotlev3b_pair failed: {rc}")
+    return lv[:n.value].copy(), lv2[:n2.value].copy()
+
+
+def rotlev3(deck_text: str, wave_path: str, kvec_path: str | None = None, kvec2_path: str | None = None):
+    """ROTLEV3 (z along r1 or r2): (first set, KMIN = 2 f set) of levels in Eh; with paths, the
+    vector files (J = 1 f with KMIN = 0 writes kvec2_path)."""
+    lv, lv2 = np.zeros(20000), np.zeros(20000)
+    n, n2 = C.c_int(0), C.c_int(0)
+    P = C.POINTER(C.c_double)
+    rc = load().oracle_rotlev3(deck_text.encode(), str(wave_path).encode(), (kvec_path or "").encode(),
+                               (kvec2_path or "").encode(), lv.ctypes.data_as(P), lv.size, C.byref(n),
+                               lv2.ctypes.data_as(P), lv2.size, C.byref(n2))
+    if rc != 0:
+        raise RuntimeError(f"oracle_rotlev3 failed: {rc}")
     return lv[:n.value].copy(), lv2[:n2.value].copy()
 
 

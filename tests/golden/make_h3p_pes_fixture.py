@@ -21,6 +21,8 @@ Morse-coordinate fit POTS through SOTV / POTV11; RJ; VLIM; VLIM1). Its coefficie
 (the DATA statements and CA(i) assignments) are not copied: they are read from the
 reference file each time the script runs. Nothing at test time reads the reference.
 
+It also writes ``h3p_jacobi_j1.npz``, the J = 1 run of the same example (main_j1).
+
 Run from the repository root:  python tests/golden/make_h3p_pes_fixture.py /path/to/reference
 """
 from __future__ import annotations
@@ -338,5 +340,78 @@ def main(ref_root: str) -> None:
           f"{len(levels)} printed levels, N = {nham3}, {len(counts)} blocks")
 
 
+DECK_J1 = "H3+Jacobi/jobs/dvrJ1.job"
+RESULT_J1 = "H3+Jacobi/results/result.H3p.J1even.dvr"
+ROT_J1 = "H3+Jacobi/jobs/rot.job"
+ROT_RESULT_J1 = "H3+Jacobi/results/result.H3p.J1even.rot"
+
+
+def printed_j1(text: str):
+    """Per k block of the J = 1 run: the printed counts, basis size and 400 levels."""
+    out = []
+    starts = [m.start() for m in re.finditer(r"point Gauss-associated Legendre integration with k =", text)]
+    for a, b in zip(starts, starts[1:] + [len(text)]):
+        out.append(printed(text[a:b]))
+    return out
+
+
+def printed_rot(text: str):
+    """ROTLEV3's two printed lists of levels in hartrees (the e set, then the J = 1 f set)."""
+    sets = []
+    for m in re.finditer(r"LOWEST\s+(\d+) EIGENVALUES IN HARTREES", text):
+        n = int(m.group(1))
+        vals = re.findall(r"[-+]?\d\.\d+D[-+]\d+", text[m.end():])[:n]
+        sets.append(np.array([_num(v) for v in vals]))
+    return sets
+
+
+def j1_deck(job: str, job_j0: str) -> str:
+    """The J = 1 job deck as the printed run used it. The printed output (a June 2010 build) gives
+    the rotational masses as 1.007276 u -- the J = 0 deck's second mass card, 1.007276470 --
+    where the job file holds 1.0075372 twice, and its k = 1 levels carry mkham1's extra term for
+    unequal vibrational and rotational masses, which the current source applies only with
+    ZX = .TRUE. (:571-577, :2166-2171). So: the J = 0 deck's rotational-mass card, and ZX on.
+    With these the oracle reproduces both blocks' 400 printed levels to their 12 digits."""
+    lines = job.splitlines()
+    lines_j0 = job_j0.splitlines()
+    lines[7] = lines_j0[7]
+    lines[1] = lines[1].replace("ztran=.true.,", "ztran=.true., zx=.true.,")
+    assert "zx=.true." in lines[1]
+    return "\n".join(lines) + "\n"
+
+
+def main_j1(ref_root: str) -> None:
+    """``h3p_jacobi_j1.npz``: the J = 1 (even, KMIN = 1) first step of the same example with the
+    potential on the grid of each k block (k = 0, 1: each has its own associated Legendre points),
+    its printed counts and levels per block, and ROTLEV3's deck (rot.job, KMIN = 2) with the two
+    printed sets of levels (``result.H3p.J1even.rot``)."""
+    ref = Path(ref_root)
+    from oracle import oracle
+
+    deck = j1_deck((ref / DECK_J1).read_text(), (ref / DECK).read_text())
+    blocks = printed_j1((ref / RESULT_J1).read_text())
+    rot = printed_rot((ref / ROT_RESULT_J1).read_text())
+    coef = read_coefficients(ref / PES)
+    d = oracle.parse_deck(deck)
+    out = {"deck": np.array(deck), "rot_deck": np.array((ref / ROT_J1).read_text()),
+           "rot_e": rot[0], "rot_f": rot[1]}
+    for k in (0, 1):
+        q = oracle.quadrature(d, k)
+        n1, n2, na = q.npnt1, q.npnt2, q.nidvr
+        r1, r2, xa = np.array(q.r1[:n1]), np.array(q.r2[:n2]), np.array(q.xalf[:na])
+        v = np.empty((na, n2, n1))
+        for ia, x in enumerate(xa):
+            for i2, b in enumerate(r2):
+                for i1, a in enumerate(r1):
+                    v[ia, i2, i1] = potv(coef, a, b, x, q.g1)
+        counts, nham3, levels = blocks[k]
+        out.update({f"v{k}": v.ravel(), f"xalf{k}": xa, f"levels{k}": levels,
+                    f"counts{k}": np.array(counts, dtype=np.int32), f"nham3_{k}": np.array(nham3)})
+    np.savez_compressed(HERE / "h3p_jacobi_j1.npz", **out)
+    print(f"J=1: {len(blocks)} blocks, {[len(b[2]) for b in blocks]} levels, ROTLEV3 sets {[len(r) for r in rot]}")
+
+
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    main(root)
+    main_j1(root)
