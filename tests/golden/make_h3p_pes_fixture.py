@@ -21,7 +21,9 @@ Morse-coordinate fit POTS through SOTV / POTV11; RJ; VLIM; VLIM1). Its coefficie
 (the DATA statements and CA(i) assignments) are not copied: they are read from the
 reference file each time the script runs. Nothing at test time reads the reference.
 
-It also writes ``h3p_jacobi_j1.npz``, the J = 1 run of the same example (main_j1).
+It also writes ``h3p_jacobi_j1.npz``, the J = 1 run of the same example (main_j1), and
+``h3p_jacobi_dip.npz``, its dipole surface dip_h3p.f tabulated at the points of its DIPOLE3 job
+(main_dip; the functional form restated here, its coefficients read from the reference file).
 
 Run from the repository root:  python tests/golden/make_h3p_pes_fixture.py /path/to/reference
 """
@@ -411,7 +413,85 @@ def main_j1(ref_root: str) -> None:
     print(f"J=1: {len(blocks)} blocks, {[len(b[2]) for b in blocks]} levels, ROTLEV3 sets {[len(r) for r in rot]}")
 
 
+DIP = "H3+Jacobi/source/dip_h3p.f"
+DIP_JOB = "H3+Jacobi/jobs/dip.job"
+
+
+def read_dipole(path: Path) -> dict:
+    """BETA, RE and the seven D coefficients of DIPD's DATA statements (dip_h3p.f :15-17), taken
+    at the precision of the DOUBLE PRECISION variables they initialise: the printed moments of
+    the example's dipole run agree with these to the printed digits, while the same literals
+    rounded to single precision first leave 2e-8 relative differences (the printing build's
+    compiler converted DATA constants to the variables' type from their text)."""
+    src = path.read_text()
+    unit = src[:src.upper().index("SUBROUTINE DIPD0")]
+    out = {}
+    for stmt in re.findall(r"(?im)^\s+DATA\s+(.*(?:\n\s+\d(.*))*)", unit):
+        text = re.sub(r"\n\s+\d", "", stmt[0])
+        for name, vals in re.findall(r"(\w+)\s*/([^/]*)/", text):
+            toks = [t.strip() for t in vals.split(",") if t.strip()]
+            out[name.upper()] = [_num(t) for t in toks]
+    return {"BETA": out["BETA"][0], "RE": out["RE"][0], "D": out["D"]}
+
+
+def h3p_dipd(c: dict, r1: float, r2: float, xcos: float, nu: int, g1: float, xmass, zembed: bool) -> float:
+    """DIPD of dip_h3p.f (the surface of Roeshe et al., J. Chem. Phys. 101, 2231 (1994)) in
+    scattering coordinates: symmetry coordinates of the Morse-type bond displacements, the
+    z and x components of the body-fixed dipole, and the component nu in the embedding of the
+    wavefunctions (z along r2 if ZEMBED, else along r1)."""
+    beta, re_, d = c["BETA"], c["RE"], c["D"]
+    sr2, sr3 = math.sqrt(2.0), math.sqrt(3.0)
+    sr6 = sr2 * sr3
+    a, b = r1 * g1, r1 - r1 * g1
+    bonds = (r1, math.sqrt(r2 * r2 + a * a - 2.0 * a * r2 * xcos), math.sqrt(r2 * r2 + b * b + 2.0 * b * r2 * xcos))
+    disp = [(1.0 - math.exp(-beta * (q / re_ - 1.0))) / beta for q in bonds]
+    sa = sum(disp) / sr3
+    sz = (2.0 * disp[0] - disp[1] - disp[2]) / sr6
+    sx = (disp[2] - disp[1]) / sr2
+    se2 = sz * sz + sx * sx
+    fz = [sz, sz * sa, sz * sa * sa, sz * sa * sa * sa, sz * sz - sx * sx, (sz * sz - sx * sx) * sa, se2 * sz]
+    fx = [sx, sx * sa, sx * sa * sa, sx * sa * sa * sa, -2.0 * sz * sx, -2.0 * sz * sx * sa, se2 * sx]
+    dipz = sum(di * f for di, f in zip(d, fz)) * r2 * sr2 / sr3 - (r2 * xmass[0] / sum(xmass) - r2 / 3.0)
+    dipx = sum(di * f for di, f in zip(d, fx)) * r1 / sr2
+    xsin = math.sqrt(1.0 - xcos * xcos)
+    if zembed:
+        return dipz + xcos * dipx if nu == 0 else dipx * xsin
+    return -(dipx + xcos * dipz) if nu == 0 else dipz * xsin
+
+
+def main_dip(ref_root: str) -> None:
+    """``h3p_jacobi_dip.npz``: the example's dipole job (dip.job: NPOT = 80, 8 x 8 levels between
+    the J = 0 odd run and the J = 1 e set of ROTLEV3), the J = 1 job deck that run's vectors came
+    from, and its DIPD evaluated, both components, at
+    every radial grid point pair and at the +-x of DIPOLE3's 80-point Gauss-Legendre rule (the
+    points DIPOLE3 calls it at), with the ket file's masses, g1 and embedding."""
+    ref = Path(ref_root)
+    from oracle import oracle
+
+    c = read_dipole(ref / DIP)
+    deck = (ref / DECK).read_text()
+    d = oracle.parse_deck(deck)
+    q = oracle.quadrature(d, 0)
+    r1, r2 = np.array(q.r1[:q.npnt1]), np.array(q.r2[:q.npnt2])
+    x, _, _, _ = oracle.dipole_quadrature(80)
+    xs = np.concatenate([np.asarray(x), -np.asarray(x)])
+    xmass = list(d.xmass[:3])
+    tab = np.empty((2, len(xs), len(r2), len(r1)))
+    for nu in (0, 1):
+        for ix, xc in enumerate(xs):
+            for i2, b in enumerate(r2):
+                for i1, a in enumerate(r1):
+                    tab[nu, ix, i2, i1] = h3p_dipd(c, a, b, xc, nu, q.g1, xmass, bool(d.zembed))
+    # the J = 1 vectors of the printed dipole run come from the J = 1 job as shipped (both mass
+    # cards 1.0075372, no ZX): its bra energies are that run's ROTLEV3 e set to 1e-8 cm-1, unlike
+    # the printed first-step and ROTLEV3 outputs of the J = 1 example (j1_deck)
+    np.savez_compressed(HERE / "h3p_jacobi_dip.npz", deck=np.array((ref / DIP_JOB).read_text()), table=tab,
+                        r1=r1, r2=r2, xcos=xs, deck_j1=np.array((ref / DECK_J1).read_text()))
+    print(f"dipole table {tab.shape}, |mu| <= {np.abs(tab).max():.4f} a.u.")
+
+
 if __name__ == "__main__":
     root = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
     main(root)
     main_j1(root)
+    main_dip(root)

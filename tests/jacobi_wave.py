@@ -26,9 +26,11 @@ def write_jacobi_wave(path, oracle_mod, deck_text: str, vgrids: dict[int, np.nda
     """Solve every k block of the deck with the oracle (vgrids[k]: the potential on block k's
     grid) and write the file. Returns {k: OracleResult}."""
     d = oracle_mod.parse_deck(deck_text)
-    if d.idia not in (1, 2) or d.jrot <= 0:
-        raise ValueError("a Jacobi deck with J > 0")
-    kd = 0 if d.kmin >= 1 else 1
+    if d.idia not in (1, 2):
+        raise ValueError("a Jacobi deck")
+    # J = 0: one block, z along r2 and KMIN = 0 whatever the deck says (insize :242-246)
+    kmin = d.kmin if d.jrot > 0 else 0
+    kd = 0 if (kmin >= 1 or d.jrot == 0) else 1
     ku = d.jrot
     res, quads = {}, {}
     for k in range(kd, ku + 1):
@@ -41,15 +43,22 @@ def write_jacobi_wave(path, oracle_mod, deck_text: str, vgrids: dict[int, np.nda
     n1, n2 = q0.npnt1, q0.npnt2
     r1, r2 = np.array(q0.r1[:n1]), np.array(q0.r2[:n2])
     idvr = q0.nidvr
-    zembed = bool(d.zembed)
+    zembed = bool(d.zembed) or d.jrot == 0
     with open(path, "wb") as f:
-        nlim = n2 if zembed else n1
-        _rec(f, struct.pack("<9i", d.idia, d.ipar, idvr, n1, n2, d.jrot, d.kmin, d.neval, nlim))
+        nlim = (n2 if zembed else n1) if d.jrot > 0 else 0
+        _rec(f, struct.pack("<9i", d.idia, d.ipar, idvr, n1, n2, d.jrot, kmin, d.neval, nlim))
         _rec(f, struct.pack("<3i", -1 if zembed else 0, -1, -1) + np.array(d.xmass[:3], "<f8").tobytes()
-             + struct.pack("<2d", q0.g1, q0.g2) + struct.pack("<2i", 0, -1))
+             + struct.pack("<2d", q0.g1, q0.g2) + struct.pack("<2i", 0 if d.jrot > 0 else -1, -1))
         _rec(f, np.array([d.re1, d.diss1, d.we1, d.re2, d.diss2, d.we2], "<f8").tobytes())
-        rm2 = 0.5 / (r2 * r2 * q0.urr2) if zembed else 0.5 / (r1 * r1 * q0.urr1)
-        _rec(f, rm2.astype("<f8").tobytes())
+        if d.jrot > 0:  # the r^-2 term of the embedding axis
+            rm2 = 0.5 / (r2 * r2 * q0.urr2) if zembed else 0.5 / (r1 * r1 * q0.urr1)
+            _rec(f, rm2.astype("<f8").tobytes())
+        else:  # one block: its basis size, first l, number of l (:835-840)
+            jdia = max(1, d.idia)
+            jstart = kmin + (1 if kmin % jdia != d.ipar else 0)
+            nang = (res[kd].maxleg - jstart) // jdia + 1
+            mbass = idvr * n1 * n2
+            _rec(f, struct.pack("<4i", mbass, jstart, nang, mbass))
         _rec(f, r1.astype("<f8").tobytes())
         _rec(f, r2.astype("<f8").tobytes())
         for k in range(kd, ku + 1):
