@@ -1,10 +1,11 @@
 """A first-step ZTRAN wavefunction file (unit IWAVE) for Jacobi coordinates written from the
-oracle's own block solves, for testing the second step (ROTLEV3) on the CPU.
+oracle's own block solves, for testing the second step (ROTLEV3) and DIPOLE3 on the CPU.
 
-The records follow the reference's writes for J > 0 with ZROT and ZTRAN
+The records follow the reference's writes with ZTRAN (and ZROT for J > 0)
 (source/dvr3drjz_segmented.f90): the header (:1178-1180: IDIA, IPAR, IDVR, NPNT1, NPNT2, JROT,
 KMIN, NEVAL, NLIM; the logical flags with the masses and g1, g2; the Morse constants), the
-r^-2 term of the embedding axis (:822-833), r1 and r2 (:843-844), then per k block its angular
+r^-2 term of the embedding axis (:822-833; for J = 0 the block's basis size, first l and number
+of l instead, :835-840), r1 and r2 (:843-844), then per k block its angular
 points, (kz, maxleg, nidvr, lincr), the Legendre functions times the DVR weights (:972-976),
 the number of levels, the levels and one amplitude record per level (trans :3733-3841).
 Test infrastructure: nothing in the product imports it.
