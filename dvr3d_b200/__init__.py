@@ -259,6 +259,32 @@ class Context:
                     kmin2=res.kmin2, nblocks=res.nblocks, dev_ms=res.dev_ms, flops=res.flops,
                     text=out.value.decode())
 
+    def ozaki_gemm(self, a, b, *, ta: bool = False, tb: bool = False, tri: int = 0, tri_b: int = 0,
+                   lower_out: bool = False, alpha: float = 1.0, beta: float = 0.0, c=None,
+                   nslice: int = 8) -> np.ndarray:
+        """alpha op(a) op(b) + beta c on the int8 tensor cores from Ozaki slices
+        (dvr3d_b200_ozaki_gemm); nslice = 0 runs the FP64 DMMA GEMM on the same operands."""
+        a = np.asfortranarray(np.asarray(a, dtype=np.float64))
+        b = np.asfortranarray(np.asarray(b, dtype=np.float64))
+        m, k = (a.shape[1], a.shape[0]) if ta else a.shape
+        n = b.shape[0] if tb else b.shape[1]
+        if (b.shape[1] if tb else b.shape[0]) != k:
+            raise ValueError("op(a) is m x k and op(b) must be k x n")
+        if c is None:
+            c = np.zeros((m, n), dtype=np.float64, order="F")
+        c = np.asfortranarray(np.array(c, dtype=np.float64))
+        lda, ldb = a.shape[0], b.shape[0]
+        if lda % 2 or ldb % 2:  # even leading dimensions: pad the stored rows
+            a = np.asfortranarray(np.vstack([a, np.zeros((lda % 2, a.shape[1]))]))
+            b = np.asfortranarray(np.vstack([b, np.zeros((ldb % 2, b.shape[1]))]))
+            lda, ldb = a.shape[0], b.shape[0]
+        dp = C.POINTER(C.c_double)
+        self._check(self._lib.dvr3d_b200_ozaki_gemm(
+            self._h, int(ta), int(tb), int(tri), int(tri_b), int(lower_out), m, n, k, float(alpha),
+            a.ctypes.data_as(dp), lda, b.ctypes.data_as(dp), ldb, float(beta), c.ctypes.data_as(dp), max(m, 1),
+            int(nslice)))
+        return c
+
     def split_gemm(self, a, b, nslice: int = 2) -> np.ndarray:
         """a^T b on the tensor cores from split-BF16 operands (dvr3d_b200_split_gemm):
         a is k x m, b is k x n (FP64); nslice 1 = one BF16 product, 2 = BF16x3."""

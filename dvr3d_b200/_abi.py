@@ -158,6 +158,9 @@ def load_library(path: str | os.PathLike | None = None) -> C.CDLL:
         "dvr3d_b200_split_gemm": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, P(C.c_double), C.c_longlong,
                                             P(C.c_double), C.c_longlong, C.c_int, P(C.c_double),
                                             C.c_longlong]),
+        "dvr3d_b200_ozaki_gemm": (C.c_int, [vp, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                            C.c_int, C.c_double, P(C.c_double), C.c_longlong, P(C.c_double),
+                                            C.c_longlong, C.c_double, P(C.c_double), C.c_longlong, C.c_int]),
         "dvr3d_b200_parse_deck": (C.c_int, [C.c_char_p, P(Deck)]),
         "dvr3d_b200_set_pes": (C.c_int, [vp, C.c_int, P(C.c_double), C.c_int]),
         "dvr3d_b200_set_pes_grid": (C.c_int, [vp, P(C.c_double), C.c_size_t]),

@@ -15,6 +15,7 @@
 #include "rotlev.cuh"
 #include "dipole.cuh"
 #include "tc_gemm.cuh"
+#include "ozaki.cuh"
 
 #define CK(x)                                          \
     do {                                               \
@@ -526,6 +527,68 @@ int dvr3d_b200_split_gemm(dvr3d_ctx *ctx, int m, int n, int k, const double *a, 
         CK(cudaMemcpyAsync(&err_host, err, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaMemcpy2DAsync(c, sizeof(double) * ldc, dc, sizeof(double) * m, sizeof(double) * m, n,
                              cudaMemcpyDeviceToHost, st));
+        CK(cudaStreamSynchronize(st));
+        if (err_host != 0) return fail_ctx(ctx, DVR3D_ERR_NOCONV, "tensor-core pipeline wait timed out");
+        return DVR3D_OK;
+    });
+}
+
+int dvr3d_b200_ozaki_gemm(dvr3d_ctx *ctx, int ta, int tb, int tri, int tri_b, int lower_out, int m, int n, int k,
+                          double alpha, const double *a, long long lda, const double *b, long long ldb, double beta,
+                          double *c, long long ldc, int nslice) {
+    const long long arow = ta ? k : m, acol = ta ? m : k, brow = tb ? n : k, bcol = tb ? k : n;
+    if (!ctx || m < 0 || n < 0 || k < 1 || !a || !b || !c || lda < arow || ldb < brow || ldc < m || (lda & 1) ||
+        (ldb & 1) || tri < 0 || tri > 2 || tri_b < 0 || tri_b > 2 || (lower_out && m != n) ||
+        (nslice != 0 && (nslice < dvr3d::kOzMinSlices || nslice > dvr3d::kOzMaxSlices)))
+        return DVR3D_ERR_ARG;
+    if (m == 0 || n == 0) return DVR3D_OK;
+    dvr3d::GemmOp g;
+    g.M = m;
+    g.N = n;
+    g.K = k;
+    g.alpha = alpha;
+    g.beta = beta;
+    g.ta = ta != 0;
+    g.tb = tb != 0;
+    g.tri = tri;
+    g.tri_b = tri_b;
+    g.lower_out = lower_out != 0;
+    g.lda = lda;
+    g.ldb = ldb;
+    g.ldc = ldc;
+    if (nslice != 0) {
+        g.A = a;  // host pointers stand in for the support check (shapes only)
+        g.B = b;
+        g.C = c;
+        if (!dvr3d::ozaki_supported(g, nslice)) return DVR3D_ERR_ARG;
+    }
+    return guarded(ctx, [&]() -> int {
+        cudaSetDevice(ctx->device);
+        cudaStream_t st = ctx->stream;
+        double *da = ctx->arena.get_t<double>("oz_a", (size_t)lda * acol);
+        double *db = ctx->arena.get_t<double>("oz_b", (size_t)ldb * bcol);
+        double *dc = ctx->arena.get_t<double>("oz_c", (size_t)ldc * n);
+        int *err = ctx->arena.get_t<int>("oz_err", 1);
+        CK(cudaMemcpyAsync(da, a, sizeof(double) * lda * acol, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(db, b, sizeof(double) * ldb * bcol, cudaMemcpyHostToDevice, st));
+        CK(cudaMemcpyAsync(dc, c, sizeof(double) * ldc * n, cudaMemcpyHostToDevice, st));
+        CK(cudaMemsetAsync(err, 0, sizeof(int), st));
+        g.A = da;
+        g.B = db;
+        g.C = dc;
+        if (nslice == 0) {
+            g.splitk = 1;
+            CK(dvr3d::launch_gemm(g, st));
+        } else {
+            const size_t wb = dvr3d::ozaki_work_bytes(g, nslice) + 1024;
+            unsigned char *w = ctx->arena.get_t<unsigned char>("oz_w", wb);
+            const uintptr_t mis = reinterpret_cast<uintptr_t>(w) & 1023u;
+            if (mis) w += 1024 - mis;
+            CK(dvr3d::launch_ozaki_gemm(g, nslice, w, wb - 1024, err, st));
+        }
+        int err_host = 0;
+        CK(cudaMemcpyAsync(&err_host, err, sizeof(int), cudaMemcpyDeviceToHost, st));
+        CK(cudaMemcpyAsync(c, dc, sizeof(double) * ldc * n, cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         if (err_host != 0) return fail_ctx(ctx, DVR3D_ERR_NOCONV, "tensor-core pipeline wait timed out");
         return DVR3D_OK;

@@ -11,11 +11,13 @@
 // needed by the shift-invert solver). Leaves (<= 64) are factored and inverted by one CTA in
 // shared memory. Work: n^3/3 (factorisation) + n^3/3 (inverse) flop, the top levels as a few
 // large GEMMs instead of one thin GEMM per 64-column panel.
+#include <algorithm>
 #include <cmath>
 
 #include "chol.cuh"
 #include "common.cuh"
 #include "gemm64.cuh"
+#include "ozaki.cuh"
 
 namespace dvr3d {
 
@@ -262,8 +264,14 @@ struct Rec {
     double *work;      // split-K scratch
     int *err;
     cudaStream_t st;
+    CholOzaki oz;      // int8-sliced products for the large GEMMs (oz.work null: DMMA only)
 
     cudaError_t gemm(GemmOp g) {
+        if (oz.work && ozaki_profitable(g) && ozaki_supported(g, oz.nslice) &&
+            ozaki_work_bytes(g, oz.nslice) <= oz.bytes) {
+            ++oz.launches;
+            return launch_ozaki_gemm(g, oz.nslice, oz.work, oz.bytes, err, st);
+        }
         g.splitk = split_of(g.M, g.N, g.K, g.lower_out != 0);
         g.work = work;
         return launch_gemm(g, st);
@@ -350,9 +358,34 @@ size_t stack_need(int n) {
     return std::max(stack_need(n1), mine + stack_need(n2));
 }
 
+// Largest Ozaki workspace any product of the recursion asks for (shapes as in Rec::run).
+size_t oz_need(int n, int nslice) {
+    if (n <= NB) return 0;
+    int n1 = ((n / 2 + NB - 1) / NB) * NB;
+    if (n1 >= n) n1 = n - NB;
+    const int n2 = n - n1;
+    static const double dummy[2] = {0.0, 0.0};
+    size_t m = 0;
+    const int shapes[4][4] = {{n2, n1, n1, 0}, {n2, n2, n1, 1}, {n2, n1, n2, 0}, {n2, n1, n1, 0}};
+    for (const auto &sh : shapes) {
+        GemmOp g;
+        g.M = sh[0];
+        g.N = sh[1];
+        g.K = sh[2];
+        g.lower_out = sh[3];
+        g.A = dummy;
+        g.B = dummy + 1;
+        g.C = const_cast<double *>(dummy);
+        if (ozaki_profitable(g) && ozaki_supported(g, nslice)) m = std::max(m, ozaki_work_bytes(g, nslice));
+    }
+    return std::max({m, oz_need(n1, nslice), oz_need(n2, nslice)});
+}
+
 }  // namespace
 
 size_t chol_work_doubles(int n) { return stack_need(n) + kSplitWork + 64; }
+
+size_t chol_ozaki_work_bytes(int n, int nslice) { return oz_need(n, nslice); }
 
 cudaError_t launch_shift_copy_lower(const double *H, long long ldh, int n, double sigma, double *A, long long lda,
                                     cudaStream_t st) {
@@ -362,11 +395,14 @@ cudaError_t launch_shift_copy_lower(const double *H, long long ldh, int n, doubl
     return cudaGetLastError();
 }
 
-cudaError_t launch_potrf_inv_lower(double *A, long long lda, int n, double *work, int *err, cudaStream_t st) {
+cudaError_t launch_potrf_inv_lower(double *A, long long lda, int n, double *work, int *err, cudaStream_t st,
+                                   CholOzaki *oz) {
     if (n <= 0) return cudaSuccess;
     if (lda & 1) return cudaErrorInvalidValue;
-    Rec r{A, lda, work + kSplitWork + 64, work, err, st};
-    return r.run(0, n, r.stack);
+    Rec r{A, lda, work + kSplitWork + 64, work, err, st, oz ? *oz : CholOzaki{}};
+    const cudaError_t e = r.run(0, n, r.stack);
+    if (oz) oz->launches = r.oz.launches;
+    return e;
 }
 
 cudaError_t launch_chol_small(double *G, int b, double *ginv, double rel_tol, int *err, cudaStream_t st) {

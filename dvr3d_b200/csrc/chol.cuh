@@ -17,7 +17,18 @@ cudaError_t launch_shift_copy_lower(const double *H, long long ldh, int n, doubl
 // doubles. A pivot that is not positive sets *err = kDevNotPosDef; the remaining kernels of
 // the factorisation then return at once and the host reads the flag.
 size_t chol_work_doubles(int n);
-cudaError_t launch_potrf_inv_lower(double *A, long long lda, int n, double *work, int *err, cudaStream_t st);
+// Products of the recursion large enough for it (ozaki_profitable) may run as FP64-accurate
+// int8-sliced tensor-core GEMMs (ozaki.cu) with nslice slices in the given workspace
+// (chol_ozaki_work_bytes(n, nslice) bytes, 1 KB aligned); launches counts them.
+struct CholOzaki {
+    void *work = nullptr;
+    size_t bytes = 0;
+    int nslice = 8;
+    int launches = 0;
+};
+size_t chol_ozaki_work_bytes(int n, int nslice);
+cudaError_t launch_potrf_inv_lower(double *A, long long lda, int n, double *work, int *err, cudaStream_t st,
+                                   CholOzaki *oz = nullptr);
 
 // Cholesky of one small SPD matrix G (b x b <= 64, ld b, lower read), in place, and the
 // inverse of its factor into ginv (ld 64). A pivot <= rel_tol * max diag(G) (or not finite)

@@ -30,6 +30,7 @@
 
 #include "band_eig.cuh"
 #include "chol.cuh"
+#include "ozaki.cuh"
 #include "common.cuh"
 #include "gemm64.cuh"
 #include "pipeline.cuh"
@@ -247,15 +248,35 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
     // ---- (1)+(2) shift, factor, invert
     tf.start(st);
     double sigma = emin_bound - std::max(1.0e-6, 1.0e-3 * std::fabs(emin_bound));
+    // the large products of the factorisation on the int8 tensor cores (Ozaki slices, FP64
+    // accuracy); DVR3D_OZAKI=0 keeps every product on the DMMA path, DVR3D_OZAKI_SLICES sets
+    // the slice count (4..8)
+    CholOzaki oz;
+    {
+        const char *oe = std::getenv("DVR3D_OZAKI");
+        const char *se = std::getenv("DVR3D_OZAKI_SLICES");
+        if (se) oz.nslice = std::max(kOzMinSlices, std::min(kOzMaxSlices, std::atoi(se)));
+        const size_t ob = (oe && oe[0] == '0') ? 0 : chol_ozaki_work_bytes(N, oz.nslice);
+        if (ob > 0) {
+            oz.work = ctx->arena.get_t<unsigned char>("si_oz", ob + 1024);
+            oz.bytes = ob + 1024;
+            const uintptr_t mis = reinterpret_cast<uintptr_t>(oz.work) & 1023u;
+            if (mis) {  // 1 KB alignment for the slice buffers
+                oz.work = static_cast<unsigned char *>(oz.work) + (1024 - mis);
+                oz.bytes -= 1024 - mis;
+            }
+        }
+    }
     bool spd = false;
     for (int attempt = 0; attempt < 4 && !spd; ++attempt) {
         CK(launch_shift_copy_lower(H3, ldh, N, sigma, Lb, ldw, st));
         CK(cudaMemsetAsync(err, 0, 2 * sizeof(int), st));
-        CK(launch_potrf_inv_lower(Lb, ldw, N, work, err, st));
+        CK(launch_potrf_inv_lower(Lb, ldw, N, work, err, st, &oz));
         int e = 0;
         CK(cudaMemcpyAsync(&e, err, sizeof(int), cudaMemcpyDeviceToHost, st));
         CK(cudaStreamSynchronize(st));
         note_d2h(sizeof(int));
+        if (e == kDevBarrierTimeout) return false;  // a tensor-core pipeline wait ran out
         if (e == 0) spd = true;
         else {
             ++ks.retries;
@@ -563,6 +584,9 @@ bool si_krylov_solve(dvr3d_ctx *ctx, const double *H3, long long ldh, int N, dou
         next = std::min(s + inc, mmax / b);
     }
     ks.factor_ms = tf.ms();
+    if (trace)
+        std::fprintf(stderr, "si_krylov: factorisation %.2f ms, %d products on the int8 tensor cores (%d slices)\n",
+                     ks.factor_ms, oz.launches, oz.nslice);
     ks.krylov_ms = tk_ms;
     ks.rr_ms = tr_ms;
     ks.gemm_ms = log_gemms ? gemm_launch_log_ms(glog) : 0.0;

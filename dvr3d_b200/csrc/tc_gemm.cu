@@ -22,10 +22,10 @@
 
 #include <cstdint>
 #include <cstring>
-#include <mutex>
 
 #include "common.cuh"
 #include "tc_gemm.cuh"
+#include "tcgen05.cuh"
 
 namespace dvr3d {
 
@@ -69,52 +69,15 @@ struct TcArgs {
     unsigned long long wait_ns;
 };
 
-__device__ __forceinline__ uint32_t smem_u32(const void *p) {
-    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
-}
-
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count));
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
-    uint32_t ok;
-    asm volatile(
-        "{\n\t.reg .pred p;\n\t"
-        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-        "selp.u32 %0, 1, 0, p;\n\t}"
-        : "=r"(ok)
-        : "r"(bar), "r"(parity)
-        : "memory");
-    return ok != 0;
-}
-
-// Wait for the phase of the given parity to complete; false once the deadline has passed.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, unsigned long long t_end) {
-    unsigned int n = 0;
-    while (!mbar_try_wait(bar, parity)) {
-        if ((++n & 63u) == 0 && global_ns() > t_end) return false;
-    }
-    return true;
-}
-
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap *map, uint32_t bar, int x, int y) {
-    asm volatile(
-        "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];" ::
-            "r"(dst),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
-        : "memory");
-}
+using tc::fence_after;
+using tc::fence_before;
+using tc::global_ns;
+using tc::mbar_expect_tx;
+using tc::mbar_init;
+using tc::mbar_wait;
+using tc::smem_u32;
+using tc::tma_load_2d;
+using tc::umma_commit;
 
 // Shared-memory matrix descriptor of a K-major tile written by TMA with the 128-byte swizzle:
 // rows of 128 bytes, 8-row groups 1024 bytes apart (stride byte offset), version 1, layout
@@ -133,26 +96,10 @@ __device__ __forceinline__ void umma_bf16(uint32_t tmem_d, uint64_t da, uint64_t
         "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(z), "r"(z), "r"(z), "r"(z));
 }
 
-__device__ __forceinline__ void umma_commit(uint32_t bar) {
-    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
-__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
-
 // 32 consecutive FP32 columns of this thread's tensor-memory lane.
 __device__ __forceinline__ void tmem_ld32(uint32_t taddr, float (&v)[32]) {
     uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-        "{%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15, "
-        "%16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+    tc::tmem_ld32(taddr, r);
 #pragma unroll
     for (int j = 0; j < 32; ++j) v[j] = __uint_as_float(r[j]);
 }
@@ -205,9 +152,9 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                      "r"((uint32_t)BN));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    tc_fence_before();
+    fence_before();
     __syncthreads();
-    tc_fence_after();
+    fence_after();
     const uint32_t tmem = tmem_slot;
 
     const int nk = (p.K + kBK - 1) / kBK;
@@ -254,7 +201,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
                 ok = false;
                 break;
             }
-            tc_fence_after();
+            fence_after();
             const uint32_t sa = ring + (uint32_t)(s * Cfg::kStage), sb = sa + 2u * Cfg::kA;
             for (int t = 0; t < nterm; ++t) {
                 // terms: A_hi B_hi, A_hi B_lo, A_lo B_hi
@@ -277,7 +224,7 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
 
     // ---- epilogue: tensor memory -> FP64
     const bool got = mbar_wait(done, 0u, t_end + wait_ns);
-    tc_fence_after();
+    fence_after();
     const bool warp_ok = __all_sync(0xffffffffu, got && *(volatile int *)&s_abort == 0);
     if (!got && lane == 0 && p.err) atomicExch(p.err, (int)kDevBarrierTimeout);
     if (warp_ok) {
@@ -319,10 +266,10 @@ __global__ void __launch_bounds__(kThreads, 1) tc_gemm_kernel(const __grid_const
             }
         }
     }
-    tc_fence_before();
+    fence_before();
     __syncthreads();
     if (warp == 0) {
-        tc_fence_after();
+        fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)BN));
     }
 }
@@ -349,23 +296,8 @@ __global__ void split_sum_kernel(const __nv_bfloat16 *__restrict__ hi, const __n
         }
 }
 
-// cuTensorMapEncodeTiled through the runtime's driver entry point (no link against libcuda).
-typedef CUresult (*EncodeTiledFn)(CUtensorMap *, CUtensorMapDataType, cuuint32_t, void *, const cuuint64_t *,
-                                  const cuuint64_t *, const cuuint32_t *, const cuuint32_t *, CUtensorMapInterleave,
-                                  CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
-
-EncodeTiledFn encode_tiled() {
-    static EncodeTiledFn fn = nullptr;
-    static std::once_flag once;
-    std::call_once(once, [] {
-        void *f = nullptr;
-        cudaDriverEntryPointQueryResult q{};
-        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
-            q == cudaDriverEntryPointSuccess)
-            fn = reinterpret_cast<EncodeTiledFn>(f);
-    });
-    return fn;
-}
+using tc::EncodeTiledFn;
+using tc::encode_tiled;
 
 // Row-major rows x K BF16 matrix (row stride ld elements), boxes of 64 K-elements x box_rows.
 bool make_map(EncodeTiledFn fn, CUtensorMap &m, const __nv_bfloat16 *ptr, int rows, int K, long long ld,

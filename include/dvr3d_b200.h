@@ -296,6 +296,22 @@ int dvr3d_b200_dipole3(dvr3d_ctx *ctx, const char *deck_text, const char *ket_pa
 int dvr3d_b200_split_gemm(dvr3d_ctx *ctx, int m, int n, int k, const double *a, long long lda, const double *b,
                           long long ldb, int nslice, double *c, long long ldc);
 
+/* An FP64 GEMM on the int8 tensor cores (Ozaki scheme), on host buffers, as the shift-invert
+ * solve uses it for the large products of its Cholesky-inverse:
+ *     c (m x n, ldc) = alpha op(a) op(b) + beta c,   column-major FP64,
+ *     op(a) = ta ? a^T (a: k x m, lda) : a (m x k, lda);  op(b) = tb ? b^T (b: n x k) : b (k x n);
+ *     tri = 1 / 2: op(a) lower / upper triangular; tri_b = 1 / 2: op(b) lower / upper
+ *     (ignored outside the triangle; the DMMA path, nslice = 0, needs zeros there);
+ *     lower_out: m == n, only c(i, j), i >= j.
+ * Each row of op(a) and column of op(b) is scaled by a power of two and cut into nslice
+ * (4..8) signed 7-bit slices; the slice products are exact int32 sums (k <= 16384) combined in
+ * FP64: with 8 slices the error per term is below 2^-49 max|op(a)(i,:)| max|op(b)(:,j)|.
+ * nslice = 0 runs the same product on the FP64 DMMA path instead (for comparisons).
+ * No counterpart in the reference (its products are LAPACK / BLAS calls). lda, ldb even. */
+int dvr3d_b200_ozaki_gemm(dvr3d_ctx *ctx, int ta, int tb, int tri, int tri_b, int lower_out, int m, int n, int k,
+                          double alpha, const double *a, long long lda, const double *b, long long ldb, double beta,
+                          double *c, long long ldc, int nslice);
+
 /* Reads a job deck in the reference's stdin format: namelist PRT (dvr3d :65, defaults of
  * block data :158-167), card 2 (insize :232), card 3 (:238), title (:372) and the setcon
  * cards (:1042-1095, in the source's order FIXCOS, XMASS, XMASSR, EMAX1/EMAX2, r1 Morse,
