@@ -431,6 +431,10 @@ def main() -> int:
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--profile-solve", action="store_true",
                     help="one solve of the workload and nothing else (for ncu captures of its kernels)")
+    ap.add_argument("--profile-ozaki", action="store_true",
+                    help="one int8-sliced FP64 product of the top-level Cholesky-inverse shape at the "
+                         "workload's size (6058 x 6144 x 6144, triangular transposed second operand) and "
+                         "nothing else (for ncu captures of oz_gemm_kernel)")
     ap.add_argument("--workload", default="cfg4", choices=["cfg4", "batch64", "dipole"],
                     help="cfg4: the headline solve; batch64: 64 independent Radau problems per step; "
                          "dipole: DIPOLE3 transition moments J=2 e<->f")
@@ -458,6 +462,19 @@ def main() -> int:
         r = ctx.solve(parse_deck(w.deck), 0, precision=prec, nlevels=args.levels)
         print(json.dumps({"profile_solve": WORKLOAD, "nham3": r.nham3, "stage_ms": list(r.stage_ms)}), flush=True)
         ctx.close()
+        return 0
+    if args.profile_ozaki:
+        # L21 = A21 inv(L11)^T of the first split of the N = 12202 factorisation (n1 = 6144,
+        # n2 = 6058): A21 dense, inv(L11) lower triangular, through dvr3d_b200_ozaki_gemm
+        import dvr3d_b200
+
+        rng = np.random.default_rng(1)
+        n1, n2 = 6144, 6058
+        a21 = np.asfortranarray(rng.standard_normal((n2, n1)))
+        l11 = np.asfortranarray(np.tril(rng.standard_normal((n1, n1))))
+        with dvr3d_b200.Context(0) as ctx:
+            c = ctx.ozaki_gemm(a21, l11, tb=True, tri_b=2)
+        print(json.dumps({"profile_ozaki": [n2, n1, n1], "checksum": float(np.abs(c).sum())}), flush=True)
         return 0
     if args.impl == "reference":
         return run_reference(args, rank, world)

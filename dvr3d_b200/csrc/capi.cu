@@ -580,11 +580,13 @@ int dvr3d_b200_ozaki_gemm(dvr3d_ctx *ctx, int ta, int tb, int tri, int tri_b, in
             g.splitk = 1;
             CK(dvr3d::launch_gemm(g, st));
         } else {
-            const size_t wb = dvr3d::ozaki_work_bytes(g, nslice) + 1024;
+            // thin products with few row tiles split K into chunks, as the Krylov steps do
+            const int kchunk = (n <= 32 && !lower_out && (m + 127) / 128 < 148) ? dvr3d::kOzKrylovChunk : 0;
+            const size_t wb = dvr3d::ozaki_work_bytes(g, nslice, false, kchunk) + 1024;
             unsigned char *w = ctx->arena.get_t<unsigned char>("oz_w", wb);
             const uintptr_t mis = reinterpret_cast<uintptr_t>(w) & 1023u;
             if (mis) w += 1024 - mis;
-            CK(dvr3d::launch_ozaki_gemm(g, nslice, w, wb - 1024, err, st));
+            CK(dvr3d::launch_ozaki_gemm(g, nslice, w, wb - 1024, err, st, nullptr, kchunk));
         }
         int err_host = 0;
         CK(cudaMemcpyAsync(&err_host, err, sizeof(int), cudaMemcpyDeviceToHost, st));

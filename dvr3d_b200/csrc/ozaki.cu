@@ -40,23 +40,24 @@ namespace dvr3d {
 namespace {
 
 constexpr int kBM = 128;       // tile rows = UMMA M = tensor-memory lanes
-constexpr int kBN = 64;        // tile columns = UMMA N = tensor-memory columns per accumulator
 constexpr int kBK = 64;        // K bytes (= int8 elements) per stage: one 64-byte swizzle row
 constexpr int kUK = 32;        // K of one kind::i8 MMA
 constexpr int kThreads = 128;  // 4 warps
-constexpr int kTmemCols = 512;
 constexpr unsigned long long kDefaultWaitNs = 4000000000ull;
 constexpr unsigned long long kNanBits = 0x7ff8000000000000ull;
 
-template <int S>
+// BN = tile columns = UMMA N = tensor-memory columns of one accumulator (64, or 32 for the
+// thin right-hand sides of the Krylov steps)
+template <int S, int BN>
 struct OzCfg {
     static constexpr int kA = kBM * kBK;  // bytes of one A slice tile (8 KB)
-    static constexpr int kB = kBN * kBK;  // bytes of one B slice tile (4 KB)
+    static constexpr int kB = BN * kBK;   // bytes of one B slice tile
     static constexpr int kStage = S * (kA + kB);
     static constexpr int kStages = (200 * 1024) / kStage;
     static constexpr int kSmem = kStages * kStage + 1024;  // + slack to align the ring to 1 KB
+    static constexpr int kCols = S * BN <= 32 ? 32 : (S * BN <= 64 ? 64 : (S * BN <= 128 ? 128 : (S * BN <= 256 ? 256 : 512)));
     static_assert(kStages >= 2, "at least double buffering");
-    static_assert(S * kBN <= kTmemCols, "one accumulator of 64 columns per weight group");
+    static_assert(S * BN <= 512, "one accumulator of BN columns per weight group");
 };
 
 struct OzMaps {
@@ -67,6 +68,8 @@ struct OzMaps {
 struct OzArgs {
     int M, N, K;
     int tri, tri_b, lower_out;
+    int kchunk;    // > 0: CTA z sums K range [z kchunk, (z + 1) kchunk) into part (no alpha, beta)
+    double *part;  // chunk z, element (i, j) at part[z M N + j M + i]
     double alpha, beta;
     double *C;
     long long ldc;
@@ -191,19 +194,32 @@ __device__ __forceinline__ int scale_exp(unsigned long long bits, bool &bad) {
     return e;
 }
 
-template <int S>
+template <int S, int BN>
 __global__ void __launch_bounds__(kThreads, 1) oz_gemm_kernel(const __grid_constant__ OzMaps maps, const OzArgs p) {
-    using Cfg = OzCfg<S>;
+    using Cfg = OzCfg<S, BN>;
     extern __shared__ __align__(1024) unsigned char oz_smem[];
     __shared__ __align__(8) unsigned long long bar_full[Cfg::kStages];
     __shared__ __align__(8) unsigned long long bar_empty[Cfg::kStages];
     __shared__ __align__(8) unsigned long long bar_done;
     __shared__ uint32_t tmem_slot;
     __shared__ int s_abort;
-    __shared__ int s_cexp[kBN];
-    __shared__ int s_cbad[kBN];
+    __shared__ int s_cexp[BN];
+    __shared__ int s_cbad[BN];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
+    // grouped launch order: consecutive CTAs walk 16 row tiles of one column tile, then the
+    // next column tile, so that a wave of CTAs shares a compact block of operand rows in L2
+    // (row-tile-fastest order made every wave read all of op(A)'s slices from HBM)
+    int ti, tj;
+    {
+        constexpr int G = 16;
+        const int tm = (int)gridDim.x, tn = (int)gridDim.y;
+        const long long t = (long long)blockIdx.y * tm + blockIdx.x, per = (long long)G * tn;
+        const int g = (int)(t / per), first = g * G, gm = min(G, tm - first);
+        const int r = (int)(t - (long long)g * per);
+        ti = first + r % gm;
+        tj = r / gm;
+    }
+    const int m0 = ti * kBM, n0 = tj * BN;
     if (p.lower_out && n0 > m0 + kBM - 1) return;  // tile strictly above the diagonal (uniform)
     const unsigned long long wait_ns = p.wait_ns;
     const unsigned long long t_end = tc::global_ns() + wait_ns;
@@ -213,9 +229,22 @@ __global__ void __launch_bounds__(kThreads, 1) oz_gemm_kernel(const __grid_const
     if (p.tri == 1) ke = min(ke, m0 + kBM);
     if (p.tri == 2) kb = max(kb, m0);
     if (p.tri_b == 1) kb = max(kb, n0);
-    if (p.tri_b == 2) ke = min(ke, n0 + kBN);
+    if (p.tri_b == 2) ke = min(ke, n0 + BN);
+    double *part = nullptr;
+    if (p.kchunk > 0) {
+        kb = max(kb, (int)blockIdx.z * p.kchunk);
+        ke = min(ke, ((int)blockIdx.z + 1) * p.kchunk);
+        part = p.part + (long long)blockIdx.z * p.M * p.N;
+    }
     kb &= ~(kBK - 1);
     const int nk = ke > kb ? (ke - kb + kBK - 1) / kBK : 0;
+    if (part && nk == 0) {  // an empty chunk of this tile: its partial sum is zero (uniform)
+        for (int q = threadIdx.x; q < kBM * BN; q += kThreads) {
+            const int i = m0 + (q % kBM), j = n0 + q / kBM;
+            if (i < p.M && j < p.N) part[(long long)j * p.M + i] = 0.0;
+        }
+        return;
+    }
 
     const uint32_t ring = (tc::smem_u32(oz_smem) + 1023u) & ~1023u;
     const uint32_t full0 = tc::smem_u32(&bar_full[0]), empty0 = tc::smem_u32(&bar_empty[0]);
@@ -229,7 +258,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_gemm_kernel(const __grid_const
         s_abort = 0;
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    if (threadIdx.x < kBN) {
+    if (threadIdx.x < BN) {
         const int c = n0 + threadIdx.x;
         bool bad = false;
         s_cexp[threadIdx.x] = c < p.N ? scale_exp(p.umax_b[c], bad) : 0;
@@ -238,7 +267,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_gemm_kernel(const __grid_const
     if (warp == 0) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(
                          tc::smem_u32(&tmem_slot)),
-                     "r"((uint32_t)kTmemCols));
+                     "r"((uint32_t)Cfg::kCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
     tc::fence_before();
@@ -277,7 +306,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_gemm_kernel(const __grid_const
         // ---- MMA issuer: pairs (i, j), i + j <= S - 1 (0-based), into accumulator i + j
         const uint32_t idesc = (2u << 4)                          // D: S32
                                | (1u << 7) | (1u << 10)            // A, B: signed 8-bit
-                               | ((uint32_t)(kBN >> 3) << 17)      // N
+                               | ((uint32_t)(BN >> 3) << 17)       // N
                                | ((uint32_t)(kBM >> 4) << 24);     // M
         bool ok = true;
         for (int it = 0; it < nk; ++it) {
@@ -295,7 +324,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_gemm_kernel(const __grid_const
 #pragma unroll
                 for (int j = 0; j + i < S; ++j) {
                     const uint64_t db = sw64_desc(sb + (uint32_t)(j * Cfg::kB));
-                    const uint32_t dst = tmem + (uint32_t)((i + j) * kBN);
+                    const uint32_t dst = tmem + (uint32_t)((i + j) * BN);
 #pragma unroll
                     for (int kk = 0; kk < kBK / kUK; ++kk)  // the first product of a group starts it
                         umma_i8(dst, da + (uint64_t)(2 * kk), db + (uint64_t)(2 * kk), idesc,
@@ -323,7 +352,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_gemm_kernel(const __grid_const
         const int er = row < p.M ? scale_exp(p.umax_a[row], rbad) : 0;
         const uint32_t lane_base = (uint32_t)(warp * 32) << 16;
 #pragma unroll 1
-        for (int c0 = 0; c0 < kBN; c0 += 32) {
+        for (int c0 = 0; c0 < BN; c0 += 32) {
             if (n0 + c0 >= p.N) break;  // uniform over the warp
             double t[32];
 #pragma unroll
@@ -332,7 +361,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_gemm_kernel(const __grid_const
 #pragma unroll 1
                 for (int q = S - 1; q >= 0; --q) {  // t = sum_q acc_q 128^-q (Horner, smallest first)
                     uint32_t r[32];
-                    tc::tmem_ld32(tmem + lane_base + (uint32_t)(q * kBN + c0), r);
+                    tc::tmem_ld32(tmem + lane_base + (uint32_t)(q * BN + c0), r);
 #pragma unroll
                     for (int j = 0; j < 32; ++j) t[j] = (double)(int)r[j] + t[j] * 0.0078125;
                 }
@@ -344,6 +373,10 @@ __global__ void __launch_bounds__(kThreads, 1) oz_gemm_kernel(const __grid_const
                 if (col >= p.N || (p.lower_out && col > row)) continue;
                 double val = ldexp(t[j], er + s_cexp[c0 + j] - 14);
                 if (rbad || s_cbad[c0 + j]) val = __longlong_as_double((long long)kNanBits);
+                if (part) {
+                    part[(long long)col * p.M + row] = val;
+                    continue;
+                }
                 double *pc = p.C + (long long)col * p.ldc + row;
                 double out = p.alpha * val;
                 if (p.beta != 0.0) out += p.beta * *pc;
@@ -355,7 +388,7 @@ __global__ void __launch_bounds__(kThreads, 1) oz_gemm_kernel(const __grid_const
     __syncthreads();
     if (warp == 0) {
         tc::fence_after();
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)kTmemCols));
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((uint32_t)Cfg::kCols));
     }
 }
 
@@ -369,46 +402,104 @@ bool make_map(tc::EncodeTiledFn fn, CUtensorMap &m, const signed char *ptr, int 
               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-template <int S>
-cudaError_t launch_cfg(const OzMaps &maps, const OzArgs &a, dim3 grid, cudaStream_t st) {
-    using Cfg = OzCfg<S>;
+// The kernel's shared-memory opt-in, once per device (kept outside stream capture by callers
+// that capture: ozaki_set_attributes).
+template <int S, int BN>
+cudaError_t set_attr() {
     static bool attr_done[kMaxAttrDevices] = {};
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return e;
     if (dev >= kMaxAttrDevices || !attr_done[dev]) {
-        e = cudaFuncSetAttribute(oz_gemm_kernel<S>, cudaFuncAttributeMaxDynamicSharedMemorySize, Cfg::kSmem);
+        e = cudaFuncSetAttribute(oz_gemm_kernel<S, BN>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 OzCfg<S, BN>::kSmem);
         if (e != cudaSuccess) return e;
         if (dev < kMaxAttrDevices) attr_done[dev] = true;
     }
+    return cudaSuccess;
+}
+
+template <int S, int BN>
+cudaError_t launch_cfg(const OzMaps &maps, const OzArgs &a, dim3 grid, cudaStream_t st) {
+    cudaError_t e = set_attr<S, BN>();
+    if (e != cudaSuccess) return e;
     DVR3D_COUNT_LAUNCH(1);
-    oz_gemm_kernel<S><<<grid, kThreads, Cfg::kSmem, st>>>(maps, a);
+    oz_gemm_kernel<S, BN><<<grid, kThreads, OzCfg<S, BN>::kSmem, st>>>(maps, a);
     return cudaGetLastError();
+}
+
+template <int BN>
+cudaError_t launch_bn(int nslice, const OzMaps &maps, const OzArgs &a, dim3 grid, cudaStream_t st) {
+    switch (nslice) {
+        case 4: return launch_cfg<4, BN>(maps, a, grid, st);
+        case 5: return launch_cfg<5, BN>(maps, a, grid, st);
+        case 6: return launch_cfg<6, BN>(maps, a, grid, st);
+        case 7: return launch_cfg<7, BN>(maps, a, grid, st);
+        default: return launch_cfg<8, BN>(maps, a, grid, st);
+    }
+}
+
+template <int BN>
+cudaError_t set_attr_bn(int nslice) {
+    switch (nslice) {
+        case 4: return set_attr<4, BN>();
+        case 5: return set_attr<5, BN>();
+        case 6: return set_attr<6, BN>();
+        case 7: return set_attr<7, BN>();
+        default: return set_attr<8, BN>();
+    }
+}
+
+// C = alpha sum_z part[z] + beta C, the chunks summed in a fixed order (deterministic).
+__global__ void oz_reduce_kernel(const double *__restrict__ part, int nchunk, int M, int N, double alpha,
+                                 double beta, double *C, long long ldc) {
+    const long long tot = (long long)M * N, stride = (long long)gridDim.x * blockDim.x;
+    for (long long t = (long long)blockIdx.x * blockDim.x + threadIdx.x; t < tot; t += stride) {
+        double v = 0.0;
+        for (int z = 0; z < nchunk; ++z) v += part[(long long)z * tot + t];
+        const int j = (int)(t / M), i = (int)(t % M);
+        double *pc = C + (long long)j * ldc + i;
+        *pc = beta != 0.0 ? alpha * v + beta * *pc : alpha * v;
+    }
 }
 
 long long rup(long long a, long long b) { return (a + b - 1) / b * b; }
 
+int tile_n_of(const GemmOp &p) { return p.N <= 32 && !p.lower_out ? 32 : 64; }
+
 struct Layout {
     int Kp;
     bool shared;  // op(B)'s rows are op(A)'s rows (A A^T): one set of slices
-    size_t umax_a, umax_b, sa, sb, total;
+    bool pre;     // op(A) sliced beforehand (OzPresliced): no A slices here
+    int nchunk;
+    size_t umax_a, umax_b, sa, sb, part, total;
 };
 
-Layout layout_of(const GemmOp &p, int nslice) {
+Layout layout_of(const GemmOp &p, int nslice, bool pre, int kchunk) {
     Layout L{};
     L.Kp = (int)rup(std::max(p.K, 1), kBK);
-    L.shared = p.A == p.B && p.lda == p.ldb && p.ta != p.tb && p.tri == 0 && p.tri_b == 0 && p.M == p.N;
+    L.pre = pre;
+    L.shared = !pre && p.A == p.B && p.lda == p.ldb && p.ta != p.tb && p.tri == 0 && p.tri_b == 0 && p.M == p.N;
+    L.nchunk = kchunk > 0 ? (p.K + kchunk - 1) / kchunk : 0;
     size_t off = 0;
     L.umax_a = off;
-    off = (size_t)rup(off + 8 * (size_t)p.M, 1024);
+    if (!pre) off = (size_t)rup(off + 8 * (size_t)p.M, 1024);
     L.umax_b = off;
     off = (size_t)rup(off + 8 * (size_t)p.N, 1024);
     L.sa = off;
-    off = (size_t)rup(off + (size_t)nslice * p.M * L.Kp, 1024);
+    if (!pre) off = (size_t)rup(off + (size_t)nslice * p.M * L.Kp, 1024);
     L.sb = L.shared ? L.sa : off;
     if (!L.shared) off = (size_t)rup(off + (size_t)nslice * p.N * L.Kp, 1024);
+    L.part = off;
+    off = (size_t)rup(off + 8 * (size_t)L.nchunk * p.M * p.N, 1024);
     L.total = off;
     return L;
+}
+
+OzOperand a_operand(const GemmOp &p, int Kp, unsigned long long *umax, signed char *S) {
+    // op(A)(i, k) = ta ? A[i lda + k] : A[k lda + i]; rows of the A side are i
+    return OzOperand{p.A, p.ta ? p.lda : 1, p.ta ? 1 : p.lda, p.M, p.K, Kp, p.tri == 1 ? 1 : (p.tri == 2 ? 2 : 0),
+                     umax, S, (long long)p.M * Kp};
 }
 
 cudaError_t slice_operand(const OzOperand &o, int nslice, cudaStream_t st) {
@@ -430,8 +521,7 @@ bool ozaki_supported(const GemmOp &p, int nslice) {
     if (p.M <= 0 || p.N <= 0 || p.K <= 0 || p.K > kOzMaxK) return false;
     if (p.lower_out && p.M != p.N) return false;
     if (!p.A || !p.B || !p.C || p.tri < 0 || p.tri > 2 || p.tri_b < 0 || p.tri_b > 2) return false;
-    if ((long long)(p.M + kBM - 1) / kBM > 0x7fffffffLL || (p.N + kBN - 1) / kBN > 65535) return false;
-    if ((p.M + 63) / 64 > 65535 || (p.N + 63) / 64 > 65535) return false;
+    if ((p.M + 63) / 64 > 65535 || (p.N + 31) / 32 > 65535) return false;
     return true;
 }
 
@@ -441,41 +531,75 @@ bool ozaki_profitable(const GemmOp &p) {
     return p.M >= 1536 && p.N >= 1536 && p.K >= 1024;
 }
 
-size_t ozaki_work_bytes(const GemmOp &p, int nslice) { return layout_of(p, nslice).total; }
+size_t ozaki_work_bytes(const GemmOp &p, int nslice, bool presliced_a, int kchunk) {
+    return layout_of(p, nslice, presliced_a, kchunk).total;
+}
+
+size_t ozaki_preslice_bytes(const GemmOp &p, int nslice) {
+    return (size_t)rup(8 * (size_t)p.M, 1024) + (size_t)nslice * p.M * rup(std::max(p.K, 1), kBK);
+}
+
+cudaError_t ozaki_preslice_a(const GemmOp &p, int nslice, void *buf, size_t bytes, OzPresliced &out,
+                             cudaStream_t st) {
+    if (!ozaki_supported(p, nslice)) return cudaErrorInvalidValue;
+    if (!buf || bytes < ozaki_preslice_bytes(p, nslice) || (reinterpret_cast<uintptr_t>(buf) & 1023u))
+        return cudaErrorInvalidValue;
+    const int Kp = (int)rup(p.K, kBK);
+    unsigned char *w = static_cast<unsigned char *>(buf);
+    auto *umax = reinterpret_cast<unsigned long long *>(w);
+    auto *S = reinterpret_cast<signed char *>(w + rup(8 * (size_t)p.M, 1024));
+    cudaError_t e = cudaMemsetAsync(umax, 0, 8 * (size_t)p.M, st);
+    if (e != cudaSuccess) return e;
+    if ((e = slice_operand(a_operand(p, Kp, umax, S), nslice, st)) != cudaSuccess) return e;
+    out = OzPresliced{S, umax, p.M, p.K, nslice, p.tri};
+    return cudaSuccess;
+}
 
 double ozaki_alg_flops(const GemmOp &p) { return gemm_alg_flops(p); }
 
+cudaError_t ozaki_set_attributes(const GemmOp &p, int nslice) {
+    if (nslice < kOzMinSlices || nslice > kOzMaxSlices) return cudaErrorInvalidValue;
+    tc::encode_tiled();
+    return tile_n_of(p) == 32 ? set_attr_bn<32>(nslice) : set_attr_bn<64>(nslice);
+}
+
 cudaError_t launch_ozaki_gemm(const GemmOp &p, int nslice, void *work, size_t work_bytes, int *err,
-                              cudaStream_t st) {
+                              cudaStream_t st, const OzPresliced *pre, int kchunk) {
     if (p.M <= 0 || p.N <= 0) return cudaSuccess;
     if (!ozaki_supported(p, nslice)) return cudaErrorInvalidValue;
-    const Layout L = layout_of(p, nslice);
+    if (pre && (pre->rows != p.M || pre->K != p.K || pre->nslice != nslice || pre->tri != p.tri || !pre->S))
+        return cudaErrorInvalidValue;
+    if (kchunk < 0 || (kchunk > 0 && (kchunk % kBK != 0 || p.lower_out || (p.K + kchunk - 1) / kchunk > 65535)))
+        return cudaErrorInvalidValue;
+    const Layout L = layout_of(p, nslice, pre != nullptr, kchunk);
     if (!work || work_bytes < L.total || (reinterpret_cast<uintptr_t>(work) & 1023u)) return cudaErrorInvalidValue;
     tc::EncodeTiledFn fn = tc::encode_tiled();
     if (!fn) return cudaErrorNotSupported;
     unsigned char *w = static_cast<unsigned char *>(work);
-    auto *umax_a = reinterpret_cast<unsigned long long *>(w + L.umax_a);
-    auto *umax_b = L.shared ? umax_a : reinterpret_cast<unsigned long long *>(w + L.umax_b);
-    auto *sa = reinterpret_cast<signed char *>(w + L.sa);
+    const unsigned long long *umax_a = pre ? pre->umax : reinterpret_cast<unsigned long long *>(w + L.umax_a);
+    auto *umax_b = L.shared ? const_cast<unsigned long long *>(umax_a)
+                            : reinterpret_cast<unsigned long long *>(w + L.umax_b);
+    const signed char *sa = pre ? pre->S : reinterpret_cast<signed char *>(w + L.sa);
     auto *sb = reinterpret_cast<signed char *>(w + L.sb);
     cudaError_t e = cudaMemsetAsync(w, 0, L.sa, st);
     if (e != cudaSuccess) return e;
 
-    // op(A)(i, k) = ta ? A[i lda + k] : A[k lda + i]; rows of the A side are i
-    OzOperand oa{p.A, p.ta ? p.lda : 1, p.ta ? 1 : p.lda, p.M, p.K, L.Kp, p.tri == 1 ? 1 : (p.tri == 2 ? 2 : 0),
-                 umax_a, sa, (long long)p.M * L.Kp};
+    if (!pre) {
+        const OzOperand oa = a_operand(p, L.Kp, const_cast<unsigned long long *>(umax_a), const_cast<signed char *>(sa));
+        if ((e = slice_operand(oa, nslice, st)) != cudaSuccess) return e;
+    }
     // op(B)(k, j) = tb ? B[k ldb + j] : B[j ldb + k]; rows of the B side are j; op(B) lower
     // (tri_b = 1) keeps k >= j, upper keeps k <= j
-    OzOperand ob{p.B, p.tb ? 1 : p.ldb, p.tb ? p.ldb : 1, p.N, p.K, L.Kp,
-                 p.tri_b == 1 ? 2 : (p.tri_b == 2 ? 1 : 0), umax_b, sb, (long long)p.N * L.Kp};
-    if ((e = slice_operand(oa, nslice, st)) != cudaSuccess) return e;
+    const OzOperand ob{p.B, p.tb ? 1 : p.ldb, p.tb ? p.ldb : 1, p.N, p.K, L.Kp,
+                       p.tri_b == 1 ? 2 : (p.tri_b == 2 ? 1 : 0), umax_b, sb, (long long)p.N * L.Kp};
     if (!L.shared && (e = slice_operand(ob, nslice, st)) != cudaSuccess) return e;
 
+    const int bn = tile_n_of(p);
     OzMaps maps;
     std::memset(&maps, 0, sizeof(maps));
     for (int sl = 0; sl < nslice; ++sl) {
         if (!make_map(fn, maps.a[sl], sa + (size_t)sl * p.M * L.Kp, p.M, L.Kp, kBM)) return cudaErrorInvalidValue;
-        if (!make_map(fn, maps.b[sl], sb + (size_t)sl * p.N * L.Kp, p.N, L.Kp, kBN)) return cudaErrorInvalidValue;
+        if (!make_map(fn, maps.b[sl], sb + (size_t)sl * p.N * L.Kp, p.N, L.Kp, bn)) return cudaErrorInvalidValue;
     }
     OzArgs a{};
     a.M = p.M;
@@ -484,6 +608,8 @@ cudaError_t launch_ozaki_gemm(const GemmOp &p, int nslice, void *work, size_t wo
     a.tri = p.tri;
     a.tri_b = p.tri_b;
     a.lower_out = p.lower_out;
+    a.kchunk = kchunk;
+    a.part = kchunk > 0 ? reinterpret_cast<double *>(w + L.part) : nullptr;
     a.alpha = p.alpha;
     a.beta = p.beta;
     a.C = p.C;
@@ -492,14 +618,15 @@ cudaError_t launch_ozaki_gemm(const GemmOp &p, int nslice, void *work, size_t wo
     a.umax_b = umax_b;
     a.err = err;
     a.wait_ns = kDefaultWaitNs;
-    const dim3 grid((unsigned)((p.M + kBM - 1) / kBM), (unsigned)((p.N + kBN - 1) / kBN));
-    switch (nslice) {
-        case 4: return launch_cfg<4>(maps, a, grid, st);
-        case 5: return launch_cfg<5>(maps, a, grid, st);
-        case 6: return launch_cfg<6>(maps, a, grid, st);
-        case 7: return launch_cfg<7>(maps, a, grid, st);
-        default: return launch_cfg<8>(maps, a, grid, st);
-    }
+    const dim3 grid((unsigned)((p.M + kBM - 1) / kBM), (unsigned)((p.N + bn - 1) / bn),
+                    (unsigned)std::max(1, L.nchunk));
+    e = bn == 32 ? launch_bn<32>(nslice, maps, a, grid, st) : launch_bn<64>(nslice, maps, a, grid, st);
+    if (e != cudaSuccess || kchunk == 0) return e;
+    const long long tot = (long long)p.M * p.N;
+    DVR3D_COUNT_LAUNCH(1);
+    oz_reduce_kernel<<<(unsigned)std::min<long long>((tot + 255) / 256, 148LL * 8), 256, 0, st>>>(
+        a.part, L.nchunk, p.M, p.N, p.alpha, p.beta, p.C, p.ldc);
+    return cudaGetLastError();
 }
 
 }  // namespace dvr3d

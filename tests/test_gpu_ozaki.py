@@ -87,6 +87,22 @@ def test_transposed_and_triangular_operands(ctx, ta, tb, tri, tri_b):
     assert np.all(np.abs(got - dmma) <= 1.5 * _bound(a_op, b_op) + 1e-15 * np.abs(c0))
 
 
+@pytest.mark.parametrize("ta,tri", [(False, 1), (True, 2)])
+def test_thin_triangular_products_in_k_chunks(ctx, ta, tri):
+    # the Krylov step's shapes: inv(L) Q_k and inv(L)^T Y with 32 columns (128 x 32 tiles, K
+    # split into chunks summed in order by a second kernel)
+    rng = np.random.default_rng(21 + tri)
+    n = 3000
+    low = np.tril(rng.standard_normal((n, n))) + n * np.eye(n)
+    a_op = low.T if ta else low
+    q = rng.standard_normal((n, 32))
+    got = ctx.ozaki_gemm(low, q, ta=ta, tri=tri)
+    ref = a_op @ q
+    assert np.all(np.abs(got - ref) <= _bound(a_op, q))
+    dmma = ctx.ozaki_gemm(low, q, ta=ta, tri=tri, nslice=0)
+    assert np.all(np.abs(got - dmma) <= 2 * _bound(a_op, q))
+
+
 def test_lower_output_update(ctx):
     # A22 <- A22 - L21 L21^T on the lower triangle only (the Cholesky's SYRK step); the upper
     # triangle of c must come back untouched
@@ -127,19 +143,21 @@ def test_rejects_k_beyond_exact_accumulation(ctx):
         ctx.ozaki_gemm(a, b)
 
 
-def _cfg2_levels(ctx, ozaki: str):
+def _cfg2_levels(ctx, ozaki: str, krylov: str = "0"):
     w = configs.config2()
     deck = parse_deck(w.deck)
     ctx.set_pes(w.pes)
-    old = os.environ.get("DVR3D_OZAKI")
-    os.environ["DVR3D_OZAKI"] = ozaki
+    keys = {"DVR3D_OZAKI": ozaki, "DVR3D_OZAKI_KRYLOV": krylov}
+    old = {k: os.environ.get(k) for k in keys}
+    os.environ.update(keys)
     try:
         return ctx.solve(deck, 0, precision=dvr3d_b200.DVR3D_PREC_MIXED_DAVIDSON, nlevels=300)
     finally:
-        if old is None:
-            del os.environ["DVR3D_OZAKI"]
-        else:
-            os.environ["DVR3D_OZAKI"] = old
+        for k, v in old.items():
+            if v is None:
+                del os.environ[k]
+            else:
+                os.environ[k] = v
 
 
 def test_shift_invert_with_int8_factorisation_matches_oracle(ctx):
@@ -150,3 +168,7 @@ def test_shift_invert_with_int8_factorisation_matches_oracle(ctx):
     lv = fx["levels"][:300]
     assert np.abs(oz.eval - lv).max() * AUTOCM <= 1e-6
     assert np.abs(oz.eval - plain.eval).max() * AUTOCM <= 1e-6
+    # the opt-in int8 Krylov products (inv(L) sliced once, 32-column blocks in K chunks)
+    kr = _cfg2_levels(ctx, "1", krylov="1")
+    assert kr.fallback == 0 and len(kr.eval) == 300
+    assert np.abs(kr.eval - lv).max() * AUTOCM <= 1e-6
